@@ -1,0 +1,295 @@
+"""Python binding of the B200 Crank-Nicolson step (libcnm_gpu.so, include/cnm_gpu.h).
+
+``CrankNicolsonModes`` mirrors the public surface of the reference class
+(include/CrankNicolsonModes.hpp:60-239): the constructor takes the same
+arguments, scalar members (R, R1, theta, Omega, dt, ...) are attributes that
+read and write the device-side solver, ``psi`` is the mode-major complex128
+state, and ``step``/``run``/``initialize``/``build_cap``/``build_damping_mask``/
+``apply_sink``/``schrodinger_rhs``/``sink_strength`` keep their meaning.
+Errors raise the Python counterparts of the reference's exceptions:
+std::invalid_argument -> ValueError, std::logic_error -> LogicError,
+std::runtime_error -> SolveError.
+
+There is no CPU fallback: if the CUDA library cannot be loaded or no GPU is
+present the constructor raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libcnm_gpu.so")
+
+CNM_OK, CNM_EINVAL, CNM_ELOGIC, CNM_ESOLVE, CNM_ECUDA, CNM_ENOMEM, CNM_EDEVICE = range(7)
+
+OPS = {"H": 0, "H0": 1, "V": 2, "V1": 3, "V2": 4, "dVdt": 5, "A": 6, "B": 7, "sink": 8,
+       "schrodinger_rhs": 9, "A_full": 10, "CAP": 11, "precond": 12}
+
+
+class LogicError(RuntimeError):
+    """std::logic_error of the reference."""
+
+
+class SolveError(RuntimeError):
+    """std::runtime_error of the reference (the CN solve failed)."""
+
+
+class CudaError(RuntimeError):
+    """CUDA failure, or the CUDA library is unavailable."""
+
+
+class cnm_params(C.Structure):
+    _fields_ = [("Nr", C.c_int32), ("L", C.c_double), ("dt", C.c_double), ("epsilon", C.c_double),
+                ("l_max", C.c_int32), ("mu", C.c_double), ("M_c", C.c_double), ("q", C.c_double),
+                ("a", C.c_double), ("R", C.c_double), ("counter", C.c_int32), ("absorption", C.c_int32),
+                ("save_every", C.c_int32), ("ramp_periods", C.c_double), ("epsilon_smear", C.c_double),
+                ("precision", C.c_int32)]
+
+
+class cnm_scalars(C.Structure):
+    _fields_ = [("t", C.c_double), ("theta", C.c_double), ("phase", C.c_double), ("Omega", C.c_double),
+                ("Omega_0", C.c_double), ("P", C.c_double), ("R", C.c_double), ("R1", C.c_double),
+                ("R2", C.c_double), ("M1", C.c_double), ("M2", C.c_double), ("q", C.c_double),
+                ("dt", C.c_double), ("p_bin", C.c_double), ("steps_per_period", C.c_double),
+                ("evolve_orbit", C.c_int32), ("ramp_secondary_potential", C.c_int32),
+                ("use_block_preconditioner", C.c_int32), ("last_solver_iterations", C.c_int32),
+                ("last_solver_residual", C.c_double), ("tolerance", C.c_double),
+                ("max_iterations", C.c_int32), ("accept_residual", C.c_double)]
+
+
+class cnm_diag(C.Structure):
+    _fields_ = [("R", C.c_double), ("theta", C.c_double), ("Omega", C.c_double), ("M1", C.c_double),
+                ("q", C.c_double), ("t", C.c_double), ("energy", C.c_double), ("p_bin", C.c_double),
+                ("p_bin_inst", C.c_double), ("dV_bin_dt", C.c_double), ("residual", C.c_double),
+                ("iterations", C.c_int32)]
+
+
+# Exported entry points of include/cnm_gpu.h, checked by the CPU test suite.
+EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "cnm_n_modes", "cnm_modes",
+           "cnm_grid", "cnm_get_scalars", "cnm_set_scalars", "cnm_set_initial_state_full", "cnm_set_state",
+           "cnm_get_state", "cnm_configure_isolated_black_hole", "cnm_initialize",
+           "cnm_set_power_average_orbits", "cnm_build_damping_mask", "cnm_build_cap", "cnm_prepare_run",
+           "cnm_refresh", "cnm_step", "cnm_should_stop", "cnm_apply", "cnm_sink_strength", "cnm_sink_active",
+           "cnm_sink_vector")
+
+_lib = None
+
+
+def load_library():
+    """Load libcnm_gpu.so (built by boson_cloud_binary_b200/Makefile); raise if absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CudaError(f"CUDA extension not built: {LIB_PATH} is missing (run __graft_entry__.build())")
+    L = C.CDLL(LIB_PATH)
+    p, i32, d = C.c_void_p, C.c_int32, C.c_double
+    dp = C.POINTER(C.c_double)
+    L.cnm_create.argtypes = [C.POINTER(cnm_params), C.POINTER(p)]
+    L.cnm_destroy.argtypes = [p]
+    L.cnm_last_error.argtypes = [p]
+    L.cnm_last_error.restype = C.c_char_p
+    L.cnm_create_error.restype = C.c_char_p
+    L.cnm_n_modes.argtypes = [p, C.POINTER(i32)]
+    L.cnm_modes.argtypes = [p, C.POINTER(i32), C.POINTER(i32)]
+    L.cnm_grid.argtypes = [p, dp]
+    L.cnm_get_scalars.argtypes = [p, C.POINTER(cnm_scalars)]
+    L.cnm_set_scalars.argtypes = [p, C.POINTER(cnm_scalars)]
+    for f in ("cnm_set_initial_state_full", "cnm_set_state", "cnm_get_state"):
+        getattr(L, f).argtypes = [p, dp, C.c_int64]
+    L.cnm_configure_isolated_black_hole.argtypes = [p, d]
+    L.cnm_initialize.argtypes = [p]
+    L.cnm_set_power_average_orbits.argtypes = [p, d]
+    L.cnm_build_damping_mask.argtypes = [p, d, d, i32]
+    L.cnm_build_cap.argtypes = [p, d, d, i32]
+    L.cnm_prepare_run.argtypes = [p, i32, d]
+    L.cnm_refresh.argtypes = [p, d]
+    L.cnm_step.argtypes = [p, i32, C.POINTER(cnm_diag), dp, dp, dp, dp]
+    L.cnm_should_stop.argtypes = [p, C.POINTER(i32)]
+    L.cnm_apply.argtypes = [p, i32, dp, dp]
+    L.cnm_sink_strength.argtypes = [p, i32, dp]
+    L.cnm_sink_active.argtypes = [p, C.POINTER(i32)]
+    L.cnm_sink_vector.argtypes = [p, i32, dp]
+    _lib = L
+    return L
+
+
+def _dptr(a):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+_SCALAR_FIELDS = {f for f, _ in cnm_scalars._fields_}
+_BOOL_FIELDS = {"evolve_orbit", "ramp_secondary_potential", "use_block_preconditioner"}
+
+
+class Diag(dict):
+    """One step's diagnostics: the values step() appends to the run's text files."""
+
+
+class CrankNicolsonModes:
+    """B200 drop-in of the reference's CrankNicolsonModes (FP64 path)."""
+
+    def __init__(self, Nx, L, dt, epsilon, l_max, mu, M_c, q, a, R, counter, absorption, save_every,
+                 ramp_periods, epsilon_smear, config_file=None):
+        lib = load_library()
+        prm = cnm_params(int(Nx), float(L), float(dt), float(epsilon), int(l_max), float(mu), float(M_c),
+                         float(q), float(a), float(R), int(bool(counter)), int(bool(absorption)),
+                         int(save_every), float(ramp_periods), float(epsilon_smear), 0)
+        h = C.c_void_p()
+        rc = lib.cnm_create(C.byref(prm), C.byref(h))
+        if rc != CNM_OK:
+            msg = lib.cnm_create_error().decode()
+            if rc == CNM_EINVAL:
+                raise ValueError(msg)
+            raise CudaError(msg)
+        self.__dict__["_h"] = h
+        self.__dict__["_lib"] = lib
+        n = C.c_int32()
+        lib.cnm_n_modes(h, C.byref(n))
+        l = np.zeros(n.value, np.int32)
+        m = np.zeros(n.value, np.int32)
+        lib.cnm_modes(h, l.ctypes.data_as(C.POINTER(C.c_int32)), m.ctypes.data_as(C.POINTER(C.c_int32)))
+        r = np.zeros(int(Nx))
+        lib.cnm_grid(h, _dptr(r))
+        self.__dict__.update(n_modes=n.value, modes=[(int(x), int(y)) for x, y in zip(l, m)], Nr=int(Nx),
+                             r=r, l_max=int(l_max), counter=bool(counter), L=float(L), mu=float(mu),
+                             M_c=float(M_c), epsilon=float(epsilon), dr=float(L) / (int(Nx) - 1),
+                             save_every=int(save_every), a=float(a), t=[], config_file=config_file)
+
+    def __del__(self):
+        h = self.__dict__.get("_h")
+        if h:
+            self._lib.cnm_destroy(h)
+            self.__dict__["_h"] = None
+
+    def _check(self, rc):
+        if rc == CNM_OK:
+            return
+        msg = self._lib.cnm_last_error(self._h).decode()
+        if rc == CNM_EINVAL:
+            raise ValueError(msg)
+        if rc == CNM_ELOGIC:
+            raise LogicError(msg)
+        if rc == CNM_ESOLVE:
+            raise SolveError(msg)
+        raise CudaError(msg)
+
+    # ---- scalar members ------------------------------------------------------------
+    def _scalars(self):
+        s = cnm_scalars()
+        self._check(self._lib.cnm_get_scalars(self._h, C.byref(s)))
+        return s
+
+    def __getattr__(self, name):
+        if name == "t_i":
+            return self._scalars().t
+        if name in _SCALAR_FIELDS:
+            v = getattr(self._scalars(), name)
+            return bool(v) if name in _BOOL_FIELDS else v
+        if name == "sink_active":
+            a = C.c_int32()
+            self._check(self._lib.cnm_sink_active(self._h, C.byref(a)))
+            return bool(a.value)
+        raise AttributeError(name)
+
+    def __setattr__(self, name, value):
+        key = "t" if name == "t_i" else name
+        if key in _SCALAR_FIELDS and not (name == "t"):
+            s = self._scalars()
+            setattr(s, key, type(getattr(s, key))(value) if not isinstance(getattr(s, key), int)
+                    else int(value))
+            self._check(self._lib.cnm_set_scalars(self._h, C.byref(s)))
+        else:
+            self.__dict__[name] = value
+
+    @property
+    def size(self):
+        return self.Nr * self.n_modes
+
+    @property
+    def psi(self):
+        out = np.zeros(2 * self.size)
+        self._check(self._lib.cnm_get_state(self._h, _dptr(out), self.size))
+        return out.view(np.complex128).copy()
+
+    @psi.setter
+    def psi(self, value):
+        v = np.ascontiguousarray(np.asarray(value, np.complex128))
+        self._check(self._lib.cnm_set_state(self._h, _dptr(v.view(np.float64)), v.size))
+
+    # ---- reference methods -------------------------------------------------------------
+    def set_initial_state_full(self, psi0):
+        v = np.ascontiguousarray(np.asarray(psi0, np.complex128))
+        self._check(self._lib.cnm_set_initial_state_full(self._h, _dptr(v.view(np.float64)), v.size))
+
+    def initialize(self):
+        self._check(self._lib.cnm_initialize(self._h))
+
+    def configure_isolated_black_hole(self, x):
+        self._check(self._lib.cnm_configure_isolated_black_hole(self._h, float(x)))
+
+    def set_power_average_orbits(self, n):
+        self._check(self._lib.cnm_set_power_average_orbits(self._h, float(n)))
+
+    def build_damping_mask(self, f, W, n):
+        self._check(self._lib.cnm_build_damping_mask(self._h, float(f), float(W), int(n)))
+
+    def build_cap(self, f, W, n):
+        self._check(self._lib.cnm_build_cap(self._h, float(f), float(W), int(n)))
+
+    def run(self, n_steps, r_ex):
+        """The computational part of run(): extraction radius, t = 0, operator refresh.
+
+        (The text output of a run lives in boson_cloud_binary_b200.output.)"""
+        self._check(self._lib.cnm_prepare_run(self._h, int(n_steps), float(r_ex)))
+        self.__dict__["t"] = [0.0]
+
+    def refresh(self, time):
+        self._check(self._lib.cnm_refresh(self._h, float(time)))
+
+    def step(self, step_id):
+        n = self.n_modes
+        d = cnm_diag()
+        ef, fl, nm, en = (np.zeros(n) for _ in range(4))
+        self._check(self._lib.cnm_step(self._h, int(step_id), C.byref(d), _dptr(ef), _dptr(fl), _dptr(nm),
+                                       _dptr(en)))
+        out = Diag({f: getattr(d, f) for f, _ in cnm_diag._fields_})
+        out.update(energy_flux=ef, flux=fl, norms=nm, energies=en)
+        t = self.__dict__["t"]
+        while len(t) <= step_id:
+            t.append(0.0)
+        t[step_id] = d.t
+        return out
+
+    def should_stop(self):
+        s = C.c_int32()
+        self._check(self._lib.cnm_should_stop(self._h, C.byref(s)))
+        return bool(s.value)
+
+    def apply(self, op, x):
+        x = np.ascontiguousarray(np.asarray(x, np.complex128))
+        y = np.zeros(2 * self.size)
+        self._check(self._lib.cnm_apply(self._h, OPS[op], _dptr(x.view(np.float64)), _dptr(y)))
+        return y.view(np.complex128).copy()
+
+    def apply_sink(self, x):
+        return self.apply("sink", x)
+
+    def schrodinger_rhs(self, x):
+        return self.apply("schrodinger_rhs", x)
+
+    def sink_strength(self, body):
+        out = C.c_double()
+        self._check(self._lib.cnm_sink_strength(self._h, int(body), C.byref(out)))
+        return out.value
+
+    def absorption_sink_active(self):
+        return self.sink_active
+
+    def sink_vector(self, body):
+        out = np.zeros(2 * self.size)
+        self._check(self._lib.cnm_sink_vector(self._h, int(body), _dptr(out)))
+        return out.view(np.complex128).copy()

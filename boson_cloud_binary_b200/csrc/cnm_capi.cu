@@ -1,0 +1,1259 @@
+// cnm_capi.cu -- the handle behind include/cnm_gpu.h: state, one CN step on the
+// device, and the host-side FP64 orbit bookkeeping of the reference class.
+//
+// Call sequence of one step (src/CrankNicolsonModes.cpp:145-234):
+//   host:   t += dt, theta += s Omega dt, phase += Omega dt; ramps and Omega
+//           (build_time_dependent_perturbation, _hamiltonian.cpp:245-268)
+//   device: hh table, absorber moments and projectors, sink projections of the
+//           old state, rhs = B psi - dt/4 Gamma psi, pivots, Woodbury set-up,
+//           BiCGSTAB (device-resident scalars), residual check, mask,
+//           fused diagnostics (one pass for H psi, V psi, dV/dt psi and dpsi/dt)
+//   host:   orbit ODE (_evolution.cpp:17-72), rolling phase average, diagnostics.
+#include "../../include/cnm_gpu.h"
+#include "cnm_coupling.h"
+#include "cnm_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <complex>
+#include <cstring>
+#include <deque>
+#include <limits>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace cnm {
+
+struct Error : std::runtime_error {
+    int code;
+    Error(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void cuda_check(cudaError_t e, const char *what)
+{
+    if (e != cudaSuccess) throw Error(e == cudaErrorMemoryAllocation ? CNM_ENOMEM : CNM_ECUDA,
+                                      std::string(what) + ": " + cudaGetErrorString(e));
+}
+#define CK(x) cuda_check((x), #x)
+
+template <class T>
+struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    void alloc(size_t count)
+    {
+        release();
+        if (count == 0) return;
+        CK(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+        CK(cudaMemset(p, 0, count * sizeof(T)));
+    }
+    void release()
+    {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+    ~DevBuf() { release(); }
+};
+
+// Rolling time average over a window of orbital phase (src/RollingPhase.cpp:24-129).
+class RollingPhaseAverage {
+public:
+    explicit RollingPhaseAverage(double n_orbits = 2.0) : window_(2.0 * M_PI * n_orbits)
+    {
+        if (n_orbits <= 0.0) throw Error(CNM_EINVAL, "RollingPhaseAverage: n_orbits must be positive");
+    }
+    double update(double time, double phase, double value)
+    {
+        if (!has_prev_) {
+            prev_ = {time, phase, value};
+            initial_phase_ = phase;
+            has_prev_ = true;
+            average_ = value;
+            return average_;
+        }
+        if (time <= prev_.time) throw Error(CNM_ESOLVE, "RollingPhaseAverage: time must increase");
+        if (phase <= prev_.phase) throw Error(CNM_ESOLVE, "RollingPhaseAverage: phase must increase");
+        Seg s{prev_.time, time, prev_.phase, phase, prev_.value, value, 0.0};
+        s.integral = 0.5 * (s.v0 + s.v1) * (s.t1 - s.t0);
+        segs_.push_back(s);
+        integral_ += s.integral;
+        duration_ += s.t1 - s.t0;
+        const double cut = phase - window_;
+        while (!segs_.empty() && segs_.front().p1 <= cut) {
+            integral_ -= segs_.front().integral;
+            duration_ -= segs_.front().t1 - segs_.front().t0;
+            segs_.pop_front();
+        }
+        if (!segs_.empty()) {
+            Seg &f = segs_.front();
+            if (f.p0 < cut && cut < f.p1) {
+                const double fr = (cut - f.p0) / (f.p1 - f.p0);
+                const double tc = f.t0 + fr * (f.t1 - f.t0), vc = f.v0 + fr * (f.v1 - f.v0);
+                integral_ -= 0.5 * (f.v0 + vc) * (tc - f.t0);
+                duration_ -= tc - f.t0;
+                f.t0 = tc;
+                f.p0 = cut;
+                f.v0 = vc;
+                f.integral = 0.5 * (f.v0 + f.v1) * (f.t1 - f.t0);
+            }
+        }
+        duration_ = std::max(duration_, 0.0);
+        average_ = duration_ > 0.0 ? integral_ / duration_ : value;
+        prev_ = {time, phase, value};
+        return average_;
+    }
+
+private:
+    struct Sample { double time, phase, value; };
+    struct Seg { double t0, t1, p0, p1, v0, v1, integral; };
+    double window_;
+    std::deque<Seg> segs_;
+    Sample prev_{};
+    bool has_prev_ = false;
+    double initial_phase_ = 0, integral_ = 0, duration_ = 0, average_ = 0;
+};
+
+// One body's absorber: kernel moments on the device, support on the host.
+struct Absorber {
+    double radius = -1.0, width = -1.0;
+    bool valid = false;
+    int lo = 0, hi = 0;            // node support [lo, hi) of the projector
+    int wlo = 0, whi = 0;          // nodes the projector kernel must (re)write
+    double strength = 0.0;         // g = A_h dr
+    DevBuf<double> mom;            // (2 l_max + 1) x Nr
+    DevBuf<double2> v;             // projector, Nr * n_modes
+};
+
+// Operator parameters frozen at the last build_time_dependent_perturbation; the
+// reference's assembled matrices keep these values until the next rebuild.
+struct OpState {
+    bool built = false;
+    double theta = 0, domega = 0, dt = 0;
+    bool cap = false;
+    bool sink_active = false;
+};
+
+struct Solver {
+    // constructor arguments and derived constants
+    int Nr, l_max, n_modes, save_every;
+    double L, dr, epsilon, mu, M_c, a_spin, epsilon_smear, ramp_periods, initial_period;
+    bool counter, absorption;
+    // evolving scalars (public members of the reference class)
+    double t_i = 0, theta = 0, phase = 0, Omega = 0, Omega_0, P, R, R1, R2, M1, M2, q, dt, p_bin = 0;
+    double steps_per_period = 50.0;
+    bool evolve_orbit = true, ramp_secondary_potential = true, use_block = true;
+    double last_residual = 0.0;
+    int last_iterations = 0;
+    double tolerance = 1e-10, accept_residual = 1e-9;
+    int max_iterations = 500;
+    // private state
+    bool isolated = false, initialized = false, sink_active = false, mask = false, cap = false;
+    double ramp_factor = 0.0, potential_ramp_factor = 0.0;
+    int idx_ex = 0;
+    double r_ex = 0.0;
+    double orbits_average = 2.0;
+    RollingPhaseAverage power_average{2.0};
+    OpState op;
+    std::vector<double> r;
+    Coupling cpl;
+    std::vector<double> capw_h, mask_h;
+
+    // device
+    cudaStream_t stream = nullptr;
+    int64_t nN;
+    int K;
+    DevBuf<double> d_r, d_hh, d_hh_aux, d_capw, d_mask, d_glx, d_glw, d_partials, d_red, d_ang00;
+    DevBuf<int> d_pair_row_ptr, d_pair_col, d_pair_term_ptr, d_term_l, d_diag_pair, d_mode_l, d_mode_m, d_status;
+    DevBuf<double> d_term_g;
+    DevBuf<double2> psi, rhs, b, x, rr, r0, p, v, s, t, y, z, yP, W0, W1, tmp, cand, dinv;
+    DevBuf<double2> d_dots;   // [0..1] psi, [2..3] psi_last, [4..5] scratch, [6..7] G set-up
+    DevBuf<double2> d_edge;   // dpsi at idx_ex (n) + psi at idx_ex-1..idx_ex+1 (3n)
+    DevBuf<Krylov> d_kr;
+    Absorber abs1, abs2;
+    int gl_n = 0;
+    int vec_blocks = 0;
+    int precond_chunk = 2048, precond_window = 256;
+    size_t apply_smem = 0, diag_smem = 0;
+    // pinned host staging
+    double *h_stage = nullptr;
+    size_t h_stage_n = 0;
+
+    Solver(const cnm_params &pr)
+        : Nr(pr.Nr), l_max(pr.l_max), save_every(pr.save_every), L(pr.L), dr(pr.L / (pr.Nr - 1)),
+          epsilon(pr.epsilon), mu(pr.mu), M_c(pr.M_c), a_spin(pr.a), epsilon_smear(pr.epsilon_smear),
+          ramp_periods(pr.ramp_periods), initial_period(2.0 * M_PI / std::sqrt((1 + pr.q) / std::pow(pr.R, 3))),
+          counter(pr.counter != 0), absorption(pr.absorption != 0), R(pr.R), q(pr.q), dt(pr.dt)
+    {
+        if (Nr < 3 || l_max < 0 || L <= 0.0 || dt <= 0.0 || save_every <= 0)
+            throw Error(CNM_EINVAL, "Require Nr >= 3, l_max >= 0, and positive L, dt, save_every");
+        if (pr.precision != CNM_FP64) throw Error(CNM_EINVAL, "unknown precision");
+        Omega = 0.0;
+        Omega_0 = std::sqrt((1.0 + q) / std::pow(R, 3));
+        P = initial_period;
+        R1 = q / (1 + q) * R;
+        R2 = 1 / (1 + q) * R;
+        M1 = 1.0;
+        M2 = q;
+        r.resize(Nr);
+        for (int i = 0; i < Nr; i++) r[i] = epsilon + i * dr;
+        cpl = build_coupling(l_max);
+        n_modes = cpl.n_modes;
+        K = 2 * l_max + 1;
+        nN = (int64_t)Nr * n_modes;
+        setup_device();
+    }
+
+    ~Solver()
+    {
+        if (h_stage) cudaFreeHost(h_stage);
+        if (stream) cudaStreamDestroy(stream);
+    }
+
+    template <class T>
+    void upload(DevBuf<T> &d, const std::vector<T> &h)
+    {
+        d.alloc(std::max<size_t>(h.size(), 1));
+        if (!h.empty()) CK(cudaMemcpy(d.p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice));
+    }
+
+    double *stage(size_t n)
+    {
+        if (n > h_stage_n) {
+            if (h_stage) cudaFreeHost(h_stage);
+            CK(cudaMallocHost(&h_stage, n * sizeof(double)));
+            h_stage_n = n;
+        }
+        return h_stage;
+    }
+
+    void setup_device()
+    {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        int nsm = 0;
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+        vec_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nN + VEC_THREADS - 1) / VEC_THREADS, (int64_t)nsm * 4));
+        upload(d_r, r);
+        upload(d_pair_row_ptr, cpl.pair_row_ptr);
+        upload(d_pair_col, cpl.pair_col);
+        upload(d_pair_term_ptr, cpl.pair_term_ptr);
+        upload(d_term_l, cpl.term_l);
+        upload(d_term_g, cpl.term_g);
+        upload(d_diag_pair, cpl.diag_pair);
+        upload(d_mode_l, cpl.mode_l);
+        upload(d_mode_m, cpl.mode_m);
+        upload(d_ang00, cpl.ang00);
+        d_hh.alloc((size_t)K * Nr);
+        d_hh_aux.alloc((size_t)K * Nr);
+        for (DevBuf<double2> *bptr : {&psi, &rhs, &b, &x, &rr, &r0, &p, &v, &s, &t, &y, &z, &yP, &W0, &W1, &tmp,
+                                      &cand, &dinv})
+            bptr->alloc(nN);
+        d_dots.alloc(8);
+        d_edge.alloc(4 * (size_t)n_modes);
+        d_kr.alloc(1);
+        d_status.alloc(1);
+        d_red.alloc(std::max(64, 2 * n_modes + 8));
+        const int diag_blocks = (Nr + APPLY_TILE - 1) / APPLY_TILE;
+        d_partials.alloc(std::max<size_t>((size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks));
+        apply_smem = (size_t)n_modes * (APPLY_TILE + 2 + APPLY_TILE + 1) * sizeof(double2) +
+                     (size_t)K * APPLY_TILE * sizeof(double);
+        diag_smem = apply_smem + (size_t)(2 * n_modes + 3) * (APPLY_THREADS / 32) * sizeof(double);
+        CK(cudaFuncSetAttribute(k_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
+        CK(cudaFuncSetAttribute(k_diagnostics, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
+        CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+    }
+
+    Grid grid() const
+    {
+        Grid g;
+        g.Nr = Nr;
+        g.n_modes = n_modes;
+        g.dr = dr;
+        g.mu = mu;
+        g.r = d_r.p;
+        g.capw = op.cap ? d_capw.p : nullptr;
+        return g;
+    }
+
+    CouplingTable table() const
+    {
+        CouplingTable c;
+        c.n_modes = n_modes;
+        c.l_max = l_max;
+        c.n_pairs = (int)cpl.pair_col.size();
+        c.n_terms = (int)cpl.term_l.size();
+        c.pair_row_ptr = d_pair_row_ptr.p;
+        c.pair_col = d_pair_col.p;
+        c.pair_term_ptr = d_pair_term_ptr.p;
+        c.term_l = d_term_l.p;
+        c.term_g = d_term_g.p;
+        c.diag_pair = d_diag_pair.p;
+        c.mode_l = d_mode_l.p;
+        c.mode_m = d_mode_m.p;
+        return c;
+    }
+
+    void sync() { CK(cudaStreamSynchronize(stream)); }
+    void launch_check() { CK(cudaGetLastError()); }
+
+    double ramp_end_time() const { return ramp_periods * initial_period; }
+
+    // -------------------------------------------------------------- set-up API
+
+    void set_initial_state_full(const double *h, int64_t n)
+    {
+        if (n != nN) throw Error(CNM_EINVAL, "Initial state size does not match the radial grid and modes");
+        std::vector<double> tmp_h(h, h + 2 * n);
+        const double sc = std::sqrt(M_c / mu);
+        for (double &e : tmp_h) e *= sc;
+        CK(cudaMemcpy(psi.p, tmp_h.data(), 2 * n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+
+    void set_state(const double *h, int64_t n)
+    {
+        if (n != nN) throw Error(CNM_EINVAL, "state size does not match the radial grid and modes");
+        CK(cudaMemcpy(psi.p, h, 2 * n * sizeof(double), cudaMemcpyHostToDevice));
+    }
+
+    void get_state(double *h, int64_t n) const
+    {
+        if (n != nN) throw Error(CNM_EINVAL, "state size does not match the radial grid and modes");
+        CK(cudaMemcpy(h, psi.p, 2 * n * sizeof(double), cudaMemcpyDeviceToHost));
+    }
+
+    void configure_isolated_black_hole(double xbh)
+    {
+        if (!std::isfinite(xbh) || std::abs(xbh) >= L)
+            throw Error(CNM_EINVAL, "The isolated BH must lie inside the radial domain");
+        if (initialized) throw Error(CNM_ELOGIC, "Configure the isolated BH before initialize()");
+        isolated = true;
+        evolve_orbit = false;
+        M1 = 1.0;
+        M2 = q = 0.0;
+        R = R1 = std::abs(xbh);
+        R2 = 0.0;
+        theta = xbh < 0.0 ? M_PI : 0.0;
+        phase = 0.0;
+        Omega = Omega_0 = 0.0;
+        ramp_periods = 0.0;
+    }
+
+    void initialize()
+    {
+        abs1.valid = abs2.valid = false;
+        t_i = 0.0;
+        build_time_dependent_perturbation(0.0);
+        initialized = true;
+    }
+
+    void build_damping_mask(double fL, double W, int n)
+    {
+        mask = true;
+        mask_h.assign(Nr, 1.0);
+        const int idx = (int)std::floor(L * fL / dr);
+        const double rm = fL * L, Lm = (1 - fL) * L;
+        for (int i = 0; i < Nr; i++)
+            if (i >= idx) mask_h[i] = std::exp(-W * std::pow((r[i] - rm) / Lm, n));
+        upload(d_mask, mask_h);
+    }
+
+    void build_cap(double fL, double W, int n)
+    {
+        cap = true;
+        capw_h.assign(Nr, 0.0);
+        const int idx = (int)std::floor(L * fL / dr);
+        const double rc = fL * L, Lc = (1 - fL) * L;
+        for (int i = std::max(idx, 0); i < Nr; i++) capw_h[i] = W * std::pow((r[i] - rc) / (r[i] - Lc), n);
+        upload(d_capw, capw_h);
+    }
+
+    // -------------------------------------------------------------- operators
+
+    void build_hh(double *dst, double a1, double a2)
+    {
+        const int64_t total = (int64_t)K * Nr;
+        k_hh_table<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(dst, d_r.p, Nr, K, R1, R2, q,
+                                                                        -mu * (M1 + M2), a1, a2);
+        launch_check();
+    }
+
+    // src/CrankNicolsonModes_hamiltonian.cpp:245-268
+    void build_time_dependent_perturbation(double time)
+    {
+        ramp_factor = 1.0;
+        if (isolated) {
+            Omega = 0.0;
+        } else if (time < ramp_end_time()) {
+            const double xr = time / ramp_end_time();
+            ramp_factor = 3.0 * xr * xr - 2.0 * xr * xr * xr;
+            Omega = Omega_0 * ramp_factor;
+        } else {
+            Omega = std::sqrt((M1 + M2) / std::pow(R, 3));
+        }
+        potential_ramp_factor = ramp_secondary_potential ? ramp_factor : 1.0;
+        build_hh(d_hh.p, 1.0, potential_ramp_factor);
+        if (absorption) build_spherical_absorption();
+        sink_active = absorption && time >= ramp_end_time();
+        op.built = true;
+        op.theta = theta;
+        op.domega = (counter ? -1.0 : 1.0) * Omega;
+        op.dt = dt;
+        op.cap = cap;
+        op.sink_active = sink_active;
+    }
+
+    // src/CrankNicolsonModes_absorption.cpp:12-81
+    void update_absorption_profile(Absorber &ab, double radius, double width)
+    {
+        if (ab.valid && ab.radius == radius && ab.width == width) return;
+        const int old_lo = ab.lo, old_hi = ab.hi;
+        ab.radius = radius;
+        ab.width = width;
+        ab.valid = true;
+        if (!ab.mom.p) {
+            ab.mom.alloc((size_t)K * Nr);
+            ab.v.alloc(nN);
+        }
+        ab.lo = ab.hi = 0;
+        if (!(width < dr || width <= 0.0 || radius < 0.0)) {
+            int lo = Nr, hi = 0;
+            for (int i = 1; i < Nr - 1; ++i)
+                if (std::abs(r[i] - radius) < width) {
+                    lo = std::min(lo, i);
+                    hi = std::max(hi, i + 1);
+                }
+            if (hi > lo) {
+                ab.lo = lo;
+                ab.hi = hi;
+            }
+        }
+        ab.wlo = std::min(old_lo, ab.lo);
+        ab.whi = std::max(old_hi, ab.hi);
+        if (old_hi <= old_lo) {
+            ab.wlo = ab.lo;
+            ab.whi = ab.hi;
+        } else if (ab.hi <= ab.lo) {
+            ab.wlo = old_lo;
+            ab.whi = old_hi;
+        }
+        if (ab.hi <= ab.lo) return;
+        const int degree = 2 * l_max;
+        const int nq = std::max(128, degree + 16);
+        if (gl_n != nq) {
+            std::vector<double> gx, gw;
+            gauss_legendre01(nq, gx, gw);
+            upload(d_glx, gx);
+            upload(d_glw, gw);
+            gl_n = nq;
+        }
+        const int threads = 128;
+        k_abs_moments<<<ab.hi - ab.lo, threads, (size_t)(degree + 1) * (threads / 32) * sizeof(double), stream>>>(
+            d_r.p, Nr, ab.lo, radius, width, nq, d_glx.p, d_glw.p, degree, ab.mom.p);
+        launch_check();
+        k_abs_normalize<<<1, 256, 0, stream>>>(d_r.p, Nr, ab.lo, ab.hi, dr, degree, ab.mom.p);
+        launch_check();
+    }
+
+    void build_projector(Absorber &ab, bool secondary)
+    {
+        const int lo = ab.wlo, hi = ab.whi;
+        if (hi <= lo) return;
+        // nodes outside the current support are written as zero (the kernel tests the geometry)
+        const int w = hi - lo;
+        const int blocks = std::max(1, std::min(1024, (w * n_modes + 255) / 256));
+        if (ab.hi > ab.lo) {
+            k_swave_projector<<<blocks, 256, 0, stream>>>(d_r.p, Nr, n_modes, lo, hi, ab.mom.p, d_ang00.p,
+                                                           d_mode_l.p, d_mode_m.p, theta, secondary ? 1 : 0, ab.v.p);
+        } else {
+            for (int j = 0; j < n_modes; ++j)
+                CK(cudaMemsetAsync(ab.v.p + (int64_t)j * Nr + lo, 0, (size_t)w * sizeof(double2), stream));
+        }
+        launch_check();
+        ab.wlo = ab.lo;
+        ab.whi = ab.hi;
+    }
+
+    // src/CrankNicolsonModes_absorption.cpp:153-182
+    void build_spherical_absorption()
+    {
+        update_absorption_profile(abs1, R1, epsilon_smear * M1);
+        update_absorption_profile(abs2, R2, epsilon_smear * M2);
+        double ramp = 1.0;
+        if (!isolated && t_i < ramp_end_time()) {
+            ramp = 0.0;
+        } else if (!isolated && t_i < ramp_end_time() + initial_period) {
+            const double xr = (t_i - ramp_end_time()) / initial_period;
+            ramp = 3.0 * xr * xr - 2.0 * xr * xr * xr;
+        }
+        const double Ah1 = 16.0 * M_PI * M1 * M1 * ramp;
+        const double Ah2 = 16.0 * M_PI * M2 * M2 * ramp;
+        if (cpl.mode00 >= 0) {
+            build_projector(abs1, false);
+            build_projector(abs2, true);
+        }
+        abs1.strength = Ah1 * dr;
+        abs2.strength = Ah2 * dr;
+    }
+
+    // Sinks that enter the CN operator: active, non-zero strength, non-empty projector
+    // (src/CrankNicolsonModes_matrices.cpp:106-110).
+    int active_sinks(const Absorber *out[2]) const
+    {
+        int k = 0;
+        if (!op.sink_active || cpl.mode00 < 0) return 0;
+        for (const Absorber *ab : {&abs1, &abs2})
+            if (ab->strength != 0.0 && ab->hi > ab->lo) out[k++] = ab;
+        return k;
+    }
+
+    void sink_dots(const double2 *xv, double2 *dots, const Absorber *const *sk, int k)
+    {
+        k_sink_dots<<<1, 512, 0, stream>>>(xv, Nr, n_modes, k, k > 0 ? sk[0]->v.p : nullptr,
+                                           k > 1 ? sk[1]->v.p : nullptr, k > 0 ? sk[0]->lo : 0,
+                                           k > 0 ? sk[0]->hi : 0, k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, dots);
+        launch_check();
+    }
+
+    ApplyArgs base_args(const double2 *xv, double2 *yv) const
+    {
+        ApplyArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.x = xv;
+        a.y = yv;
+        a.hh = d_hh.p;
+        a.theta = op.theta;
+        a.domega = op.domega;
+        return a;
+    }
+
+    void launch_apply(const ApplyArgs &a)
+    {
+        const unsigned blocks = (unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE);
+        k_apply<<<blocks, APPLY_THREADS, apply_smem, stream>>>(grid(), table(), a);
+        launch_check();
+    }
+
+    // y = A_full x (sparse CN operator plus dt/4 Gamma) with the sink projections of x at `dots`.
+    void apply_A(const double2 *xv, double2 *yv, const Absorber *const *sk, int k, const double2 *dots, double dtv)
+    {
+        ApplyArgs a = base_args(xv, yv);
+        a.alpha = cmake(1.0, 0.0);
+        a.beta = cmake(0.0, 0.5 * dtv);
+        a.use_h0 = 1;
+        a.use_cap = 1;
+        a.vpart = V_POT;
+        a.n_sinks = k;
+        a.sink_dots = dots;
+        for (int i = 0; i < k; ++i) {
+            a.sink_v[i] = sk[i]->v.p;
+            a.sink_coef[i] = 0.25 * dtv * sk[i]->strength;
+            a.sink_lo[i] = sk[i]->lo;
+            a.sink_hi[i] = sk[i]->hi;
+        }
+        launch_apply(a);
+    }
+
+    // -------------------------------------------------------------- preconditioner
+
+    double2 offdiag(double dtv) const
+    {
+        // A's radial off-diagonal: i dt/2 * (-1/(2 mu dr^2))
+        const double alpha_d = 1.0 / (dr * dr);
+        return cmake(0.0, 0.5 * dtv * (-alpha_d / (2 * mu)));
+    }
+
+    // Warm-up window of the chunked scans: the recurrences contract by rho = |off| / |p+|
+    // per node, p+ the attracting pivot of a block whose diagonal sits 1% below the
+    // free one.  The window forgets the chunk's start value to exp(-40).
+    void choose_window(double dtv)
+    {
+        const double kappa = std::abs(offdiag(dtv).y);
+        const std::complex<double> a(1.0, 2.0 * kappa * 0.99), c(-kappa * kappa, 0.0);
+        const std::complex<double> sq = std::sqrt(a * a - 4.0 * c);
+        const double pp = std::max(std::abs((a + sq) * 0.5), std::abs((a - sq) * 0.5));
+        const double rho = kappa / pp;
+        int w = rho < 1.0 ? (int)std::ceil(40.0 / -std::log(rho)) + 16 : 4096;
+        precond_window = std::max(32, std::min(4096, w));
+        precond_chunk = 2048;
+    }
+
+    void factorize(double dtv)
+    {
+        choose_window(dtv);
+        const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
+        CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
+        k_precond_factor<<<dim3(chunks, n_modes), SCAN_THREADS, 0, stream>>>(
+            grid(), table(), d_hh.p, 0.5 * dtv, offdiag(dtv), precond_chunk, precond_window / 2 + 16, dinv.p,
+            d_status.p);
+        launch_check();
+    }
+
+    void precond(const double2 *bv, double2 *xv, double dtv)
+    {
+        const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
+        const size_t smem = (size_t)(std::min(Nr, precond_chunk + 2 * precond_window) + SCAN_THREADS) * sizeof(double2);
+        k_precond_solve<<<dim3(chunks, n_modes), SCAN_THREADS, smem, stream>>>(Nr, precond_chunk, precond_window,
+                                                                               offdiag(dtv), dinv.p, bv, xv);
+        launch_check();
+    }
+
+    // -------------------------------------------------------------- reductions
+
+    // red[0..2*nq-1] = sum conj(a_q) b_q (re, im pairs), synchronous read if `host`.
+    void dots(int nq, const double2 *a0, const double2 *b0, const double2 *a1 = nullptr, const double2 *b1 = nullptr,
+              const double2 *a2 = nullptr, const double2 *b2 = nullptr)
+    {
+        k_dots<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, nq, a0, b0, a1, b1, a2, b2, d_partials.p);
+        launch_check();
+        k_sum_partials<<<1, 256, 0, stream>>>(d_partials.p, vec_blocks, 2 * nq, d_red.p);
+        launch_check();
+    }
+
+    double read_red(int idx)
+    {
+        double vv = 0;
+        CK(cudaMemcpyAsync(&vv, d_red.p + idx, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        sync();
+        return vv;
+    }
+
+    void axpby(double2 al, const double2 *xv, double2 be, const double2 *wv, double2 *yv)
+    {
+        k_axpby<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, al, xv, be, wv, yv);
+        launch_check();
+    }
+
+    // -------------------------------------------------------------- CN solve
+
+    // src/CrankNicolsonModes_matrices.cpp:94-215 with the radial block preconditioner.
+    void solve_CN()
+    {
+        const double dtv = op.dt;
+        dots(1, rhs.p, rhs.p);
+        const double rhs_norm = std::sqrt(read_red(0));
+        if (rhs_norm == 0.0) {
+            CK(cudaMemsetAsync(psi.p, 0, nN * sizeof(double2), stream));
+            last_residual = 0.0;
+            last_iterations = 0;
+            return;
+        }
+        const Absorber *sk[2];
+        const int k = active_sinks(sk);
+        axpby(cmake(1.0 / rhs_norm, 0), rhs.p, cmake(0, 0), nullptr, b.p);
+        axpby(cmake(1.0 / rhs_norm, 0), psi.p, cmake(0, 0), nullptr, x.p);
+        factorize(dtv);
+        Krylov kr;
+        std::memset(&kr, 0, sizeof(kr));
+        kr.n_sinks = k;
+        if (k > 0) {
+            // Woodbury: W_a = P^{-1} v_a, G = diag(1 / (dt/4 g_a)) + v_a^dag W_b (_matrices.cpp:133-145)
+            precond(sk[0]->v.p, W0.p, dtv);
+            if (k > 1) precond(sk[1]->v.p, W1.p, dtv);
+            sink_dots(W0.p, d_dots.p + 4, sk, k);
+            if (k > 1) sink_dots(W1.p, d_dots.p + 6, sk, k);
+            double2 hd[8];
+            CK(cudaMemcpyAsync(hd, d_dots.p, sizeof(hd), cudaMemcpyDeviceToHost, stream));
+            sync();
+            std::complex<double> G[2][2] = {{0, 0}, {0, 0}};
+            for (int a2 = 0; a2 < k; ++a2) {
+                G[a2][a2] += 1.0 / (0.25 * dtv * sk[a2]->strength);
+                for (int b2 = 0; b2 < k; ++b2) {
+                    const double2 vw = hd[4 + 2 * b2 + a2];  // v_a . W_b
+                    G[a2][b2] += std::complex<double>(vw.x, vw.y);
+                    kr.vW[a2][b2] = vw;
+                }
+            }
+            std::complex<double> Gi[2][2];
+            if (k == 1) {
+                Gi[0][0] = 1.0 / G[0][0];
+            } else {
+                const std::complex<double> det = G[0][0] * G[1][1] - G[0][1] * G[1][0];
+                Gi[0][0] = G[1][1] / det;
+                Gi[0][1] = -G[0][1] / det;
+                Gi[1][0] = -G[1][0] / det;
+                Gi[1][1] = G[0][0] / det;
+            }
+            for (int a2 = 0; a2 < 2; ++a2)
+                for (int b2 = 0; b2 < 2; ++b2) kr.Gi[a2][b2] = cmake(Gi[a2][b2].real(), Gi[a2][b2].imag());
+        }
+        // r = b - A_full x; r0 = r
+        sink_dots(x.p, d_dots.p, sk, k);
+        apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv);
+        axpby(cmake(1, 0), b.p, cmake(-1, 0), tmp.p, rr.p);
+        CK(cudaMemcpyAsync(r0.p, rr.p, nN * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+        CK(cudaMemsetAsync(p.p, 0, nN * sizeof(double2), stream));
+        CK(cudaMemsetAsync(v.p, 0, nN * sizeof(double2), stream));
+        dots(2, rr.p, rr.p, b.p, b.p);
+        double hr[4];
+        CK(cudaMemcpyAsync(hr, d_red.p, sizeof(hr), cudaMemcpyDeviceToHost, stream));
+        sync();
+        const double r0n2 = hr[0], b2 = hr[2];
+        const bool eigen_path = k == 0;
+        kr.rho = kr.alpha = kr.omega = cmake(1.0, 0.0);
+        kr.thr = tolerance * tolerance * b2;
+        const double eps = std::numeric_limits<double>::epsilon();
+        kr.restart_thr = eigen_path ? eps * eps * r0n2 : 1e-32 * r0n2;
+        kr.r2 = r0n2;
+        kr.r0r = cmake(r0n2, 0.0);
+        kr.max_iterations = max_iterations;
+        kr.iterations = 0;
+        kr.done = !(r0n2 > kr.thr) || max_iterations <= 0;
+        CK(cudaMemcpyAsync(d_kr.p, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
+        int restarts = 0;
+        Krylov *dk = d_kr.p;
+        const double *red = d_red.p;
+        while (!kr.done) {
+            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_BETA, red);
+            launch_check();
+            CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
+            sync();
+            if (kr.restart) {
+                // Lost biorthogonality: restart from the current residual (_matrices.cpp:69-75)
+                sink_dots(x.p, d_dots.p, sk, k);
+                apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv);
+                axpby(cmake(1, 0), b.p, cmake(-1, 0), tmp.p, rr.p);
+                CK(cudaMemcpyAsync(r0.p, rr.p, nN * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+                dots(1, rr.p, rr.p);
+                const double nr2 = read_red(0);
+                kr.rho = cmake(nr2, 0.0);
+                if (eigen_path) {
+                    kr.restart_thr = eps * eps * nr2;
+                    if (restarts++ == 0) kr.iterations = 0;
+                }
+                kr.beta = cmul(cdiv(kr.rho, kr.rho_old), cdiv(kr.alpha, kr.omega));
+                kr.restart = 0;
+                CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
+            }
+            // p = r + beta (p - omega v); y = M p
+            k_bicg_p<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, rr.p, v.p, p.p);
+            launch_check();
+            const double2 *yv = yP.p;
+            if (k > 0) {
+                precond(p.p, yP.p, dtv);
+                sink_dots(yP.p, d_dots.p + 4, sk, k);
+                k_wood_scalar<<<1, 32, 0, stream>>>(dk, 0, d_dots.p + 4);
+                k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, 0, yP.p, W0.p, W1.p, y.p);
+                launch_check();
+                yv = y.p;
+            } else {
+                precond(p.p, y.p, dtv);
+                yv = y.p;
+            }
+            // v = A y; alpha = rho / r0.v
+            apply_A(yv, v.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[0][0]), dtv);
+            dots(1, r0.p, v.p);
+            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_ALPHA, red);
+            // s = r - alpha v; z = M s
+            k_bicg_s<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, rr.p, v.p, s.p);
+            launch_check();
+            if (k > 0) {
+                precond(s.p, yP.p, dtv);
+                sink_dots(yP.p, d_dots.p + 4, sk, k);
+                k_wood_scalar<<<1, 32, 0, stream>>>(dk, 1, d_dots.p + 4);
+                k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, 1, yP.p, W0.p, W1.p, z.p);
+                launch_check();
+            } else {
+                precond(s.p, z.p, dtv);
+            }
+            // t = A z; omega = t.s / |t|^2
+            apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv);
+            dots(2, t.p, s.p, t.p, t.p);
+            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_OMEGA, red);
+            // x += alpha y + omega z; r = s - omega t
+            k_bicg_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, yv, z.p, rr.p, s.p, t.p, r0.p,
+                                                                   d_partials.p);
+            launch_check();
+            k_sum_partials<<<1, 256, 0, stream>>>(d_partials.p, vec_blocks, 3, d_red.p);
+            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_UPDATE, red);
+            launch_check();
+            CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
+            sync();
+        }
+        last_iterations = kr.iterations;
+        // candidate = x * |rhs|; residual = |A_full candidate - rhs| / |rhs|
+        axpby(cmake(rhs_norm, 0), x.p, cmake(0, 0), nullptr, cand.p);
+        sink_dots(cand.p, d_dots.p, sk, k);
+        apply_A(cand.p, tmp.p, sk, k, d_dots.p, dtv);
+        axpby(cmake(1, 0), tmp.p, cmake(-1, 0), rhs.p, tmp.p);
+        dots(1, tmp.p, tmp.p);
+        int status = 0;
+        CK(cudaMemcpyAsync(&status, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        const double res2 = read_red(0);
+        last_residual = std::isfinite(res2) ? std::sqrt(res2) / rhs_norm : std::numeric_limits<double>::infinity();
+        if (status != 0)
+            throw Error(CNM_ESOLVE, "Radial preconditioner factorization failed (zero or non-finite pivot)");
+        if (!(last_residual <= accept_residual))
+            throw Error(CNM_ESOLVE, "Crank-Nicolson solve failed the relative residual check");
+        k_scale_mask<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, Nr, 1.0, mask ? d_mask.p : nullptr, cand.p, psi.p);
+        launch_check();
+    }
+
+    // -------------------------------------------------------------- step
+
+    void set_extraction_radius(double rex, int n_steps)
+    {
+        r_ex = rex;
+        idx_ex = (int)std::floor(r_ex / dr);
+        if (n_steps < 1 || idx_ex < 1 || idx_ex >= Nr - 1)
+            throw Error(CNM_EINVAL, "Require at least one time sample and an interior extraction radius");
+    }
+
+    void prepare_run(int n_steps, double rex)
+    {
+        set_extraction_radius(rex, n_steps);
+        t_i = 0.0;
+        build_time_dependent_perturbation(t_i);
+        sync();
+    }
+
+    void step(int step_id, cnm_diag *dg, double *ef, double *fl, double *nm, double *en)
+    {
+        if (!initialized) throw Error(CNM_ELOGIC, "initialize() must be called before step()");
+        if (idx_ex < 1) throw Error(CNM_ELOGIC, "run() (cnm_prepare_run) must set the extraction radius first");
+        const double step_start = t_i;
+        t_i += dt;
+        theta += (counter ? -1.0 : 1.0) * Omega * dt;
+        phase += Omega * dt;
+        build_time_dependent_perturbation(t_i);
+        // projections of the old state on the new sinks (for the midpoint accretion rate)
+        const Absorber *all[2] = {&abs1, &abs2};
+        const bool have_sinks = absorption && cpl.mode00 >= 0;
+        if (have_sinks) sink_dots(psi.p, d_dots.p + 2, all, 2);
+        // rhs = B psi - dt/4 Gamma psi
+        const Absorber *sk[2];
+        const int k = active_sinks(sk);
+        sink_dots(psi.p, d_dots.p, sk, k);
+        {
+            ApplyArgs a = base_args(psi.p, rhs.p);
+            a.alpha = cmake(1.0, 0.0);
+            a.beta = cmake(0.0, -0.5 * op.dt);
+            a.use_h0 = 1;
+            a.use_cap = 1;
+            a.vpart = V_POT;
+            a.n_sinks = k;
+            a.sink_dots = d_dots.p;
+            for (int i = 0; i < k; ++i) {
+                a.sink_v[i] = sk[i]->v.p;
+                a.sink_coef[i] = -0.25 * op.dt * sk[i]->strength;
+                a.sink_lo[i] = sk[i]->lo;
+                a.sink_hi[i] = sk[i]->hi;
+            }
+            launch_apply(a);
+        }
+        solve_CN();
+        // diagnostics on the masked end-of-step state with the step's operators
+        sink_dots(psi.p, d_dots.p, sk, k);
+        if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2);
+        const unsigned dblocks = (unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE);
+        k_diagnostics<<<dblocks, APPLY_THREADS, diag_smem, stream>>>(
+            grid(), table(), d_hh.p, op.theta, op.domega, psi.p, idx_ex, k, k > 0 ? sk[0]->v.p : nullptr,
+            k > 1 ? sk[1]->v.p : nullptr, d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
+            k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
+            k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes);
+        launch_check();
+        const int nslots = 2 * n_modes + 3;
+        k_sum_slots<<<(nslots + 127) / 128, 128, 0, stream>>>(d_partials.p, (int)dblocks, nslots, d_red.p);
+        launch_check();
+        double *hs = stage(nslots + 8 * n_modes + 16);
+        CK(cudaMemcpyAsync(hs, d_red.p, nslots * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hs + nslots, d_edge.p, 4 * n_modes * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hs + nslots + 8 * n_modes, d_dots.p, 8 * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+        sync();
+        const double *redh = hs;
+        const double2 *edge = reinterpret_cast<const double2 *>(hs + nslots);
+        const double2 *dh = reinterpret_cast<const double2 *>(hs + nslots + 8 * n_modes);
+        // orbit (src/CrankNicolsonModes.cpp:189-195)
+        if (!isolated && evolve_orbit && t_i > ramp_end_time()) {
+            const double orbit_dt = t_i - std::max(step_start, ramp_end_time());
+            double md[2] = {0.0, 0.0};
+            if (have_sinks)
+                for (int a2 = 0; a2 < 2; ++a2) {
+                    const Absorber *ab = all[a2];
+                    if (ab->strength == 0.0) continue;
+                    // v^dag psi_mid = (v^dag psi + v^dag psi_last) / 2
+                    const std::complex<double> pm(0.5 * (dh[4 + a2].x + dh[2 + a2].x),
+                                                  0.5 * (dh[4 + a2].y + dh[2 + a2].y));
+                    md[a2] = mu * dr * ab->strength * std::norm(pm);
+                }
+            update_time_dependent_increment(orbit_dt, md[0], md[1]);
+        }
+        // diagnostics (src/CrankNicolsonModes_extraction.cpp)
+        const int n = n_modes;
+        const double rx = r[idx_ex];
+        double energy_sum = 0.0;
+        for (int j = 0; j < n; ++j) {
+            const std::complex<double> pl(edge[n + 3 * j].x, edge[n + 3 * j].y);
+            const std::complex<double> pc(edge[n + 3 * j + 1].x, edge[n + 3 * j + 1].y);
+            const std::complex<double> pr(edge[n + 3 * j + 2].x, edge[n + 3 * j + 2].y);
+            const std::complex<double> dpsi(edge[j].x, edge[j].y);
+            const std::complex<double> dU = (pr - pl) / (2.0 * dr) - pc / rx;
+            if (fl) fl[j] = (std::conj(pc) * dU).imag();
+            if (ef) ef[j] = (std::conj(dpsi) * dU).real() / mu;
+            if (nm) nm[j] = redh[j] * dr;
+            if (en) en[j] = redh[n + j] * dr;
+            energy_sum += redh[n + j];
+        }
+        const double energy = (energy_sum + redh[2 * n]) * dr;
+        const double p_bin_inst = redh[2 * n + 1] * dr;
+        const double dV = redh[2 * n + 2] * dr;
+        p_bin = isolated ? 0.0 : power_average.update(t_i, phase, p_bin_inst);
+        if (dg) {
+            dg->R = R;
+            dg->theta = theta;
+            dg->Omega = Omega;
+            dg->M1 = M1;
+            dg->q = q;
+            dg->t = t_i;
+            dg->energy = energy;
+            dg->p_bin = p_bin;
+            dg->p_bin_inst = p_bin_inst;
+            dg->dV_bin_dt = dV;
+            dg->residual = last_residual;
+            dg->iterations = last_iterations;
+        }
+        (void)step_id;
+    }
+
+    // src/CrankNicolsonModes_evolution.cpp:17-72
+    void update_time_dependent_increment(double orbit_dt, double Mdot1, double Mdot2)
+    {
+        double ramp = 1.0;
+        if (t_i < ramp_end_time()) ramp = 0.0;
+        else if (t_i < ramp_end_time() + initial_period) {
+            const double xr = (t_i - ramp_end_time()) / initial_period;
+            ramp = 3.0 * xr * xr - 2.0 * xr * xr * xr;
+        }
+        const double dR_gw = -(64.0 / 5.0) * M1 * M2 * (M1 + M2) / std::pow(R, 3);
+        const double dR_cloud = -2.0 * R * R * p_bin / (M1 * M2);
+        const double dRdt = (dR_gw + dR_cloud) * ramp;
+        R += dRdt * orbit_dt;
+        M1 += Mdot1 * orbit_dt;
+        M2 += Mdot2 * orbit_dt;
+        q = M2 / M1;
+        const double Mt = M1 + M2;
+        R1 = M2 / Mt * R;
+        R2 = M1 / Mt * R;
+        Omega = std::sqrt(Mt / std::pow(R, 3));
+        P = 2.0 * M_PI / Omega;
+        if (ramp_factor == 1.0) dt = P / steps_per_period;
+    }
+
+    // -------------------------------------------------------------- cnm_apply
+
+    void apply_op(int opc, const double *xh, double *yh)
+    {
+        if (!op.built) throw Error(CNM_ELOGIC, "operators exist only after initialize()");
+        CK(cudaMemcpyAsync(tmp.p, xh, nN * sizeof(double2), cudaMemcpyHostToDevice, stream));
+        const Absorber *sk[2];
+        const int k = active_sinks(sk);
+        ApplyArgs a = base_args(tmp.p, cand.p);
+        a.alpha = cmake(0, 0);
+        a.beta = cmake(1, 0);
+        auto with_sinks = [&](double coef) {
+            sink_dots(tmp.p, d_dots.p + 6, sk, k);
+            a.n_sinks = k;
+            a.sink_dots = d_dots.p + 6;
+            for (int i = 0; i < k; ++i) {
+                a.sink_v[i] = sk[i]->v.p;
+                a.sink_coef[i] = coef * sk[i]->strength;
+                a.sink_lo[i] = sk[i]->lo;
+                a.sink_hi[i] = sk[i]->hi;
+            }
+        };
+        switch (opc) {
+        case CNM_OP_H: a.use_h0 = 1; a.use_cap = 1; a.vpart = V_POT; break;
+        case CNM_OP_H0: a.use_h0 = 1; break;
+        case CNM_OP_V: a.vpart = V_POT; break;
+        case CNM_OP_V1: build_hh(d_hh_aux.p, 1.0, 0.0); a.vpart = V_POT; a.hh = d_hh_aux.p; break;
+        case CNM_OP_V2: build_hh(d_hh_aux.p, 0.0, 1.0); a.vpart = V_POT; a.hh = d_hh_aux.p; break;
+        case CNM_OP_DVDT: a.vpart = V_DVDT; break;
+        case CNM_OP_A:
+        case CNM_OP_B:
+        case CNM_OP_AFULL:
+            a.alpha = cmake(1, 0);
+            a.beta = cmake(0, (opc == CNM_OP_B ? -0.5 : 0.5) * op.dt);
+            a.use_h0 = 1;
+            a.use_cap = 1;
+            a.vpart = V_POT;
+            if (opc == CNM_OP_AFULL) with_sinks(0.25 * op.dt);
+            break;
+        case CNM_OP_SINK: a.beta = cmake(0, 0); with_sinks(1.0); break;
+        case CNM_OP_RHS:
+            a.beta = cmake(0, -1);
+            a.use_h0 = 1;
+            a.use_cap = 1;
+            a.vpart = V_POT;
+            with_sinks(-0.5);
+            break;
+        case CNM_OP_CAP: a.use_cap = 1; break;
+        case CNM_OP_PRECOND:
+            factorize(op.dt);
+            precond(tmp.p, cand.p, op.dt);
+            break;
+        default: throw Error(CNM_EINVAL, "unknown operator");
+        }
+        if (opc != CNM_OP_PRECOND) launch_apply(a);
+        CK(cudaMemcpyAsync(yh, cand.p, nN * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+        sync();
+    }
+
+    double sink_strength(int body)
+    {
+        const Absorber &ab = body == 1 ? abs1 : abs2;
+        if (!op.sink_active || ab.strength == 0.0 || ab.hi <= ab.lo || cpl.mode00 < 0) return 0.0;
+        const Absorber *one[1] = {&ab};
+        sink_dots(ab.v.p, d_dots.p + 6, one, 1);
+        double2 vv;
+        CK(cudaMemcpyAsync(&vv, d_dots.p + 6, sizeof(vv), cudaMemcpyDeviceToHost, stream));
+        sync();
+        return ab.strength * vv.x;
+    }
+};
+
+}  // namespace cnm
+
+// ==================================================================== C ABI
+
+struct cnm_handle {
+    cnm::Solver *s = nullptr;
+    std::string err;
+};
+
+static thread_local std::string g_create_error;
+
+template <class F>
+static int guarded(cnm_handle *h, F &&f)
+{
+    if (!h || !h->s) return CNM_EINVAL;
+    try {
+        f(*h->s);
+        return CNM_OK;
+    } catch (const cnm::Error &e) {
+        h->err = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        h->err = e.what();
+        return CNM_ECUDA;
+    }
+}
+
+extern "C" {
+
+int cnm_create(const cnm_params *params, cnm_handle **out)
+{
+    if (!params || !out) return CNM_EINVAL;
+    *out = nullptr;
+    try {
+        cnm_handle *h = new cnm_handle;
+        h->s = new cnm::Solver(*params);
+        *out = h;
+        return CNM_OK;
+    } catch (const cnm::Error &e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return CNM_ECUDA;
+    }
+}
+
+int cnm_destroy(cnm_handle *h)
+{
+    if (!h) return CNM_OK;
+    delete h->s;
+    delete h;
+    return CNM_OK;
+}
+
+const char *cnm_last_error(const cnm_handle *h) { return h ? h->err.c_str() : g_create_error.c_str(); }
+const char *cnm_create_error(void) { return g_create_error.c_str(); }
+
+int cnm_n_modes(const cnm_handle *h, int32_t *n)
+{
+    if (!h || !n) return CNM_EINVAL;
+    *n = h->s->n_modes;
+    return CNM_OK;
+}
+
+int cnm_modes(const cnm_handle *h, int32_t *l, int32_t *m)
+{
+    if (!h || !l || !m) return CNM_EINVAL;
+    for (int j = 0; j < h->s->n_modes; ++j) {
+        l[j] = h->s->cpl.mode_l[j];
+        m[j] = h->s->cpl.mode_m[j];
+    }
+    return CNM_OK;
+}
+
+int cnm_grid(const cnm_handle *h, double *r)
+{
+    if (!h || !r) return CNM_EINVAL;
+    std::copy(h->s->r.begin(), h->s->r.end(), r);
+    return CNM_OK;
+}
+
+int cnm_get_scalars(const cnm_handle *h, cnm_scalars *o)
+{
+    if (!h || !o) return CNM_EINVAL;
+    const cnm::Solver &s = *h->s;
+    o->t = s.t_i;
+    o->theta = s.theta;
+    o->phase = s.phase;
+    o->Omega = s.Omega;
+    o->Omega_0 = s.Omega_0;
+    o->P = s.P;
+    o->R = s.R;
+    o->R1 = s.R1;
+    o->R2 = s.R2;
+    o->M1 = s.M1;
+    o->M2 = s.M2;
+    o->q = s.q;
+    o->dt = s.dt;
+    o->p_bin = s.p_bin;
+    o->steps_per_period = s.steps_per_period;
+    o->evolve_orbit = s.evolve_orbit;
+    o->ramp_secondary_potential = s.ramp_secondary_potential;
+    o->use_block_preconditioner = s.use_block;
+    o->last_solver_iterations = s.last_iterations;
+    o->last_solver_residual = s.last_residual;
+    o->tolerance = s.tolerance;
+    o->max_iterations = s.max_iterations;
+    o->accept_residual = s.accept_residual;
+    return CNM_OK;
+}
+
+int cnm_set_scalars(cnm_handle *h, const cnm_scalars *i)
+{
+    if (!h || !i) return CNM_EINVAL;
+    cnm::Solver &s = *h->s;
+    s.t_i = i->t;
+    s.theta = i->theta;
+    s.phase = i->phase;
+    s.Omega = i->Omega;
+    s.Omega_0 = i->Omega_0;
+    s.P = i->P;
+    s.R = i->R;
+    s.R1 = i->R1;
+    s.R2 = i->R2;
+    s.M1 = i->M1;
+    s.M2 = i->M2;
+    s.q = i->q;
+    s.dt = i->dt;
+    s.p_bin = i->p_bin;
+    s.steps_per_period = i->steps_per_period;
+    s.evolve_orbit = i->evolve_orbit != 0;
+    s.ramp_secondary_potential = i->ramp_secondary_potential != 0;
+    s.use_block = i->use_block_preconditioner != 0;
+    s.last_iterations = i->last_solver_iterations;
+    s.last_residual = i->last_solver_residual;
+    s.tolerance = i->tolerance;
+    s.max_iterations = i->max_iterations;
+    s.accept_residual = i->accept_residual;
+    return CNM_OK;
+}
+
+int cnm_set_initial_state_full(cnm_handle *h, const double *psi0, int64_t n)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.set_initial_state_full(psi0, n); });
+}
+
+int cnm_set_state(cnm_handle *h, const double *psi, int64_t n)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.set_state(psi, n); });
+}
+
+int cnm_get_state(const cnm_handle *h, double *psi, int64_t n)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) { s.get_state(psi, n); });
+}
+
+int cnm_configure_isolated_black_hole(cnm_handle *h, double x)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.configure_isolated_black_hole(x); });
+}
+
+int cnm_initialize(cnm_handle *h)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        s.initialize();
+        s.sync();
+    });
+}
+
+int cnm_set_power_average_orbits(cnm_handle *h, double n_orbits)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        s.power_average = cnm::RollingPhaseAverage(n_orbits);
+        s.orbits_average = n_orbits;
+    });
+}
+
+int cnm_build_damping_mask(cnm_handle *h, double f, double W, int32_t n)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.build_damping_mask(f, W, n); });
+}
+
+int cnm_build_cap(cnm_handle *h, double f, double W, int32_t n)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.build_cap(f, W, n); });
+}
+
+int cnm_prepare_run(cnm_handle *h, int32_t n_steps, double r_ex)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.prepare_run(n_steps, r_ex); });
+}
+
+int cnm_refresh(cnm_handle *h, double time)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        s.build_time_dependent_perturbation(time);
+        s.sync();
+    });
+}
+
+int cnm_step(cnm_handle *h, int32_t step_id, cnm_diag *d, double *ef, double *fl, double *nm, double *en)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.step(step_id, d, ef, fl, nm, en); });
+}
+
+int cnm_should_stop(const cnm_handle *h, int32_t *stop)
+{
+    if (!h || !stop) return CNM_EINVAL;
+    const cnm::Solver &s = *h->s;
+    *stop = (!s.isolated && s.evolve_orbit && s.R <= 6.0) ? 1 : 0;
+    return CNM_OK;
+}
+
+int cnm_apply(cnm_handle *h, int32_t op, const double *x, double *y)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.apply_op(op, x, y); });
+}
+
+int cnm_sink_strength(const cnm_handle *h, int32_t body, double *out)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) { *out = s.sink_strength(body); });
+}
+
+int cnm_sink_active(const cnm_handle *h, int32_t *active)
+{
+    if (!h || !active) return CNM_EINVAL;
+    *active = h->s->sink_active ? 1 : 0;
+    return CNM_OK;
+}
+
+int cnm_sink_vector(const cnm_handle *h, int32_t body, double *out)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) {
+        const cnm::Absorber &ab = body == 1 ? s.abs1 : s.abs2;
+        if (ab.v.p) cnm::cuda_check(cudaMemcpy(out, ab.v.p, s.nN * sizeof(double2), cudaMemcpyDeviceToHost), "cudaMemcpy");
+        else std::fill(out, out + 2 * s.nN, 0.0);
+    });
+}
+
+}  // extern "C"

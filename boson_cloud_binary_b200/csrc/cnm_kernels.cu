@@ -1,0 +1,825 @@
+// cnm_kernels.cu -- sm_100a kernels of the Crank-Nicolson step (FP64 drop-in path).
+//
+// Every kernel here is memory-streaming or FMA work on complex128 vectors in the
+// reference's mode-major layout; see cnm_common.cuh for the data layout.
+#include "cnm_kernels.cuh"
+
+#include <cuda_runtime.h>
+
+namespace cnm {
+
+// ------------------------------------------------------------------ reductions
+
+__device__ __forceinline__ double warp_sum(double v)
+{
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Deterministic block sum of NV doubles per thread; result valid in thread 0.
+template <int NV>
+__device__ void block_sum(double (&v)[NV], double *scratch /* NV * 32 */)
+{
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) scratch[q * 32 + warp] = v[q];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            double s = lane < nw ? scratch[q * 32 + lane] : 0.0;
+            v[q] = warp_sum(s);
+        }
+    }
+    __syncthreads();
+}
+
+// ------------------------------------------------------------------ radial weights
+
+// hh[l][i] = scale * (a1 F1_l(r_i) + a2 (-1)^l F2_l(r_i)) on interior nodes, zero on the
+// two boundary nodes (the reference fills radial_f1/f2 for i = 1..Nr-2 only,
+// src/CrankNicolsonModes_hamiltonian.cpp:178-185).
+__global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
+                           double scale, double a1, double a2)
+{
+    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (int64_t)K * Nr) return;
+    const int l = (int)(idx / Nr), i = (int)(idx % Nr);
+    if (i == 0 || i == Nr - 1) {
+        hh[idx] = 0.0;
+        return;
+    }
+    const double ri = r[i];
+    double f1, f2;
+    if (ri >= R1) f1 = 1 / (1 + q) * pow(R1, l) / pow(ri, l + 1);
+    else f1 = 1 / (1 + q) * pow(ri, l) / pow(R1, l + 1);
+    if (ri >= R2) f2 = 1.0 * q / (1 + q) * pow(R2, l) / pow(ri, l + 1);
+    else f2 = 1.0 * q / (1 + q) * pow(ri, l) / pow(R2, l + 1);
+    const double par = (l & 1) ? -1.0 : 1.0;
+    hh[idx] = scale * (a1 * f1 + a2 * par * f2);
+}
+
+// ------------------------------------------------------------------ operator application
+
+// One CTA owns APPLY_TILE consecutive radial nodes of every mode.  The tile of x
+// (with a one-node halo for the stencil), its phase-rotated copy z = D^dag x and
+// the tile of the hh table sit in shared memory; warp w computes rows
+// j = w, w + nwarps, ... with lane = node, so the coupling term list is read
+// warp-uniformly (broadcast) and every shared-memory access is conflict-free.
+__global__ void __launch_bounds__(APPLY_THREADS) k_apply(Grid g, CouplingTable ct, ApplyArgs a)
+{
+    extern __shared__ double2 smem2[];
+    const int n = g.n_modes, Nr = g.Nr;
+    const int K = 2 * ct.l_max + 1;
+    const int i0 = blockIdx.x * APPLY_TILE;
+    double2 *xs = smem2;                                   // n * (TILE + 2)
+    double2 *zs = xs + n * (APPLY_TILE + 2);               // n * TILE
+    double2 *ph = zs + n * APPLY_TILE;                     // n: exp(i m_k theta)
+    double *hs = reinterpret_cast<double *>(ph + n);       // K * TILE
+    const bool vp = a.vpart != V_NONE;
+
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double s, c;
+        sincos((double)ct.mode_m[k] * a.theta, &s, &c);
+        ph[k] = cmake(c, s);
+    }
+    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
+        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
+        const int i = i0 - 1 + c;
+        xs[e] = (i >= 0 && i < Nr) ? a.x[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
+    }
+    if (vp)
+        for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
+            const int l = e / APPLY_TILE, c = e % APPLY_TILE;
+            const int i = i0 + c;
+            hs[e] = i < Nr ? a.hh[(int64_t)l * Nr + i] : 0.0;
+        }
+    __syncthreads();
+    if (vp)
+        for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
+            const int k = e / APPLY_TILE, c = e % APPLY_TILE;
+            zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
+        }
+    __syncthreads();
+
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int c = lane;  // APPLY_TILE == 32
+    const int i = i0 + c;
+    if (i >= Nr) return;
+    const bool interior = i >= 1 && i <= Nr - 2;
+    const double alpha_d = 1.0 / (g.dr * g.dr);
+    const double ri = g.r[i];
+    for (int j = warp; j < n; j += nw) {
+        const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
+        double2 acc = cmake(0.0, 0.0);
+        if (a.use_h0 && interior) {
+            const int l = ct.mode_l[j];
+            const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+            const double off = -alpha_d / (2 * g.mu);
+            const double2 xl = xs[j * (APPLY_TILE + 2) + c], xr = xs[j * (APPLY_TILE + 2) + c + 2];
+            acc = cadd(cscale(xv, diag), cscale(cadd(xl, xr), off));
+        }
+        if (vp && interior) {
+            double2 av = cmake(0.0, 0.0), am = cmake(0.0, 0.0);
+            const int pb = ct.pair_row_ptr[j], pe = ct.pair_row_ptr[j + 1];
+            for (int p = pb; p < pe; ++p) {
+                const int k = __ldg(ct.pair_col + p);
+                const int tb = __ldg(ct.pair_term_ptr + p), te = __ldg(ct.pair_term_ptr + p + 1);
+                double s = 0.0;
+                for (int t = tb; t < te; ++t) s += __ldg(ct.term_g + t) * hs[__ldg(ct.term_l + t) * APPLY_TILE + c];
+                const double2 zk = zs[k * APPLY_TILE + c];
+                av.x += s * zk.x;
+                av.y += s * zk.y;
+                if (a.vpart == V_DVDT) {
+                    const double sm = s * (double)ct.mode_m[k];
+                    am.x += sm * zk.x;
+                    am.y += sm * zk.y;
+                }
+            }
+            double2 vj;
+            if (a.vpart == V_DVDT) {
+                // (dV/dt x)_j = i s Omega e^{-i m_j theta} sum_k Ahat_jk (m_k - m_j) z_k
+                const double mj = (double)ct.mode_m[j];
+                const double2 d = cmake(am.x - mj * av.x, am.y - mj * av.y);
+                vj = cmuli(cscale(d, a.domega));
+            } else {
+                vj = av;
+            }
+            acc = cadd(acc, cmul(cconj(ph[j]), vj));
+        }
+        if (a.use_cap && g.capw) acc = cadd(acc, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));  // (-i w) x
+        double2 y = cadd(cmul(a.alpha, xv), cmul(a.beta, acc));
+        for (int s = 0; s < a.n_sinks; ++s)
+            if (i >= a.sink_lo[s] && i < a.sink_hi[s]) {
+                const double2 cf = cscale(a.sink_dots[s], a.sink_coef[s]);
+                y = cadd(y, cmul(cf, a.sink_v[s][(int64_t)j * Nr + i]));
+            }
+        a.y[(int64_t)j * Nr + i] = y;
+    }
+}
+
+// ------------------------------------------------------------------ sink projections
+
+// dots[s] = v_s^dagger x over the support of v_s (v_s vanishes elsewhere), one CTA,
+// fixed summation order.
+__global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
+                            const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots)
+{
+    __shared__ double scratch[4 * 32];
+    double acc[4] = {0, 0, 0, 0};
+    for (int s = 0; s < n_sinks; ++s) {
+        const double2 *v = s == 0 ? v0 : v1;
+        const int lo = s == 0 ? lo0 : lo1, hi = s == 0 ? hi0 : hi1;
+        const int w = hi - lo;
+        if (w <= 0) continue;
+        for (int e = threadIdx.x; e < w * n_modes; e += blockDim.x) {
+            const int j = e / w, i = lo + e % w;
+            const int64_t k = (int64_t)j * Nr + i;
+            const double2 d = cconjmul(v[k], x[k]);
+            acc[2 * s] += d.x;
+            acc[2 * s + 1] += d.y;
+        }
+    }
+    block_sum<4>(acc, scratch);
+    if (threadIdx.x == 0) {
+        dots[0] = cmake(acc[0], acc[1]);
+        dots[1] = cmake(acc[2], acc[3]);
+    }
+}
+
+// ------------------------------------------------------------------ preconditioner
+
+// Diagonal of the sparse CN operator A = 1 + i dt/2 (H0 + V + CAP) at (j, i)
+// (src/CrankNicolsonModes_matrices.cpp:27-40).
+__device__ __forceinline__ double2 a_diag(const Grid &g, const CouplingTable &ct, const double *hh, double half_dt,
+                                          int j, int i)
+{
+    double hre = 0.0, him = 0.0;
+    if (i >= 1 && i <= g.Nr - 2) {
+        const int l = ct.mode_l[j];
+        const double alpha_d = 1.0 / (g.dr * g.dr);
+        const double ri = g.r[i];
+        hre = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+        const int p = ct.diag_pair[j];
+        if (p >= 0)
+            for (int t = ct.pair_term_ptr[p]; t < ct.pair_term_ptr[p + 1]; ++t)
+                hre += ct.term_g[t] * hh[(int64_t)ct.term_l[t] * g.Nr + i];
+    }
+    if (g.capw) him = -g.capw[i];
+    // 1 + i (dt/2) (hre + i him) = (1 - dt/2 him) + i dt/2 hre
+    return cmake(1.0 - half_dt * him, half_dt * hre);
+}
+
+// 2x2 complex matrix (Moebius map p -> (m00 p + m01) / (m10 p + m11)).
+struct Mob {
+    double2 m00, m01, m10, m11;
+};
+
+__device__ __forceinline__ Mob mob_mul(const Mob &A, const Mob &B)  // A after B
+{
+    Mob C;
+    C.m00 = cadd(cmul(A.m00, B.m00), cmul(A.m01, B.m10));
+    C.m01 = cadd(cmul(A.m00, B.m01), cmul(A.m01, B.m11));
+    C.m10 = cadd(cmul(A.m10, B.m00), cmul(A.m11, B.m10));
+    C.m11 = cadd(cmul(A.m10, B.m01), cmul(A.m11, B.m11));
+    return C;
+}
+
+__device__ __forceinline__ void mob_normalize(Mob &A)
+{
+    double s = fmax(fmax(fabs(A.m00.x), fabs(A.m00.y)), fmax(fabs(A.m01.x), fabs(A.m01.y)));
+    s = fmax(s, fmax(fmax(fabs(A.m10.x), fabs(A.m10.y)), fmax(fabs(A.m11.x), fabs(A.m11.y))));
+    if (s > 0.0 && isfinite(s)) {
+        // scale by a power of two: exact, and the map is scale invariant
+        int e;
+        frexp(s, &e);
+        const double f = ldexp(1.0, -e);
+        A.m00 = cscale(A.m00, f);
+        A.m01 = cscale(A.m01, f);
+        A.m10 = cscale(A.m10, f);
+        A.m11 = cscale(A.m11, f);
+    }
+}
+
+// Pivot map of node i of one radial block (include/RadialBlockPreconditioner.hpp:59-76):
+// p_i = a_i - l_i d_{i-1} u_{i-1}; with l_i = u_{i-1} = off for 2 <= i <= Nr-2 and zero
+// couplings to the two boundary nodes, p_i = a_i - c / p_{i-1} (c = off^2) in the
+// interior and p_i = a_i at i = 0, 1 and Nr-1.
+__device__ __forceinline__ Mob pivot_map(double2 ai, int i, int Nr, double2 c)
+{
+    Mob M;
+    if (i >= 2 && i <= Nr - 2) {
+        M.m00 = ai;
+        M.m01 = cmake(-c.x, -c.y);
+        M.m10 = cmake(1.0, 0.0);
+        M.m11 = cmake(0.0, 0.0);
+    } else {
+        M.m00 = cmake(0.0, 0.0);
+        M.m01 = ai;
+        M.m10 = cmake(0.0, 0.0);
+        M.m11 = cmake(1.0, 0.0);
+    }
+    return M;
+}
+
+__device__ __forceinline__ double2 mob_apply(const Mob &M, double2 p)
+{
+    return cdiv(cadd(cmul(M.m00, p), M.m01), cadd(cmul(M.m10, p), M.m11));
+}
+
+// Inverse Thomas pivots d_i = 1 / p_i of every radial block.  Grid (chunks, modes);
+// each CTA recomputes the pivot recurrence over its chunk preceded by a warm-up
+// window: the map p -> a - c/p contracts towards the local pivot, so the window
+// start value is forgotten to rounding.  Inside the CTA the recurrence is a
+// parallel scan of 2x2 Moebius matrices.
+__global__ void __launch_bounds__(SCAN_THREADS) k_precond_factor(Grid g, CouplingTable ct, const double *hh,
+                                                                  double half_dt, double2 off, int chunk, int window,
+                                                                  double2 *dinv, int *status)
+{
+    __shared__ Mob tmat[SCAN_THREADS];
+    const int Nr = g.Nr, j = blockIdx.y;
+    const int c0 = blockIdx.x * chunk, c1 = min(Nr, c0 + chunk);
+    const int lo = max(0, c0 - window), hi = c1;
+    const int len = hi - lo;
+    const int per = (len + blockDim.x - 1) / blockDim.x;
+    const int s0 = lo + threadIdx.x * per, s1 = min(hi, s0 + per);
+    const double2 c = cmul(off, off);
+    Mob acc;
+    acc.m00 = cmake(1, 0);
+    acc.m01 = cmake(0, 0);
+    acc.m10 = cmake(0, 0);
+    acc.m11 = cmake(1, 0);
+    for (int i = s0; i < s1; ++i) {
+        acc = mob_mul(pivot_map(a_diag(g, ct, hh, half_dt, j, i), i, Nr, c), acc);
+        mob_normalize(acc);
+    }
+    tmat[threadIdx.x] = acc;
+    __syncthreads();
+    // Hillis-Steele inclusive scan over threads (t composes after t-1).
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        Mob mine = tmat[threadIdx.x];
+        Mob prev;
+        const bool has = threadIdx.x >= (unsigned)o;
+        if (has) prev = tmat[threadIdx.x - o];
+        __syncthreads();
+        if (has) {
+            mine = mob_mul(mine, prev);
+            mob_normalize(mine);
+            tmat[threadIdx.x] = mine;
+        }
+        __syncthreads();
+    }
+    // start value before node lo: any finite guess; exact when lo == 0 (node 0's map is constant)
+    double2 p = a_diag(g, ct, hh, half_dt, j, lo);
+    if (threadIdx.x > 0) p = mob_apply(tmat[threadIdx.x - 1], p);
+    for (int i = s0; i < s1; ++i) {
+        p = mob_apply(pivot_map(a_diag(g, ct, hh, half_dt, j, i), i, Nr, c), p);
+        if (i >= c0) {
+            const double m = cabs2(p);
+            if (!(m > 0.0) || !isfinite(m)) {
+                atomicOr(status, 1);
+                dinv[(int64_t)j * Nr + i] = cmake(0.0, 0.0);
+            } else {
+                dinv[(int64_t)j * Nr + i] = crcp(p);
+            }
+        }
+    }
+}
+
+// Affine map y -> A y + B.
+struct Aff {
+    double2 A, B;
+};
+
+__device__ __forceinline__ Aff aff_then(const Aff &first, const Aff &second)  // second(first(y))
+{
+    Aff r;
+    r.A = cmul(second.A, first.A);
+    r.B = cadd(cmul(second.A, first.B), second.B);
+    return r;
+}
+
+// x = P^{-1} b for the per-mode tridiagonal blocks (include/RadialBlockPreconditioner.hpp:80-98):
+// forward y_i = d_i (b_i - l_i y_{i-1}), backward x_i = y_i - u_i d_i x_{i+1}.  Both sweeps
+// are linear recurrences solved by an in-CTA scan of affine maps over the chunk and
+// its warm-up windows (the recurrences contract, |l_i d_i| < 1).  If `fuse` is set
+// the input is b = r + beta (p - omega v) and b is also stored to `bout` (the
+// BiCGSTAB search direction), or b = r - alpha v (fuse == 2).
+__global__ void __launch_bounds__(SCAN_THREADS) k_precond_solve(int Nr, int chunk, int window, double2 off,
+                                                                 const double2 *dinv, const double2 *b, double2 *x)
+{
+    extern __shared__ double2 ys[];
+    __shared__ Aff tf[SCAN_THREADS];
+    const int j = blockIdx.y;
+    const int c0 = blockIdx.x * chunk, c1 = min(Nr, c0 + chunk);
+    const int lo = max(0, c0 - window), hi = min(Nr, c1 + window);
+    const int len = hi - lo;
+    int per = (len + blockDim.x - 1) / blockDim.x;
+    per |= 1;  // odd stride: conflict-free 16-byte shared-memory accesses
+    const int s0 = lo + threadIdx.x * per, s1 = min(hi, s0 + per);
+    const int64_t base = (int64_t)j * Nr;
+
+    // forward sweep
+    Aff acc{cmake(1, 0), cmake(0, 0)};
+    for (int i = s0; i < s1; ++i) {
+        const double2 d = dinv[base + i];
+        const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        const Aff m{cmake(-(l.x * d.x - l.y * d.y), -(l.x * d.y + l.y * d.x)), cmul(d, b[base + i])};
+        acc = aff_then(acc, m);
+    }
+    tf[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        Aff mine = tf[threadIdx.x], prev;
+        const bool has = threadIdx.x >= (unsigned)o;
+        if (has) prev = tf[threadIdx.x - o];
+        __syncthreads();
+        if (has) tf[threadIdx.x] = aff_then(prev, mine);
+        __syncthreads();
+    }
+    double2 y = threadIdx.x > 0 ? tf[threadIdx.x - 1].B : cmake(0, 0);
+    for (int i = s0; i < s1; ++i) {
+        const double2 d = dinv[base + i];
+        const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        y = cmul(d, csub(b[base + i], cmul(l, y)));
+        ys[i - lo] = y;
+    }
+    __syncthreads();
+    // backward sweep, right to left
+    Aff bcc{cmake(1, 0), cmake(0, 0)};
+    for (int i = s1 - 1; i >= s0; --i) {
+        const double2 d = dinv[base + i];
+        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        const Aff m{cmake(-(u.x * d.x - u.y * d.y), -(u.x * d.y + u.y * d.x)), ys[i - lo]};
+        bcc = aff_then(bcc, m);
+    }
+    tf[threadIdx.x] = bcc;
+    __syncthreads();
+    const int T = blockDim.x;
+    for (int o = 1; o < T; o <<= 1) {
+        Aff mine = tf[threadIdx.x], prev;
+        const bool has = (int)threadIdx.x + o < T;
+        if (has) prev = tf[threadIdx.x + o];
+        __syncthreads();
+        if (has) tf[threadIdx.x] = aff_then(prev, mine);
+        __syncthreads();
+    }
+    double2 xv = (int)threadIdx.x + 1 < T ? tf[threadIdx.x + 1].B : cmake(0, 0);
+    for (int i = s1 - 1; i >= s0; --i) {
+        const double2 d = dinv[base + i];
+        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        xv = csub(ys[i - lo], cmul(cmul(u, d), xv));
+        if (i >= c0 && i < c1) x[base + i] = xv;
+    }
+}
+
+// ------------------------------------------------------------------ vector kernels
+
+// Per-CTA partial sums of up to three complex inner products conj(a_q) . b_q over n
+// elements (grid-stride, fixed assignment, deterministic).
+__global__ void __launch_bounds__(VEC_THREADS) k_dots(int64_t n, int nq, const double2 *a0, const double2 *b0,
+                                                       const double2 *a1, const double2 *b1, const double2 *a2,
+                                                       const double2 *b2, double *partials)
+{
+    __shared__ double scratch[6 * 32];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double2 d = cconjmul(a0[e], b0[e]);
+        acc[0] += d.x;
+        acc[1] += d.y;
+        if (nq > 1) {
+            d = cconjmul(a1[e], b1[e]);
+            acc[2] += d.x;
+            acc[3] += d.y;
+        }
+        if (nq > 2) {
+            d = cconjmul(a2[e], b2[e]);
+            acc[4] += d.x;
+            acc[5] += d.y;
+        }
+    }
+    block_sum<6>(acc, scratch);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 6; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = acc[q];
+}
+
+// out[q] = sum over `nblocks` partials of slot q (fixed order), q < nslots.
+__global__ void k_sum_partials(const double *partials, int nblocks, int nslots, double *out)
+{
+    __shared__ double scratch[6 * 32];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        for (int q = 0; q < nslots; ++q) acc[q] += partials[(int64_t)q * nblocks + b];
+    block_sum<6>(acc, scratch);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < nslots; ++q) out[q] = acc[q];
+}
+
+// y = a x (+ b w): scaled copies and combinations with host-side scalars.
+__global__ void k_axpby(int64_t n, double2 a, const double2 *x, double2 b, const double2 *w, double2 *y)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double2 v = cmul(a, x[e]);
+        if (w) v = cadd(v, cmul(b, w[e]));
+        y[e] = v;
+    }
+}
+
+// y *= mask(i) (the damping mask is one profile shared by every mode).
+__global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y)
+{
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const double f = mask ? s * mask[e % Nr] : s;
+        y[e] = cscale(x[e], f);
+    }
+}
+
+// ---- BiCGSTAB (src/CrankNicolsonModes_matrices.cpp:47-91), device-resident scalars
+
+__global__ void k_bicg_p(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *p)
+{
+    const double2 beta = kr->beta, w = kr->omega;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        p[e] = cadd(r[e], cmul(beta, csub(p[e], cmul(w, v[e]))));
+}
+
+__global__ void k_bicg_s(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *s)
+{
+    const double2 al = kr->alpha;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        s[e] = csub(r[e], cmul(al, v[e]));
+}
+
+// x += alpha y + omega z; r = s - omega t; per-CTA partials of |r|^2 and r0 . r.
+__global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, const Krylov *kr, double2 *x, const double2 *y,
+                                                              const double2 *z, double2 *r, const double2 *s,
+                                                              const double2 *t, const double2 *r0, double *partials)
+{
+    __shared__ double scratch[3 * 32];
+    const double2 al = kr->alpha, w = kr->omega;
+    double acc[3] = {0, 0, 0};
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        x[e] = cadd(x[e], cadd(cmul(al, y[e]), cmul(w, z[e])));
+        const double2 rv = csub(s[e], cmul(w, t[e]));
+        r[e] = rv;
+        acc[0] += cabs2(rv);
+        const double2 d = cconjmul(r0[e], rv);
+        acc[1] += d.x;
+        acc[2] += d.y;
+    }
+    block_sum<3>(acc, scratch);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 3; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = acc[q];
+}
+
+// Woodbury correction y = yP - sum_a W_a c_a on the vector (src/CrankNicolsonModes_matrices.cpp:146-153).
+__global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2 *yP, const double2 *W0,
+                           const double2 *W1, double2 *y)
+{
+    const double2 c0 = kr->wc[which][0], c1 = kr->wc[which][1];
+    const int k = kr->n_sinks;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double2 corr = cmul(W0[e], c0);
+        if (k > 1) corr = cadd(corr, cmul(W1[e], c1));
+        y[e] = csub(yP[e], corr);
+    }
+}
+
+// Scalar steps of the recurrence, one thread.
+__global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
+{
+    if (threadIdx.x != 0) return;
+    switch (stage) {
+    case KS_BETA: {  // rho_old = rho; rho = r0 . r; restart check; beta
+        const double2 rho_old = kr->rho;
+        kr->rho = kr->r0r;
+        kr->restart = sqrt(cabs2(kr->rho)) < kr->restart_thr ? 1 : 0;
+        kr->rho_old = rho_old;
+        kr->beta = cmul(cdiv(kr->rho, rho_old), cdiv(kr->alpha, kr->omega));
+        break;
+    }
+    case KS_ALPHA:  // alpha = rho / (r0 . v); red = {re, im}
+        kr->alpha = cdiv(kr->rho, cmake(red[0], red[1]));
+        break;
+    case KS_OMEGA: {  // red = {ts.re, ts.im, tt}
+        const double tt = red[2];
+        kr->omega = tt > 0.0 ? cscale(cmake(red[0], red[1]), 1.0 / tt) : cmake(0.0, 0.0);
+        break;
+    }
+    case KS_UPDATE:  // red = {|r|^2, r0.r re, im}
+        kr->r2 = red[0];
+        kr->r0r = cmake(red[1], red[2]);
+        kr->iterations += 1;
+        kr->done = !(kr->r2 > kr->thr) || kr->iterations >= kr->max_iterations;
+        break;
+    default: break;
+    }
+}
+
+// Woodbury projections: with proj_a = v_a^dag yP (dots), c = G^{-1} proj and the sink
+// dots of the corrected vector, v_a^dag y = proj_a - sum_b (v_a^dag W_b) c_b.
+__global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj)
+{
+    if (threadIdx.x != 0) return;
+    const int k = kr->n_sinks;
+    double2 c[2] = {cmake(0, 0), cmake(0, 0)};
+    for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) c[a] = cadd(c[a], cmul(kr->Gi[a][b], proj[b]));
+    for (int a = 0; a < 2; ++a) kr->wc[which][a] = c[a];
+    for (int a = 0; a < k; ++a) {
+        double2 d = proj[a];
+        for (int b = 0; b < k; ++b) d = csub(d, cmul(kr->vW[a][b], c[b]));
+        kr->sdots[which][a] = d;
+    }
+}
+
+// ------------------------------------------------------------------ absorbers
+
+// Legendre moments 2 pi int K(s) P_l(cos gamma) d cos gamma of one body's kernel at one
+// radial node per CTA (src/CrankNicolsonModes_absorption.cpp:35-70): Gauss-Legendre
+// quadrature over the angular cap z = 1 - cos(gamma) in [0, cap], one quadrature node
+// per thread, Legendre recurrence to degree 2 l_max.
+__global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
+                              const double *gl_x, const double *gl_w, int degree, double *mom)
+{
+    extern __shared__ double sh[];  // (degree + 1) * nwarps
+    const int i = lo + blockIdx.x;
+    if (i < 1 || i > Nr - 2) return;
+    const double delta = r[i] - radius;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (fabs(delta) >= width) {
+        for (int l = threadIdx.x; l <= degree; l += blockDim.x) mom[(int64_t)l * Nr + i] = 0.0;
+        return;
+    }
+    if (radius == 0.0) {
+        if (threadIdx.x == 0) {
+            const double x = r[i] / width;
+            mom[i] = 4.0 * M_PI * exp(-1.0 / (1.0 - x * x));
+            for (int l = 1; l <= degree; ++l) mom[(int64_t)l * Nr + i] = 0.0;
+        }
+        return;
+    }
+    const double product = 2.0 * r[i] * radius;
+    const double cap = fmin(2.0, (width * width - delta * delta) / product);
+    for (int l = 0; l <= degree; ++l) {
+        double part = 0.0;
+        for (int k = threadIdx.x; k < nq; k += blockDim.x) {
+            const double z = cap * gl_x[k];
+            const double u = 1.0 - z;
+            const double d2 = delta * delta + product * z;
+            const double weight = 2.0 * M_PI * cap * gl_w[k] * exp(-1.0 / (1.0 - d2 / (width * width)));
+            double pl;
+            if (l == 0) pl = 1.0;
+            else {
+                double prev = 1.0, cur = u;
+                for (int m = 2; m <= l; ++m) {
+                    const double next = ((2 * m - 1) * u * cur - (m - 1) * prev) / m;
+                    prev = cur;
+                    cur = next;
+                }
+                pl = cur;
+            }
+            part += weight * pl;
+        }
+        part = warp_sum(part);
+        if (lane == 0) sh[l * nw + warp] = part;
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l <= degree; l += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += sh[l * nw + w];
+        mom[(int64_t)l * Nr + i] = s;
+    }
+}
+
+// Discrete volume normalisation sum_i dr r_i^2 K_0(r_i) = 1 (_absorption.cpp:71-80), one CTA.
+__global__ void k_abs_normalize(const double *r, int Nr, int lo, int hi, double dr, int degree, double *mom)
+{
+    __shared__ double scratch[32];
+    __shared__ double norm_s;
+    double acc[1] = {0.0};
+    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x)
+        if (i >= 1 && i <= Nr - 2) acc[0] += dr * r[i] * r[i] * mom[i];
+    block_sum<1>(acc, scratch);
+    if (threadIdx.x == 0) norm_s = acc[0];
+    __syncthreads();
+    const double norm = norm_s;
+    if (norm > 0.0)
+        for (int e = threadIdx.x; e < (degree + 1) * (hi - lo); e += blockDim.x) {
+            const int l = e / (hi - lo), i = lo + e % (hi - lo);
+            mom[(int64_t)l * Nr + i] /= norm;
+        }
+}
+
+// v[j, i] = r_i sqrt(4 pi) parity_j kappa_j(r_i), kappa_j = mom_{l_j}(r_i) ang_j e^{-i m_j theta}
+// (_absorption.cpp:127-151; the only Gaunt term of the pair (j, (0,0)) has l* = l_j and
+// m* = -m_j).  Writes the support [lo, hi) of every mode.
+__global__ void k_swave_projector(const double *r, int Nr, int n_modes, int lo, int hi, const double *mom,
+                                  const double *ang00, const int *mode_l, const int *mode_m, double theta,
+                                  int secondary, double2 *v)
+{
+    const int w = hi - lo;
+    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < w * n_modes; e += gridDim.x * blockDim.x) {
+        const int j = e / w, i = lo + e % w;
+        double2 val = cmake(0.0, 0.0);
+        if (i >= 1 && i <= Nr - 2 && ang00[j] != 0.0) {
+            const int ms = -mode_m[j];
+            double sn, cs;
+            sincos((double)ms * theta, &sn, &cs);
+            const double parity = (secondary && (ms & 1)) ? -1.0 : 1.0;
+            const double m = mom[(int64_t)mode_l[j] * Nr + i];
+            const double2 kappa = cscale(cmake(cs, sn), m * ang00[j]);
+            val = cscale(kappa, r[i] * sqrt(4.0 * M_PI) * parity);
+        }
+        v[(int64_t)j * Nr + i] = val;
+    }
+}
+
+// ------------------------------------------------------------------ diagnostics
+
+// One pass over nodes 0..idx_ex for every mode (src/CrankNicolsonModes_extraction.cpp:8-129):
+// with Hx, Vx and dV/dt x rebuilt on chip (same tiling as k_apply) it accumulates per CTA
+//   norms_j  = sum_{i < idx_ex} |psi|^2,  energies_j = sum_{i < idx_ex} Re conj(psi) (H psi),
+//   e_edge   = sum_j Re conj(psi) (H psi) at i = idx_ex,
+//   p_bin    = sum_{i <= idx_ex} Re conj(psi) (dVdt psi),
+//   dV       = sum_{i <= idx_ex} Re conj(dpsi/dt) (V psi),  dpsi/dt = -i H psi - Gamma psi / 2,
+// and stores dpsi/dt at idx_ex for the energy flux.  Partials layout: [slot][block],
+// slots 0..n-1 norms, n..2n-1 energies, 2n e_edge, 2n+1 p_bin, 2n+2 dV.
+__global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics(Grid g, CouplingTable ct, const double *hh,
+                                                                double theta, double domega, const double2 *psi,
+                                                                int idx_ex, int n_sinks, const double2 *sv0,
+                                                                const double2 *sv1, const double2 *sink_dots,
+                                                                double sink_coef0, double sink_coef1, int slo0,
+                                                                int shi0, int slo1, int shi1, double *partials,
+                                                                double2 *dpsi_edge, double2 *psi_edge)
+{
+    extern __shared__ double2 smem2[];
+    const int n = g.n_modes, Nr = g.Nr;
+    const int K = 2 * ct.l_max + 1;
+    const int i0 = blockIdx.x * APPLY_TILE;
+    double2 *xs = smem2;
+    double2 *zs = xs + n * (APPLY_TILE + 2);
+    double2 *ph = zs + n * APPLY_TILE;
+    double *hs = reinterpret_cast<double *>(ph + n);
+    double *red = hs + K * APPLY_TILE;  // (2n + 3) * nwarps
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double s, c;
+        sincos((double)ct.mode_m[k] * theta, &s, &c);
+        ph[k] = cmake(c, s);
+    }
+    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
+        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
+        const int i = i0 - 1 + c;
+        xs[e] = (i >= 0 && i < Nr) ? psi[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
+    }
+    for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
+        const int l = e / APPLY_TILE, c = e % APPLY_TILE;
+        const int i = i0 + c;
+        hs[e] = i < Nr ? hh[(int64_t)l * Nr + i] : 0.0;
+    }
+    for (int e = threadIdx.x; e < (2 * n + 3) * nw; e += blockDim.x) red[e] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
+        const int k = e / APPLY_TILE, c = e % APPLY_TILE;
+        zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
+    }
+    __syncthreads();
+
+    const int c = lane;
+    const int i = i0 + c;
+    const bool active = i < Nr && i <= idx_ex;
+    const bool interior = i >= 1 && i <= Nr - 2;
+    const double alpha_d = 1.0 / (g.dr * g.dr);
+    double e_edge = 0.0, pb = 0.0, dv = 0.0;
+    for (int j = warp; j < n; j += nw) {
+        double nrm = 0.0, en = 0.0;
+        if (active) {
+            const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
+            double2 hx = cmake(0.0, 0.0), vx = cmake(0.0, 0.0), dx = cmake(0.0, 0.0);
+            if (interior) {
+                const int l = ct.mode_l[j];
+                const double ri = g.r[i];
+                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+                const double off = -alpha_d / (2 * g.mu);
+                hx = cadd(cscale(xv, diag),
+                          cscale(cadd(xs[j * (APPLY_TILE + 2) + c], xs[j * (APPLY_TILE + 2) + c + 2]), off));
+                double2 av = cmake(0.0, 0.0), am = cmake(0.0, 0.0);
+                for (int p = ct.pair_row_ptr[j]; p < ct.pair_row_ptr[j + 1]; ++p) {
+                    const int k = __ldg(ct.pair_col + p);
+                    double s = 0.0;
+                    for (int t = __ldg(ct.pair_term_ptr + p); t < __ldg(ct.pair_term_ptr + p + 1); ++t)
+                        s += __ldg(ct.term_g + t) * hs[__ldg(ct.term_l + t) * APPLY_TILE + c];
+                    const double2 zk = zs[k * APPLY_TILE + c];
+                    av.x += s * zk.x;
+                    av.y += s * zk.y;
+                    const double sm = s * (double)ct.mode_m[k];
+                    am.x += sm * zk.x;
+                    am.y += sm * zk.y;
+                }
+                const double mj = (double)ct.mode_m[j];
+                vx = cmul(cconj(ph[j]), av);
+                dx = cmul(cconj(ph[j]), cmuli(cscale(cmake(am.x - mj * av.x, am.y - mj * av.y), domega)));
+                hx = cadd(hx, vx);
+            }
+            if (g.capw) hx = cadd(hx, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
+            // dpsi/dt = -i H psi - Gamma psi / 2
+            double2 dp = cmake(hx.y, -hx.x);
+            if (n_sinks > 0 && i >= slo0 && i < shi0)
+                dp = cadd(dp, cmul(cscale(sink_dots[0], sink_coef0), sv0[(int64_t)j * Nr + i]));
+            if (n_sinks > 1 && i >= slo1 && i < shi1)
+                dp = cadd(dp, cmul(cscale(sink_dots[1], sink_coef1), sv1[(int64_t)j * Nr + i]));
+            const double ce = cconjmul(xv, hx).x;
+            if (i < idx_ex) {
+                nrm = cabs2(xv);
+                en = ce;
+            } else {
+                e_edge += ce;
+                dpsi_edge[j] = dp;
+                psi_edge[3 * j] = xs[j * (APPLY_TILE + 2) + c];
+                psi_edge[3 * j + 1] = xv;
+                psi_edge[3 * j + 2] = xs[j * (APPLY_TILE + 2) + c + 2];
+            }
+            pb += cconjmul(xv, dx).x;
+            dv += cconjmul(dp, vx).x;
+        }
+        nrm = warp_sum(nrm);
+        en = warp_sum(en);
+        if (lane == 0) {
+            red[j * nw + warp] = nrm;
+            red[(n + j) * nw + warp] = en;
+        }
+    }
+    e_edge = warp_sum(e_edge);
+    pb = warp_sum(pb);
+    dv = warp_sum(dv);
+    if (lane == 0) {
+        red[(2 * n) * nw + warp] = e_edge;
+        red[(2 * n + 1) * nw + warp] = pb;
+        red[(2 * n + 2) * nw + warp] = dv;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 2 * n + 3; q += blockDim.x) {
+        double s = 0.0;
+        for (int w = 0; w < nw; ++w) s += red[q * nw + w];
+        partials[(int64_t)q * gridDim.x + blockIdx.x] = s;
+    }
+}
+
+// out[q] = sum_b partials[q][b] for q < nslots (fixed order); one thread per slot.
+__global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out)
+{
+    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    if (q >= nslots) return;
+    double s = 0.0;
+    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)q * nblocks + b];
+    out[q] = s;
+}
+
+}  // namespace cnm

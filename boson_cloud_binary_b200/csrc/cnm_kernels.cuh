@@ -1,0 +1,65 @@
+// cnm_kernels.cuh -- kernel declarations and launch constants.
+#pragma once
+
+#include "cnm_common.cuh"
+
+namespace cnm {
+
+constexpr int APPLY_TILE = 32;      // radial nodes per CTA in the operator kernels (= warp width)
+constexpr int APPLY_THREADS = 256;  // 8 warps share the rows of a tile
+constexpr int SCAN_THREADS = 256;   // preconditioner scan CTAs
+constexpr int VEC_THREADS = 256;    // streaming vector kernels
+
+// Device-resident scalars of one BiCGSTAB solve (src/CrankNicolsonModes_matrices.cpp:47-91)
+// and of its Woodbury correction (:133-157).
+struct Krylov {
+    double2 rho, rho_old, alpha, omega, beta;
+    double2 r0r;          // r0 . r of the current residual
+    double r2;            // |r|^2
+    double thr;           // tol^2 |b|^2
+    double restart_thr;   // 1e-32 |r0|^2 (sink path) or eps^2 |r0|^2 (Eigen path)
+    int iterations, max_iterations, done, restart;
+    int n_sinks;
+    double2 Gi[2][2];     // G^{-1}
+    double2 vW[2][2];     // v_a . W_b
+    double2 wc[2][2];     // c = G^{-1} proj for the two preconditioner calls of an iteration
+    double2 sdots[2][2];  // sink projections of the corrected vectors y and z
+};
+
+enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3 };
+
+__global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
+                           double scale, double a1, double a2);
+__global__ void k_apply(Grid g, CouplingTable ct, ApplyArgs a);
+__global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
+                            const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots);
+__global__ void k_precond_factor(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off,
+                                 int chunk, int window, double2 *dinv, int *status);
+__global__ void k_precond_solve(int Nr, int chunk, int window, double2 off, const double2 *dinv,
+                                const double2 *b, double2 *x);
+__global__ void k_dots(int64_t n, int nq, const double2 *a0, const double2 *b0, const double2 *a1,
+                       const double2 *b1, const double2 *a2, const double2 *b2, double *partials);
+__global__ void k_sum_partials(const double *partials, int nblocks, int nslots, double *out);
+__global__ void k_axpby(int64_t n, double2 a, const double2 *x, double2 b, const double2 *w, double2 *y);
+__global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y);
+__global__ void k_bicg_p(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *p);
+__global__ void k_bicg_s(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *s);
+__global__ void k_bicg_update(int64_t n, const Krylov *kr, double2 *x, const double2 *y, const double2 *z,
+                              double2 *r, const double2 *s, const double2 *t, const double2 *r0, double *partials);
+__global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2 *yP, const double2 *W0,
+                           const double2 *W1, double2 *y);
+__global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red);
+__global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj);
+__global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
+                              const double *gl_x, const double *gl_w, int degree, double *mom);
+__global__ void k_abs_normalize(const double *r, int Nr, int lo, int hi, double dr, int degree, double *mom);
+__global__ void k_swave_projector(const double *r, int Nr, int n_modes, int lo, int hi, const double *mom,
+                                  const double *ang00, const int *mode_l, const int *mode_m, double theta,
+                                  int secondary, double2 *v);
+__global__ void k_diagnostics(Grid g, CouplingTable ct, const double *hh, double theta, double domega,
+                              const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
+                              const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0,
+                              int slo1, int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge);
+__global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out);
+
+}  // namespace cnm

@@ -1,0 +1,189 @@
+/*
+ * cnm_gpu.h -- C ABI of the B200 Crank-Nicolson step of CrankNicolsonModes.
+ *
+ * The reference (rdellamonica/boson-cloud-binary) exposes its solver as the C++
+ * class CrankNicolsonModes (include/CrankNicolsonModes.hpp:60-455).  This header
+ * is the flat interface underneath a drop-in replacement of that class: plain
+ * pointers and sizes, no Eigen or torch types.  Every entry point names the
+ * reference member it replaces.
+ *
+ * Conventions
+ *  - A handle owns all device memory of one binary; host buffers belong to the
+ *    caller.  A handle must not be used from two threads at once.
+ *  - States are complex128, stored as interleaved (re, im) doubles, mode-major:
+ *    entry j*Nr+i is mode j at radial node i, exactly the reference's layout
+ *    (include/CrankNicolsonModes.hpp:10-12).
+ *  - Every function returns CNM_OK (0) or an error code; cnm_last_error()
+ *    gives the message.  The codes map one to one onto the exceptions the
+ *    reference throws: CNM_EINVAL <-> std::invalid_argument,
+ *    CNM_ELOGIC <-> std::logic_error, CNM_ESOLVE <-> std::runtime_error.
+ *  - Calls are synchronous with respect to the host.
+ */
+#ifndef CNM_GPU_H
+#define CNM_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum cnm_status {
+    CNM_OK = 0,
+    CNM_EINVAL = 1,   /* std::invalid_argument in the reference */
+    CNM_ELOGIC = 2,   /* std::logic_error */
+    CNM_ESOLVE = 3,   /* std::runtime_error: the CN solve failed its residual check */
+    CNM_ECUDA = 4,    /* CUDA runtime error, or the CUDA kernels are unavailable */
+    CNM_ENOMEM = 5,   /* device allocation failed */
+    CNM_EDEVICE = 6   /* a device-side check failed (non-finite pivot, scan window) */
+};
+
+enum cnm_precision {
+    CNM_FP64 = 0      /* complex128 everywhere: the drop-in path */
+};
+
+/* Operators for cnm_apply (all of size Nr*n_modes). */
+enum cnm_operator {
+    CNM_OP_H = 0,      /* conservative Hamiltonian H = H0 + V (+ CAP)               */
+    CNM_OP_H0 = 1,     /* free radial Hamiltonian with the centrifugal term         */
+    CNM_OP_V = 2,      /* active potential V1 + ramp * V2                           */
+    CNM_OP_V1 = 3,     /* primary's potential                                      */
+    CNM_OP_V2 = 4,     /* companion's potential                                    */
+    CNM_OP_DVDT = 5,   /* dV/dt from the orbital rotation                          */
+    CNM_OP_A = 6,      /* sparse CN operator 1 + i dt H / 2                        */
+    CNM_OP_B = 7,      /* sparse CN operator 1 - i dt H / 2                        */
+    CNM_OP_SINK = 8,   /* Gamma = sum_a g_a v_a v_a^dagger (zero when inactive)    */
+    CNM_OP_RHS = 9,    /* schrodinger_rhs: -i H x - Gamma x / 2                    */
+    CNM_OP_AFULL = 10, /* A + (dt/4) Gamma, the operator BiCGSTAB inverts          */
+    CNM_OP_CAP = 11,   /* diagonal complex absorbing potential (zero if not built) */
+    CNM_OP_PRECOND = 12 /* inverse of the per-mode radial blocks of A              */
+};
+
+typedef struct cnm_handle cnm_handle;
+
+/* Constructor arguments, in the order of CrankNicolsonModes::CrankNicolsonModes
+ * (include/CrankNicolsonModes.hpp:84; src/CrankNicolsonModes.cpp:11-50). */
+typedef struct cnm_params {
+    int32_t Nr;
+    double L;
+    double dt;
+    double epsilon;
+    int32_t l_max;
+    double mu;
+    double M_c;
+    double q;
+    double a;
+    double R;
+    int32_t counter;
+    int32_t absorption;
+    int32_t save_every;
+    double ramp_periods;
+    double epsilon_smear;
+    int32_t precision;   /* enum cnm_precision */
+} cnm_params;
+
+/* The evolving public scalars of the class (include/CrankNicolsonModes.hpp:88-158)
+ * plus the private time t_i, the phase-averaged p_bin and the solver knobs that
+ * the reference hard-codes (src/CrankNicolsonModes_matrices.cpp:19-20). */
+typedef struct cnm_scalars {
+    double t;              /* t_i, time of the current state                    */
+    double theta, phase, Omega, Omega_0, P;
+    double R, R1, R2, M1, M2, q;
+    double dt;
+    double p_bin;
+    double steps_per_period;
+    int32_t evolve_orbit;
+    int32_t ramp_secondary_potential;
+    int32_t use_block_preconditioner;
+    int32_t last_solver_iterations;
+    double last_solver_residual;
+    double tolerance;      /* BiCGSTAB relative tolerance, reference 1e-10       */
+    int32_t max_iterations;/* reference 500                                      */
+    double accept_residual;/* acceptance of the true residual, reference 1e-9    */
+} cnm_scalars;
+
+/* One step's diagnostics: the rows step() appends to R.txt ... energy_modes.txt
+ * (src/CrankNicolsonModes.cpp:197-226).  The four per-mode arrays are written to
+ * caller buffers of n_modes doubles each (any of them may be NULL). */
+typedef struct cnm_diag {
+    double R, theta, Omega, M1, q, t;
+    double energy, p_bin, p_bin_inst, dV_bin_dt;
+    double residual;
+    int32_t iterations;
+} cnm_diag;
+
+/* --- lifetime ---------------------------------------------------------------- */
+
+/* CrankNicolsonModes::CrankNicolsonModes (src/CrankNicolsonModes.cpp:11-50):
+ * builds the grid, the (l, m) list with even l-m, and the free Hamiltonian. */
+int cnm_create(const cnm_params *params, cnm_handle **out);
+int cnm_destroy(cnm_handle *h);
+const char *cnm_last_error(const cnm_handle *h);
+/* Message of the last failed cnm_create (no handle exists then). */
+const char *cnm_create_error(void);
+
+/* --- geometry ---------------------------------------------------------------- */
+
+int cnm_n_modes(const cnm_handle *h, int32_t *n_modes);       /* member n_modes */
+int cnm_modes(const cnm_handle *h, int32_t *l, int32_t *m);   /* member modes   */
+int cnm_grid(const cnm_handle *h, double *r);                 /* member r       */
+
+/* --- scalar members ---------------------------------------------------------- */
+
+int cnm_get_scalars(const cnm_handle *h, cnm_scalars *out);
+int cnm_set_scalars(cnm_handle *h, const cnm_scalars *in);
+
+/* --- state -------------------------------------------------------------------- */
+
+/* set_initial_state_full (src/CrankNicolsonModes.cpp:130-143): copies psi_0 and
+ * scales it by sqrt(M_c / mu).  CNM_EINVAL if n != Nr * n_modes. */
+int cnm_set_initial_state_full(cnm_handle *h, const double *psi0, int64_t n);
+/* Raw access to member psi (no scaling). */
+int cnm_set_state(cnm_handle *h, const double *psi, int64_t n);
+int cnm_get_state(const cnm_handle *h, double *psi, int64_t n);
+
+/* --- set-up ------------------------------------------------------------------- */
+
+/* configure_isolated_black_hole (src/CrankNicolsonModes.cpp:58-74). */
+int cnm_configure_isolated_black_hole(cnm_handle *h, double x);
+/* initialize (src/CrankNicolsonModes.cpp:76-98): coupling tables, t = 0 operator. */
+int cnm_initialize(cnm_handle *h);
+/* set_power_average_orbits (src/CrankNicolsonModes.cpp:52-56). */
+int cnm_set_power_average_orbits(cnm_handle *h, double n_orbits);
+/* build_damping_mask / build_cap (src/CrankNicolsonModes_outgoing.cpp:10-62). */
+int cnm_build_damping_mask(cnm_handle *h, double L_factor, double W, int32_t n);
+int cnm_build_cap(cnm_handle *h, double L_factor, double W, int32_t n);
+
+/* --- evolution ---------------------------------------------------------------- */
+
+/* The computational part of run() (src/CrankNicolsonModes.cpp:236-259,261-270):
+ * validates r_ex against the grid, sets t = 0 and refreshes the operator. */
+int cnm_prepare_run(cnm_handle *h, int32_t n_steps, double r_ex);
+/* build_time_dependent_perturbation(time) (_hamiltonian.cpp:245-268). */
+int cnm_refresh(cnm_handle *h, double time);
+/* step(step_id) (src/CrankNicolsonModes.cpp:145-234) without the text writes:
+ * the CN solve, mask, orbit update and all diagnostics of the step. */
+int cnm_step(cnm_handle *h, int32_t step_id, cnm_diag *diag, double *energy_flux,
+             double *flux, double *norms, double *energies);
+/* The stop test of evolve() (src/CrankNicolsonModes.cpp:276-282): 1 when R <= 6
+ * on an evolving binary orbit. */
+int cnm_should_stop(const cnm_handle *h, int32_t *stop);
+
+/* --- operators ------------------------------------------------------------------ */
+
+/* y = op x for an interleaved complex128 vector of length Nr * n_modes, with
+ * the operators of the current time (H, V, dVdt, A, B, apply_sink and
+ * schrodinger_rhs of include/CrankNicolsonModes.hpp:197-213). */
+int cnm_apply(cnm_handle *h, int32_t op, const double *x, double *y);
+/* sink_strength(body) (_absorption.cpp:119-125). */
+int cnm_sink_strength(const cnm_handle *h, int32_t body, double *out);
+/* absorption_sink_active(). */
+int cnm_sink_active(const cnm_handle *h, int32_t *active);
+/* The projector v_a of one body's sink (interleaved, Nr * n_modes). */
+int cnm_sink_vector(const cnm_handle *h, int32_t body, double *out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CNM_GPU_H */
