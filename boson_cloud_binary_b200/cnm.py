@@ -69,11 +69,13 @@ class cnm_diag(C.Structure):
 
 # Exported entry points of include/cnm_gpu.h, checked by the CPU test suite.
 EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "cnm_n_modes", "cnm_modes",
-           "cnm_grid", "cnm_get_scalars", "cnm_set_scalars", "cnm_set_initial_state_full", "cnm_set_state",
+           "cnm_grid", "cnm_coupling_info", "cnm_get_scalars", "cnm_set_scalars", "cnm_set_initial_state_full", "cnm_set_state",
            "cnm_get_state", "cnm_configure_isolated_black_hole", "cnm_initialize",
            "cnm_set_power_average_orbits", "cnm_build_damping_mask", "cnm_build_cap", "cnm_prepare_run",
            "cnm_refresh", "cnm_step", "cnm_should_stop", "cnm_apply", "cnm_sink_strength", "cnm_sink_active",
-           "cnm_sink_vector")
+           "cnm_sink_vector", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop")
+
+KERNELS = {"apply": 0, "precond_solve": 1, "precond_factor": 2, "diagnostics": 3}
 
 _lib = None
 
@@ -96,6 +98,7 @@ def load_library():
     L.cnm_n_modes.argtypes = [p, C.POINTER(i32)]
     L.cnm_modes.argtypes = [p, C.POINTER(i32), C.POINTER(i32)]
     L.cnm_grid.argtypes = [p, dp]
+    L.cnm_coupling_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32)]
     L.cnm_get_scalars.argtypes = [p, C.POINTER(cnm_scalars)]
     L.cnm_set_scalars.argtypes = [p, C.POINTER(cnm_scalars)]
     for f in ("cnm_set_initial_state_full", "cnm_set_state", "cnm_get_state"):
@@ -113,8 +116,20 @@ def load_library():
     L.cnm_sink_strength.argtypes = [p, i32, dp]
     L.cnm_sink_active.argtypes = [p, C.POINTER(i32)]
     L.cnm_sink_vector.argtypes = [p, i32, dp]
+    L.cnm_select_device.argtypes = [i32]
+    L.cnm_set_profiling.argtypes = [p, i32]
+    L.cnm_kernel_times.argtypes = [p, i32, dp, C.POINTER(C.c_int64)]
+    L.cnm_timer_start.argtypes = [p]
+    L.cnm_timer_stop.argtypes = [p, dp]
     _lib = L
     return L
+
+
+def select_device(device: int) -> None:
+    """Make `device` current (for one-process-per-GPU runs) before creating solvers."""
+    lib = load_library()
+    if lib.cnm_select_device(int(device)) != CNM_OK:
+        raise CudaError(lib.cnm_create_error().decode())
 
 
 def _dptr(a):
@@ -264,6 +279,12 @@ class CrankNicolsonModes:
         t[step_id] = d.t
         return out
 
+    def coupling_info(self):
+        """(number of coupled mode pairs, number of Gaunt terms) of the coupling cache."""
+        a, b = C.c_int32(), C.c_int32()
+        self._check(self._lib.cnm_coupling_info(self._h, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
     def should_stop(self):
         s = C.c_int32()
         self._check(self._lib.cnm_should_stop(self._h, C.byref(s)))
@@ -293,3 +314,23 @@ class CrankNicolsonModes:
         out = np.zeros(2 * self.size)
         self._check(self._lib.cnm_sink_vector(self._h, int(body), _dptr(out)))
         return out.view(np.complex128).copy()
+
+    # ---- measurement hooks ------------------------------------------------------------
+    def set_profiling(self, on=True):
+        self._check(self._lib.cnm_set_profiling(self._h, int(bool(on))))
+
+    def kernel_times(self, name):
+        """(total device milliseconds, launches) of one hot kernel class since profiling began."""
+        ms = C.c_double()
+        n = C.c_int64()
+        self._check(self._lib.cnm_kernel_times(self._h, KERNELS[name], C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+    def timer_start(self):
+        self._check(self._lib.cnm_timer_start(self._h))
+
+    def timer_stop(self):
+        """Device milliseconds on the solver's stream since timer_start()."""
+        ms = C.c_double()
+        self._check(self._lib.cnm_timer_stop(self._h, C.byref(ms)))
+        return ms.value

@@ -37,7 +37,7 @@ void cuda_check(cudaError_t e, const char *what)
     if (e != cudaSuccess) throw Error(e == cudaErrorMemoryAllocation ? CNM_ENOMEM : CNM_ECUDA,
                                       std::string(what) + ": " + cudaGetErrorString(e));
 }
-#define CK(x) cuda_check((x), #x)
+#define CK(x) ::cnm::cuda_check((x), #x)
 
 template <class T>
 struct DevBuf {
@@ -134,9 +134,25 @@ struct Absorber {
 struct OpState {
     bool built = false;
     double theta = 0, domega = 0, dt = 0;
+    double R1 = 0, R2 = 0, q = 0, Mtot = 0, w = 0;  // geometry of the hh table
     bool cap = false;
     bool sink_active = false;
 };
+
+// Device-event timing of one class of kernel launches (profiling hook).
+struct KernelTimer {
+    std::vector<cudaEvent_t> a, b;
+    int used = 0;
+    double ms = 0.0;
+    int64_t launches = 0;
+    ~KernelTimer()
+    {
+        for (cudaEvent_t e : a) cudaEventDestroy(e);
+        for (cudaEvent_t e : b) cudaEventDestroy(e);
+    }
+};
+
+enum TimedKernel : int { TK_APPLY = 0, TK_PSOLVE = 1, TK_PFACTOR = 2, TK_DIAG = 3, TK_COUNT = 4 };
 
 struct Solver {
     // constructor arguments and derived constants
@@ -182,6 +198,48 @@ struct Solver {
     // pinned host staging
     double *h_stage = nullptr;
     size_t h_stage_n = 0;
+    // profiling
+    bool profiling = false;
+    KernelTimer ktime[TK_COUNT];
+    cudaEvent_t region_a = nullptr, region_b = nullptr;
+
+    void kt_begin(int k)
+    {
+        if (!profiling) return;
+        KernelTimer &t = ktime[k];
+        if (t.used == (int)t.a.size()) {
+            if (t.a.size() >= 4096) kt_flush();
+            else {
+                cudaEvent_t e1, e2;
+                CK(cudaEventCreate(&e1));
+                CK(cudaEventCreate(&e2));
+                t.a.push_back(e1);
+                t.b.push_back(e2);
+            }
+        }
+        CK(cudaEventRecord(t.a[t.used], stream));
+    }
+    void kt_end(int k)
+    {
+        if (!profiling) return;
+        KernelTimer &t = ktime[k];
+        CK(cudaEventRecord(t.b[t.used], stream));
+        ++t.used;
+        ++t.launches;
+    }
+    void kt_flush()
+    {
+        if (!profiling) return;
+        CK(cudaStreamSynchronize(stream));
+        for (KernelTimer &t : ktime) {
+            for (int i = 0; i < t.used; ++i) {
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, t.a[i], t.b[i]));
+                t.ms += ms;
+            }
+            t.used = 0;
+        }
+    }
 
     Solver(const cnm_params &pr)
         : Nr(pr.Nr), l_max(pr.l_max), save_every(pr.save_every), L(pr.L), dr(pr.L / (pr.Nr - 1)),
@@ -210,6 +268,8 @@ struct Solver {
 
     ~Solver()
     {
+        if (region_a) cudaEventDestroy(region_a);
+        if (region_b) cudaEventDestroy(region_b);
         if (h_stage) cudaFreeHost(h_stage);
         if (stream) cudaStreamDestroy(stream);
     }
@@ -375,11 +435,12 @@ struct Solver {
 
     // -------------------------------------------------------------- operators
 
+    // hh table of the geometry frozen in `op` (set by build_time_dependent_perturbation).
     void build_hh(double *dst, double a1, double a2)
     {
         const int64_t total = (int64_t)K * Nr;
-        k_hh_table<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(dst, d_r.p, Nr, K, R1, R2, q,
-                                                                        -mu * (M1 + M2), a1, a2);
+        k_hh_table<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(dst, d_r.p, Nr, K, op.R1, op.R2, op.q,
+                                                                        -mu * op.Mtot, a1, a2);
         launch_check();
     }
 
@@ -397,6 +458,11 @@ struct Solver {
             Omega = std::sqrt((M1 + M2) / std::pow(R, 3));
         }
         potential_ramp_factor = ramp_secondary_potential ? ramp_factor : 1.0;
+        op.R1 = R1;
+        op.R2 = R2;
+        op.q = q;
+        op.Mtot = M1 + M2;
+        op.w = potential_ramp_factor;
         build_hh(d_hh.p, 1.0, potential_ramp_factor);
         if (absorption) build_spherical_absorption();
         sink_active = absorption && time >= ramp_end_time();
@@ -535,8 +601,10 @@ struct Solver {
     void launch_apply(const ApplyArgs &a)
     {
         const unsigned blocks = (unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE);
+        kt_begin(TK_APPLY);
         k_apply<<<blocks, APPLY_THREADS, apply_smem, stream>>>(grid(), table(), a);
         launch_check();
+        kt_end(TK_APPLY);
     }
 
     // y = A_full x (sparse CN operator plus dt/4 Gamma) with the sink projections of x at `dots`.
@@ -588,19 +656,23 @@ struct Solver {
         choose_window(dtv);
         const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
         CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
+        kt_begin(TK_PFACTOR);
         k_precond_factor<<<dim3(chunks, n_modes), SCAN_THREADS, 0, stream>>>(
             grid(), table(), d_hh.p, 0.5 * dtv, offdiag(dtv), precond_chunk, precond_window / 2 + 16, dinv.p,
             d_status.p);
         launch_check();
+        kt_end(TK_PFACTOR);
     }
 
     void precond(const double2 *bv, double2 *xv, double dtv)
     {
         const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
         const size_t smem = (size_t)(std::min(Nr, precond_chunk + 2 * precond_window) + SCAN_THREADS) * sizeof(double2);
+        kt_begin(TK_PSOLVE);
         k_precond_solve<<<dim3(chunks, n_modes), SCAN_THREADS, smem, stream>>>(Nr, precond_chunk, precond_window,
                                                                                offdiag(dtv), dinv.p, bv, xv);
         launch_check();
+        kt_end(TK_PSOLVE);
     }
 
     // -------------------------------------------------------------- reductions
@@ -851,12 +923,14 @@ struct Solver {
         sink_dots(psi.p, d_dots.p, sk, k);
         if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2);
         const unsigned dblocks = (unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE);
+        kt_begin(TK_DIAG);
         k_diagnostics<<<dblocks, APPLY_THREADS, diag_smem, stream>>>(
             grid(), table(), d_hh.p, op.theta, op.domega, psi.p, idx_ex, k, k > 0 ? sk[0]->v.p : nullptr,
             k > 1 ? sk[1]->v.p : nullptr, d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
             k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
             k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes);
         launch_check();
+        kt_end(TK_DIAG);
         const int nslots = 2 * n_modes + 3;
         k_sum_slots<<<(nslots + 127) / 128, 128, 0, stream>>>(d_partials.p, (int)dblocks, nslots, d_red.p);
         launch_check();
@@ -903,6 +977,7 @@ struct Solver {
         const double p_bin_inst = redh[2 * n + 1] * dr;
         const double dV = redh[2 * n + 2] * dr;
         p_bin = isolated ? 0.0 : power_average.update(t_i, phase, p_bin_inst);
+        kt_flush();
         if (dg) {
             dg->R = R;
             dg->theta = theta;
@@ -1045,6 +1120,16 @@ static int guarded(cnm_handle *h, F &&f)
 
 extern "C" {
 
+int cnm_select_device(int32_t device)
+{
+    const cudaError_t e = cudaSetDevice(device);
+    if (e != cudaSuccess) {
+        g_create_error = std::string("cudaSetDevice: ") + cudaGetErrorString(e);
+        return CNM_ECUDA;
+    }
+    return CNM_OK;
+}
+
 int cnm_create(const cnm_params *params, cnm_handle **out)
 {
     if (!params || !out) return CNM_EINVAL;
@@ -1088,6 +1173,14 @@ int cnm_modes(const cnm_handle *h, int32_t *l, int32_t *m)
         l[j] = h->s->cpl.mode_l[j];
         m[j] = h->s->cpl.mode_m[j];
     }
+    return CNM_OK;
+}
+
+int cnm_coupling_info(const cnm_handle *h, int32_t *n_pairs, int32_t *n_terms)
+{
+    if (!h || !n_pairs || !n_terms) return CNM_EINVAL;
+    *n_pairs = (int32_t)h->s->cpl.pair_col.size();
+    *n_terms = (int32_t)h->s->cpl.term_l.size();
     return CNM_OK;
 }
 
@@ -1253,6 +1346,52 @@ int cnm_sink_vector(const cnm_handle *h, int32_t body, double *out)
         const cnm::Absorber &ab = body == 1 ? s.abs1 : s.abs2;
         if (ab.v.p) cnm::cuda_check(cudaMemcpy(out, ab.v.p, s.nN * sizeof(double2), cudaMemcpyDeviceToHost), "cudaMemcpy");
         else std::fill(out, out + 2 * s.nN, 0.0);
+    });
+}
+
+int cnm_set_profiling(cnm_handle *h, int32_t on)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        s.kt_flush();
+        s.profiling = on != 0;
+        for (cnm::KernelTimer &t : s.ktime) {
+            t.ms = 0.0;
+            t.launches = 0;
+            t.used = 0;
+        }
+    });
+}
+
+int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *launches)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        if (which < 0 || which >= cnm::TK_COUNT) throw cnm::Error(CNM_EINVAL, "unknown kernel class");
+        s.kt_flush();
+        *total_ms = s.ktime[which].ms;
+        *launches = s.ktime[which].launches;
+    });
+}
+
+int cnm_timer_start(cnm_handle *h)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        if (!s.region_a) {
+            CK(cudaEventCreate(&s.region_a));
+            CK(cudaEventCreate(&s.region_b));
+        }
+        CK(cudaEventRecord(s.region_a, s.stream));
+    });
+}
+
+int cnm_timer_stop(cnm_handle *h, double *ms)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        if (!s.region_a) throw cnm::Error(CNM_ELOGIC, "cnm_timer_start was not called");
+        CK(cudaEventRecord(s.region_b, s.stream));
+        CK(cudaEventSynchronize(s.region_b));
+        float f = 0.f;
+        CK(cudaEventElapsedTime(&f, s.region_a, s.region_b));
+        *ms = f;
     });
 }
 

@@ -70,6 +70,17 @@ struct CouplingTable {
     const int *mode_m;         // [n_modes]
 };
 
+// Register-blocked layout of the same coupling (see BlockedCoupling in cnm_coupling.h).
+constexpr int ROW_BLOCK = 4;
+struct BlockTable {
+    int n_chunks;
+    const int *chunk_l;     // [n_chunks]
+    const int *chunk_rows;  // [n_chunks * ROW_BLOCK]
+    const int *chunk_goff;  // [n_chunks * (l_max + 1)]
+    const int *l_off;       // [l_max + 2]
+    const double *g;
+};
+
 // Grid description shared by all kernels.
 struct Grid {
     int Nr;

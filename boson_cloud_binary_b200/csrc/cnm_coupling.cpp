@@ -164,4 +164,52 @@ Coupling build_coupling(int l_max)
     return c;
 }
 
+BlockedCoupling block_coupling(const Coupling &c, int rb)
+{
+    BlockedCoupling b;
+    b.rb = rb;
+    const int L = c.l_max;
+    b.l_off.assign(L + 2, 0);
+    for (int j = 0; j < c.n_modes; ++j) b.l_off[c.mode_l[j] + 1] = j + 1;
+    for (int l = 1; l <= L + 1; ++l) b.l_off[l] = std::max(b.l_off[l], b.l_off[l - 1]);
+    // term lookup: (j, k, l*) -> g
+    std::vector<std::vector<double>> dense(c.n_modes * (size_t)c.n_modes);
+    for (int j = 0; j < c.n_modes; ++j)
+        for (int p = c.pair_row_ptr[j]; p < c.pair_row_ptr[j + 1]; ++p) {
+            std::vector<double> &v = dense[(size_t)j * c.n_modes + c.pair_col[p]];
+            v.assign(2 * L + 1, 0.0);
+            for (int t = c.pair_term_ptr[p]; t < c.pair_term_ptr[p + 1]; ++t) v[c.term_l[t]] = c.term_g[t];
+        }
+    // chunks, heaviest first so warps that take chunks round-robin stay balanced
+    struct Ch { int l, first, count; double cost; };
+    std::vector<Ch> chunks;
+    for (int l = 0; l <= L; ++l) {
+        const int first = b.l_off[l], count = b.l_off[l + 1] - b.l_off[l];
+        double cost = 0;
+        for (int l1 = 0; l1 <= L; ++l1) cost += (l1 + 1) * (std::min(l, l1) + 3);
+        for (int r0 = 0; r0 < count; r0 += rb) chunks.push_back({l, first + r0, std::min(rb, count - r0), cost});
+    }
+    std::stable_sort(chunks.begin(), chunks.end(), [](const Ch &a, const Ch &b2) { return a.cost > b2.cost; });
+    b.n_chunks = (int)chunks.size();
+    for (const Ch &ch : chunks) {
+        b.chunk_l.push_back(ch.l);
+        for (int rr = 0; rr < rb; ++rr) b.chunk_rows.push_back(rr < ch.count ? ch.first + rr : -1);
+        for (int l1 = 0; l1 <= L; ++l1) {
+            b.chunk_goff.push_back((int)b.g.size());
+            const int L0 = std::abs(ch.l - l1), S = std::min(ch.l, l1) + 1;
+            for (int k = b.l_off[l1]; k < b.l_off[l1 + 1]; ++k)
+                for (int rr = 0; rr < rb; ++rr)
+                    for (int s2 = 0; s2 < S; ++s2) {
+                        double gv = 0.0;
+                        if (rr < ch.count) {
+                            const std::vector<double> &v = dense[(size_t)(ch.first + rr) * c.n_modes + k];
+                            if (!v.empty()) gv = v[L0 + 2 * s2];
+                        }
+                        b.g.push_back(gv);
+                    }
+        }
+    }
+    return b;
+}
+
 }  // namespace cnm

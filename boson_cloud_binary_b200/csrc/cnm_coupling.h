@@ -27,4 +27,22 @@ struct Coupling {
 
 Coupling build_coupling(int l_max);
 
+// The coupling cache regrouped for the register-blocked kernels: rows with the same
+// l are taken `rb` at a time ("row chunks"); for every chunk and every column
+// degree l1 the Gaunt weights of the (l, l1) block are stored densely as
+// [column m1][row][s] with l* = |l - l1| + 2 s, s < min(l, l1) + 1 (zero where a
+// pair has no term at that l*), so the kernel's inner loops have compile-time
+// trip counts.
+struct BlockedCoupling {
+    int rb = 4;
+    int n_chunks = 0;
+    std::vector<int> chunk_l;      // [n_chunks]
+    std::vector<int> chunk_rows;   // [n_chunks * rb], -1 pads
+    std::vector<int> chunk_goff;   // [n_chunks * (l_max + 1)] offset of block (chunk, l1) in g
+    std::vector<int> l_off;        // [l_max + 2] first mode index of each l
+    std::vector<double> g;
+};
+
+BlockedCoupling block_coupling(const Coupling &c, int rb);
+
 }  // namespace cnm

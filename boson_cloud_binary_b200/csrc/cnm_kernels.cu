@@ -163,6 +163,318 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_apply(Grid g, CouplingTable c
     }
 }
 
+// ------------------------------------------------------------------ register-blocked coupling
+
+// Multipole cut of one tile: the largest l* whose weight exceeds 1e-18 of the
+// monopole weight at some node of the tile.  Smaller terms cannot change an FP64
+// result (they lie far below the rounding of the diagonal), and at radii well
+// outside the binary they make up most of the Gaunt terms.
+__device__ int tile_lcut(const double *hs, int K, int lane)
+{
+    int lc = -1;
+    const double h0 = fabs(hs[lane]);
+    if (h0 > 0.0) {
+        lc = 0;
+        for (int l = K - 1; l > 0; --l)
+            if (fabs(hs[l * APPLY_TILE + lane]) > 1e-18 * h0) {
+                lc = l;
+                break;
+            }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) lc = max(lc, __shfl_xor_sync(0xffffffffu, lc, o));
+    return lc;
+}
+
+// One (row chunk, l1) block: for the S_EFF leading multipoles l* = L0 + 2s held in
+// registers, Ahat_jk = sum_s g[k][row][s] h_s for the ROW_BLOCK rows of the chunk and
+// the l1 + 1 columns k = col0 .. col0 + ncols - 1, accumulated into acc (and into
+// accm with weight m_k for dV/dt).
+template <int S_EFF, bool DVDT>
+__device__ __forceinline__ void coupling_block(const double *__restrict__ g, int stride, int ncols, int col0,
+                                               const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
+                                               double2 (&acc)[ROW_BLOCK], double2 (&accm)[ROW_BLOCK])
+{
+    double h[S_EFF];
+#pragma unroll
+    for (int s2 = 0; s2 < S_EFF; ++s2) h[s2] = hs_l0[2 * s2 * APPLY_TILE + lane];
+    for (int kk = 0; kk < ncols; ++kk) {
+        const double2 z = zs[(col0 + kk) * APPLY_TILE + lane];
+        const double *gk = g + kk * ROW_BLOCK * stride;
+        const double mk = DVDT ? (double)mode_m[col0 + kk] : 0.0;
+#pragma unroll
+        for (int rr = 0; rr < ROW_BLOCK; ++rr) {
+            double a = 0.0;
+#pragma unroll
+            for (int s2 = 0; s2 < S_EFF; ++s2) a = fma(__ldg(gk + rr * stride + s2), h[s2], a);
+            acc[rr].x = fma(a, z.x, acc[rr].x);
+            acc[rr].y = fma(a, z.y, acc[rr].y);
+            if (DVDT) {
+                const double am = a * mk;
+                accm[rr].x = fma(am, z.x, accm[rr].x);
+                accm[rr].y = fma(am, z.y, accm[rr].y);
+            }
+        }
+    }
+}
+
+template <bool DVDT>
+__device__ __forceinline__ void coupling_dispatch(int s_eff, const double *g, int stride, int ncols, int col0,
+                                                  const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
+                                                  double2 (&acc)[ROW_BLOCK], double2 (&accm)[ROW_BLOCK])
+{
+#define CNM_CASE(S)                                                                                      \
+    case S: coupling_block<S, DVDT>(g, stride, ncols, col0, zs, hs_l0, mode_m, lane, acc, accm); break;
+    switch (s_eff) {
+        CNM_CASE(1) CNM_CASE(2) CNM_CASE(3) CNM_CASE(4) CNM_CASE(5) CNM_CASE(6) CNM_CASE(7) CNM_CASE(8)
+        CNM_CASE(9) CNM_CASE(10) CNM_CASE(11) CNM_CASE(12) CNM_CASE(13) CNM_CASE(14) CNM_CASE(15)
+        CNM_CASE(16) CNM_CASE(17) CNM_CASE(18) CNM_CASE(19) CNM_CASE(20) CNM_CASE(21) CNM_CASE(22)
+        CNM_CASE(23) CNM_CASE(24) CNM_CASE(25)
+    default: break;
+    }
+#undef CNM_CASE
+}
+
+// Ahat z (and Ahat M z) for the rows of one chunk at the warp's 32 nodes.
+template <bool DVDT>
+__device__ __forceinline__ void coupling_chunk(const BlockTable &bt, int l_max, int ci, int lcut, const double2 *zs,
+                                               const double *hs, const int *mode_m, int lane,
+                                               double2 (&acc)[ROW_BLOCK], double2 (&accm)[ROW_BLOCK])
+{
+#pragma unroll
+    for (int rr = 0; rr < ROW_BLOCK; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
+    const int l = bt.chunk_l[ci];
+    for (int l1 = 0; l1 <= l_max; ++l1) {
+        const int L0 = abs(l - l1), S = min(l, l1) + 1;
+        if (lcut < L0) continue;
+        const int s_eff = min(S, (lcut - L0) / 2 + 1);
+        const int col0 = bt.l_off[l1];
+        coupling_dispatch<DVDT>(s_eff, bt.g + bt.chunk_goff[ci * (l_max + 1) + l1], S, l1 + 1, col0, zs,
+                                hs + L0 * APPLY_TILE, mode_m, lane, acc, accm);
+    }
+}
+
+// Operator application, register-blocked: warps take row chunks round-robin.
+__global__ void __launch_bounds__(APPLY_THREADS) k_apply2(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a)
+{
+    extern __shared__ double2 smem2[];
+    __shared__ int s_lcut;
+    const int n = g.n_modes, Nr = g.Nr;
+    const int K = 2 * ct.l_max + 1;
+    const int i0 = blockIdx.x * APPLY_TILE;
+    double2 *xs = smem2;                              // n * (TILE + 2)
+    double2 *zs = xs + n * (APPLY_TILE + 2);          // n * TILE
+    double2 *ph = zs + n * APPLY_TILE;                // n
+    double *hs = reinterpret_cast<double *>(ph + n);  // K * TILE
+    const bool vp = a.vpart != V_NONE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double sn, cs;
+        sincos((double)ct.mode_m[k] * a.theta, &sn, &cs);
+        ph[k] = cmake(cs, sn);
+    }
+    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
+        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
+        const int i = i0 - 1 + c;
+        xs[e] = (i >= 0 && i < Nr) ? a.x[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
+    }
+    if (vp)
+        for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
+            const int l = e / APPLY_TILE, c = e % APPLY_TILE;
+            const int i = i0 + c;
+            hs[e] = i < Nr ? a.hh[(int64_t)l * Nr + i] : 0.0;
+        }
+    __syncthreads();
+    if (vp) {
+        for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
+            const int k = e / APPLY_TILE, c = e % APPLY_TILE;
+            zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
+        }
+        if (warp == 0) {
+            const int lc = tile_lcut(hs, K, lane);
+            if (lane == 0) s_lcut = lc;
+        }
+    }
+    __syncthreads();
+    const int lcut = vp ? s_lcut : -1;
+    const int c = lane;
+    const int i = i0 + c;
+    const bool interior = i >= 1 && i <= Nr - 2;
+    const double alpha_d = 1.0 / (g.dr * g.dr);
+    const double ri = i < Nr ? g.r[i] : 1.0;
+    for (int ci = warp; ci < bt.n_chunks; ci += nw) {
+        double2 acc[ROW_BLOCK], accm[ROW_BLOCK];
+        if (vp && lcut >= 0) {
+            if (a.vpart == V_DVDT) coupling_chunk<true>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
+            else coupling_chunk<false>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
+        } else {
+#pragma unroll
+            for (int rr = 0; rr < ROW_BLOCK; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
+        }
+        if (i >= Nr) continue;
+#pragma unroll
+        for (int rr = 0; rr < ROW_BLOCK; ++rr) {
+            const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
+            if (j < 0) continue;
+            const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
+            double2 h = cmake(0.0, 0.0);
+            if (a.use_h0 && interior) {
+                const int l = ct.mode_l[j];
+                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+                const double off = -alpha_d / (2 * g.mu);
+                h = cadd(cscale(xv, diag),
+                         cscale(cadd(xs[j * (APPLY_TILE + 2) + c], xs[j * (APPLY_TILE + 2) + c + 2]), off));
+            }
+            if (vp && interior) {
+                double2 vj;
+                if (a.vpart == V_DVDT) {
+                    const double mj = (double)ct.mode_m[j];
+                    vj = cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), a.domega));
+                } else {
+                    vj = acc[rr];
+                }
+                h = cadd(h, cmul(cconj(ph[j]), vj));
+            }
+            if (a.use_cap && g.capw) h = cadd(h, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
+            double2 y = cadd(cmul(a.alpha, xv), cmul(a.beta, h));
+            for (int s2 = 0; s2 < a.n_sinks; ++s2)
+                if (i >= a.sink_lo[s2] && i < a.sink_hi[s2])
+                    y = cadd(y, cmul(cscale(a.sink_dots[s2], a.sink_coef[s2]), a.sink_v[s2][(int64_t)j * Nr + i]));
+            a.y[(int64_t)j * Nr + i] = y;
+        }
+    }
+}
+
+// Fused diagnostics, register-blocked (same outputs and partial layout as k_diagnostics).
+__global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics2(Grid g, CouplingTable ct, BlockTable bt,
+                                                                 const double *hh, double theta, double domega,
+                                                                 const double2 *psi, int idx_ex, int n_sinks,
+                                                                 const double2 *sv0, const double2 *sv1,
+                                                                 const double2 *sink_dots, double sink_coef0,
+                                                                 double sink_coef1, int slo0, int shi0, int slo1,
+                                                                 int shi1, double *partials, double2 *dpsi_edge,
+                                                                 double2 *psi_edge)
+{
+    extern __shared__ double2 smem2[];
+    __shared__ int s_lcut;
+    const int n = g.n_modes, Nr = g.Nr;
+    const int K = 2 * ct.l_max + 1;
+    const int i0 = blockIdx.x * APPLY_TILE;
+    double2 *xs = smem2;
+    double2 *zs = xs + n * (APPLY_TILE + 2);
+    double2 *ph = zs + n * APPLY_TILE;
+    double *hs = reinterpret_cast<double *>(ph + n);
+    double *red = hs + K * APPLY_TILE;  // (2n + 3) * nwarps
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double sn, cs;
+        sincos((double)ct.mode_m[k] * theta, &sn, &cs);
+        ph[k] = cmake(cs, sn);
+    }
+    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
+        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
+        const int i = i0 - 1 + c;
+        xs[e] = (i >= 0 && i < Nr) ? psi[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
+    }
+    for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
+        const int l = e / APPLY_TILE, c = e % APPLY_TILE;
+        const int i = i0 + c;
+        hs[e] = i < Nr ? hh[(int64_t)l * Nr + i] : 0.0;
+    }
+    for (int e = threadIdx.x; e < (2 * n + 3) * nw; e += blockDim.x) red[e] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
+        const int k = e / APPLY_TILE, c = e % APPLY_TILE;
+        zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
+    }
+    if (warp == 0) {
+        const int lc = tile_lcut(hs, K, lane);
+        if (lane == 0) s_lcut = lc;
+    }
+    __syncthreads();
+    const int lcut = s_lcut;
+    const int c = lane;
+    const int i = i0 + c;
+    const bool active = i < Nr && i <= idx_ex;
+    const bool interior = i >= 1 && i <= Nr - 2;
+    const double alpha_d = 1.0 / (g.dr * g.dr);
+    const double ri = i < Nr ? g.r[i] : 1.0;
+    double e_edge = 0.0, pb = 0.0, dv = 0.0;
+    // tiles entirely beyond the extraction node hold no diagnostics
+    const bool tile_active = i0 <= idx_ex;
+    for (int ci = warp; tile_active && ci < bt.n_chunks; ci += nw) {
+        double2 acc[ROW_BLOCK], accm[ROW_BLOCK];
+        if (lcut >= 0) coupling_chunk<true>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
+        else {
+#pragma unroll
+            for (int rr = 0; rr < ROW_BLOCK; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
+        }
+#pragma unroll
+        for (int rr = 0; rr < ROW_BLOCK; ++rr) {
+            const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
+            if (j < 0) continue;
+            double nrm = 0.0, en = 0.0;
+            if (active) {
+                const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
+                double2 hx = cmake(0.0, 0.0), vx = cmake(0.0, 0.0), dx = cmake(0.0, 0.0);
+                if (interior) {
+                    const int l = ct.mode_l[j];
+                    const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+                    const double off = -alpha_d / (2 * g.mu);
+                    hx = cadd(cscale(xv, diag),
+                              cscale(cadd(xs[j * (APPLY_TILE + 2) + c], xs[j * (APPLY_TILE + 2) + c + 2]), off));
+                    const double mj = (double)ct.mode_m[j];
+                    vx = cmul(cconj(ph[j]), acc[rr]);
+                    dx = cmul(cconj(ph[j]),
+                              cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), domega)));
+                    hx = cadd(hx, vx);
+                }
+                if (g.capw) hx = cadd(hx, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
+                double2 dp = cmake(hx.y, -hx.x);  // -i H psi
+                if (n_sinks > 0 && i >= slo0 && i < shi0)
+                    dp = cadd(dp, cmul(cscale(sink_dots[0], sink_coef0), sv0[(int64_t)j * Nr + i]));
+                if (n_sinks > 1 && i >= slo1 && i < shi1)
+                    dp = cadd(dp, cmul(cscale(sink_dots[1], sink_coef1), sv1[(int64_t)j * Nr + i]));
+                const double ce = cconjmul(xv, hx).x;
+                if (i < idx_ex) {
+                    nrm = cabs2(xv);
+                    en = ce;
+                } else {
+                    e_edge += ce;
+                    dpsi_edge[j] = dp;
+                    psi_edge[3 * j] = xs[j * (APPLY_TILE + 2) + c];
+                    psi_edge[3 * j + 1] = xv;
+                    psi_edge[3 * j + 2] = xs[j * (APPLY_TILE + 2) + c + 2];
+                }
+                pb += cconjmul(xv, dx).x;
+                dv += cconjmul(dp, vx).x;
+            }
+            nrm = warp_sum(nrm);
+            en = warp_sum(en);
+            if (lane == 0) {
+                red[j * nw + warp] = nrm;
+                red[(n + j) * nw + warp] = en;
+            }
+        }
+    }
+    e_edge = warp_sum(e_edge);
+    pb = warp_sum(pb);
+    dv = warp_sum(dv);
+    if (lane == 0) {
+        red[(2 * n) * nw + warp] = e_edge;
+        red[(2 * n + 1) * nw + warp] = pb;
+        red[(2 * n + 2) * nw + warp] = dv;
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < 2 * n + 3; q += blockDim.x) {
+        double sm = 0.0;
+        for (int w = 0; w < nw; ++w) sm += red[q * nw + w];
+        partials[(int64_t)q * gridDim.x + blockIdx.x] = sm;
+    }
+}
+
 // ------------------------------------------------------------------ sink projections
 
 // dots[s] = v_s^dagger x over the support of v_s (v_s vanishes elsewhere), one CTA,

@@ -31,6 +31,12 @@ enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3 
 __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
                            double scale, double a1, double a2);
 __global__ void k_apply(Grid g, CouplingTable ct, ApplyArgs a);
+__global__ void k_apply2(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a);
+__global__ void k_diagnostics2(Grid g, CouplingTable ct, BlockTable bt, const double *hh, double theta,
+                               double domega, const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0,
+                               const double2 *sv1, const double2 *sink_dots, double sink_coef0, double sink_coef1,
+                               int slo0, int shi0, int slo1, int shi1, double *partials, double2 *dpsi_edge,
+                               double2 *psi_edge);
 __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
                             const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots);
 __global__ void k_precond_factor(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off,

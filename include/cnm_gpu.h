@@ -117,6 +117,9 @@ typedef struct cnm_diag {
 /* CrankNicolsonModes::CrankNicolsonModes (src/CrankNicolsonModes.cpp:11-50):
  * builds the grid, the (l, m) list with even l-m, and the free Hamiltonian. */
 int cnm_create(const cnm_params *params, cnm_handle **out);
+/* Make `device` current for the calling thread before cnm_create (one process per
+ * GPU; the handle stays on the device that was current when it was created). */
+int cnm_select_device(int32_t device);
 int cnm_destroy(cnm_handle *h);
 const char *cnm_last_error(const cnm_handle *h);
 /* Message of the last failed cnm_create (no handle exists then). */
@@ -127,6 +130,9 @@ const char *cnm_create_error(void);
 int cnm_n_modes(const cnm_handle *h, int32_t *n_modes);       /* member n_modes */
 int cnm_modes(const cnm_handle *h, int32_t *l, int32_t *m);   /* member modes   */
 int cnm_grid(const cnm_handle *h, double *r);                 /* member r       */
+/* Size of the coupling cache (mode_pairs and their Gaunt terms,
+ * src/CrankNicolsonModes_hamiltonian.cpp:68-104). */
+int cnm_coupling_info(const cnm_handle *h, int32_t *n_pairs, int32_t *n_terms);
 
 /* --- scalar members ---------------------------------------------------------- */
 
@@ -181,6 +187,16 @@ int cnm_sink_strength(const cnm_handle *h, int32_t body, double *out);
 int cnm_sink_active(const cnm_handle *h, int32_t *active);
 /* The projector v_a of one body's sink (interleaved, Nr * n_modes). */
 int cnm_sink_vector(const cnm_handle *h, int32_t body, double *out);
+
+/* --- measurement hooks (no counterpart in the reference) -------------------------
+ * Device-event timing of the handle's stream, used by the benchmark: whole regions
+ * (start/stop) and, while profiling is on, every launch of the four hot kernel
+ * classes: 0 operator apply, 1 preconditioner solve, 2 pivot factorisation,
+ * 3 fused diagnostics. */
+int cnm_set_profiling(cnm_handle *h, int32_t on);
+int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *launches);
+int cnm_timer_start(cnm_handle *h);
+int cnm_timer_stop(cnm_handle *h, double *ms);
 
 #ifdef __cplusplus
 }
