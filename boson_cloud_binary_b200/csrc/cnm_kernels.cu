@@ -643,6 +643,61 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_precond_factor(Grid g, Couplin
     }
 }
 
+// The pivot kernel above for a caller-supplied diagonal: a_i = diag[j * Nr + i] instead
+// of the diagonal rebuilt from the Hamiltonian.  Same chunking, window and scan.
+__global__ void __launch_bounds__(SCAN_THREADS) k_precond_factor_diag(const double2 *diag, int Nr, double2 off,
+                                                                       int chunk, int window, double2 *dinv,
+                                                                       int *status)
+{
+    __shared__ Mob tmat[SCAN_THREADS];
+    const int j = blockIdx.y;
+    const int64_t base = (int64_t)j * Nr;
+    const int c0 = blockIdx.x * chunk, c1 = min(Nr, c0 + chunk);
+    const int lo = max(0, c0 - window), hi = c1;
+    const int len = hi - lo;
+    const int per = (len + blockDim.x - 1) / blockDim.x;
+    const int s0 = lo + threadIdx.x * per, s1 = min(hi, s0 + per);
+    const double2 c = cmul(off, off);
+    Mob acc;
+    acc.m00 = cmake(1, 0);
+    acc.m01 = cmake(0, 0);
+    acc.m10 = cmake(0, 0);
+    acc.m11 = cmake(1, 0);
+    for (int i = s0; i < s1; ++i) {
+        acc = mob_mul(pivot_map(diag[base + i], i, Nr, c), acc);
+        mob_normalize(acc);
+    }
+    tmat[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        Mob mine = tmat[threadIdx.x];
+        Mob prev;
+        const bool has = threadIdx.x >= (unsigned)o;
+        if (has) prev = tmat[threadIdx.x - o];
+        __syncthreads();
+        if (has) {
+            mine = mob_mul(mine, prev);
+            mob_normalize(mine);
+            tmat[threadIdx.x] = mine;
+        }
+        __syncthreads();
+    }
+    double2 p = diag[base + lo];
+    if (threadIdx.x > 0) p = mob_apply(tmat[threadIdx.x - 1], p);
+    for (int i = s0; i < s1; ++i) {
+        p = mob_apply(pivot_map(diag[base + i], i, Nr, c), p);
+        if (i >= c0) {
+            const double m = cabs2(p);
+            if (!(m > 0.0) || !isfinite(m)) {
+                atomicOr(status, 1);
+                dinv[base + i] = cmake(0.0, 0.0);
+            } else {
+                dinv[base + i] = crcp(p);
+            }
+        }
+    }
+}
+
 // Affine map y -> A y + B.
 struct Aff {
     double2 A, B;

@@ -41,6 +41,8 @@ __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, 
                             const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots);
 __global__ void k_precond_factor(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off,
                                  int chunk, int window, double2 *dinv, int *status);
+__global__ void k_precond_factor_diag(const double2 *diag, int Nr, double2 off, int chunk, int window,
+                                      double2 *dinv, int *status);
 __global__ void k_precond_solve(int Nr, int chunk, int window, double2 off, const double2 *dinv,
                                 const double2 *b, double2 *x);
 __global__ void k_dots(int64_t n, int nq, const double2 *a0, const double2 *b0, const double2 *a1,

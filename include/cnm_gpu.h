@@ -198,6 +198,34 @@ int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *la
 int cnm_timer_start(cnm_handle *h);
 int cnm_timer_stop(cnm_handle *h, double *ms);
 
+/* --- radial block solve without allocation (no counterpart in the reference) -----
+ * For callers that cannot call cudaMalloc -- a host code that gives the solver a
+ * fixed, pre-reserved device arena and allows no other allocation, a driver that
+ * launches from a region where allocation is forbidden, a plug-in that only
+ * receives device pointers -- and so cannot create a handle.  Solves, for every
+ * mode j, the tridiagonal radial block of the preconditioner
+ * (include/RadialBlockPreconditioner.hpp:44-98 of the reference):
+ *     diag[j,i] x[j,i] + off (x[j,i-1] + x[j,i+1]) = b[j,i]   for 1 <= i <= Nr-2,
+ *     diag[j,i] x[j,i] = b[j,i]                                for i = 0, Nr-1,
+ * with the same kernels as cnm_apply(..., CNM_OP_PRECOND, ...).
+ *   diag, b, x  device pointers to Nr * n_modes interleaved complex128 values,
+ *               mode-major (x may not alias diag or b);
+ *   off         the constant off-diagonal (re, im);
+ *   stream      a cudaStream_t (NULL: the legacy default stream); the call returns
+ *               after the solve has finished on it.
+ * It allocates nothing: the inverse pivots live in one file-scope device array
+ * of CNM_NOALLOC_MAX_UNKNOWNS complex values (16 MiB per GPU, held from the
+ * library's load until the process exits).  Larger problems (Nr * n_modes above
+ * the maximum) are rejected with CNM_EINVAL before any GPU work.  The first call on
+ * a device looks up the array's device address (and sets the solve kernel's
+ * shared-memory limit); make that first call before any stream capture.  Every call
+ * shares the one array, so calls that overlap on the GPU (concurrent streams or
+ * threads) race and must be serialised by the caller.  Returns CNM_EDEVICE if a
+ * pivot is zero or not finite, CNM_ECUDA on a CUDA error. */
+#define CNM_NOALLOC_MAX_UNKNOWNS (1 << 20)
+int cnm_radial_solve_noalloc(const double *diag, double off_re, double off_im, int32_t Nr, int32_t n_modes,
+                             const double *b, double *x, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
