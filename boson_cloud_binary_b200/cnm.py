@@ -73,7 +73,7 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_get_state", "cnm_configure_isolated_black_hole", "cnm_initialize",
            "cnm_set_power_average_orbits", "cnm_build_damping_mask", "cnm_build_cap", "cnm_prepare_run",
            "cnm_refresh", "cnm_step", "cnm_should_stop", "cnm_apply", "cnm_sink_strength", "cnm_sink_active",
-           "cnm_sink_vector", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop")
+           "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop")
 
 KERNELS = {"apply": 0, "precond_solve": 1, "precond_factor": 2, "diagnostics": 3}
 
@@ -116,6 +116,9 @@ def load_library():
     L.cnm_sink_strength.argtypes = [p, i32, dp]
     L.cnm_sink_active.argtypes = [p, C.POINTER(i32)]
     L.cnm_sink_vector.argtypes = [p, i32, dp]
+    L.cnm_save_checkpoint.argtypes = [p, i32, C.c_void_p, C.c_int64, C.POINTER(C.c_int64)]
+    L.cnm_load_checkpoint.argtypes = [p, i32, C.c_void_p, C.c_int64, C.POINTER(i32)]
+    L.cnm_replay_power_average.argtypes = [p, dp, dp, dp, i32]
     L.cnm_select_device.argtypes = [i32]
     L.cnm_set_profiling.argtypes = [p, i32]
     L.cnm_kernel_times.argtypes = [p, i32, dp, C.POINTER(C.c_int64)]
@@ -314,6 +317,21 @@ class CrankNicolsonModes:
         out = np.zeros(2 * self.size)
         self._check(self._lib.cnm_sink_vector(self._h, int(body), _dptr(out)))
         return out.view(np.complex128).copy()
+
+    # ---- checkpoints --------------------------------------------------------------------
+    def save_checkpoint(self, step_id):
+        """The bytes of checkpoint.bin for step_id (reference layout GMCKPT01)."""
+        n = C.c_int64()
+        self._check(self._lib.cnm_save_checkpoint(self._h, int(step_id), None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value)
+        self._check(self._lib.cnm_save_checkpoint(self._h, int(step_id), buf, n.value, C.byref(n)))
+        return buf.raw[:n.value]
+
+    def load_checkpoint(self, step_id, blob):
+        """Restore from checkpoint bytes; False (state untouched) if they do not match."""
+        ok = C.c_int32()
+        self._check(self._lib.cnm_load_checkpoint(self._h, int(step_id), blob, len(blob), C.byref(ok)))
+        return bool(ok.value)
 
     # ---- measurement hooks ------------------------------------------------------------
     def set_profiling(self, on=True):

@@ -83,6 +83,7 @@ public:
         segs_.push_back(s);
         integral_ += s.integral;
         duration_ += s.t1 - s.t0;
+        if (phase - initial_phase_ >= window_) ready_ = true;
         const double cut = phase - window_;
         while (!segs_.empty() && segs_.front().p1 <= cut) {
             integral_ -= segs_.front().integral;
@@ -108,13 +109,63 @@ public:
         return average_;
     }
 
+    // Exact state in the byte layout of the reference's RollingPhaseAverage::save
+    // (src/RollingPhase.cpp:169-184): window, previous sample (3 doubles), two bools,
+    // initial phase, integral, duration, average, u64 count, then 7 doubles per segment.
+    size_t blob_size() const { return 8 + 24 + 1 + 1 + 4 * 8 + 8 + 56 * segs_.size(); }
+    void save(std::vector<char> &out) const
+    {
+        auto put = [&](const void *p, size_t n) {
+            const char *c = static_cast<const char *>(p);
+            out.insert(out.end(), c, c + n);
+        };
+        put(&window_, 8);
+        put(&prev_, 24);
+        put(&has_prev_, 1);
+        put(&ready_, 1);
+        put(&initial_phase_, 8);
+        put(&integral_, 8);
+        put(&duration_, 8);
+        put(&average_, 8);
+        const uint64_t n = segs_.size();
+        put(&n, 8);
+        for (const Seg &sg : segs_) put(&sg, 56);
+    }
+    // Returns false on a truncated blob (the reference throws there and the caller
+    // treats the checkpoint as unusable).
+    bool load(const char *p, size_t size, size_t &used)
+    {
+        size_t o = 0;
+        auto get = [&](void *dst, size_t n) {
+            if (o + n > size) return false;
+            std::memcpy(dst, p + o, n);
+            o += n;
+            return true;
+        };
+        RollingPhaseAverage r(1.0);
+        uint64_t n = 0;
+        if (!(get(&r.window_, 8) && get(&r.prev_, 24) && get(&r.has_prev_, 1) && get(&r.ready_, 1) &&
+              get(&r.initial_phase_, 8) && get(&r.integral_, 8) && get(&r.duration_, 8) && get(&r.average_, 8) &&
+              get(&n, 8)))
+            return false;
+        for (uint64_t i = 0; i < n; ++i) {
+            Seg sg;
+            if (!get(&sg, 56)) return false;
+            r.segs_.push_back(sg);
+        }
+        *this = r;
+        used = o;
+        return true;
+    }
+
 private:
     struct Sample { double time, phase, value; };
     struct Seg { double t0, t1, p0, p1, v0, v1, integral; };
+    static_assert(sizeof(Sample) == 24 && sizeof(Seg) == 56, "checkpoint layout");
     double window_;
     std::deque<Seg> segs_;
     Sample prev_{};
-    bool has_prev_ = false;
+    bool has_prev_ = false, ready_ = false;
     double initial_phase_ = 0, integral_ = 0, duration_ = 0, average_ = 0;
 };
 
@@ -186,7 +237,13 @@ struct Solver {
     DevBuf<double> d_r, d_hh, d_hh_aux, d_capw, d_mask, d_glx, d_glw, d_partials, d_red, d_ang00;
     DevBuf<int> d_pair_row_ptr, d_pair_col, d_pair_term_ptr, d_term_l, d_diag_pair, d_mode_l, d_mode_m, d_status;
     DevBuf<double> d_term_g;
-    DevBuf<double2> psi, rhs, b, x, rr, r0, p, v, s, t, y, z, yP, W0, W1, tmp, cand, dinv;
+    BlockedCoupling bcpl, bcpl2;  // 4-row chunks (diagnostics), 2-row chunks (operator kernel)
+    DevBuf<int> d_chunk_l, d_chunk_nrows, d_chunk_rows, d_chunk_goff, d_l_off;
+    DevBuf<double> d_block_g;
+    DevBuf<int> d2_chunk_l, d2_chunk_nrows, d2_chunk_rows, d2_chunk_goff, d2_l_off;
+    DevBuf<double> d2_block_g;
+    size_t apply3_smem = 0;
+    DevBuf<double2> psi, rhs, b, x, rr, r0, p, p2, v, s, t, y, z, yP, W0, W1, tmp, cand, dinv;
     DevBuf<double2> d_dots;   // [0..1] psi, [2..3] psi_last, [4..5] scratch, [6..7] G set-up
     DevBuf<double2> d_edge;   // dpsi at idx_ex (n) + psi at idx_ex-1..idx_ex+1 (3n)
     DevBuf<Krylov> d_kr;
@@ -309,9 +366,23 @@ struct Solver {
         upload(d_mode_l, cpl.mode_l);
         upload(d_mode_m, cpl.mode_m);
         upload(d_ang00, cpl.ang00);
+        bcpl = block_coupling(cpl, ROW_BLOCK);
+        upload(d_chunk_l, bcpl.chunk_l);
+        upload(d_chunk_nrows, bcpl.chunk_nrows);
+        upload(d_chunk_rows, bcpl.chunk_rows);
+        upload(d_chunk_goff, bcpl.chunk_goff);
+        upload(d_l_off, bcpl.l_off);
+        upload(d_block_g, bcpl.g);
+        bcpl2 = block_coupling(cpl, 2);
+        upload(d2_chunk_l, bcpl2.chunk_l);
+        upload(d2_chunk_nrows, bcpl2.chunk_nrows);
+        upload(d2_chunk_rows, bcpl2.chunk_rows);
+        upload(d2_chunk_goff, bcpl2.chunk_goff);
+        upload(d2_l_off, bcpl2.l_off);
+        upload(d2_block_g, bcpl2.g);
         d_hh.alloc((size_t)K * Nr);
         d_hh_aux.alloc((size_t)K * Nr);
-        for (DevBuf<double2> *bptr : {&psi, &rhs, &b, &x, &rr, &r0, &p, &v, &s, &t, &y, &z, &yP, &W0, &W1, &tmp,
+        for (DevBuf<double2> *bptr : {&psi, &rhs, &b, &x, &rr, &r0, &p, &p2, &v, &s, &t, &y, &z, &yP, &W0, &W1, &tmp,
                                       &cand, &dinv})
             bptr->alloc(nN);
         d_dots.alloc(8);
@@ -319,14 +390,22 @@ struct Solver {
         d_kr.alloc(1);
         d_status.alloc(1);
         d_red.alloc(std::max(64, 2 * n_modes + 8));
-        const int diag_blocks = (Nr + APPLY_TILE - 1) / APPLY_TILE;
-        d_partials.alloc(std::max<size_t>((size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks));
+        const int diag_blocks = 2 * ((Nr + APPLY_TILE - 1) / APPLY_TILE);  // node tiles x row split
+        d_partials.alloc(std::max<size_t>({(size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks,
+                                           (size_t)4 * 4 * ((Nr + 63) / 64)}));
+        // the hh tile doubles as the scratch of the fused reductions (4 x 32 doubles)
         apply_smem = (size_t)n_modes * (APPLY_TILE + 2 + APPLY_TILE + 1) * sizeof(double2) +
-                     (size_t)K * APPLY_TILE * sizeof(double);
+                     (size_t)std::max(K, 4) * APPLY_TILE * sizeof(double);
         diag_smem = apply_smem + (size_t)(2 * n_modes + 3) * (APPLY_THREADS / 32) * sizeof(double);
         CK(cudaFuncSetAttribute(k_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
+        CK(set_operator_smem((int)apply_smem, (int)diag_smem));
+        apply3_smem = (size_t)n_modes * (APPLY3_TILE + 1) * sizeof(double2) +
+                      (size_t)std::max(K, 4) * APPLY3_TILE * sizeof(double);
+        CK(set_apply3_smem((int)apply3_smem));
         CK(cudaFuncSetAttribute(k_diagnostics, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
         CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CK(cudaFuncSetAttribute(k_precond_solve2, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
+        CK(cudaFuncSetAttribute(k_precond_factor2, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
     }
 
     Grid grid() const
@@ -357,6 +436,32 @@ struct Solver {
         c.mode_l = d_mode_l.p;
         c.mode_m = d_mode_m.p;
         return c;
+    }
+
+    BlockTable btable() const
+    {
+        BlockTable b;
+        b.n_chunks = bcpl.n_chunks;
+        b.chunk_l = d_chunk_l.p;
+        b.chunk_nrows = d_chunk_nrows.p;
+        b.chunk_rows = d_chunk_rows.p;
+        b.chunk_goff = d_chunk_goff.p;
+        b.l_off = d_l_off.p;
+        b.g = d_block_g.p;
+        return b;
+    }
+
+    BlockTable btable2() const
+    {
+        BlockTable b;
+        b.n_chunks = bcpl2.n_chunks;
+        b.chunk_l = d2_chunk_l.p;
+        b.chunk_nrows = d2_chunk_nrows.p;
+        b.chunk_rows = d2_chunk_rows.p;
+        b.chunk_goff = d2_chunk_goff.p;
+        b.l_off = d2_l_off.p;
+        b.g = d2_block_g.p;
+        return b;
     }
 
     void sync() { CK(cudaStreamSynchronize(stream)); }
@@ -598,19 +703,50 @@ struct Solver {
         return a;
     }
 
+    // Row chunks of a tile are split across this many CTAs (one round of chunks per warp).
+    int apply_split() const { return bcpl.n_chunks > APPLY_THREADS / 32 ? 2 : 1; }
+    dim3 apply_grid() const { return dim3((unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE), (unsigned)apply_split()); }
+
+    // Operator kernel grid: 64-node tiles x enough CTAs per tile that each warp takes about
+    // one two-row chunk.
+    dim3 apply3_grid() const
+    {
+        const int split = std::max(1, std::min(4, (bcpl2.n_chunks + APPLY_THREADS / 32 - 1) / (APPLY_THREADS / 32)));
+        return dim3((unsigned)((Nr + APPLY3_TILE - 1) / APPLY3_TILE), (unsigned)split);
+    }
+
     void launch_apply(const ApplyArgs &a)
     {
-        const unsigned blocks = (unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE);
+        const dim3 blocks3 = apply3_grid();
         kt_begin(TK_APPLY);
-        k_apply<<<blocks, APPLY_THREADS, apply_smem, stream>>>(grid(), table(), a);
+        ::cnm::launch_apply3(l_max, blocks3, apply3_smem, stream, grid(), table(), btable2(), a);
         launch_check();
         kt_end(TK_APPLY);
     }
 
-    // y = A_full x (sparse CN operator plus dt/4 Gamma) with the sink projections of x at `dots`.
-    void apply_A(const double2 *xv, double2 *yv, const Absorber *const *sk, int k, const double2 *dots, double dtv)
+    void launch_apply_v2(const ApplyArgs &a)
+    {
+        const dim3 blocks = apply_grid();
+        kt_begin(TK_APPLY);
+        ::cnm::launch_apply(l_max, blocks, apply_smem, stream, grid(), table(), btable(), a);
+        launch_check();
+        kt_end(TK_APPLY);
+    }
+
+    // y = A_full x (sparse CN operator plus dt/4 Gamma) with the sink projections of x at `dots`;
+    // optionally with up to two inner products of y (ApplyArgs::dot_kind) reduced into
+    // per-CTA partials.
+    void apply_A(const double2 *xv, double2 *yv, const Absorber *const *sk, int k, const double2 *dots, double dtv,
+                 int ndots = 0, int kind0 = 0, const double2 *ext0 = nullptr, int kind1 = 0,
+                 const double2 *ext1 = nullptr)
     {
         ApplyArgs a = base_args(xv, yv);
+        a.n_dots = ndots;
+        a.dot_kind[0] = kind0;
+        a.dot_kind[1] = kind1;
+        a.dot_ext[0] = ext0;
+        a.dot_ext[1] = ext1;
+        a.dot_partials = d_partials.p;
         a.alpha = cmake(1.0, 0.0);
         a.beta = cmake(0.0, 0.5 * dtv);
         a.use_h0 = 1;
@@ -639,16 +775,39 @@ struct Solver {
     // Warm-up window of the chunked scans: the recurrences contract by rho = |off| / |p+|
     // per node, p+ the attracting pivot of a block whose diagonal sits 1% below the
     // free one.  The window forgets the chunk's start value to exp(-40).
+    // Largest |Ahat_jj(r)| over modes and interior nodes for the frozen geometry:
+    // |h_l*(r)| <= mu (M1+M2) [1/((1+q) max(r,R1)) + |w| q/((1+q) max(r,R2))] and
+    // |Ahat_jj| <= (sum_l* |g_jjl*|) max_l* |h_l*|.
+    double diag_potential_bound() const
+    {
+        double gsum = 0.0;
+        for (int j = 0; j < n_modes; ++j) {
+            const int p = cpl.diag_pair[j];
+            double s2 = 0.0;
+            if (p >= 0)
+                for (int t = cpl.pair_term_ptr[p]; t < cpl.pair_term_ptr[p + 1]; ++t) s2 += std::abs(cpl.term_g[t]);
+            gsum = std::max(gsum, s2);
+        }
+        const double r1 = std::max(r[1], 1e-300);
+        const double h = mu * op.Mtot * (1.0 / ((1 + op.q) * std::max(r1, op.R1)) +
+                                         std::abs(op.w) * op.q / ((1 + op.q) * std::max(r1, op.R2)));
+        return gsum * h;
+    }
+
     void choose_window(double dtv)
     {
         const double kappa = std::abs(offdiag(dtv).y);
-        const std::complex<double> a(1.0, 2.0 * kappa * 0.99), c(-kappa * kappa, 0.0);
+        // the potential can only lower the imaginary part of the diagonal 2 kappa (1 + ...)
+        // by (dt/2) |Ahat_jj|; CAP and centrifugal terms only strengthen the decay
+        const double depress = std::min(0.5, 0.5 * dtv * diag_potential_bound() / (2.0 * kappa));
+        const std::complex<double> a(1.0, 2.0 * kappa * (1.0 - depress)), c(-kappa * kappa, 0.0);
         const std::complex<double> sq = std::sqrt(a * a - 4.0 * c);
         const double pp = std::max(std::abs((a + sq) * 0.5), std::abs((a - sq) * 0.5));
         const double rho = kappa / pp;
         int w = rho < 1.0 ? (int)std::ceil(40.0 / -std::log(rho)) + 16 : 4096;
-        precond_window = std::max(32, std::min(4096, w));
         precond_chunk = 2048;
+        // two staged solve CTAs per SM: (chunk + 2 window) * 32 bytes <= 96 KiB where possible
+        precond_window = std::max(32, std::min((6720 - precond_chunk) / 2, w));
     }
 
     void factorize(double dtv)
@@ -656,21 +815,26 @@ struct Solver {
         choose_window(dtv);
         const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
         CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
+        const int fwin = precond_window / 2 + 16;
+        const size_t smem = (size_t)std::min(Nr, precond_chunk + fwin) * sizeof(double2);
         kt_begin(TK_PFACTOR);
-        k_precond_factor<<<dim3(chunks, n_modes), SCAN_THREADS, 0, stream>>>(
-            grid(), table(), d_hh.p, 0.5 * dtv, offdiag(dtv), precond_chunk, precond_window / 2 + 16, dinv.p,
-            d_status.p);
+        k_precond_factor2<<<dim3(chunks, n_modes), SCAN2_THREADS, smem, stream>>>(
+            grid(), table(), d_hh.p, 0.5 * dtv, offdiag(dtv), precond_chunk, fwin, dinv.p, d_status.p);
         launch_check();
         kt_end(TK_PFACTOR);
     }
 
-    void precond(const double2 *bv, double2 *xv, double dtv)
+    unsigned apply_blocks() const { return apply3_grid().x * apply3_grid().y; }
+
+    void precond(const double2 *bv, double2 *xv, double dtv, PrecondInput in = PrecondInput{PI_PLAIN, nullptr,
+                                                                                             nullptr, nullptr,
+                                                                                             nullptr, nullptr})
     {
         const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
-        const size_t smem = (size_t)(std::min(Nr, precond_chunk + 2 * precond_window) + SCAN_THREADS) * sizeof(double2);
+        const size_t smem = (size_t)2 * std::min(Nr, precond_chunk + 2 * precond_window) * sizeof(double2);
         kt_begin(TK_PSOLVE);
-        k_precond_solve<<<dim3(chunks, n_modes), SCAN_THREADS, smem, stream>>>(Nr, precond_chunk, precond_window,
-                                                                               offdiag(dtv), dinv.p, bv, xv);
+        k_precond_solve2<<<dim3(chunks, n_modes), SCAN2_THREADS, smem, stream>>>(Nr, precond_chunk, precond_window,
+                                                                                offdiag(dtv), dinv.p, bv, xv, in);
         launch_check();
         kt_end(TK_PSOLVE);
     }
@@ -683,7 +847,7 @@ struct Solver {
     {
         k_dots<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, nq, a0, b0, a1, b1, a2, b2, d_partials.p);
         launch_check();
-        k_sum_partials<<<1, 256, 0, stream>>>(d_partials.p, vec_blocks, 2 * nq, d_red.p);
+        k_sum_partials<<<1, 512, 0, stream>>>(d_partials.p, vec_blocks, 2 * nq, d_red.p);
         launch_check();
     }
 
@@ -704,152 +868,126 @@ struct Solver {
     // -------------------------------------------------------------- CN solve
 
     // src/CrankNicolsonModes_matrices.cpp:94-215 with the radial block preconditioner.
+    // Scalars live on the device (Krylov); the host synchronises once before the
+    // loop, once per iteration (convergence / restart) and once for the residual.
     void solve_CN()
     {
         const double dtv = op.dt;
-        dots(1, rhs.p, rhs.p);
-        const double rhs_norm = std::sqrt(read_red(0));
-        if (rhs_norm == 0.0) {
-            CK(cudaMemsetAsync(psi.p, 0, nN * sizeof(double2), stream));
-            last_residual = 0.0;
-            last_iterations = 0;
-            return;
-        }
         const Absorber *sk[2];
         const int k = active_sinks(sk);
-        axpby(cmake(1.0 / rhs_norm, 0), rhs.p, cmake(0, 0), nullptr, b.p);
-        axpby(cmake(1.0 / rhs_norm, 0), psi.p, cmake(0, 0), nullptr, x.p);
-        factorize(dtv);
+        Krylov *dk = d_kr.p;
+        const double *red = d_red.p;
         Krylov kr;
         std::memset(&kr, 0, sizeof(kr));
         kr.n_sinks = k;
+        kr.tol = tolerance;
+        kr.max_iterations = max_iterations;
+        kr.eigen_path = k == 0;
+        CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
+        // b = rhs / |rhs|, x = psi / |rhs|, r = r0 = b - A_full x in one pass
+        dots(1, rhs.p, rhs.p);
+        k_krylov_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, red, rhs.p, psi.p, b.p, x.p, rr.p, r0.p,
+                                                                d_partials.p);
+        launch_check();
+        k_sum_partials<<<1, 512, 0, stream>>>(d_partials.p, vec_blocks, 4, d_red.p + 8);
+        launch_check();
+        factorize(dtv);
         if (k > 0) {
             // Woodbury: W_a = P^{-1} v_a, G = diag(1 / (dt/4 g_a)) + v_a^dag W_b (_matrices.cpp:133-145)
             precond(sk[0]->v.p, W0.p, dtv);
             if (k > 1) precond(sk[1]->v.p, W1.p, dtv);
             sink_dots(W0.p, d_dots.p + 4, sk, k);
             if (k > 1) sink_dots(W1.p, d_dots.p + 6, sk, k);
-            double2 hd[8];
-            CK(cudaMemcpyAsync(hd, d_dots.p, sizeof(hd), cudaMemcpyDeviceToHost, stream));
-            sync();
-            std::complex<double> G[2][2] = {{0, 0}, {0, 0}};
-            for (int a2 = 0; a2 < k; ++a2) {
-                G[a2][a2] += 1.0 / (0.25 * dtv * sk[a2]->strength);
-                for (int b2 = 0; b2 < k; ++b2) {
-                    const double2 vw = hd[4 + 2 * b2 + a2];  // v_a . W_b
-                    G[a2][b2] += std::complex<double>(vw.x, vw.y);
-                    kr.vW[a2][b2] = vw;
-                }
-            }
-            std::complex<double> Gi[2][2];
-            if (k == 1) {
-                Gi[0][0] = 1.0 / G[0][0];
-            } else {
-                const std::complex<double> det = G[0][0] * G[1][1] - G[0][1] * G[1][0];
-                Gi[0][0] = G[1][1] / det;
-                Gi[0][1] = -G[0][1] / det;
-                Gi[1][0] = -G[1][0] / det;
-                Gi[1][1] = G[0][0] / det;
-            }
-            for (int a2 = 0; a2 < 2; ++a2)
-                for (int b2 = 0; b2 < 2; ++b2) kr.Gi[a2][b2] = cmake(Gi[a2][b2].real(), Gi[a2][b2].imag());
+            k_wood_setup<<<1, 32, 0, stream>>>(dk, d_dots.p + 4, 0.25 * dtv * sk[0]->strength,
+                                              k > 1 ? 0.25 * dtv * sk[1]->strength : 1.0);
+            launch_check();
         }
-        // r = b - A_full x; r0 = r
-        sink_dots(x.p, d_dots.p, sk, k);
-        apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv);
-        axpby(cmake(1, 0), b.p, cmake(-1, 0), tmp.p, rr.p);
-        CK(cudaMemcpyAsync(r0.p, rr.p, nN * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
+        // Krylov scalars from |r0|^2 and |b|^2 (reduced by k_krylov_start into red[8..11])
         CK(cudaMemsetAsync(p.p, 0, nN * sizeof(double2), stream));
         CK(cudaMemsetAsync(v.p, 0, nN * sizeof(double2), stream));
-        dots(2, rr.p, rr.p, b.p, b.p);
-        double hr[4];
-        CK(cudaMemcpyAsync(hr, d_red.p, sizeof(hr), cudaMemcpyDeviceToHost, stream));
+        const double2 *p_cur = p.p;
+        k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_INIT, red + 8);
+        launch_check();
+        CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
         sync();
-        const double r0n2 = hr[0], b2 = hr[2];
+        if (kr.zero_rhs) {
+            CK(cudaMemsetAsync(psi.p, 0, nN * sizeof(double2), stream));
+            last_residual = 0.0;
+            last_iterations = 0;
+            return;
+        }
         const bool eigen_path = k == 0;
-        kr.rho = kr.alpha = kr.omega = cmake(1.0, 0.0);
-        kr.thr = tolerance * tolerance * b2;
         const double eps = std::numeric_limits<double>::epsilon();
-        kr.restart_thr = eigen_path ? eps * eps * r0n2 : 1e-32 * r0n2;
-        kr.r2 = r0n2;
-        kr.r0r = cmake(r0n2, 0.0);
-        kr.max_iterations = max_iterations;
-        kr.iterations = 0;
-        kr.done = !(r0n2 > kr.thr) || max_iterations <= 0;
-        CK(cudaMemcpyAsync(d_kr.p, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
         int restarts = 0;
-        Krylov *dk = d_kr.p;
-        const double *red = d_red.p;
         while (!kr.done) {
-            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_BETA, red);
-            launch_check();
-            CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
-            sync();
             if (kr.restart) {
-                // Lost biorthogonality: restart from the current residual (_matrices.cpp:69-75)
+                // Lost biorthogonality: restart from the current residual (_matrices.cpp:69-75).
+                const double2 rho_old = kr.rho;
                 sink_dots(x.p, d_dots.p, sk, k);
                 apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv);
                 axpby(cmake(1, 0), b.p, cmake(-1, 0), tmp.p, rr.p);
                 CK(cudaMemcpyAsync(r0.p, rr.p, nN * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
                 dots(1, rr.p, rr.p);
                 const double nr2 = read_red(0);
+                kr.rho_old = rho_old;
                 kr.rho = cmake(nr2, 0.0);
                 if (eigen_path) {
                     kr.restart_thr = eps * eps * nr2;
                     if (restarts++ == 0) kr.iterations = 0;
                 }
-                kr.beta = cmul(cdiv(kr.rho, kr.rho_old), cdiv(kr.alpha, kr.omega));
+                kr.beta = cmul(cdiv(kr.rho, rho_old), cdiv(kr.alpha, kr.omega));
                 kr.restart = 0;
                 CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
+            } else {
+                k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_BETA, red);
+                launch_check();
             }
-            // p = r + beta (p - omega v); y = M p
-            k_bicg_p<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, rr.p, v.p, p.p);
-            launch_check();
-            const double2 *yv = yP.p;
+            // p = r + beta (p - omega v) formed inside the preconditioner pass; y = M p
+            double2 *p_new = p_cur == p.p ? p2.p : p.p;
+            const PrecondInput pin{PI_P, dk, rr.p, p_cur, v.p, p_new};
+            p_cur = p_new;
             if (k > 0) {
-                precond(p.p, yP.p, dtv);
+                precond(nullptr, yP.p, dtv, pin);
                 sink_dots(yP.p, d_dots.p + 4, sk, k);
                 k_wood_scalar<<<1, 32, 0, stream>>>(dk, 0, d_dots.p + 4);
                 k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, 0, yP.p, W0.p, W1.p, y.p);
                 launch_check();
-                yv = y.p;
             } else {
-                precond(p.p, y.p, dtv);
-                yv = y.p;
+                precond(nullptr, y.p, dtv, pin);
             }
-            // v = A y; alpha = rho / r0.v
-            apply_A(yv, v.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[0][0]), dtv);
-            dots(1, r0.p, v.p);
-            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_ALPHA, red);
-            // s = r - alpha v; z = M s
-            k_bicg_s<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, rr.p, v.p, s.p);
+            // v = A y with r0 . v reduced in the same pass; alpha = rho / r0.v
+            apply_A(y.p, v.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[0][0]), dtv, 1, 1, r0.p);
+            k_reduce_stage<<<1, 512, 0, stream>>>(d_partials.p, (int)apply_blocks(), 2, d_red.p, dk, KS_ALPHA);
             launch_check();
+            // s = r - alpha v formed inside the preconditioner pass; z = M s
+            const PrecondInput sin{PI_S, dk, rr.p, nullptr, v.p, s.p};
             if (k > 0) {
-                precond(s.p, yP.p, dtv);
+                precond(nullptr, yP.p, dtv, sin);
                 sink_dots(yP.p, d_dots.p + 4, sk, k);
                 k_wood_scalar<<<1, 32, 0, stream>>>(dk, 1, d_dots.p + 4);
                 k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, 1, yP.p, W0.p, W1.p, z.p);
                 launch_check();
             } else {
-                precond(s.p, z.p, dtv);
+                precond(nullptr, z.p, dtv, sin);
             }
-            // t = A z; omega = t.s / |t|^2
-            apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv);
-            dots(2, t.p, s.p, t.p, t.p);
-            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_OMEGA, red);
+            // t = A z with t . s and |t|^2 reduced in the same pass; omega = t.s / |t|^2
+            apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv, 2, 2, s.p, 3,
+                    nullptr);
+            k_reduce_stage<<<1, 512, 0, stream>>>(d_partials.p, (int)apply_blocks(), 4, d_red.p, dk, KS_OMEGA);
+            launch_check();
             // x += alpha y + omega z; r = s - omega t
-            k_bicg_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, yv, z.p, rr.p, s.p, t.p, r0.p,
+            k_bicg_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, y.p, z.p, rr.p, s.p, t.p, r0.p,
                                                                    d_partials.p);
             launch_check();
-            k_sum_partials<<<1, 256, 0, stream>>>(d_partials.p, vec_blocks, 3, d_red.p);
-            k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_UPDATE, red);
+            k_reduce_stage<<<1, 512, 0, stream>>>(d_partials.p, vec_blocks, 3, d_red.p, dk, KS_UPDATE);
             launch_check();
             CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
             sync();
         }
         last_iterations = kr.iterations;
-        // candidate = x * |rhs|; residual = |A_full candidate - rhs| / |rhs|
-        axpby(cmake(rhs_norm, 0), x.p, cmake(0, 0), nullptr, cand.p);
+        // candidate = x |rhs|; residual = |A_full candidate - rhs| / |rhs|
+        k_scale_candidate<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, cand.p);
+        launch_check();
         sink_dots(cand.p, d_dots.p, sk, k);
         apply_A(cand.p, tmp.p, sk, k, d_dots.p, dtv);
         axpby(cmake(1, 0), tmp.p, cmake(-1, 0), rhs.p, tmp.p);
@@ -857,6 +995,7 @@ struct Solver {
         int status = 0;
         CK(cudaMemcpyAsync(&status, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
         const double res2 = read_red(0);
+        const double rhs_norm = kr.rhs_norm;
         last_residual = std::isfinite(res2) ? std::sqrt(res2) / rhs_norm : std::numeric_limits<double>::infinity();
         if (status != 0)
             throw Error(CNM_ESOLVE, "Radial preconditioner factorization failed (zero or non-finite pivot)");
@@ -922,17 +1061,18 @@ struct Solver {
         // diagnostics on the masked end-of-step state with the step's operators
         sink_dots(psi.p, d_dots.p, sk, k);
         if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2);
-        const unsigned dblocks = (unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE);
+        const dim3 dgrid = apply_grid();
+        const unsigned dblocks = dgrid.x * dgrid.y;
         kt_begin(TK_DIAG);
-        k_diagnostics<<<dblocks, APPLY_THREADS, diag_smem, stream>>>(
-            grid(), table(), d_hh.p, op.theta, op.domega, psi.p, idx_ex, k, k > 0 ? sk[0]->v.p : nullptr,
+        ::cnm::launch_diagnostics(
+            l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p, idx_ex, k, k > 0 ? sk[0]->v.p : nullptr,
             k > 1 ? sk[1]->v.p : nullptr, d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
             k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
             k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes);
         launch_check();
         kt_end(TK_DIAG);
         const int nslots = 2 * n_modes + 3;
-        k_sum_slots<<<(nslots + 127) / 128, 128, 0, stream>>>(d_partials.p, (int)dblocks, nslots, d_red.p);
+        k_sum_slots<<<nslots, 256, 0, stream>>>(d_partials.p, (int)dblocks, nslots, d_red.p);
         launch_check();
         double *hs = stage(nslots + 8 * n_modes + 16);
         CK(cudaMemcpyAsync(hs, d_red.p, nslots * sizeof(double), cudaMemcpyDeviceToHost, stream));
@@ -1017,6 +1157,67 @@ struct Solver {
         Omega = std::sqrt(Mt / std::pow(R, 3));
         P = 2.0 * M_PI / Omega;
         if (ramp_factor == 1.0) dt = P / steps_per_period;
+    }
+
+    // -------------------------------------------------------------- checkpoint
+
+    // src/CrankNicolsonModes_restart.cpp:139-177: "GMCKPT01", int32 {step, Nr, n_modes},
+    // 13 f64 {t, theta, phase, R, M1, M2, q, R1, R2, Omega, P, dt, p_bin}, u64 size,
+    // psi as complex128, the rolling-average blob.
+    std::vector<char> checkpoint(int step_id) const
+    {
+        std::vector<char> out;
+        auto put = [&](const void *p, size_t n) {
+            const char *c = static_cast<const char *>(p);
+            out.insert(out.end(), c, c + n);
+        };
+        put("GMCKPT01", 8);
+        const int32_t header[3] = {step_id, Nr, n_modes};
+        put(header, sizeof(header));
+        const double values[13] = {t_i, theta, phase, R, M1, M2, q, R1, R2, Omega, P, dt, p_bin};
+        put(values, sizeof(values));
+        const uint64_t size = (uint64_t)nN;
+        put(&size, 8);
+        const size_t at = out.size();
+        out.resize(at + (size_t)nN * sizeof(double2));
+        CK(cudaMemcpy(out.data() + at, psi.p, (size_t)nN * sizeof(double2), cudaMemcpyDeviceToHost));
+        power_average.save(out);
+        return out;
+    }
+
+    // src/CrankNicolsonModes_restart.cpp:179-233: false (state untouched) unless the blob
+    // is a complete checkpoint of this step and geometry.
+    bool restore(int step_id, const char *p, size_t size)
+    {
+        const size_t head = 8 + 12 + 13 * 8 + 8;
+        if (size < head || std::memcmp(p, "GMCKPT01", 8) != 0) return false;
+        int32_t header[3];
+        std::memcpy(header, p + 8, sizeof(header));
+        if (header[0] != step_id || header[1] != Nr || header[2] != n_modes) return false;
+        double values[13];
+        std::memcpy(values, p + 20, sizeof(values));
+        uint64_t n = 0;
+        std::memcpy(&n, p + 20 + 104, 8);
+        if (n != (uint64_t)nN || size < head + n * sizeof(double2)) return false;
+        RollingPhaseAverage avg(orbits_average);
+        size_t used = 0;
+        if (!avg.load(p + head + n * sizeof(double2), size - head - n * sizeof(double2), used)) return false;
+        CK(cudaMemcpy(psi.p, p + head, (size_t)n * sizeof(double2), cudaMemcpyHostToDevice));
+        t_i = values[0];
+        theta = values[1];
+        phase = values[2];
+        R = values[3];
+        M1 = values[4];
+        M2 = values[5];
+        q = values[6];
+        R1 = values[7];
+        R2 = values[8];
+        Omega = values[9];
+        P = values[10];
+        dt = values[11];
+        p_bin = values[12];
+        power_average = avg;
+        return true;
     }
 
     // -------------------------------------------------------------- cnm_apply
@@ -1346,6 +1547,35 @@ int cnm_sink_vector(const cnm_handle *h, int32_t body, double *out)
         const cnm::Absorber &ab = body == 1 ? s.abs1 : s.abs2;
         if (ab.v.p) cnm::cuda_check(cudaMemcpy(out, ab.v.p, s.nN * sizeof(double2), cudaMemcpyDeviceToHost), "cudaMemcpy");
         else std::fill(out, out + 2 * s.nN, 0.0);
+    });
+}
+
+int cnm_save_checkpoint(const cnm_handle *h, int32_t step_id, void *buf, int64_t capacity, int64_t *size)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) {
+        const std::vector<char> blob = s.checkpoint(step_id);
+        *size = (int64_t)blob.size();
+        if (buf) {
+            if (capacity < (int64_t)blob.size()) throw cnm::Error(CNM_EINVAL, "checkpoint buffer too small");
+            std::memcpy(buf, blob.data(), blob.size());
+        }
+    });
+}
+
+int cnm_load_checkpoint(cnm_handle *h, int32_t step_id, const void *buf, int64_t size, int32_t *loaded)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        *loaded = (buf && size > 0 && s.restore(step_id, static_cast<const char *>(buf), (size_t)size)) ? 1 : 0;
+    });
+}
+
+int cnm_replay_power_average(cnm_handle *h, const double *times, const double *phases, const double *values,
+                             int32_t n)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        if (n < 0 || (n > 0 && (!times || !phases || !values))) throw cnm::Error(CNM_EINVAL, "bad samples");
+        s.power_average = cnm::RollingPhaseAverage(s.orbits_average);
+        for (int32_t k = 0; k < n; ++k) s.power_average.update(times[k], phases[k], values[k]);
     });
 }
 

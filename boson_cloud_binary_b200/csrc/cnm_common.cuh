@@ -75,6 +75,7 @@ constexpr int ROW_BLOCK = 4;
 struct BlockTable {
     int n_chunks;
     const int *chunk_l;     // [n_chunks]
+    const int *chunk_nrows; // [n_chunks]
     const int *chunk_rows;  // [n_chunks * ROW_BLOCK]
     const int *chunk_goff;  // [n_chunks * (l_max + 1)]
     const int *l_off;       // [l_max + 2]
@@ -112,6 +113,12 @@ struct ApplyArgs {
     const double2 *sink_dots;   // device: v_a^dag x for each sink
     double sink_coef[2];
     int sink_lo[2], sink_hi[2]; // node support [lo, hi) of each v_a
+    // fused inner products of the output y with itself or another vector, as per-CTA
+    // partials [slot][block]: kind 1 conj(ext) . y, 2 conj(y) . ext, 3 |y|^2 (real)
+    int n_dots;
+    int dot_kind[2];
+    const double2 *dot_ext[2];
+    double *dot_partials;
 };
 
 }  // namespace cnm

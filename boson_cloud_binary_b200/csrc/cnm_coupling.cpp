@@ -185,26 +185,32 @@ BlockedCoupling block_coupling(const Coupling &c, int rb)
     std::vector<Ch> chunks;
     for (int l = 0; l <= L; ++l) {
         const int first = b.l_off[l], count = b.l_off[l + 1] - b.l_off[l];
-        double cost = 0;
-        for (int l1 = 0; l1 <= L; ++l1) cost += (l1 + 1) * (std::min(l, l1) + 3);
-        for (int r0 = 0; r0 < count; r0 += rb) chunks.push_back({l, first + r0, std::min(rb, count - r0), cost});
+        const int nch = (count + rb - 1) / rb;
+        int r0 = 0;
+        for (int c2 = 0; c2 < nch; ++c2) {
+            const int size = count / nch + (c2 < count % nch ? 1 : 0);
+            double cost = 0;
+            for (int l1 = 0; l1 <= L; ++l1) cost += (l1 + 1) * size * (std::min(l, l1) + 3);
+            chunks.push_back({l, first + r0, size, cost});
+            r0 += size;
+        }
     }
     std::stable_sort(chunks.begin(), chunks.end(), [](const Ch &a, const Ch &b2) { return a.cost > b2.cost; });
     b.n_chunks = (int)chunks.size();
     for (const Ch &ch : chunks) {
         b.chunk_l.push_back(ch.l);
+        b.chunk_nrows.push_back(ch.count);
         for (int rr = 0; rr < rb; ++rr) b.chunk_rows.push_back(rr < ch.count ? ch.first + rr : -1);
         for (int l1 = 0; l1 <= L; ++l1) {
             b.chunk_goff.push_back((int)b.g.size());
             const int L0 = std::abs(ch.l - l1), S = std::min(ch.l, l1) + 1;
+            const int stride = (S + 1) & ~1;
             for (int k = b.l_off[l1]; k < b.l_off[l1 + 1]; ++k)
-                for (int rr = 0; rr < rb; ++rr)
-                    for (int s2 = 0; s2 < S; ++s2) {
+                for (int rr = 0; rr < ch.count; ++rr)
+                    for (int s2 = 0; s2 < stride; ++s2) {
                         double gv = 0.0;
-                        if (rr < ch.count) {
-                            const std::vector<double> &v = dense[(size_t)(ch.first + rr) * c.n_modes + k];
-                            if (!v.empty()) gv = v[L0 + 2 * s2];
-                        }
+                        const std::vector<double> &v = dense[(size_t)(ch.first + rr) * c.n_modes + k];
+                        if (s2 < S && !v.empty()) gv = v[L0 + 2 * s2];
                         b.g.push_back(gv);
                     }
         }

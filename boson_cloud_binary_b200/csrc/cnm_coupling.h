@@ -31,12 +31,15 @@ Coupling build_coupling(int l_max);
 // l are taken `rb` at a time ("row chunks"); for every chunk and every column
 // degree l1 the Gaunt weights of the (l, l1) block are stored densely as
 // [column m1][row][s] with l* = |l - l1| + 2 s, s < min(l, l1) + 1 (zero where a
-// pair has no term at that l*), so the kernel's inner loops have compile-time
-// trip counts.
+// pair has no term at that l*; the s stride is rounded up to an even count so
+// pairs of weights load as one 16-byte word), so the kernel's inner loops have
+// compile-time trip counts.  The l + 1 rows of a degree are split into chunks of
+// near-equal size, at most rb each, so no chunk carries empty rows.
 struct BlockedCoupling {
-    int rb = 4;
+    int rb = 4;                    // most rows per chunk
     int n_chunks = 0;
     std::vector<int> chunk_l;      // [n_chunks]
+    std::vector<int> chunk_nrows;  // [n_chunks] rows in the chunk (1..rb)
     std::vector<int> chunk_rows;   // [n_chunks * rb], -1 pads
     std::vector<int> chunk_goff;   // [n_chunks * (l_max + 1)] offset of block (chunk, l1) in g
     std::vector<int> l_off;        // [l_max + 2] first mode index of each l

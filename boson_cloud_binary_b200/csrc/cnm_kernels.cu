@@ -187,26 +187,34 @@ __device__ int tile_lcut(const double *hs, int K, int lane)
 }
 
 // One (row chunk, l1) block: for the S_EFF leading multipoles l* = L0 + 2s held in
-// registers, Ahat_jk = sum_s g[k][row][s] h_s for the ROW_BLOCK rows of the chunk and
-// the l1 + 1 columns k = col0 .. col0 + ncols - 1, accumulated into acc (and into
-// accm with weight m_k for dV/dt).
-template <int S_EFF, bool DVDT>
+// registers, Ahat_jk = sum_s g[k][row][s] h_s for the RB rows of the chunk and the
+// l1 + 1 columns k = col0 .. col0 + ncols - 1, accumulated into acc (and into accm with
+// weight m_k for dV/dt).  Weights come in 16-byte pairs (even stride) and feed two
+// independent FMA chains.
+template <int S_EFF, int RB, bool DVDT>
 __device__ __forceinline__ void coupling_block(const double *__restrict__ g, int stride, int ncols, int col0,
                                                const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
-                                               double2 (&acc)[ROW_BLOCK], double2 (&accm)[ROW_BLOCK])
+                                               double2 (&acc)[RB], double2 (&accm)[RB])
 {
     double h[S_EFF];
 #pragma unroll
     for (int s2 = 0; s2 < S_EFF; ++s2) h[s2] = hs_l0[2 * s2 * APPLY_TILE + lane];
     for (int kk = 0; kk < ncols; ++kk) {
         const double2 z = zs[(col0 + kk) * APPLY_TILE + lane];
-        const double *gk = g + kk * ROW_BLOCK * stride;
+        const double *gk = g + kk * RB * stride;
         const double mk = DVDT ? (double)mode_m[col0 + kk] : 0.0;
 #pragma unroll
-        for (int rr = 0; rr < ROW_BLOCK; ++rr) {
-            double a = 0.0;
+        for (int rr = 0; rr < RB; ++rr) {
+            const double *gr = gk + rr * stride;
+            double a0 = 0.0, a1 = 0.0;
 #pragma unroll
-            for (int s2 = 0; s2 < S_EFF; ++s2) a = fma(__ldg(gk + rr * stride + s2), h[s2], a);
+            for (int s2 = 0; s2 + 1 < S_EFF; s2 += 2) {
+                const double2 gg = __ldg(reinterpret_cast<const double2 *>(gr + s2));
+                a0 = fma(gg.x, h[s2], a0);
+                a1 = fma(gg.y, h[s2 + 1], a1);
+            }
+            if (S_EFF & 1) a0 = fma(__ldg(gr + S_EFF - 1), h[S_EFF - 1], a0);
+            const double a = a0 + a1;
             acc[rr].x = fma(a, z.x, acc[rr].x);
             acc[rr].y = fma(a, z.y, acc[rr].y);
             if (DVDT) {
@@ -218,13 +226,19 @@ __device__ __forceinline__ void coupling_block(const double *__restrict__ g, int
     }
 }
 
-template <bool DVDT>
+template <int SMAX, int RB, bool DVDT>
 __device__ __forceinline__ void coupling_dispatch(int s_eff, const double *g, int stride, int ncols, int col0,
                                                   const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
-                                                  double2 (&acc)[ROW_BLOCK], double2 (&accm)[ROW_BLOCK])
+                                                  double2 (&acc)[RB], double2 (&accm)[RB])
 {
-#define CNM_CASE(S)                                                                                      \
-    case S: coupling_block<S, DVDT>(g, stride, ncols, col0, zs, hs_l0, mode_m, lane, acc, accm); break;
+    // Blocks of up to SMAX multipoles: the instantiation for an l_max allocates
+    // registers for its own widest block only.
+#define CNM_CASE(S)                                                                                  \
+    case S:                                                                                          \
+        if (S <= SMAX)                                                                               \
+            coupling_block<(S <= SMAX ? S : 1), RB, DVDT>(g, stride, ncols, col0, zs, hs_l0, mode_m, \
+                                                          lane, acc, accm);                          \
+        break;
     switch (s_eff) {
         CNM_CASE(1) CNM_CASE(2) CNM_CASE(3) CNM_CASE(4) CNM_CASE(5) CNM_CASE(6) CNM_CASE(7) CNM_CASE(8)
         CNM_CASE(9) CNM_CASE(10) CNM_CASE(11) CNM_CASE(12) CNM_CASE(13) CNM_CASE(14) CNM_CASE(15)
@@ -235,27 +249,148 @@ __device__ __forceinline__ void coupling_dispatch(int s_eff, const double *g, in
 #undef CNM_CASE
 }
 
-// Ahat z (and Ahat M z) for the rows of one chunk at the warp's 32 nodes.
-template <bool DVDT>
+// Ahat z (and Ahat M z) for the RB rows of one chunk at the warp's 32 nodes.
+template <int SMAX, int RB, bool DVDT>
 __device__ __forceinline__ void coupling_chunk(const BlockTable &bt, int l_max, int ci, int lcut, const double2 *zs,
-                                               const double *hs, const int *mode_m, int lane,
-                                               double2 (&acc)[ROW_BLOCK], double2 (&accm)[ROW_BLOCK])
+                                               const double *hs, const int *mode_m, int lane, double2 (&acc)[RB],
+                                               double2 (&accm)[RB])
 {
 #pragma unroll
-    for (int rr = 0; rr < ROW_BLOCK; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
+    for (int rr = 0; rr < RB; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
+    if (lcut < 0) return;
     const int l = bt.chunk_l[ci];
     for (int l1 = 0; l1 <= l_max; ++l1) {
         const int L0 = abs(l - l1), S = min(l, l1) + 1;
         if (lcut < L0) continue;
         const int s_eff = min(S, (lcut - L0) / 2 + 1);
-        const int col0 = bt.l_off[l1];
-        coupling_dispatch<DVDT>(s_eff, bt.g + bt.chunk_goff[ci * (l_max + 1) + l1], S, l1 + 1, col0, zs,
-                                hs + L0 * APPLY_TILE, mode_m, lane, acc, accm);
+        coupling_dispatch<SMAX, RB, DVDT>(s_eff, bt.g + bt.chunk_goff[ci * (l_max + 1) + l1], (S + 1) & ~1, l1 + 1,
+                                          bt.l_off[l1], zs, hs + L0 * APPLY_TILE, mode_m, lane, acc, accm);
     }
 }
 
-// Operator application, register-blocked: warps take row chunks round-robin.
-__global__ void __launch_bounds__(APPLY_THREADS) k_apply2(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a)
+// Everything an operator kernel's warp needs about its tile and node.
+struct TileCtx {
+    const double2 *xs, *zs, *ph;
+    const double *hs;
+    int lane, i, lcut;
+    bool interior;
+    double ri;
+};
+
+// Output of one chunk for k_apply2: stencil, potential, CAP, sinks, store, fused dots.
+template <int SMAX, int RB, int VP>
+__device__ __forceinline__ void apply_chunk(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
+                                            const ApplyArgs &a, const TileCtx &t, int ci, double (&dacc)[4])
+{
+    double2 acc[RB], accm[RB];
+    if (VP != V_NONE) coupling_chunk<SMAX, RB, VP == V_DVDT>(bt, ct.l_max, ci, t.lcut, t.zs, t.hs, ct.mode_m, t.lane, acc, accm);
+    const int Nr = g.Nr, c = t.lane, i = t.i;
+    if (i >= Nr) return;
+    const double alpha_d = 1.0 / (g.dr * g.dr);
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) {
+        const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
+        const double2 xv = t.xs[j * (APPLY_TILE + 2) + c + 1];
+        double2 h = cmake(0.0, 0.0);
+        if (a.use_h0 && t.interior) {
+            const int l = ct.mode_l[j];
+            const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (t.ri * t.ri)) / (2 * g.mu);
+            const double off = -alpha_d / (2 * g.mu);
+            h = cadd(cscale(xv, diag), cscale(cadd(t.xs[j * (APPLY_TILE + 2) + c], t.xs[j * (APPLY_TILE + 2) + c + 2]), off));
+        }
+        if (VP != V_NONE && t.interior) {
+            double2 vj;
+            if (VP == V_DVDT) {
+                const double mj = (double)ct.mode_m[j];
+                vj = cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), a.domega));
+            } else {
+                vj = acc[rr];
+            }
+            h = cadd(h, cmul(cconj(t.ph[j]), vj));
+        }
+        if (a.use_cap && g.capw) h = cadd(h, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
+        double2 y = cadd(cmul(a.alpha, xv), cmul(a.beta, h));
+        for (int s2 = 0; s2 < a.n_sinks; ++s2)
+            if (i >= a.sink_lo[s2] && i < a.sink_hi[s2])
+                y = cadd(y, cmul(cscale(a.sink_dots[s2], a.sink_coef[s2]), a.sink_v[s2][(int64_t)j * Nr + i]));
+        a.y[(int64_t)j * Nr + i] = y;
+        for (int q = 0; q < a.n_dots; ++q) {
+            double2 d;
+            if (a.dot_kind[q] == 1) d = cconjmul(a.dot_ext[q][(int64_t)j * Nr + i], y);
+            else if (a.dot_kind[q] == 2) d = cconjmul(y, a.dot_ext[q][(int64_t)j * Nr + i]);
+            else d = cmake(cabs2(y), 0.0);
+            dacc[2 * q] += d.x;
+            dacc[2 * q + 1] += d.y;
+        }
+    }
+}
+
+// Fused diagnostics of one chunk (see k_diagnostics2).
+template <int SMAX, int RB>
+__device__ __forceinline__ void diag_chunk(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
+                                           const TileCtx &t, int ci, bool active, int idx_ex, double domega,
+                                           int n_sinks, const double2 *sv0, const double2 *sv1,
+                                           const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0,
+                                           int shi0, int slo1, int shi1, double2 *dpsi_edge, double2 *psi_edge,
+                                           double *red, int nw, int warp, double &e_edge, double &pb, double &dv)
+{
+    double2 acc[RB], accm[RB];
+    coupling_chunk<SMAX, RB, true>(bt, ct.l_max, ci, t.lcut, t.zs, t.hs, ct.mode_m, t.lane, acc, accm);
+    const int Nr = g.Nr, c = t.lane, i = t.i, n = g.n_modes;
+    const double alpha_d = 1.0 / (g.dr * g.dr);
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) {
+        const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
+        double nrm = 0.0, en = 0.0;
+        if (active) {
+            const double2 xv = t.xs[j * (APPLY_TILE + 2) + c + 1];
+            double2 hx = cmake(0.0, 0.0), vx = cmake(0.0, 0.0), dx = cmake(0.0, 0.0);
+            if (t.interior) {
+                const int l = ct.mode_l[j];
+                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (t.ri * t.ri)) / (2 * g.mu);
+                const double off = -alpha_d / (2 * g.mu);
+                hx = cadd(cscale(xv, diag),
+                          cscale(cadd(t.xs[j * (APPLY_TILE + 2) + c], t.xs[j * (APPLY_TILE + 2) + c + 2]), off));
+                const double mj = (double)ct.mode_m[j];
+                vx = cmul(cconj(t.ph[j]), acc[rr]);
+                dx = cmul(cconj(t.ph[j]), cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), domega)));
+                hx = cadd(hx, vx);
+            }
+            if (g.capw) hx = cadd(hx, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
+            double2 dp = cmake(hx.y, -hx.x);  // -i H psi
+            if (n_sinks > 0 && i >= slo0 && i < shi0)
+                dp = cadd(dp, cmul(cscale(sink_dots[0], sink_coef0), sv0[(int64_t)j * Nr + i]));
+            if (n_sinks > 1 && i >= slo1 && i < shi1)
+                dp = cadd(dp, cmul(cscale(sink_dots[1], sink_coef1), sv1[(int64_t)j * Nr + i]));
+            const double ce = cconjmul(xv, hx).x;
+            if (i < idx_ex) {
+                nrm = cabs2(xv);
+                en = ce;
+            } else {
+                e_edge += ce;
+                dpsi_edge[j] = dp;
+                psi_edge[3 * j] = t.xs[j * (APPLY_TILE + 2) + c];
+                psi_edge[3 * j + 1] = xv;
+                psi_edge[3 * j + 2] = t.xs[j * (APPLY_TILE + 2) + c + 2];
+            }
+            pb += cconjmul(xv, dx).x;
+            dv += cconjmul(dp, vx).x;
+        }
+        nrm = warp_sum(nrm);
+        en = warp_sum(en);
+        if (t.lane == 0) {
+            red[j * nw + warp] = nrm;
+            red[(n + j) * nw + warp] = en;
+        }
+    }
+}
+
+// Operator application, register-blocked.  grid.x = node tiles, grid.y splits the row
+// chunks of a tile between CTAs (chunk ci goes to CTA ci % gridDim.y); inside a CTA the
+// warps take its chunks round-robin.
+// SMAX: widest (l, l1) block (l_max + 1 rounded up); VP: the potential part (VPart).
+template <int SMAX, int VP>
+__global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply2(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a)
 {
     extern __shared__ double2 smem2[];
     __shared__ int s_lcut;
@@ -265,8 +400,8 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_apply2(Grid g, CouplingTable 
     double2 *xs = smem2;                              // n * (TILE + 2)
     double2 *zs = xs + n * (APPLY_TILE + 2);          // n * TILE
     double2 *ph = zs + n * APPLY_TILE;                // n
-    double *hs = reinterpret_cast<double *>(ph + n);  // K * TILE
-    const bool vp = a.vpart != V_NONE;
+    double *hs = reinterpret_cast<double *>(ph + n);  // max(K, 4) * TILE
+    constexpr bool vp = VP != V_NONE;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
 
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
@@ -297,56 +432,46 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_apply2(Grid g, CouplingTable 
         }
     }
     __syncthreads();
-    const int lcut = vp ? s_lcut : -1;
-    const int c = lane;
-    const int i = i0 + c;
-    const bool interior = i >= 1 && i <= Nr - 2;
-    const double alpha_d = 1.0 / (g.dr * g.dr);
-    const double ri = i < Nr ? g.r[i] : 1.0;
-    for (int ci = warp; ci < bt.n_chunks; ci += nw) {
-        double2 acc[ROW_BLOCK], accm[ROW_BLOCK];
-        if (vp && lcut >= 0) {
-            if (a.vpart == V_DVDT) coupling_chunk<true>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
-            else coupling_chunk<false>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
-        } else {
-#pragma unroll
-            for (int rr = 0; rr < ROW_BLOCK; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
+    TileCtx t;
+    t.xs = xs;
+    t.zs = zs;
+    t.ph = ph;
+    t.hs = hs;
+    t.lane = lane;
+    t.i = i0 + lane;
+    t.lcut = vp ? s_lcut : -1;
+    t.interior = t.i >= 1 && t.i <= Nr - 2;
+    t.ri = t.i < Nr ? g.r[t.i] : 1.0;
+    double dacc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int ci = blockIdx.y + gridDim.y * warp; ci < bt.n_chunks; ci += gridDim.y * nw) {
+        switch (bt.chunk_nrows[ci]) {
+        case 1: apply_chunk<SMAX, 1, VP>(g, ct, bt, a, t, ci, dacc); break;
+        case 2: apply_chunk<SMAX, 2, VP>(g, ct, bt, a, t, ci, dacc); break;
+        case 3: apply_chunk<SMAX, 3, VP>(g, ct, bt, a, t, ci, dacc); break;
+        default: apply_chunk<SMAX, 4, VP>(g, ct, bt, a, t, ci, dacc); break;
         }
-        if (i >= Nr) continue;
+    }
+    if (a.n_dots > 0) {
+        // deterministic CTA reduction of the fused inner products into per-CTA partials
+        __syncthreads();
+        double *red = hs;  // the hh tile is no longer needed
 #pragma unroll
-        for (int rr = 0; rr < ROW_BLOCK; ++rr) {
-            const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
-            if (j < 0) continue;
-            const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
-            double2 h = cmake(0.0, 0.0);
-            if (a.use_h0 && interior) {
-                const int l = ct.mode_l[j];
-                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
-                const double off = -alpha_d / (2 * g.mu);
-                h = cadd(cscale(xv, diag),
-                         cscale(cadd(xs[j * (APPLY_TILE + 2) + c], xs[j * (APPLY_TILE + 2) + c + 2]), off));
-            }
-            if (vp && interior) {
-                double2 vj;
-                if (a.vpart == V_DVDT) {
-                    const double mj = (double)ct.mode_m[j];
-                    vj = cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), a.domega));
-                } else {
-                    vj = acc[rr];
-                }
-                h = cadd(h, cmul(cconj(ph[j]), vj));
-            }
-            if (a.use_cap && g.capw) h = cadd(h, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
-            double2 y = cadd(cmul(a.alpha, xv), cmul(a.beta, h));
-            for (int s2 = 0; s2 < a.n_sinks; ++s2)
-                if (i >= a.sink_lo[s2] && i < a.sink_hi[s2])
-                    y = cadd(y, cmul(cscale(a.sink_dots[s2], a.sink_coef[s2]), a.sink_v[s2][(int64_t)j * Nr + i]));
-            a.y[(int64_t)j * Nr + i] = y;
+        for (int q = 0; q < 4; ++q) dacc[q] = warp_sum(dacc[q]);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) red[q * 32 + warp] = dacc[q];
+        __syncthreads();
+        const int nblocks = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
+        if (threadIdx.x < 2 * a.n_dots) {
+            double sm = 0.0;
+            for (int w = 0; w < nw; ++w) sm += red[threadIdx.x * 32 + w];
+            a.dot_partials[(int64_t)threadIdx.x * nblocks + blk] = sm;
         }
     }
 }
 
 // Fused diagnostics, register-blocked (same outputs and partial layout as k_diagnostics).
+template <int SMAX>
 __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics2(Grid g, CouplingTable ct, BlockTable bt,
                                                                  const double *hh, double theta, double domega,
                                                                  const double2 *psi, int idx_ex, int n_sinks,
@@ -394,70 +519,31 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics2(Grid g, Coupling
         if (lane == 0) s_lcut = lc;
     }
     __syncthreads();
-    const int lcut = s_lcut;
-    const int c = lane;
-    const int i = i0 + c;
-    const bool active = i < Nr && i <= idx_ex;
-    const bool interior = i >= 1 && i <= Nr - 2;
-    const double alpha_d = 1.0 / (g.dr * g.dr);
-    const double ri = i < Nr ? g.r[i] : 1.0;
+    TileCtx t;
+    t.xs = xs;
+    t.zs = zs;
+    t.ph = ph;
+    t.hs = hs;
+    t.lane = lane;
+    t.i = i0 + lane;
+    t.lcut = s_lcut;
+    t.interior = t.i >= 1 && t.i <= Nr - 2;
+    t.ri = t.i < Nr ? g.r[t.i] : 1.0;
+    const bool active = t.i < Nr && t.i <= idx_ex;
     double e_edge = 0.0, pb = 0.0, dv = 0.0;
     // tiles entirely beyond the extraction node hold no diagnostics
     const bool tile_active = i0 <= idx_ex;
-    for (int ci = warp; tile_active && ci < bt.n_chunks; ci += nw) {
-        double2 acc[ROW_BLOCK], accm[ROW_BLOCK];
-        if (lcut >= 0) coupling_chunk<true>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
-        else {
-#pragma unroll
-            for (int rr = 0; rr < ROW_BLOCK; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
+    for (int ci = blockIdx.y + gridDim.y * warp; tile_active && ci < bt.n_chunks; ci += gridDim.y * nw) {
+#define CNM_DIAG(RB)                                                                                          \
+    diag_chunk<SMAX, RB>(g, ct, bt, t, ci, active, idx_ex, domega, n_sinks, sv0, sv1, sink_dots, sink_coef0, \
+                         sink_coef1, slo0, shi0, slo1, shi1, dpsi_edge, psi_edge, red, nw, warp, e_edge, pb, dv)
+        switch (bt.chunk_nrows[ci]) {
+        case 1: CNM_DIAG(1); break;
+        case 2: CNM_DIAG(2); break;
+        case 3: CNM_DIAG(3); break;
+        default: CNM_DIAG(4); break;
         }
-#pragma unroll
-        for (int rr = 0; rr < ROW_BLOCK; ++rr) {
-            const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
-            if (j < 0) continue;
-            double nrm = 0.0, en = 0.0;
-            if (active) {
-                const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
-                double2 hx = cmake(0.0, 0.0), vx = cmake(0.0, 0.0), dx = cmake(0.0, 0.0);
-                if (interior) {
-                    const int l = ct.mode_l[j];
-                    const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
-                    const double off = -alpha_d / (2 * g.mu);
-                    hx = cadd(cscale(xv, diag),
-                              cscale(cadd(xs[j * (APPLY_TILE + 2) + c], xs[j * (APPLY_TILE + 2) + c + 2]), off));
-                    const double mj = (double)ct.mode_m[j];
-                    vx = cmul(cconj(ph[j]), acc[rr]);
-                    dx = cmul(cconj(ph[j]),
-                              cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), domega)));
-                    hx = cadd(hx, vx);
-                }
-                if (g.capw) hx = cadd(hx, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
-                double2 dp = cmake(hx.y, -hx.x);  // -i H psi
-                if (n_sinks > 0 && i >= slo0 && i < shi0)
-                    dp = cadd(dp, cmul(cscale(sink_dots[0], sink_coef0), sv0[(int64_t)j * Nr + i]));
-                if (n_sinks > 1 && i >= slo1 && i < shi1)
-                    dp = cadd(dp, cmul(cscale(sink_dots[1], sink_coef1), sv1[(int64_t)j * Nr + i]));
-                const double ce = cconjmul(xv, hx).x;
-                if (i < idx_ex) {
-                    nrm = cabs2(xv);
-                    en = ce;
-                } else {
-                    e_edge += ce;
-                    dpsi_edge[j] = dp;
-                    psi_edge[3 * j] = xs[j * (APPLY_TILE + 2) + c];
-                    psi_edge[3 * j + 1] = xv;
-                    psi_edge[3 * j + 2] = xs[j * (APPLY_TILE + 2) + c + 2];
-                }
-                pb += cconjmul(xv, dx).x;
-                dv += cconjmul(dp, vx).x;
-            }
-            nrm = warp_sum(nrm);
-            en = warp_sum(en);
-            if (lane == 0) {
-                red[j * nw + warp] = nrm;
-                red[(n + j) * nw + warp] = en;
-            }
-        }
+#undef CNM_DIAG
     }
     e_edge = warp_sum(e_edge);
     pb = warp_sum(pb);
@@ -468,11 +554,319 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics2(Grid g, Coupling
         red[(2 * n + 2) * nw + warp] = dv;
     }
     __syncthreads();
+    const int nblocks = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
     for (int q = threadIdx.x; q < 2 * n + 3; q += blockDim.x) {
         double sm = 0.0;
         for (int w = 0; w < nw; ++w) sm += red[q * nw + w];
-        partials[(int64_t)q * gridDim.x + blockIdx.x] = sm;
+        partials[(int64_t)q * nblocks + blk] = sm;
     }
+}
+
+// ------------------------------------------------------------------ operator kernel, two nodes per thread
+
+// Tiles of TILE3 = 64 nodes: lane l of every warp owns nodes l and l + 32, so each
+// warp-uniform Gaunt weight loaded for a chunk of at most two rows feeds the FMA
+// chains of both nodes.  z = D^dag x and the hh tile sit in shared memory; x itself
+// is read through L1 where the stencil and the output need it.
+constexpr int TILE3 = 64;
+
+template <int S_EFF, int RB, bool DVDT>
+__device__ __forceinline__ void coupling_block3(const double *__restrict__ g, int stride, int ncols, int col0,
+                                                const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
+                                                double2 (&acc)[RB][2], double2 (&accm)[RB][2])
+{
+    double h0[S_EFF], h1[S_EFF];
+#pragma unroll
+    for (int s2 = 0; s2 < S_EFF; ++s2) {
+        h0[s2] = hs_l0[2 * s2 * TILE3 + lane];
+        h1[s2] = hs_l0[2 * s2 * TILE3 + lane + 32];
+    }
+    for (int kk = 0; kk < ncols; ++kk) {
+        const double2 z0 = zs[(col0 + kk) * TILE3 + lane];
+        const double2 z1 = zs[(col0 + kk) * TILE3 + lane + 32];
+        const double *gk = g + kk * RB * stride;
+        const double mk = DVDT ? (double)mode_m[col0 + kk] : 0.0;
+#pragma unroll
+        for (int rr = 0; rr < RB; ++rr) {
+            const double *gr = gk + rr * stride;
+            double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+            for (int s2 = 0; s2 + 1 < S_EFF; s2 += 2) {
+                const double2 gg = __ldg(reinterpret_cast<const double2 *>(gr + s2));
+                a0 = fma(gg.x, h0[s2], a0);
+                a1 = fma(gg.y, h0[s2 + 1], a1);
+                b0 = fma(gg.x, h1[s2], b0);
+                b1 = fma(gg.y, h1[s2 + 1], b1);
+            }
+            if (S_EFF & 1) {
+                const double gl = __ldg(gr + S_EFF - 1);
+                a0 = fma(gl, h0[S_EFF - 1], a0);
+                b0 = fma(gl, h1[S_EFF - 1], b0);
+            }
+            const double a = a0 + a1, b = b0 + b1;
+            acc[rr][0].x = fma(a, z0.x, acc[rr][0].x);
+            acc[rr][0].y = fma(a, z0.y, acc[rr][0].y);
+            acc[rr][1].x = fma(b, z1.x, acc[rr][1].x);
+            acc[rr][1].y = fma(b, z1.y, acc[rr][1].y);
+            if (DVDT) {
+                const double am = a * mk, bm = b * mk;
+                accm[rr][0].x = fma(am, z0.x, accm[rr][0].x);
+                accm[rr][0].y = fma(am, z0.y, accm[rr][0].y);
+                accm[rr][1].x = fma(bm, z1.x, accm[rr][1].x);
+                accm[rr][1].y = fma(bm, z1.y, accm[rr][1].y);
+            }
+        }
+    }
+}
+
+template <int SMAX, int RB, bool DVDT>
+__device__ __forceinline__ void coupling_chunk3(const BlockTable &bt, int l_max, int ci, int lcut, const double2 *zs,
+                                                const double *hs, const int *mode_m, int lane, double2 (&acc)[RB][2],
+                                                double2 (&accm)[RB][2])
+{
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) acc[rr][0] = acc[rr][1] = accm[rr][0] = accm[rr][1] = cmake(0.0, 0.0);
+    if (lcut < 0) return;
+    const int l = bt.chunk_l[ci];
+    for (int l1 = 0; l1 <= l_max; ++l1) {
+        const int L0 = abs(l - l1), S = min(l, l1) + 1;
+        if (lcut < L0) continue;
+        const int s_eff = min(S, (lcut - L0) / 2 + 1);
+        const double *g = bt.g + bt.chunk_goff[ci * (l_max + 1) + l1];
+        const int stride = (S + 1) & ~1, col0 = bt.l_off[l1];
+        const double *hs_l0 = hs + L0 * TILE3;
+#define CNM_CASE3(S2)                                                                                            \
+    case S2:                                                                                                     \
+        if (S2 <= SMAX)                                                                                          \
+            coupling_block3<(S2 <= SMAX ? S2 : 1), RB, DVDT>(g, stride, l1 + 1, col0, zs, hs_l0, mode_m, lane, \
+                                                             acc, accm);                                        \
+        break;
+        switch (s_eff) {
+            CNM_CASE3(1) CNM_CASE3(2) CNM_CASE3(3) CNM_CASE3(4) CNM_CASE3(5) CNM_CASE3(6) CNM_CASE3(7)
+            CNM_CASE3(8) CNM_CASE3(9) CNM_CASE3(10) CNM_CASE3(11) CNM_CASE3(12) CNM_CASE3(13) CNM_CASE3(14)
+            CNM_CASE3(15) CNM_CASE3(16) CNM_CASE3(17) CNM_CASE3(18) CNM_CASE3(19) CNM_CASE3(20) CNM_CASE3(21)
+            CNM_CASE3(22) CNM_CASE3(23) CNM_CASE3(24) CNM_CASE3(25)
+        default: break;
+        }
+#undef CNM_CASE3
+    }
+}
+
+template <int SMAX, int RB, int VP>
+__device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
+                                             const ApplyArgs &a, const double2 *zs, const double2 *ph,
+                                             const double *hs, int lane, int i0, int lcut, int ci, double (&dacc)[4])
+{
+    double2 acc[RB][2], accm[RB][2];
+    if (VP != V_NONE) coupling_chunk3<SMAX, RB, VP == V_DVDT>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
+    const int Nr = g.Nr;
+    const double alpha_d = 1.0 / (g.dr * g.dr);
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) {
+        const int j = bt.chunk_rows[ci * 2 + rr];
+        const double2 *xr = a.x + (int64_t)j * Nr;
+#pragma unroll
+        for (int nb = 0; nb < 2; ++nb) {
+            const int i = i0 + lane + 32 * nb;
+            if (i >= Nr) continue;
+            const bool interior = i >= 1 && i <= Nr - 2;
+            const double2 xv = xr[i];
+            double2 h = cmake(0.0, 0.0);
+            if (a.use_h0 && interior) {
+                const int l = ct.mode_l[j];
+                const double ri = g.r[i];
+                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+                const double off = -alpha_d / (2 * g.mu);
+                h = cadd(cscale(xv, diag), cscale(cadd(xr[i - 1], xr[i + 1]), off));
+            }
+            if (VP != V_NONE && interior) {
+                double2 vj;
+                if (VP == V_DVDT) {
+                    const double mj = (double)ct.mode_m[j];
+                    vj = cmuli(cscale(cmake(accm[rr][nb].x - mj * acc[rr][nb].x, accm[rr][nb].y - mj * acc[rr][nb].y),
+                                      a.domega));
+                } else {
+                    vj = acc[rr][nb];
+                }
+                h = cadd(h, cmul(cconj(ph[j]), vj));
+            }
+            if (a.use_cap && g.capw) h = cadd(h, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
+            double2 y = cadd(cmul(a.alpha, xv), cmul(a.beta, h));
+            for (int s2 = 0; s2 < a.n_sinks; ++s2)
+                if (i >= a.sink_lo[s2] && i < a.sink_hi[s2])
+                    y = cadd(y, cmul(cscale(a.sink_dots[s2], a.sink_coef[s2]), a.sink_v[s2][(int64_t)j * Nr + i]));
+            a.y[(int64_t)j * Nr + i] = y;
+            for (int q = 0; q < a.n_dots; ++q) {
+                double2 d;
+                if (a.dot_kind[q] == 1) d = cconjmul(a.dot_ext[q][(int64_t)j * Nr + i], y);
+                else if (a.dot_kind[q] == 2) d = cconjmul(y, a.dot_ext[q][(int64_t)j * Nr + i]);
+                else d = cmake(cabs2(y), 0.0);
+                dacc[2 * q] += d.x;
+                dacc[2 * q + 1] += d.y;
+            }
+        }
+    }
+}
+
+template <int SMAX, int VP>
+__global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a)
+{
+    extern __shared__ double2 smem3[];
+    __shared__ int s_lcut;
+    const int n = g.n_modes, Nr = g.Nr;
+    const int K = 2 * ct.l_max + 1;
+    const int i0 = blockIdx.x * TILE3;
+    double2 *zs = smem3;                              // n * TILE3
+    double2 *ph = zs + n * TILE3;                     // n
+    double *hs = reinterpret_cast<double *>(ph + n);  // max(K, 4) * TILE3
+    constexpr bool vp = VP != V_NONE;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double sn, cs;
+        sincos((double)ct.mode_m[k] * a.theta, &sn, &cs);
+        ph[k] = cmake(cs, sn);
+    }
+    if (vp)
+        for (int e = threadIdx.x; e < K * TILE3; e += blockDim.x) {
+            const int l = e / TILE3, c = e % TILE3;
+            const int i = i0 + c;
+            hs[e] = i < Nr ? a.hh[(int64_t)l * Nr + i] : 0.0;
+        }
+    __syncthreads();
+    if (vp) {
+        for (int e = threadIdx.x; e < n * TILE3; e += blockDim.x) {
+            const int k = e / TILE3, c = e % TILE3;
+            const int i = i0 + c;
+            zs[e] = i < Nr ? cmul(ph[k], a.x[(int64_t)k * Nr + i]) : cmake(0.0, 0.0);
+        }
+        if (warp == 0) {
+            // multipole cut over both halves of the tile
+            int lc = -1;
+            for (int half = 0; half < 2; ++half) {
+                const int c = lane + 32 * half;
+                const double h0 = fabs(hs[c]);
+                if (h0 > 0.0) {
+                    int lcc = 0;
+                    for (int l = K - 1; l > 0; --l)
+                        if (fabs(hs[l * TILE3 + c]) > 1e-18 * h0) {
+                            lcc = l;
+                            break;
+                        }
+                    lc = max(lc, lcc);
+                }
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) lc = max(lc, __shfl_xor_sync(0xffffffffu, lc, o));
+            if (lane == 0) s_lcut = lc;
+        }
+    }
+    __syncthreads();
+    const int lcut = vp ? s_lcut : -1;
+    double dacc[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int ci = blockIdx.y + gridDim.y * warp; ci < bt.n_chunks; ci += gridDim.y * nw) {
+        if (bt.chunk_nrows[ci] == 1) apply_chunk3<SMAX, 1, VP>(g, ct, bt, a, zs, ph, hs, lane, i0, lcut, ci, dacc);
+        else apply_chunk3<SMAX, 2, VP>(g, ct, bt, a, zs, ph, hs, lane, i0, lcut, ci, dacc);
+    }
+    if (a.n_dots > 0) {
+        __syncthreads();
+        double *red = hs;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) dacc[q] = warp_sum(dacc[q]);
+        if (lane == 0)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) red[q * 32 + warp] = dacc[q];
+        __syncthreads();
+        const int nblocks = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
+        if (threadIdx.x < 2 * a.n_dots) {
+            double sm = 0.0;
+            for (int w = 0; w < nw; ++w) sm += red[threadIdx.x * 32 + w];
+            a.dot_partials[(int64_t)threadIdx.x * nblocks + blk] = sm;
+        }
+    }
+}
+
+// ---- launchers of the templated operator kernels
+
+static int smax_for(int l_max)
+{
+    const int need = l_max + 1;
+    return need <= 5 ? 5 : need <= 9 ? 9 : need <= 13 ? 13 : need <= 17 ? 17 : 25;
+}
+
+#define CNM_FOR_SMAX(MACRO) MACRO(5) MACRO(9) MACRO(13) MACRO(17) MACRO(25)
+
+cudaError_t set_operator_smem(int apply_bytes, int diag_bytes)
+{
+    cudaError_t e = cudaSuccess;
+#define CNM_ATTR(S)                                                                                          \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply2<S, V_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, apply_bytes); \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply2<S, V_POT>, cudaFuncAttributeMaxDynamicSharedMemorySize, apply_bytes);  \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply2<S, V_DVDT>, cudaFuncAttributeMaxDynamicSharedMemorySize, apply_bytes); \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diagnostics2<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_bytes);
+    CNM_FOR_SMAX(CNM_ATTR)
+#undef CNM_ATTR
+    return e;
+}
+
+cudaError_t set_apply3_smem(int bytes)
+{
+    cudaError_t e = cudaSuccess;
+#define CNM_ATTR3(S)                                                                                           \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply3<S, V_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply3<S, V_POT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);  \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply3<S, V_DVDT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    CNM_FOR_SMAX(CNM_ATTR3)
+#undef CNM_ATTR3
+    return e;
+}
+
+void launch_apply3(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
+                   const BlockTable &bt, const ApplyArgs &a)
+{
+    const int smax = smax_for(l_max);
+#define CNM_LAUNCH3(S)                                                                                     \
+    if (smax == S) {                                                                                       \
+        if (a.vpart == V_POT) k_apply3<S, V_POT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);       \
+        else if (a.vpart == V_DVDT) k_apply3<S, V_DVDT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);\
+        else k_apply3<S, V_NONE><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);                       \
+        return;                                                                                            \
+    }
+    CNM_FOR_SMAX(CNM_LAUNCH3)
+#undef CNM_LAUNCH3
+}
+
+void launch_apply(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
+                  const BlockTable &bt, const ApplyArgs &a)
+{
+    const int smax = smax_for(l_max);
+#define CNM_LAUNCH(S)                                                                                        \
+    if (smax == S) {                                                                                         \
+        if (a.vpart == V_POT) k_apply2<S, V_POT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);         \
+        else if (a.vpart == V_DVDT) k_apply2<S, V_DVDT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);  \
+        else k_apply2<S, V_NONE><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);                         \
+        return;                                                                                              \
+    }
+    CNM_FOR_SMAX(CNM_LAUNCH)
+#undef CNM_LAUNCH
+}
+
+void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
+                        const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
+                        const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
+                        const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0, int slo1,
+                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge)
+{
+    const int smax = smax_for(l_max);
+#define CNM_LAUNCH(S)                                                                                        \
+    if (smax == S) {                                                                                         \
+        k_diagnostics2<S><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, hh, theta, domega, psi, idx_ex,    \
+                                                               n_sinks, sv0, sv1, sink_dots, sink_coef0,     \
+                                                               sink_coef1, slo0, shi0, slo1, shi1, partials, \
+                                                               dpsi_edge, psi_edge);                         \
+        return;                                                                                              \
+    }
+    CNM_FOR_SMAX(CNM_LAUNCH)
+#undef CNM_LAUNCH
 }
 
 // ------------------------------------------------------------------ sink projections
@@ -785,6 +1179,196 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_precond_solve(int Nr, int chun
     }
 }
 
+// x = P^{-1} b with the chunk, its windows, the pivots and the right-hand side staged in
+// shared memory by coalesced loads; the sweeps run in place in shared memory.
+__global__ void __launch_bounds__(SCAN2_THREADS) k_precond_solve2(int Nr, int chunk, int window, double2 off,
+                                                                  const double2 *dinv, const double2 *b, double2 *x,
+                                                                  PrecondInput in)
+{
+    extern __shared__ double2 sm2[];
+    __shared__ Aff tf[SCAN2_THREADS];
+    const int j = blockIdx.y;
+    const int c0 = blockIdx.x * chunk, c1 = min(Nr, c0 + chunk);
+    const int lo = max(0, c0 - window), hi = min(Nr, c1 + window);
+    const int len = hi - lo;
+    const int cap = min(Nr, chunk + 2 * window);
+    double2 *D = sm2, *Y = sm2 + cap;
+    const int64_t base = (int64_t)j * Nr + lo;
+    if (in.mode == PI_PLAIN) {
+        for (int e = threadIdx.x; e < len; e += blockDim.x) {
+            D[e] = dinv[base + e];
+            Y[e] = b[base + e];
+        }
+    } else {
+        // the right-hand side is a BiCGSTAB combination formed here and also stored
+        // (own chunk only) as the search direction p or the vector s
+        const double2 beta = in.kr->beta, omega = in.kr->omega, alpha = in.kr->alpha;
+        for (int e = threadIdx.x; e < len; e += blockDim.x) {
+            D[e] = dinv[base + e];
+            const int64_t k = base + e;
+            double2 rhsv;
+            if (in.mode == PI_P) rhsv = cadd(in.r[k], cmul(beta, csub(in.p_old[k], cmul(omega, in.v[k]))));
+            else rhsv = csub(in.r[k], cmul(alpha, in.v[k]));
+            Y[e] = rhsv;
+            const int i = lo + e;
+            if (i >= c0 && i < c1) in.out[k] = rhsv;
+        }
+    }
+    __syncthreads();
+    int per = (len + blockDim.x - 1) / blockDim.x;
+    per |= 1;
+    const int s0 = threadIdx.x * per, s1 = min(len, s0 + per);
+    // forward: y_i = d_i (b_i - l_i y_{i-1})
+    Aff acc{cmake(1, 0), cmake(0, 0)};
+    for (int e = s0; e < s1; ++e) {
+        const int i = lo + e;
+        const double2 d = D[e];
+        const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        const Aff m{cmake(-(l.x * d.x - l.y * d.y), -(l.x * d.y + l.y * d.x)), cmul(d, Y[e])};
+        acc = aff_then(acc, m);
+    }
+    tf[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        Aff mine = tf[threadIdx.x], prev;
+        const bool has = threadIdx.x >= (unsigned)o;
+        if (has) prev = tf[threadIdx.x - o];
+        __syncthreads();
+        if (has) tf[threadIdx.x] = aff_then(prev, mine);
+        __syncthreads();
+    }
+    double2 y = threadIdx.x > 0 ? tf[threadIdx.x - 1].B : cmake(0, 0);
+    for (int e = s0; e < s1; ++e) {
+        const int i = lo + e;
+        const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        y = cmul(D[e], csub(Y[e], cmul(l, y)));
+        Y[e] = y;
+    }
+    __syncthreads();
+    // backward: x_i = y_i - u_i d_i x_{i+1}
+    Aff bcc{cmake(1, 0), cmake(0, 0)};
+    for (int e = s1 - 1; e >= s0; --e) {
+        const int i = lo + e;
+        const double2 d = D[e];
+        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        const Aff m{cmake(-(u.x * d.x - u.y * d.y), -(u.x * d.y + u.y * d.x)), Y[e]};
+        bcc = aff_then(bcc, m);
+    }
+    tf[threadIdx.x] = bcc;
+    __syncthreads();
+    const int T = blockDim.x;
+    for (int o = 1; o < T; o <<= 1) {
+        Aff mine = tf[threadIdx.x], prev;
+        const bool has = (int)threadIdx.x + o < T;
+        if (has) prev = tf[threadIdx.x + o];
+        __syncthreads();
+        if (has) tf[threadIdx.x] = aff_then(prev, mine);
+        __syncthreads();
+    }
+    double2 xv = (int)threadIdx.x + 1 < T ? tf[threadIdx.x + 1].B : cmake(0, 0);
+    for (int e = s1 - 1; e >= s0; --e) {
+        const int i = lo + e;
+        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        xv = csub(Y[e], cmul(cmul(u, D[e]), xv));
+        Y[e] = xv;
+    }
+    __syncthreads();
+    for (int e = (c0 - lo) + threadIdx.x; e < (c1 - lo); e += blockDim.x) x[base + e] = Y[e];
+}
+
+// Pivots with the chunk's diagonal staged in shared memory by coalesced passes over
+// the hh table; the recurrence then runs from shared memory and the inverse pivots
+// leave through one coalesced store.
+__global__ void __launch_bounds__(SCAN2_THREADS) k_precond_factor2(Grid g, CouplingTable ct, const double *hh,
+                                                                   double half_dt, double2 off, int chunk, int window,
+                                                                   double2 *dinv, int *status)
+{
+    extern __shared__ double2 sm2[];
+    __shared__ Mob tmat[SCAN2_THREADS];
+    const int Nr = g.Nr, j = blockIdx.y;
+    const int c0 = blockIdx.x * chunk, c1 = min(Nr, c0 + chunk);
+    const int lo = max(0, c0 - window), hi = c1;
+    const int len = hi - lo;
+    double2 *A = sm2;
+    // diagonal of A = 1 + i dt/2 (H0 + V + CAP) staged term by term: every pass over the
+    // nodes reads one row of the hh table with coalesced, independent loads
+    {
+        const int l = ct.mode_l[j];
+        const double alpha_d = 1.0 / (g.dr * g.dr);
+        for (int e = threadIdx.x; e < len; e += blockDim.x) {
+            const int i = lo + e;
+            double hre = 0.0;
+            if (i >= 1 && i <= Nr - 2) {
+                const double ri = g.r[i];
+                hre = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+            }
+            A[e] = cmake(0.0, hre);
+        }
+        const int p = ct.diag_pair[j];
+        if (p >= 0)
+            for (int t = ct.pair_term_ptr[p]; t < ct.pair_term_ptr[p + 1]; ++t) {
+                const double gt = ct.term_g[t];
+                const double *row = hh + (int64_t)ct.term_l[t] * Nr + lo;
+                for (int e = threadIdx.x; e < len; e += blockDim.x) {
+                    const int i = lo + e;
+                    if (i >= 1 && i <= Nr - 2) A[e].y += gt * row[e];
+                }
+            }
+        for (int e = threadIdx.x; e < len; e += blockDim.x) {
+            const double him = g.capw ? -g.capw[lo + e] : 0.0;
+            // 1 + i (dt/2) (hre + i him) = (1 - dt/2 him) + i dt/2 hre
+            A[e] = cmake(1.0 - half_dt * him, half_dt * A[e].y);
+        }
+    }
+    __syncthreads();
+    const double2 pstart = A[0];  // start value before node lo (exact when lo == 0)
+    int per = (len + blockDim.x - 1) / blockDim.x;
+    per |= 1;
+    const int s0 = threadIdx.x * per, s1 = min(len, s0 + per);
+    const double2 c = cmul(off, off);
+    Mob acc;
+    acc.m00 = cmake(1, 0);
+    acc.m01 = cmake(0, 0);
+    acc.m10 = cmake(0, 0);
+    acc.m11 = cmake(1, 0);
+    for (int e = s0; e < s1; ++e) {
+        acc = mob_mul(pivot_map(A[e], lo + e, Nr, c), acc);
+        mob_normalize(acc);
+    }
+    tmat[threadIdx.x] = acc;
+    __syncthreads();
+    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
+        Mob mine = tmat[threadIdx.x];
+        Mob prev;
+        const bool has = threadIdx.x >= (unsigned)o;
+        if (has) prev = tmat[threadIdx.x - o];
+        __syncthreads();
+        if (has) {
+            mine = mob_mul(mine, prev);
+            mob_normalize(mine);
+            tmat[threadIdx.x] = mine;
+        }
+        __syncthreads();
+    }
+    double2 p = pstart;
+    if (threadIdx.x > 0 && s0 < len) p = mob_apply(tmat[threadIdx.x - 1], p);
+    int bad = 0;
+    for (int e = s0; e < s1; ++e) {
+        p = mob_apply(pivot_map(A[e], lo + e, Nr, c), p);
+        const double m = cabs2(p);
+        if (!(m > 0.0) || !isfinite(m)) {
+            if (lo + e >= c0) bad = 1;
+            A[e] = cmake(0.0, 0.0);
+        } else {
+            A[e] = crcp(p);
+        }
+    }
+    if (bad) atomicOr(status, 1);
+    __syncthreads();
+    const int64_t base = (int64_t)j * Nr + lo;
+    for (int e = (c0 - lo) + threadIdx.x; e < len; e += blockDim.x) dinv[base + e] = A[e];
+}
+
 // ------------------------------------------------------------------ vector kernels
 
 // Per-CTA partial sums of up to three complex inner products conj(a_q) . b_q over n
@@ -897,10 +1481,9 @@ __global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2
     }
 }
 
-// Scalar steps of the recurrence, one thread.
-__global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
+// Scalar steps of the recurrence.
+__device__ void bicg_stage(Krylov *kr, int stage, const double *red)
 {
-    if (threadIdx.x != 0) return;
     switch (stage) {
     case KS_BETA: {  // rho_old = rho; rho = r0 . r; restart check; beta
         const double2 rho_old = kr->rho;
@@ -918,14 +1501,119 @@ __global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
         kr->omega = tt > 0.0 ? cscale(cmake(red[0], red[1]), 1.0 / tt) : cmake(0.0, 0.0);
         break;
     }
-    case KS_UPDATE:  // red = {|r|^2, r0.r re, im}
+    case KS_UPDATE:  // red = {|r|^2, r0.r re, im}; also flags the next iteration's restart
         kr->r2 = red[0];
         kr->r0r = cmake(red[1], red[2]);
         kr->iterations += 1;
         kr->done = !(kr->r2 > kr->thr) || kr->iterations >= kr->max_iterations;
+        kr->restart = sqrt(cabs2(kr->r0r)) < kr->restart_thr ? 1 : 0;
         break;
+    case KS_INIT: {  // red = {|r0|^2, 0, |b|^2, 0}
+        const double r0n2 = red[0], b2 = red[2];
+        kr->rho = kr->alpha = kr->omega = cmake(1.0, 0.0);
+        kr->thr = kr->tol * kr->tol * b2;
+        const double eps = 2.220446049250313e-16;
+        kr->restart_thr = kr->eigen_path ? eps * eps * r0n2 : 1e-32 * r0n2;
+        kr->r2 = r0n2;
+        kr->r0r = cmake(r0n2, 0.0);
+        kr->iterations = 0;
+        kr->done = !(r0n2 > kr->thr) || kr->max_iterations <= 0;
+        kr->restart = 0;
+        break;
+    }
     default: break;
     }
+}
+
+__global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
+{
+    if (threadIdx.x == 0) bicg_stage(kr, stage, red);
+}
+
+// Woodbury set-up on the device (src/CrankNicolsonModes_matrices.cpp:133-145):
+// G = diag(1 / (dt/4 g_a)) + v_a^dag W_b from vw[2 b + a] = v_a^dag W_b, and G^{-1}.
+__global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1)
+{
+    if (threadIdx.x != 0) return;
+    const int k = kr->n_sinks;
+    double2 G[2][2];
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) {
+            const double2 v = (a < k && b < k) ? vw[2 * b + a] : cmake(0.0, 0.0);
+            kr->vW[a][b] = v;
+            G[a][b] = v;
+        }
+    G[0][0].x += 1.0 / c0;
+    if (k > 1) G[1][1].x += 1.0 / c1;
+    for (int a = 0; a < 2; ++a)
+        for (int b = 0; b < 2; ++b) kr->Gi[a][b] = cmake(0.0, 0.0);
+    if (k == 1) {
+        kr->Gi[0][0] = crcp(G[0][0]);
+    } else if (k == 2) {
+        const double2 det = csub(cmul(G[0][0], G[1][1]), cmul(G[0][1], G[1][0]));
+        const double2 id = crcp(det);
+        kr->Gi[0][0] = cmul(G[1][1], id);
+        kr->Gi[0][1] = cmul(cmake(-G[0][1].x, -G[0][1].y), id);
+        kr->Gi[1][0] = cmul(cmake(-G[1][0].x, -G[1][0].y), id);
+        kr->Gi[1][1] = cmul(G[0][0], id);
+    }
+}
+
+// b = rhs / |rhs|, x = psi / |rhs| with |rhs|^2 = red[0]; a zero right-hand side is
+// flagged (kr->zero_rhs) and leaves b = x = 0.
+__global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
+                                double2 *b, double2 *x)
+{
+    const double nrm = sqrt(red[0]);
+    const double s = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        kr->rhs_norm = nrm;
+        kr->zero_rhs = nrm == 0.0;
+    }
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        b[e] = cscale(rhs[e], s);
+        x[e] = cscale(psi[e], s);
+    }
+}
+
+// Start of the solve in one pass: with s = 1/|rhs| (|rhs|^2 = red[0]),
+//   b = s rhs, x = s psi, r = r0 = b - A_full x = 2 s (rhs - psi)
+// because A_full + B_full = 2 I and rhs = B_full psi (src/CrankNicolsonModes.cpp:170-172,
+// _matrices.cpp:36-37); per-CTA partials of |r|^2 and |b|^2 for KS_INIT.
+__global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov *kr, const double *red,
+                                                               const double2 *rhs, const double2 *psi, double2 *b,
+                                                               double2 *x, double2 *r, double2 *r0, double *partials)
+{
+    __shared__ double scratch[4 * 32];
+    const double nrm = sqrt(red[0]);
+    const double sc = nrm > 0.0 ? 1.0 / nrm : 0.0;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        kr->rhs_norm = nrm;
+        kr->zero_rhs = nrm == 0.0;
+    }
+    double acc[4] = {0, 0, 0, 0};
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const double2 hv = rhs[e], pv = psi[e];
+        const double2 bv = cscale(hv, sc);
+        const double2 rv = cscale(csub(hv, pv), 2.0 * sc);
+        b[e] = bv;
+        x[e] = cscale(pv, sc);
+        r[e] = rv;
+        r0[e] = rv;
+        acc[0] += cabs2(rv);
+        acc[2] += cabs2(bv);
+    }
+    block_sum<4>(acc, scratch);
+    if (threadIdx.x == 0)
+        for (int q = 0; q < 4; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = acc[q];
+}
+
+// candidate = x |rhs|.
+__global__ void k_scale_candidate(int64_t n, const Krylov *kr, const double2 *x, double2 *cand)
+{
+    const double s = kr->rhs_norm;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
+        cand[e] = cscale(x[e], s);
 }
 
 // Woodbury projections: with proj_a = v_a^dag yP (dots), c = G^{-1} proj and the sink
@@ -1179,14 +1867,31 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics(Grid g, CouplingT
     }
 }
 
-// out[q] = sum_b partials[q][b] for q < nslots (fixed order); one thread per slot.
+// out[q] = sum_b partials[q][b]: one CTA per slot, coalesced loads, fixed-order tree.
 __global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out)
 {
-    const int q = blockIdx.x * blockDim.x + threadIdx.x;
+    __shared__ double scratch[32];
+    const int q = blockIdx.x;
     if (q >= nslots) return;
-    double s = 0.0;
-    for (int b = 0; b < nblocks; ++b) s += partials[(int64_t)q * nblocks + b];
-    out[q] = s;
+    double acc[1] = {0.0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc[0] += partials[(int64_t)q * nblocks + b];
+    block_sum<1>(acc, scratch);
+    if (threadIdx.x == 0) out[q] = acc[0];
+}
+
+// Sum the per-CTA partials of nslots values into red[0..nslots) and run one scalar stage
+// of the recurrence on them, in one launch.
+__global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage)
+{
+    __shared__ double scratch[6 * 32];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        for (int q = 0; q < nslots; ++q) acc[q] += partials[(int64_t)q * nblocks + b];
+    block_sum<6>(acc, scratch);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < nslots; ++q) red[q] = acc[q];
+        bicg_stage(kr, stage, red);
+    }
 }
 
 }  // namespace cnm

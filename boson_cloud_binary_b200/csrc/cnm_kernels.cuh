@@ -7,7 +7,8 @@ namespace cnm {
 
 constexpr int APPLY_TILE = 32;      // radial nodes per CTA in the operator kernels (= warp width)
 constexpr int APPLY_THREADS = 256;  // 8 warps share the rows of a tile
-constexpr int SCAN_THREADS = 256;   // preconditioner scan CTAs
+constexpr int SCAN_THREADS = 256;   // preconditioner scan CTAs (per-thread chunk kernels)
+constexpr int SCAN2_THREADS = 512;  // staged preconditioner scan CTAs
 constexpr int VEC_THREADS = 256;    // streaming vector kernels
 
 // Device-resident scalars of one BiCGSTAB solve (src/CrankNicolsonModes_matrices.cpp:47-91)
@@ -24,19 +25,43 @@ struct Krylov {
     double2 vW[2][2];     // v_a . W_b
     double2 wc[2][2];     // c = G^{-1} proj for the two preconditioner calls of an iteration
     double2 sdots[2][2];  // sink projections of the corrected vectors y and z
+    double tol;           // relative tolerance
+    int eigen_path;       // 1: Eigen's restart rule (no sinks), 0: the sink path's
+    int zero_rhs;
+    double rhs_norm;
 };
 
-enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3 };
+// Right-hand side of a preconditioner solve: b itself, or a BiCGSTAB combination
+// formed while staging (PI_P: p = r + beta (p_old - omega v); PI_S: s = r - alpha v),
+// which is also written to `out`.
+enum PrecondMode : int { PI_PLAIN = 0, PI_P = 1, PI_S = 2 };
+struct PrecondInput {
+    int mode;
+    const struct Krylov *kr;
+    const double2 *r, *p_old, *v;
+    double2 *out;
+};
+
+enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3, KS_INIT = 4 };
 
 __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
                            double scale, double a1, double a2);
 __global__ void k_apply(Grid g, CouplingTable ct, ApplyArgs a);
-__global__ void k_apply2(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a);
-__global__ void k_diagnostics2(Grid g, CouplingTable ct, BlockTable bt, const double *hh, double theta,
-                               double domega, const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0,
-                               const double2 *sv1, const double2 *sink_dots, double sink_coef0, double sink_coef1,
-                               int slo0, int shi0, int slo1, int shi1, double *partials, double2 *dpsi_edge,
-                               double2 *psi_edge);
+// Register-blocked operator kernels (templated on the widest Gaunt block), launched
+// through these host functions.
+cudaError_t set_operator_smem(int apply_bytes, int diag_bytes);
+// Two-nodes-per-thread operator kernel on 64-node tiles with a two-row blocked table.
+constexpr int APPLY3_TILE = 64;
+cudaError_t set_apply3_smem(int bytes);
+void launch_apply3(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
+                   const BlockTable &bt, const ApplyArgs &a);
+void launch_apply(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
+                  const BlockTable &bt, const ApplyArgs &a);
+void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
+                        const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
+                        const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
+                        const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0, int slo1,
+                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge);
 __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
                             const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots);
 __global__ void k_precond_factor(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off,
@@ -58,6 +83,16 @@ __global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2
                            const double2 *W1, double2 *y);
 __global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red);
 __global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj);
+__global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1);
+__global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
+                                double2 *b, double2 *x);
+__global__ void k_krylov_start(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
+                               double2 *b, double2 *x, double2 *r, double2 *r0, double *partials);
+__global__ void k_scale_candidate(int64_t n, const Krylov *kr, const double2 *x, double2 *cand);
+__global__ void k_precond_solve2(int Nr, int chunk, int window, double2 off, const double2 *dinv, const double2 *b,
+                                 double2 *x, PrecondInput in);
+__global__ void k_precond_factor2(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int chunk,
+                                  int window, double2 *dinv, int *status);
 __global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
                               const double *gl_x, const double *gl_w, int degree, double *mom);
 __global__ void k_abs_normalize(const double *r, int Nr, int lo, int hi, double dr, int degree, double *mom);
@@ -69,5 +104,6 @@ __global__ void k_diagnostics(Grid g, CouplingTable ct, const double *hh, double
                               const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0,
                               int slo1, int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge);
 __global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out);
+__global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage);
 
 }  // namespace cnm

@@ -175,6 +175,26 @@ int cnm_step(cnm_handle *h, int32_t step_id, cnm_diag *diag, double *energy_flux
  * on an evolving binary orbit. */
 int cnm_should_stop(const cnm_handle *h, int32_t *stop);
 
+/* --- checkpoints --------------------------------------------------------------- */
+
+/* save_checkpoint (src/CrankNicolsonModes_restart.cpp:139-177): the exact bytes of
+ * checkpoint.bin -- "GMCKPT01", int32 {step_id, Nr, n_modes}, 13 doubles {t, theta,
+ * phase, R, M1, M2, q, R1, R2, Omega, P, dt, p_bin}, uint64 size, psi as complex128,
+ * then the rolling-average state of src/RollingPhase.cpp:169-184.  Writes *size; the
+ * bytes go to buf when buf is non-NULL and capacity >= *size.  The caller writes the
+ * file (the reference replaces it atomically through a .tmp file). */
+int cnm_save_checkpoint(const cnm_handle *h, int32_t step_id, void *buf, int64_t capacity, int64_t *size);
+/* load_checkpoint (src/CrankNicolsonModes_restart.cpp:179-233): restores psi, the
+ * evolving scalars and the rolling average when buf is a complete checkpoint of
+ * step_id for this grid; *loaded = 1 then, else 0 and nothing changes. */
+int cnm_load_checkpoint(cnm_handle *h, int32_t step_id, const void *buf, int64_t size, int32_t *loaded);
+
+/* reconstruct_state_from_diagnostics (src/CrankNicolsonModes_restart.cpp:238-286): reset
+ * the rolling phase average of p_bin and feed it the n stored samples (time, phase,
+ * p_bin_inst) of the diagnostic rows. */
+int cnm_replay_power_average(cnm_handle *h, const double *times, const double *phases, const double *values,
+                             int32_t n);
+
 /* --- operators ------------------------------------------------------------------ */
 
 /* y = op x for an interleaved complex128 vector of length Nr * n_modes, with
