@@ -251,6 +251,9 @@ struct Solver {
     int gl_n = 0;
     int vec_blocks = 0;
     int precond_chunk = 2048, precond_window = 256;
+    // exact cluster scans: nodes per thread (odd) and CTAs per radial block; 0 = the
+    // windowed scans are used instead
+    int pcl_per = 0, pcl_cs = 0;
     size_t apply_smem = 0, diag_smem = 0;
     // pinned host staging
     double *h_stage = nullptr;
@@ -406,6 +409,71 @@ struct Solver {
         CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CK(cudaFuncSetAttribute(k_precond_solve2, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
         CK(cudaFuncSetAttribute(k_precond_factor2, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
+        plan_cluster_scans();
+    }
+
+    // Cluster plan of the exact preconditioner scans: the fewest nodes per thread (odd)
+    // that cover a radial block with at most 8 CTAs (16 where the device allows
+    // non-portable clusters), the solve's two staged vectors within the opt-in shared
+    // memory, and at least one such cluster resident on the device.
+    void plan_cluster_scans()
+    {
+        pcl_per = pcl_cs = 0;
+        int optin = 0, dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        for (int cs_max : {8, 16}) {
+            const int per = ((Nr + cs_max * PCL_THREADS - 1) / (cs_max * PCL_THREADS)) | 1;
+            const int cs = (Nr + PCL_THREADS * per - 1) / (PCL_THREADS * per);
+            const size_t smem = (size_t)2 * PCL_THREADS * per * sizeof(double2);
+            if (smem > (size_t)optin) continue;
+            if (cs > 8) {
+                if (cudaFuncSetAttribute(k_precond_solve_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                        cudaSuccess ||
+                    cudaFuncSetAttribute(k_precond_factor_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
+                        cudaSuccess) {
+                    cudaGetLastError();
+                    continue;
+                }
+            }
+            CK(cudaFuncSetAttribute(k_precond_solve_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+            CK(cudaFuncSetAttribute(k_precond_factor_cl, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    (int)(smem / 2)));
+            cudaLaunchConfig_t cfg = cluster_config(cs, n_modes, smem);
+            cudaLaunchAttribute at;
+            cluster_attr(at, cs);
+            cfg.attrs = &at;
+            int nclusters = 0;
+            if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_precond_solve_cl, &cfg) != cudaSuccess ||
+                nclusters < 1) {
+                cudaGetLastError();
+                continue;
+            }
+            pcl_per = per;
+            pcl_cs = cs;
+            return;
+        }
+    }
+
+    cudaLaunchConfig_t cluster_config(int cs, int blocks_y, size_t smem) const
+    {
+        cudaLaunchConfig_t cfg;
+        std::memset(&cfg, 0, sizeof(cfg));
+        cfg.gridDim = dim3((unsigned)cs, (unsigned)blocks_y, 1);
+        cfg.blockDim = dim3(PCL_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = smem;
+        cfg.stream = stream;
+        cfg.numAttrs = 1;
+        return cfg;
+    }
+
+    static void cluster_attr(cudaLaunchAttribute &at, int cs)
+    {
+        std::memset(&at, 0, sizeof(at));
+        at.id = cudaLaunchAttributeClusterDimension;
+        at.val.clusterDim.x = (unsigned)cs;
+        at.val.clusterDim.y = 1;
+        at.val.clusterDim.z = 1;
     }
 
     Grid grid() const
@@ -812,9 +880,21 @@ struct Solver {
 
     void factorize(double dtv)
     {
+        CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
+        if (pcl_per > 0) {
+            const size_t smem = (size_t)PCL_THREADS * pcl_per * sizeof(double2);
+            cudaLaunchConfig_t cfg = cluster_config(pcl_cs, n_modes, smem);
+            cudaLaunchAttribute at;
+            cluster_attr(at, pcl_cs);
+            cfg.attrs = &at;
+            kt_begin(TK_PFACTOR);
+            CK(cudaLaunchKernelEx(&cfg, k_precond_factor_cl, grid(), table(), (const double *)d_hh.p, 0.5 * dtv,
+                                  offdiag(dtv), pcl_per, dinv.p, d_status.p));
+            kt_end(TK_PFACTOR);
+            return;
+        }
         choose_window(dtv);
         const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
-        CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
         const int fwin = precond_window / 2 + 16;
         const size_t smem = (size_t)std::min(Nr, precond_chunk + fwin) * sizeof(double2);
         kt_begin(TK_PFACTOR);
@@ -830,6 +910,10 @@ struct Solver {
                                                                                              nullptr, nullptr,
                                                                                              nullptr, nullptr})
     {
+        if (pcl_per > 0) {
+            precond_cl(bv, xv, nullptr, nullptr, dtv, in);
+            return;
+        }
         const int chunks = (Nr + precond_chunk - 1) / precond_chunk;
         const size_t smem = (size_t)2 * std::min(Nr, precond_chunk + 2 * precond_window) * sizeof(double2);
         kt_begin(TK_PSOLVE);
@@ -837,6 +921,31 @@ struct Solver {
                                                                                 offdiag(dtv), dinv.p, bv, xv, in);
         launch_check();
         kt_end(TK_PSOLVE);
+    }
+
+    // Exact cluster solve; with b2/x2 set the launch solves both right-hand sides.
+    void precond_cl(const double2 *bv, double2 *xv, const double2 *b2, double2 *x2, double dtv, PrecondInput in)
+    {
+        const size_t smem = (size_t)2 * PCL_THREADS * pcl_per * sizeof(double2);
+        cudaLaunchConfig_t cfg = cluster_config(pcl_cs, b2 ? 2 * n_modes : n_modes, smem);
+        cudaLaunchAttribute at;
+        cluster_attr(at, pcl_cs);
+        cfg.attrs = &at;
+        kt_begin(TK_PSOLVE);
+        CK(cudaLaunchKernelEx(&cfg, k_precond_solve_cl, Nr, n_modes, pcl_per, offdiag(dtv), (const double2 *)dinv.p,
+                              bv, xv, b2, x2, in));
+        kt_end(TK_PSOLVE);
+    }
+
+    // x0 = P^{-1} b0 and x1 = P^{-1} b1 (one launch where the cluster scans run).
+    void precond_pair(const double2 *b0, double2 *x0, const double2 *b1, double2 *x1, double dtv)
+    {
+        if (pcl_per > 0) {
+            precond_cl(b0, x0, b1, x1, dtv, PrecondInput{PI_PLAIN, nullptr, nullptr, nullptr, nullptr, nullptr});
+        } else {
+            precond(b0, x0, dtv);
+            precond(b1, x1, dtv);
+        }
     }
 
     // -------------------------------------------------------------- reductions
@@ -894,8 +1003,8 @@ struct Solver {
         factorize(dtv);
         if (k > 0) {
             // Woodbury: W_a = P^{-1} v_a, G = diag(1 / (dt/4 g_a)) + v_a^dag W_b (_matrices.cpp:133-145)
-            precond(sk[0]->v.p, W0.p, dtv);
-            if (k > 1) precond(sk[1]->v.p, W1.p, dtv);
+            if (k > 1) precond_pair(sk[0]->v.p, W0.p, sk[1]->v.p, W1.p, dtv);
+            else precond(sk[0]->v.p, W0.p, dtv);
             sink_dots(W0.p, d_dots.p + 4, sk, k);
             if (k > 1) sink_dots(W1.p, d_dots.p + 6, sk, k);
             k_wood_setup<<<1, 32, 0, stream>>>(dk, d_dots.p + 4, 0.25 * dtv * sk[0]->strength,

@@ -4,6 +4,7 @@
 // reference's mode-major layout; see cnm_common.cuh for the data layout.
 #include "cnm_kernels.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 namespace cnm {
@@ -1367,6 +1368,315 @@ __global__ void __launch_bounds__(SCAN2_THREADS) k_precond_factor2(Grid g, Coupl
     __syncthreads();
     const int64_t base = (int64_t)j * Nr + lo;
     for (int e = (c0 - lo) + threadIdx.x; e < len; e += blockDim.x) dinv[base + e] = A[e];
+}
+
+// ------------------------------------------------------------------ exact cluster scans
+
+// One thread-block cluster per radial block (mode): the cluster's CTAs split the Nr
+// nodes into consecutive chunks of PCL_THREADS * per nodes, every thread owns `per`
+// consecutive nodes (odd, so the threads' 16-byte shared-memory accesses are
+// conflict-free).  A recurrence is solved exactly, without warm-up windows:
+//   thread:  compose the maps of its nodes,
+//   warp:    shuffle scan of the thread maps,
+//   CTA:     composition of the warp totals,
+//   cluster: every CTA reads the totals of the CTAs before it (after it, for a
+//            backward sweep) from their shared memory and folds them into its start
+//            value; then each thread replays its nodes from its exact start value.
+
+__device__ __forceinline__ Aff aff_identity() { return Aff{cmake(1.0, 0.0), cmake(0.0, 0.0)}; }
+__device__ __forceinline__ double2 aff_apply(const Aff &m, double2 y) { return cadd(cmul(m.A, y), m.B); }
+
+__device__ __forceinline__ Aff shfl_up_aff(const Aff &a, int o)
+{
+    Aff r;
+    r.A.x = __shfl_up_sync(0xffffffffu, a.A.x, o);
+    r.A.y = __shfl_up_sync(0xffffffffu, a.A.y, o);
+    r.B.x = __shfl_up_sync(0xffffffffu, a.B.x, o);
+    r.B.y = __shfl_up_sync(0xffffffffu, a.B.y, o);
+    return r;
+}
+
+__device__ __forceinline__ Aff shfl_down_aff(const Aff &a, int o)
+{
+    Aff r;
+    r.A.x = __shfl_down_sync(0xffffffffu, a.A.x, o);
+    r.A.y = __shfl_down_sync(0xffffffffu, a.A.y, o);
+    r.B.x = __shfl_down_sync(0xffffffffu, a.B.x, o);
+    r.B.y = __shfl_down_sync(0xffffffffu, a.B.y, o);
+    return r;
+}
+
+__device__ __forceinline__ Mob shfl_up_mob(const Mob &a, int o)
+{
+    Mob r;
+    r.m00 = cmake(__shfl_up_sync(0xffffffffu, a.m00.x, o), __shfl_up_sync(0xffffffffu, a.m00.y, o));
+    r.m01 = cmake(__shfl_up_sync(0xffffffffu, a.m01.x, o), __shfl_up_sync(0xffffffffu, a.m01.y, o));
+    r.m10 = cmake(__shfl_up_sync(0xffffffffu, a.m10.x, o), __shfl_up_sync(0xffffffffu, a.m10.y, o));
+    r.m11 = cmake(__shfl_up_sync(0xffffffffu, a.m11.x, o), __shfl_up_sync(0xffffffffu, a.m11.y, o));
+    return r;
+}
+
+__device__ __forceinline__ Mob mob_identity()
+{
+    Mob m;
+    m.m00 = cmake(1, 0);
+    m.m01 = cmake(0, 0);
+    m.m10 = cmake(0, 0);
+    m.m11 = cmake(1, 0);
+    return m;
+}
+
+// x = P^{-1} b for every radial block, exact (see the scan scheme above).  Grid
+// (cluster size, blocks): blockIdx.y selects the mode j = blockIdx.y % n_modes and,
+// for blockIdx.y >= n_modes, the second right-hand side / output pair (b2, x2), so
+// one launch can carry two independent solves.  PrecondInput fuses the BiCGSTAB
+// combinations as in k_precond_solve2.
+__global__ void __launch_bounds__(PCL_THREADS) k_precond_solve_cl(int Nr, int n_modes, int per, double2 off,
+                                                                   const double2 *dinv, const double2 *b, double2 *x,
+                                                                   const double2 *b2, double2 *x2, PrecondInput in)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ double2 smc[];
+    __shared__ Aff wagg[PCL_THREADS / 32];
+    __shared__ double2 win[PCL_THREADS / 32];
+    __shared__ Aff cagg_f, cagg_b;
+    const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
+    const int second = blockIdx.y >= (unsigned)n_modes;
+    const int j = blockIdx.y - (second ? n_modes : 0);
+    const double2 *bv = second ? b2 : b;
+    double2 *xv = second ? x2 : x;
+    const int T = PCL_THREADS, NW = PCL_THREADS / 32;
+    const int Lc = T * per;
+    const int c0 = rank * Lc, c1 = min(Nr, c0 + Lc), len = max(0, c1 - c0);
+    double2 *D = smc, *Y = smc + Lc;
+    const int64_t base = (int64_t)j * Nr + c0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (in.mode == PI_PLAIN) {
+        for (int e = tid; e < len; e += T) {
+            D[e] = dinv[base + e];
+            Y[e] = bv[base + e];
+        }
+    } else {
+        const double2 beta = in.kr->beta, omega = in.kr->omega, alpha = in.kr->alpha;
+        for (int e = tid; e < len; e += T) {
+            D[e] = dinv[base + e];
+            const int64_t k = base + e;
+            double2 rhsv;
+            if (in.mode == PI_P) rhsv = cadd(in.r[k], cmul(beta, csub(in.p_old[k], cmul(omega, in.v[k]))));
+            else rhsv = csub(in.r[k], cmul(alpha, in.v[k]));
+            Y[e] = rhsv;
+            in.out[k] = rhsv;
+        }
+    }
+    __syncthreads();
+    const int s0 = tid * per, s1 = min(len, s0 + per);
+
+    // ---- forward: y_i = d_i (b_i - l_i y_{i-1})
+    Aff acc = aff_identity();
+    for (int e = s0; e < s1; ++e) {
+        const int i = c0 + e;
+        const double2 d = D[e];
+        const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        const Aff m{cmake(-(l.x * d.x - l.y * d.y), -(l.x * d.y + l.y * d.x)), cmul(d, Y[e])};
+        acc = aff_then(acc, m);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Aff prev = shfl_up_aff(acc, o);
+        if (lane >= o) acc = aff_then(prev, acc);
+    }
+    Aff excl = shfl_up_aff(acc, 1);
+    if (lane == 0) excl = aff_identity();
+    if (lane == 31) wagg[warp] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        Aff c = aff_identity();
+        for (int w = 0; w < NW; ++w) c = aff_then(c, wagg[w]);
+        cagg_f = c;
+    }
+    cl.sync();
+    if (tid == 0) {
+        double2 y = cmake(0.0, 0.0);
+        for (int q = 0; q < rank; ++q) y = aff_apply(*cl.map_shared_rank(&cagg_f, q), y);
+        for (int w = 0; w < NW; ++w) {
+            win[w] = y;
+            y = aff_apply(wagg[w], y);
+        }
+    }
+    __syncthreads();
+    {
+        double2 y = aff_apply(excl, win[warp]);
+        for (int e = s0; e < s1; ++e) {
+            const int i = c0 + e;
+            const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+            y = cmul(D[e], csub(Y[e], cmul(l, y)));
+            Y[e] = y;
+        }
+    }
+
+    // ---- backward: x_i = y_i - u_i d_i x_{i+1}
+    Aff bcc = aff_identity();
+    for (int e = s1 - 1; e >= s0; --e) {
+        const int i = c0 + e;
+        const double2 d = D[e];
+        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+        const Aff m{cmake(-(u.x * d.x - u.y * d.y), -(u.x * d.y + u.y * d.x)), Y[e]};
+        bcc = aff_then(bcc, m);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Aff nxt = shfl_down_aff(bcc, o);
+        if (lane + o < 32) bcc = aff_then(nxt, bcc);
+    }
+    Aff bexcl = shfl_down_aff(bcc, 1);
+    if (lane == 31) bexcl = aff_identity();
+    __syncthreads();  // every thread has read win[] of the forward sweep
+    if (lane == 0) wagg[warp] = bcc;
+    __syncthreads();
+    if (tid == 0) {
+        Aff c = aff_identity();
+        for (int w = NW - 1; w >= 0; --w) c = aff_then(c, wagg[w]);
+        cagg_b = c;
+    }
+    cl.sync();
+    if (tid == 0) {
+        double2 xr = cmake(0.0, 0.0);
+        for (int q = cs - 1; q > rank; --q) xr = aff_apply(*cl.map_shared_rank(&cagg_b, q), xr);
+        for (int w = NW - 1; w >= 0; --w) {
+            win[w] = xr;
+            xr = aff_apply(wagg[w], xr);
+        }
+    }
+    // the other CTAs read cagg_b only before this arrive; the matching wait is the
+    // last statement, so a CTA's shared memory outlives every remote read of it
+    cl.barrier_arrive();
+    __syncthreads();
+    {
+        double2 xr = aff_apply(bexcl, win[warp]);
+        for (int e = s1 - 1; e >= s0; --e) {
+            const int i = c0 + e;
+            const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
+            xr = csub(Y[e], cmul(cmul(u, D[e]), xr));
+            Y[e] = xr;
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < len; e += T) xv[base + e] = Y[e];
+    cl.barrier_wait();
+}
+
+// Inverse Thomas pivots d_i = 1 / p_i, exact: the pivot recurrence p_i = a_i - c / p_{i-1}
+// is a chain of Moebius maps composed by the cluster scan above (2x2 complex matrices,
+// rescaled by powers of two as they grow).  Grid (cluster size, modes).
+__global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, CouplingTable ct, const double *hh,
+                                                                    double half_dt, double2 off, int per,
+                                                                    double2 *dinv, int *status)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ double2 smc[];
+    __shared__ Mob wmob[PCL_THREADS / 32];
+    __shared__ double2 pwin[PCL_THREADS / 32];
+    __shared__ Mob cmob;
+    const int rank = (int)cl.block_rank();
+    const int Nr = g.Nr, j = blockIdx.y;
+    const int T = PCL_THREADS, NW = PCL_THREADS / 32;
+    const int Lc = T * per;
+    const int c0 = rank * Lc, c1 = min(Nr, c0 + Lc), len = max(0, c1 - c0);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    double2 *A = smc;
+    // diagonal of A = 1 + i dt/2 (H0 + V + CAP), staged term by term with coalesced
+    // passes over the hh rows (as k_precond_factor2)
+    {
+        const int l = ct.mode_l[j];
+        const double alpha_d = 1.0 / (g.dr * g.dr);
+        for (int e = tid; e < len; e += T) {
+            const int i = c0 + e;
+            double hre = 0.0;
+            if (i >= 1 && i <= Nr - 2) {
+                const double ri = g.r[i];
+                hre = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+            }
+            A[e] = cmake(0.0, hre);
+        }
+        const int p = ct.diag_pair[j];
+        if (p >= 0)
+            for (int t = ct.pair_term_ptr[p]; t < ct.pair_term_ptr[p + 1]; ++t) {
+                const double gt = ct.term_g[t];
+                const double *row = hh + (int64_t)ct.term_l[t] * Nr + c0;
+                for (int e = tid; e < len; e += T) {
+                    const int i = c0 + e;
+                    if (i >= 1 && i <= Nr - 2) A[e].y += gt * row[e];
+                }
+            }
+        for (int e = tid; e < len; e += T) {
+            const double him = g.capw ? -g.capw[c0 + e] : 0.0;
+            A[e] = cmake(1.0 - half_dt * him, half_dt * A[e].y);
+        }
+    }
+    __syncthreads();
+    const int s0 = tid * per, s1 = min(len, s0 + per);
+    const double2 c = cmul(off, off);
+    Mob acc = mob_identity();
+    for (int e = s0; e < s1; ++e) {
+        acc = mob_mul(pivot_map(A[e], c0 + e, Nr, c), acc);
+        if (((e - s0) & 3) == 3) mob_normalize(acc);
+    }
+    mob_normalize(acc);
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Mob prev = shfl_up_mob(acc, o);
+        if (lane >= o) {
+            acc = mob_mul(acc, prev);
+            mob_normalize(acc);
+        }
+    }
+    const Mob excl = shfl_up_mob(acc, 1);
+    if (lane == 31) wmob[warp] = acc;
+    __syncthreads();
+    if (tid == 0) {
+        Mob m = mob_identity();
+        for (int w = 0; w < NW; ++w) {
+            m = mob_mul(wmob[w], m);
+            mob_normalize(m);
+        }
+        cmob = m;
+    }
+    cl.sync();
+    if (tid == 0) {
+        // node 0's map is constant (p_0 = a_0), so any finite start value is exact
+        double2 p = cmake(1.0, 0.0);
+        for (int q = 0; q < rank; ++q) p = mob_apply(*cl.map_shared_rank(&cmob, q), p);
+        for (int w = 0; w < NW; ++w) {
+            pwin[w] = p;
+            if (w + 1 < NW) p = mob_apply(wmob[w], p);
+        }
+    }
+    cl.barrier_arrive();
+    __syncthreads();
+    double2 p = pwin[warp];
+    if (lane > 0) p = mob_apply(excl, p);
+    int bad = 0;
+    double2 dprev = crcp(p);
+    for (int e = s0; e < s1; ++e) {
+        const int i = c0 + e;
+        const double2 a = A[e];
+        p = (i >= 2 && i <= Nr - 2) ? csub(a, cmul(c, dprev)) : a;
+        const double m = cabs2(p);
+        if (!(m > 0.0) || !isfinite(m)) {
+            bad = 1;
+            dprev = cmake(0.0, 0.0);
+        } else {
+            dprev = crcp(p);
+        }
+        A[e] = dprev;
+    }
+    if (bad) atomicOr(status, 1);
+    __syncthreads();
+    const int64_t base = (int64_t)j * Nr + c0;
+    for (int e = tid; e < len; e += T) dinv[base + e] = A[e];
+    cl.barrier_wait();
 }
 
 // ------------------------------------------------------------------ vector kernels

@@ -9,6 +9,7 @@ constexpr int APPLY_TILE = 32;      // radial nodes per CTA in the operator kern
 constexpr int APPLY_THREADS = 256;  // 8 warps share the rows of a tile
 constexpr int SCAN_THREADS = 256;   // preconditioner scan CTAs (per-thread chunk kernels)
 constexpr int SCAN2_THREADS = 512;  // staged preconditioner scan CTAs
+constexpr int PCL_THREADS = 256;    // cluster preconditioner scan CTAs
 constexpr int VEC_THREADS = 256;    // streaming vector kernels
 
 // Device-resident scalars of one BiCGSTAB solve (src/CrankNicolsonModes_matrices.cpp:47-91)
@@ -93,6 +94,10 @@ __global__ void k_precond_solve2(int Nr, int chunk, int window, double2 off, con
                                  double2 *x, PrecondInput in);
 __global__ void k_precond_factor2(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int chunk,
                                   int window, double2 *dinv, int *status);
+__global__ void k_precond_solve_cl(int Nr, int n_modes, int per, double2 off, const double2 *dinv, const double2 *b,
+                                   double2 *x, const double2 *b2, double2 *x2, PrecondInput in);
+__global__ void k_precond_factor_cl(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int per,
+                                    double2 *dinv, int *status);
 __global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
                               const double *gl_x, const double *gl_w, int degree, double *mom);
 __global__ void k_abs_normalize(const double *r, int Nr, int lo, int hi, double dr, int degree, double *mom);
