@@ -60,6 +60,18 @@ struct DevBuf {
     ~DevBuf() { release(); }
 };
 
+// Fused reductions of an operator launch: up to two inner products of its output
+// (ApplyArgs::dot_kind), optionally finished by the last CTA into `red` with a scalar
+// stage (KS_*; KS_NONE only stores the sums).
+struct DotSpec {
+    int n = 0;
+    int kind[2] = {0, 0};
+    const double2 *ext[2] = {nullptr, nullptr};
+    double scale = 1.0;
+    int stage = -1;
+    double *red = nullptr;
+};
+
 // Rolling time average over a window of orbital phase (src/RollingPhase.cpp:24-129).
 class RollingPhaseAverage {
 public:
@@ -237,7 +249,11 @@ struct Solver {
     DevBuf<double> d_r, d_hh, d_hh_aux, d_capw, d_mask, d_glx, d_glw, d_partials, d_red, d_ang00;
     DevBuf<int> d_pair_row_ptr, d_pair_col, d_pair_term_ptr, d_term_l, d_diag_pair, d_mode_l, d_mode_m, d_status;
     DevBuf<double> d_term_g;
-    BlockedCoupling bcpl, bcpl2;  // 4-row chunks (diagnostics), 2-row chunks (operator kernel)
+    BlockedCoupling bcpl;         // 4-row chunks (diagnostics)
+    CouplingPlan plan3;           // operator kernel work plan (its blocks: 1-2 row chunks in list order)
+    bool apply3_gsm = false;      // group weights staged in shared memory
+    DevBuf<int> d3_list_ptr, d3_group_goff;
+    DevBuf<double> d_ir2;
     DevBuf<int> d_chunk_l, d_chunk_nrows, d_chunk_rows, d_chunk_goff, d_l_off;
     DevBuf<double> d_block_g;
     DevBuf<int> d2_chunk_l, d2_chunk_nrows, d2_chunk_rows, d2_chunk_goff, d2_l_off;
@@ -254,6 +270,9 @@ struct Solver {
     // exact cluster scans: nodes per thread (odd) and CTAs per radial block; 0 = the
     // windowed scans are used instead
     int pcl_per = 0, pcl_cs = 0;
+    DevBuf<unsigned> d_tickets;  // completion tickets (zero between launches)
+    DevBuf<double> d_wpart;      // partials of the Woodbury projections
+    static constexpr int RED_RHS = 16, RED_RES = 20;  // red slots: |rhs|^2, final residual^2
     size_t apply_smem = 0, diag_smem = 0;
     // pinned host staging
     double *h_stage = nullptr;
@@ -376,13 +395,11 @@ struct Solver {
         upload(d_chunk_goff, bcpl.chunk_goff);
         upload(d_l_off, bcpl.l_off);
         upload(d_block_g, bcpl.g);
-        bcpl2 = block_coupling(cpl, 2);
-        upload(d2_chunk_l, bcpl2.chunk_l);
-        upload(d2_chunk_nrows, bcpl2.chunk_nrows);
-        upload(d2_chunk_rows, bcpl2.chunk_rows);
-        upload(d2_chunk_goff, bcpl2.chunk_goff);
-        upload(d2_l_off, bcpl2.l_off);
-        upload(d2_block_g, bcpl2.g);
+        {
+            std::vector<double> ir2(Nr, 0.0);
+            for (int i = 0; i < Nr; ++i) ir2[i] = r[i] > 0.0 ? 1.0 / (r[i] * r[i]) : 0.0;
+            upload(d_ir2, ir2);
+        }
         d_hh.alloc((size_t)K * Nr);
         d_hh_aux.alloc((size_t)K * Nr);
         for (DevBuf<double2> *bptr : {&psi, &rhs, &b, &x, &rr, &r0, &p, &p2, &v, &s, &t, &y, &z, &yP, &W0, &W1, &tmp,
@@ -393,52 +410,104 @@ struct Solver {
         d_kr.alloc(1);
         d_status.alloc(1);
         d_red.alloc(std::max(64, 2 * n_modes + 8));
+        d_tickets.alloc(TK_COUNT_T);
         const int diag_blocks = 2 * ((Nr + APPLY_TILE - 1) / APPLY_TILE);  // node tiles x row split
         d_partials.alloc(std::max<size_t>({(size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks,
-                                           (size_t)4 * 4 * ((Nr + 63) / 64)}));
+                                           (size_t)4 * 8 * ((Nr + 63) / 64)}));
         // the hh tile doubles as the scratch of the fused reductions (4 x 32 doubles)
         apply_smem = (size_t)n_modes * (APPLY_TILE + 2 + APPLY_TILE + 1) * sizeof(double2) +
                      (size_t)std::max(K, 4) * APPLY_TILE * sizeof(double);
         diag_smem = apply_smem + (size_t)(2 * n_modes + 3) * (APPLY_THREADS / 32) * sizeof(double);
         CK(cudaFuncSetAttribute(k_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
         CK(set_operator_smem((int)apply_smem, (int)diag_smem));
-        apply3_smem = (size_t)n_modes * (APPLY3_TILE + 1) * sizeof(double2) +
-                      (size_t)std::max(K, 4) * APPLY3_TILE * sizeof(double);
-        CK(set_apply3_smem((int)apply3_smem));
+        plan_operator(nsm);
         CK(cudaFuncSetAttribute(k_diagnostics, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
         CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CK(cudaFuncSetAttribute(k_precond_solve2, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
         CK(cudaFuncSetAttribute(k_precond_factor2, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
         plan_cluster_scans();
+        d_wpart.alloc((size_t)8 * std::max(1, pcl_cs) * 2 * n_modes);
     }
 
-    // Cluster plan of the exact preconditioner scans: the fewest nodes per thread (odd)
-    // that cover a radial block with at most 8 CTAs (16 where the device allows
-    // non-portable clusters), the solve's two staged vectors within the opt-in shared
-    // memory, and at least one such cluster resident on the device.
+    // Work plan of the operator kernel: for 1..8 CTA groups per 64-node tile, the LPT
+    // warp lists (cnm::plan_coupling) and the resident CTAs per SM give an estimated
+    // time  waves x heaviest warp list; the cheapest plan is kept.  A group's weights
+    // are staged in shared memory when they fit beside the tile.
+    void plan_operator(int nsm)
+    {
+        int optin = 0, dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa;
+        CK(cudaFuncGetAttributes(&fa, apply3_kernel(l_max, V_POT, true)));
+        const int dyn_max = optin - (int)fa.sharedSizeBytes;
+        CK(set_apply3_smem(dyn_max));
+        const size_t base = (size_t)n_modes * (APPLY3_TILE + 1) * sizeof(double2) +
+                            (size_t)std::max(K, 4) * APPLY3_TILE * sizeof(double);
+        if (base > (size_t)dyn_max) throw Error(CNM_EINVAL, "Too many modes for the operator kernel's shared tile");
+        const int tiles = (Nr + APPLY3_TILE - 1) / APPLY3_TILE;
+        double best = 0.0;
+        for (int ng = 1; ng <= 8; ++ng) {
+            CouplingPlan pl = plan_coupling(cpl, ng, APPLY_THREADS / 32);
+            const size_t with_g = base + (size_t)pl.max_group_g * sizeof(double);
+            const bool gsm = with_g <= (size_t)dyn_max;
+            const size_t smem = gsm ? with_g : base;
+            int occ = 0;
+            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, apply3_kernel(l_max, V_POT, gsm), APPLY_THREADS,
+                                                             smem));
+            if (occ < 1) continue;
+            const int waves = (tiles * ng + occ * nsm - 1) / (occ * nsm);
+            const double est = waves * pl.max_list_cost * (gsm ? 1.0 : 1.25);
+            if (plan3.list_ptr.empty() || est < best) {
+                best = est;
+                plan3 = std::move(pl);
+                apply3_gsm = gsm;
+                apply3_smem = smem;
+            }
+        }
+        if (plan3.list_ptr.empty()) throw Error(CNM_EINVAL, "No resident configuration of the operator kernel");
+        const BlockedCoupling &b = plan3.blocks;
+        upload(d2_chunk_l, b.chunk_l);
+        upload(d2_chunk_nrows, b.chunk_nrows);
+        upload(d2_chunk_rows, b.chunk_rows);
+        upload(d2_chunk_goff, b.chunk_goff);
+        upload(d2_l_off, b.l_off);
+        upload(d2_block_g, b.g);
+        upload(d3_list_ptr, plan3.list_ptr);
+        upload(d3_group_goff, plan3.group_goff);
+    }
+
+    // Cluster plan of the exact preconditioner scans.  Candidates: every odd count of
+    // nodes per thread whose cluster (CTAs per radial block) has at most 16 CTAs (more
+    // than 8 only where the device allows non-portable clusters) and whose two staged
+    // vectors fit the opt-in shared memory.  The plan minimises the estimated time
+    //   rounds x per,  rounds = ceil(blocks / clusters resident at once),
+    // so that, where possible, every radial block's cluster is resident in one round.
     void plan_cluster_scans()
     {
         pcl_per = pcl_cs = 0;
         int optin = 0, dev = 0;
         CK(cudaGetDevice(&dev));
         CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
-        for (int cs_max : {8, 16}) {
-            const int per = ((Nr + cs_max * PCL_THREADS - 1) / (cs_max * PCL_THREADS)) | 1;
+        bool nonportable = true;
+        for (const void *kern : {(const void *)k_precond_solve_cl, (const void *)k_precond_factor_cl})
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+                cudaGetLastError();
+                nonportable = false;
+            }
+        // dynamic shared memory may use what the kernels' static arrays leave of the opt-in limit
+        cudaFuncAttributes fs, ff;
+        CK(cudaFuncGetAttributes(&fs, k_precond_solve_cl));
+        CK(cudaFuncGetAttributes(&ff, k_precond_factor_cl));
+        const int dyn_max = optin - (int)std::max(fs.sharedSizeBytes, ff.sharedSizeBytes);
+        CK(cudaFuncSetAttribute(k_precond_solve_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
+        CK(cudaFuncSetAttribute(k_precond_factor_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn_max));
+        const int cs_max = nonportable ? 16 : 8;
+        double best = 0.0;
+        for (int per = ((Nr + cs_max * PCL_THREADS - 1) / (cs_max * PCL_THREADS)) | 1;; per += 2) {
             const int cs = (Nr + PCL_THREADS * per - 1) / (PCL_THREADS * per);
             const size_t smem = (size_t)2 * PCL_THREADS * per * sizeof(double2);
-            if (smem > (size_t)optin) continue;
-            if (cs > 8) {
-                if (cudaFuncSetAttribute(k_precond_solve_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-                        cudaSuccess ||
-                    cudaFuncSetAttribute(k_precond_factor_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1) !=
-                        cudaSuccess) {
-                    cudaGetLastError();
-                    continue;
-                }
-            }
-            CK(cudaFuncSetAttribute(k_precond_solve_cl, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-            CK(cudaFuncSetAttribute(k_precond_factor_cl, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    (int)(smem / 2)));
+            if (smem > (size_t)dyn_max) break;
             cudaLaunchConfig_t cfg = cluster_config(cs, n_modes, smem);
             cudaLaunchAttribute at;
             cluster_attr(at, cs);
@@ -447,11 +516,15 @@ struct Solver {
             if (cudaOccupancyMaxActiveClusters(&nclusters, (const void *)k_precond_solve_cl, &cfg) != cudaSuccess ||
                 nclusters < 1) {
                 cudaGetLastError();
-                continue;
+            } else {
+                const double est = (double)((n_modes + nclusters - 1) / nclusters) * per;
+                if (pcl_per == 0 || est < best) {
+                    best = est;
+                    pcl_per = per;
+                    pcl_cs = cs;
+                }
             }
-            pcl_per = per;
-            pcl_cs = cs;
-            return;
+            if (cs == 1) break;
         }
     }
 
@@ -485,6 +558,7 @@ struct Solver {
         g.mu = mu;
         g.r = d_r.p;
         g.capw = op.cap ? d_capw.p : nullptr;
+        g.ir2 = d_ir2.p;
         return g;
     }
 
@@ -522,7 +596,7 @@ struct Solver {
     BlockTable btable2() const
     {
         BlockTable b;
-        b.n_chunks = bcpl2.n_chunks;
+        b.n_chunks = plan3.blocks.n_chunks;
         b.chunk_l = d2_chunk_l.p;
         b.chunk_nrows = d2_chunk_nrows.p;
         b.chunk_rows = d2_chunk_rows.p;
@@ -530,6 +604,14 @@ struct Solver {
         b.l_off = d2_l_off.p;
         b.g = d2_block_g.p;
         return b;
+    }
+
+    ApplyPlan aplan() const
+    {
+        ApplyPlan p;
+        p.list_ptr = d3_list_ptr.p;
+        p.group_goff = d3_group_goff.p;
+        return p;
     }
 
     void sync() { CK(cudaStreamSynchronize(stream)); }
@@ -751,6 +833,8 @@ struct Solver {
         return k;
     }
 
+    int sink_slot(const Absorber *ab) const { return ab == &abs1 ? 0 : 1; }
+
     void sink_dots(const double2 *xv, double2 *dots, const Absorber *const *sk, int k)
     {
         k_sink_dots<<<1, 512, 0, stream>>>(xv, Nr, n_modes, k, k > 0 ? sk[0]->v.p : nullptr,
@@ -768,6 +852,8 @@ struct Solver {
         a.hh = d_hh.p;
         a.theta = op.theta;
         a.domega = op.domega;
+        a.stage = -1;
+        a.dot_scale = 1.0;
         return a;
     }
 
@@ -775,19 +861,17 @@ struct Solver {
     int apply_split() const { return bcpl.n_chunks > APPLY_THREADS / 32 ? 2 : 1; }
     dim3 apply_grid() const { return dim3((unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE), (unsigned)apply_split()); }
 
-    // Operator kernel grid: 64-node tiles x enough CTAs per tile that each warp takes about
-    // one two-row chunk.
+    // Operator kernel grid: 64-node tiles x the plan's CTA groups.
     dim3 apply3_grid() const
     {
-        const int split = std::max(1, std::min(4, (bcpl2.n_chunks + APPLY_THREADS / 32 - 1) / (APPLY_THREADS / 32)));
-        return dim3((unsigned)((Nr + APPLY3_TILE - 1) / APPLY3_TILE), (unsigned)split);
+        return dim3((unsigned)((Nr + APPLY3_TILE - 1) / APPLY3_TILE), (unsigned)plan3.n_groups);
     }
 
     void launch_apply(const ApplyArgs &a)
     {
         const dim3 blocks3 = apply3_grid();
         kt_begin(TK_APPLY);
-        ::cnm::launch_apply3(l_max, blocks3, apply3_smem, stream, grid(), table(), btable2(), a);
+        ::cnm::launch_apply3(l_max, apply3_gsm, blocks3, apply3_smem, stream, grid(), table(), btable2(), aplan(), a);
         launch_check();
         kt_end(TK_APPLY);
     }
@@ -805,16 +889,17 @@ struct Solver {
     // optionally with up to two inner products of y (ApplyArgs::dot_kind) reduced into
     // per-CTA partials.
     void apply_A(const double2 *xv, double2 *yv, const Absorber *const *sk, int k, const double2 *dots, double dtv,
-                 int ndots = 0, int kind0 = 0, const double2 *ext0 = nullptr, int kind1 = 0,
-                 const double2 *ext1 = nullptr)
+                 const DotSpec &ds = DotSpec())
     {
         ApplyArgs a = base_args(xv, yv);
-        a.n_dots = ndots;
-        a.dot_kind[0] = kind0;
-        a.dot_kind[1] = kind1;
-        a.dot_ext[0] = ext0;
-        a.dot_ext[1] = ext1;
+        a.n_dots = ds.n;
+        a.dot_kind[0] = ds.kind[0];
+        a.dot_kind[1] = ds.kind[1];
+        a.dot_ext[0] = ds.ext[0];
+        a.dot_ext[1] = ds.ext[1];
+        a.dot_scale = ds.scale;
         a.dot_partials = d_partials.p;
+        set_finish(a, ds);
         a.alpha = cmake(1.0, 0.0);
         a.beta = cmake(0.0, 0.5 * dtv);
         a.use_h0 = 1;
@@ -830,6 +915,16 @@ struct Solver {
         }
         launch_apply(a);
     }
+
+    void set_finish(ApplyArgs &a, const DotSpec &ds)
+    {
+        a.stage = ds.n > 0 ? ds.stage : -1;
+        a.kr = d_kr.p;
+        a.ticket = ticket(TK_APPLY_T);
+        a.red = ds.red ? ds.red : d_red.p;
+    }
+
+    unsigned *ticket(int which) const { return d_tickets.p + which; }
 
     // -------------------------------------------------------------- preconditioner
 
@@ -924,7 +1019,9 @@ struct Solver {
     }
 
     // Exact cluster solve; with b2/x2 set the launch solves both right-hand sides.
-    void precond_cl(const double2 *bv, double2 *xv, const double2 *b2, double2 *x2, double dtv, PrecondInput in)
+    void precond_cl(const double2 *bv, double2 *xv, const double2 *b2, double2 *x2, double dtv, PrecondInput in,
+                    WoodArgs wd = WoodArgs{WD_NONE, 0, 0, nullptr, nullptr, 0, 0, 0, 0, 0.0, 0.0, nullptr, nullptr,
+                                           nullptr})
     {
         const size_t smem = (size_t)2 * PCL_THREADS * pcl_per * sizeof(double2);
         cudaLaunchConfig_t cfg = cluster_config(pcl_cs, b2 ? 2 * n_modes : n_modes, smem);
@@ -933,19 +1030,8 @@ struct Solver {
         cfg.attrs = &at;
         kt_begin(TK_PSOLVE);
         CK(cudaLaunchKernelEx(&cfg, k_precond_solve_cl, Nr, n_modes, pcl_per, offdiag(dtv), (const double2 *)dinv.p,
-                              bv, xv, b2, x2, in));
+                              bv, xv, b2, x2, in, wd));
         kt_end(TK_PSOLVE);
-    }
-
-    // x0 = P^{-1} b0 and x1 = P^{-1} b1 (one launch where the cluster scans run).
-    void precond_pair(const double2 *b0, double2 *x0, const double2 *b1, double2 *x1, double dtv)
-    {
-        if (pcl_per > 0) {
-            precond_cl(b0, x0, b1, x1, dtv, PrecondInput{PI_PLAIN, nullptr, nullptr, nullptr, nullptr, nullptr});
-        } else {
-            precond(b0, x0, dtv);
-            precond(b1, x1, dtv);
-        }
     }
 
     // -------------------------------------------------------------- reductions
@@ -977,15 +1063,16 @@ struct Solver {
     // -------------------------------------------------------------- CN solve
 
     // src/CrankNicolsonModes_matrices.cpp:94-215 with the radial block preconditioner.
-    // Scalars live on the device (Krylov); the host synchronises once before the
-    // loop, once per iteration (convergence / restart) and once for the residual.
+    // Scalars live on the device (Krylov): every launch that produces a reduction
+    // finishes the matching scalar stage in its last CTA, so an iteration is seven
+    // launches (five without sinks) and one host synchronisation (convergence and
+    // restart test).  |rhs|^2 is left in red[RED_RHS] by the right-hand-side apply.
     void solve_CN()
     {
         const double dtv = op.dt;
         const Absorber *sk[2];
         const int k = active_sinks(sk);
         Krylov *dk = d_kr.p;
-        const double *red = d_red.p;
         Krylov kr;
         std::memset(&kr, 0, sizeof(kr));
         kr.n_sinks = k;
@@ -993,30 +1080,14 @@ struct Solver {
         kr.max_iterations = max_iterations;
         kr.eigen_path = k == 0;
         CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
-        // b = rhs / |rhs|, x = psi / |rhs|, r = r0 = b - A_full x in one pass
-        dots(1, rhs.p, rhs.p);
-        k_krylov_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, red, rhs.p, psi.p, b.p, x.p, rr.p, r0.p,
-                                                                d_partials.p);
-        launch_check();
-        k_sum_partials<<<1, 512, 0, stream>>>(d_partials.p, vec_blocks, 4, d_red.p + 8);
+        // b = rhs / |rhs|, x = psi / |rhs|, r = r0 = b - A_full x in one pass; its last
+        // CTA runs KS_INIT (and the first beta) on |r0|^2 and |b|^2
+        k_krylov_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, d_red.p + RED_RHS, rhs.p, psi.p, b.p, x.p,
+                                                                rr.p, r0.p, d_partials.p, d_red.p + 8,
+                                                                ticket(TK_START_T));
         launch_check();
         factorize(dtv);
-        if (k > 0) {
-            // Woodbury: W_a = P^{-1} v_a, G = diag(1 / (dt/4 g_a)) + v_a^dag W_b (_matrices.cpp:133-145)
-            if (k > 1) precond_pair(sk[0]->v.p, W0.p, sk[1]->v.p, W1.p, dtv);
-            else precond(sk[0]->v.p, W0.p, dtv);
-            sink_dots(W0.p, d_dots.p + 4, sk, k);
-            if (k > 1) sink_dots(W1.p, d_dots.p + 6, sk, k);
-            k_wood_setup<<<1, 32, 0, stream>>>(dk, d_dots.p + 4, 0.25 * dtv * sk[0]->strength,
-                                              k > 1 ? 0.25 * dtv * sk[1]->strength : 1.0);
-            launch_check();
-        }
-        // Krylov scalars from |r0|^2 and |b|^2 (reduced by k_krylov_start into red[8..11])
-        CK(cudaMemsetAsync(p.p, 0, nN * sizeof(double2), stream));
-        CK(cudaMemsetAsync(v.p, 0, nN * sizeof(double2), stream));
-        const double2 *p_cur = p.p;
-        k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_INIT, red + 8);
-        launch_check();
+        if (k > 0) wood_setup(sk, k, dtv);
         CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
         sync();
         if (kr.zero_rhs) {
@@ -1028,6 +1099,7 @@ struct Solver {
         const bool eigen_path = k == 0;
         const double eps = std::numeric_limits<double>::epsilon();
         int restarts = 0;
+        const double2 *p_cur = nullptr;  // no search direction yet: p = r
         while (!kr.done) {
             if (kr.restart) {
                 // Lost biorthogonality: restart from the current residual (_matrices.cpp:69-75).
@@ -1047,70 +1119,130 @@ struct Solver {
                 kr.beta = cmul(cdiv(kr.rho, rho_old), cdiv(kr.alpha, kr.omega));
                 kr.restart = 0;
                 CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
-            } else {
-                k_bicg_scalar<<<1, 32, 0, stream>>>(dk, KS_BETA, red);
-                launch_check();
             }
             // p = r + beta (p - omega v) formed inside the preconditioner pass; y = M p
             double2 *p_new = p_cur == p.p ? p2.p : p.p;
-            const PrecondInput pin{PI_P, dk, rr.p, p_cur, v.p, p_new};
+            precond_M(PrecondInput{PI_P, dk, rr.p, p_cur, v.p, p_new}, 0, sk, k, dtv, y.p);
             p_cur = p_new;
-            if (k > 0) {
-                precond(nullptr, yP.p, dtv, pin);
-                sink_dots(yP.p, d_dots.p + 4, sk, k);
-                k_wood_scalar<<<1, 32, 0, stream>>>(dk, 0, d_dots.p + 4);
-                k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, 0, yP.p, W0.p, W1.p, y.p);
-                launch_check();
-            } else {
-                precond(nullptr, y.p, dtv, pin);
-            }
             // v = A y with r0 . v reduced in the same pass; alpha = rho / r0.v
-            apply_A(y.p, v.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[0][0]), dtv, 1, 1, r0.p);
-            k_reduce_stage<<<1, 512, 0, stream>>>(d_partials.p, (int)apply_blocks(), 2, d_red.p, dk, KS_ALPHA);
-            launch_check();
-            // s = r - alpha v formed inside the preconditioner pass; z = M s
-            const PrecondInput sin{PI_S, dk, rr.p, nullptr, v.p, s.p};
-            if (k > 0) {
-                precond(nullptr, yP.p, dtv, sin);
-                sink_dots(yP.p, d_dots.p + 4, sk, k);
-                k_wood_scalar<<<1, 32, 0, stream>>>(dk, 1, d_dots.p + 4);
-                k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, 1, yP.p, W0.p, W1.p, z.p);
-                launch_check();
-            } else {
-                precond(nullptr, z.p, dtv, sin);
+            {
+                DotSpec ds;
+                ds.n = 1;
+                ds.kind[0] = 1;
+                ds.ext[0] = r0.p;
+                ds.stage = KS_ALPHA;
+                apply_A(y.p, v.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[0][0]), dtv, ds);
             }
+            // s = r - alpha v formed inside the preconditioner pass; z = M s
+            precond_M(PrecondInput{PI_S, dk, rr.p, nullptr, v.p, s.p}, 1, sk, k, dtv, z.p);
             // t = A z with t . s and |t|^2 reduced in the same pass; omega = t.s / |t|^2
-            apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv, 2, 2, s.p, 3,
-                    nullptr);
-            k_reduce_stage<<<1, 512, 0, stream>>>(d_partials.p, (int)apply_blocks(), 4, d_red.p, dk, KS_OMEGA);
-            launch_check();
-            // x += alpha y + omega z; r = s - omega t
+            {
+                DotSpec ds;
+                ds.n = 2;
+                ds.kind[0] = 2;
+                ds.ext[0] = s.p;
+                ds.kind[1] = 3;
+                ds.stage = KS_OMEGA;
+                apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv, ds);
+            }
+            // x += alpha y + omega z; r = s - omega t; then KS_UPDATE and the next beta
             k_bicg_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, y.p, z.p, rr.p, s.p, t.p, r0.p,
-                                                                   d_partials.p);
-            launch_check();
-            k_reduce_stage<<<1, 512, 0, stream>>>(d_partials.p, vec_blocks, 3, d_red.p, dk, KS_UPDATE);
+                                                                   d_partials.p, d_red.p, ticket(TK_UPDATE_T));
             launch_check();
             CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
             sync();
         }
         last_iterations = kr.iterations;
-        // candidate = x |rhs|; residual = |A_full candidate - rhs| / |rhs|
-        k_scale_candidate<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, cand.p);
-        launch_check();
-        sink_dots(cand.p, d_dots.p, sk, k);
-        apply_A(cand.p, tmp.p, sk, k, d_dots.p, dtv);
-        axpby(cmake(1, 0), tmp.p, cmake(-1, 0), rhs.p, tmp.p);
-        dots(1, tmp.p, tmp.p);
-        int status = 0;
-        CK(cudaMemcpyAsync(&status, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        const double res2 = read_red(0);
+        // candidate = |rhs| x; residual |A candidate - rhs| / |rhs| = | |rhs| (A x) - rhs | / |rhs|
         const double rhs_norm = kr.rhs_norm;
+        sink_dots(x.p, d_dots.p, sk, k);
+        {
+            DotSpec ds;
+            ds.n = 1;
+            ds.kind[0] = 4;
+            ds.ext[0] = rhs.p;
+            ds.scale = rhs_norm;
+            ds.stage = KS_NONE;
+            ds.red = d_red.p + RED_RES;
+            apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv, ds);
+        }
+        double *hres = stage(2);
+        CK(cudaMemcpyAsync(hres, d_red.p + RED_RES, sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hres + 1, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
+        sync();
+        const double res2 = hres[0];
+        int status = 0;
+        std::memcpy(&status, hres + 1, sizeof(int));
         last_residual = std::isfinite(res2) ? std::sqrt(res2) / rhs_norm : std::numeric_limits<double>::infinity();
         if (status != 0)
             throw Error(CNM_ESOLVE, "Radial preconditioner factorization failed (zero or non-finite pivot)");
         if (!(last_residual <= accept_residual))
             throw Error(CNM_ESOLVE, "Crank-Nicolson solve failed the relative residual check");
-        k_scale_mask<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, Nr, 1.0, mask ? d_mask.p : nullptr, cand.p, psi.p);
+        // psi = mask (|rhs| x)
+        k_scale_mask<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, Nr, rhs_norm, mask ? d_mask.p : nullptr, x.p,
+                                                              psi.p);
+        launch_check();
+    }
+
+    // Woodbury set-up (src/CrankNicolsonModes_matrices.cpp:133-145): W_a = P^{-1} v_a and
+    // G = diag(1 / (dt/4 g_a)) + v_a^dag W_b with its inverse, into the Krylov struct.
+    void wood_setup(const Absorber *const *sk, int k, double dtv)
+    {
+        const double c0 = 0.25 * dtv * sk[0]->strength, c1 = k > 1 ? 0.25 * dtv * sk[1]->strength : 1.0;
+        if (pcl_per > 0) {
+            WoodArgs wd = wood_args(WD_SETUP, 0, sk, k);
+            wd.c0 = c0;
+            wd.c1 = c1;
+            const PrecondInput plain{PI_PLAIN, nullptr, nullptr, nullptr, nullptr, nullptr};
+            if (k > 1) precond_cl(sk[0]->v.p, W0.p, sk[1]->v.p, W1.p, dtv, plain, wd);
+            else precond_cl(sk[0]->v.p, W0.p, nullptr, nullptr, dtv, plain, wd);
+            return;
+        }
+        precond(sk[0]->v.p, W0.p, dtv);
+        if (k > 1) precond(sk[1]->v.p, W1.p, dtv);
+        sink_dots(W0.p, d_dots.p + 4, sk, k);
+        if (k > 1) sink_dots(W1.p, d_dots.p + 6, sk, k);
+        k_wood_setup<<<1, 32, 0, stream>>>(d_kr.p, d_dots.p + 4, c0, c1);
+        launch_check();
+    }
+
+    WoodArgs wood_args(int mode, int which, const Absorber *const *sk, int k)
+    {
+        WoodArgs wd;
+        std::memset(&wd, 0, sizeof(wd));
+        wd.mode = k > 0 ? mode : WD_NONE;
+        wd.which = which;
+        wd.n_sinks = k;
+        wd.v0 = k > 0 ? sk[0]->v.p : nullptr;
+        wd.v1 = k > 1 ? sk[1]->v.p : nullptr;
+        wd.lo0 = k > 0 ? sk[0]->lo : 0;
+        wd.hi0 = k > 0 ? sk[0]->hi : 0;
+        wd.lo1 = k > 1 ? sk[1]->lo : 0;
+        wd.hi1 = k > 1 ? sk[1]->hi : 0;
+        wd.partials = d_wpart.p;
+        wd.ticket = ticket(TK_WOOD_T);
+        wd.kr = d_kr.p;
+        return wd;
+    }
+
+    // out = M b (src/CrankNicolsonModes_matrices.cpp:146-153): out = P^{-1} b without sinks;
+    // with sinks yP = P^{-1} b, c = G^{-1} v^dag yP (in the solve's last CTA) and
+    // out = yP - W c.  `in` forms b inside the solve (PI_P / PI_S).
+    void precond_M(const PrecondInput &in, int which, const Absorber *const *sk, int k, double dtv, double2 *out)
+    {
+        if (k == 0) {
+            precond(nullptr, out, dtv, in);
+            return;
+        }
+        if (pcl_per > 0) {
+            precond_cl(nullptr, yP.p, nullptr, nullptr, dtv, in, wood_args(WD_PROJ, which, sk, k));
+        } else {
+            precond(nullptr, yP.p, dtv, in);
+            sink_dots(yP.p, d_dots.p + 4, sk, k);
+            k_wood_scalar<<<1, 32, 0, stream>>>(d_kr.p, which, d_dots.p + 4);
+            launch_check();
+        }
+        k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_kr.p, which, yP.p, W0.p, W1.p, out);
         launch_check();
     }
 
@@ -1144,20 +1276,30 @@ struct Solver {
         // projections of the old state on the new sinks (for the midpoint accretion rate)
         const Absorber *all[2] = {&abs1, &abs2};
         const bool have_sinks = absorption && cpl.mode00 >= 0;
+        // v_a^dag psi on both sinks (d_dots[2..3]); the active sinks are a contiguous
+        // subsequence of (abs1, abs2), so their projections are read in place
         if (have_sinks) sink_dots(psi.p, d_dots.p + 2, all, 2);
-        // rhs = B psi - dt/4 Gamma psi
+        // rhs = B psi - dt/4 Gamma psi, with |rhs|^2 into red[RED_RHS]
         const Absorber *sk[2];
         const int k = active_sinks(sk);
-        sink_dots(psi.p, d_dots.p, sk, k);
         {
             ApplyArgs a = base_args(psi.p, rhs.p);
+            DotSpec ds;
+            ds.n = 1;
+            ds.kind[0] = 3;
+            ds.stage = KS_NONE;
+            ds.red = d_red.p + RED_RHS;
+            a.n_dots = 1;
+            a.dot_kind[0] = 3;
+            a.dot_partials = d_partials.p;
+            set_finish(a, ds);
             a.alpha = cmake(1.0, 0.0);
             a.beta = cmake(0.0, -0.5 * op.dt);
             a.use_h0 = 1;
             a.use_cap = 1;
             a.vpart = V_POT;
             a.n_sinks = k;
-            a.sink_dots = d_dots.p;
+            a.sink_dots = k > 0 ? d_dots.p + 2 + sink_slot(sk[0]) : d_dots.p;
             for (int i = 0; i < k; ++i) {
                 a.sink_v[i] = sk[i]->v.p;
                 a.sink_coef[i] = -0.25 * op.dt * sk[i]->strength;
@@ -1168,14 +1310,14 @@ struct Solver {
         }
         solve_CN();
         // diagnostics on the masked end-of-step state with the step's operators
-        sink_dots(psi.p, d_dots.p, sk, k);
         if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2);
         const dim3 dgrid = apply_grid();
         const unsigned dblocks = dgrid.x * dgrid.y;
         kt_begin(TK_DIAG);
         ::cnm::launch_diagnostics(
             l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p, idx_ex, k, k > 0 ? sk[0]->v.p : nullptr,
-            k > 1 ? sk[1]->v.p : nullptr, d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
+            k > 1 ? sk[1]->v.p : nullptr, k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p,
+            k > 0 ? -0.5 * sk[0]->strength : 0.0,
             k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
             k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes);
         launch_check();

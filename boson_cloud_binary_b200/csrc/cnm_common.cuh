@@ -90,6 +90,15 @@ struct Grid {
     double mu;
     const double *r;     // [Nr]
     const double *capw;  // [Nr] or null: CAP = -i capw(r) (all modes)
+    const double *ir2;   // [Nr] 1 / r^2 (0 at r = 0)
+};
+
+// Work plan of the operator kernel (host side: cnm::CouplingPlan): warp list b of
+// the CTA group y = b / warps is the chunk range [list_ptr[b], list_ptr[b + 1]); the
+// group's Gaunt weights are g[group_goff[y] .. group_goff[y + 1]).
+struct ApplyPlan {
+    const int *list_ptr;
+    const int *group_goff;
 };
 
 // Components of a generic operator application
@@ -115,10 +124,18 @@ struct ApplyArgs {
     int sink_lo[2], sink_hi[2]; // node support [lo, hi) of each v_a
     // fused inner products of the output y with itself or another vector, as per-CTA
     // partials [slot][block]: kind 1 conj(ext) . y, 2 conj(y) . ext, 3 |y|^2 (real)
+    // (kind 4: |dot_scale y - ext|^2, real)
     int n_dots;
     int dot_kind[2];
     const double2 *dot_ext[2];
     double *dot_partials;
+    double dot_scale;
+    // completion (stage >= 0): the CTA that finishes last sums the partials into red
+    // and runs that scalar stage of the Krylov recurrence (see finish_stage)
+    int stage;
+    struct Krylov *kr;
+    unsigned *ticket;
+    double *red;
 };
 
 }  // namespace cnm

@@ -218,4 +218,82 @@ BlockedCoupling block_coupling(const Coupling &c, int rb)
     return b;
 }
 
+CouplingPlan plan_coupling(const Coupling &c, int n_groups, int warps)
+{
+    CouplingPlan pl;
+    pl.n_groups = n_groups;
+    pl.warps = warps;
+    BlockedCoupling &b = pl.blocks;
+    b.rb = 2;
+    const int L = c.l_max;
+    b.l_off.assign(L + 2, 0);
+    for (int j = 0; j < c.n_modes; ++j) b.l_off[c.mode_l[j] + 1] = j + 1;
+    for (int l = 1; l <= L + 1; ++l) b.l_off[l] = std::max(b.l_off[l], b.l_off[l - 1]);
+    std::vector<std::vector<double>> dense(c.n_modes * (size_t)c.n_modes);
+    for (int j = 0; j < c.n_modes; ++j)
+        for (int p = c.pair_row_ptr[j]; p < c.pair_row_ptr[j + 1]; ++p) {
+            std::vector<double> &v = dense[(size_t)j * c.n_modes + c.pair_col[p]];
+            v.assign(2 * L + 1, 0.0);
+            for (int t = c.pair_term_ptr[p]; t < c.pair_term_ptr[p + 1]; ++t) v[c.term_l[t]] = c.term_g[t];
+        }
+    std::vector<double> row_cost(L + 1, 0.0);
+    for (int l = 0; l <= L; ++l)
+        for (int l1 = 0; l1 <= L; ++l1) row_cost[l] += (l1 + 1) * (std::min(l, l1) + 3);
+    for (int l = 0; l <= L; ++l) pl.total_cost += (b.l_off[l + 1] - b.l_off[l]) * row_cost[l];
+    const int n_lists = n_groups * warps;
+    const double target = pl.total_cost / n_lists;
+    struct Ch { int l, first, count; double cost; };
+    std::vector<Ch> chunks;
+    for (int l = 0; l <= L; ++l) {
+        const int first = b.l_off[l], count = b.l_off[l + 1] - b.l_off[l];
+        const int size = 2 * row_cost[l] <= target ? 2 : 1;
+        for (int r0 = 0; r0 < count; r0 += size) {
+            const int sz = std::min(size, count - r0);
+            chunks.push_back({l, first + r0, sz, sz * row_cost[l]});
+        }
+    }
+    std::stable_sort(chunks.begin(), chunks.end(), [](const Ch &a, const Ch &b2) { return a.cost > b2.cost; });
+    std::vector<double> load(n_lists, 0.0);
+    std::vector<std::vector<int>> lists(n_lists);
+    for (int ci = 0; ci < (int)chunks.size(); ++ci) {
+        int best = 0;
+        for (int q = 1; q < n_lists; ++q)
+            if (load[q] < load[best]) best = q;
+        load[best] += chunks[ci].cost;
+        lists[best].push_back(ci);
+    }
+    pl.max_list_cost = *std::max_element(load.begin(), load.end());
+    pl.list_ptr.assign(1, 0);
+    pl.group_goff.assign(1, 0);
+    for (int q = 0; q < n_lists; ++q) {
+        for (int ci : lists[q]) {
+            const Ch &ch = chunks[ci];
+            b.chunk_l.push_back(ch.l);
+            b.chunk_nrows.push_back(ch.count);
+            for (int rr = 0; rr < 2; ++rr) b.chunk_rows.push_back(rr < ch.count ? ch.first + rr : -1);
+            for (int l1 = 0; l1 <= L; ++l1) {
+                b.chunk_goff.push_back((int)b.g.size());
+                const int L0 = std::abs(ch.l - l1), S = std::min(ch.l, l1) + 1;
+                const int stride = (S + 1) & ~1;
+                for (int k = b.l_off[l1]; k < b.l_off[l1 + 1]; ++k)
+                    for (int rr = 0; rr < ch.count; ++rr)
+                        for (int s2 = 0; s2 < stride; ++s2) {
+                            double gv = 0.0;
+                            const std::vector<double> &v = dense[(size_t)(ch.first + rr) * c.n_modes + k];
+                            if (s2 < S && !v.empty()) gv = v[L0 + 2 * s2];
+                            b.g.push_back(gv);
+                        }
+            }
+        }
+        pl.list_ptr.push_back((int)b.chunk_l.size());
+        if ((q + 1) % warps == 0) {
+            pl.group_goff.push_back((int)b.g.size());
+            const int gsz = pl.group_goff.back() - pl.group_goff[pl.group_goff.size() - 2];
+            pl.max_group_g = std::max(pl.max_group_g, gsz);
+        }
+    }
+    b.n_chunks = (int)b.chunk_l.size();
+    return pl;
+}
+
 }  // namespace cnm

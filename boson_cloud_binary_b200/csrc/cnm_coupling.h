@@ -48,4 +48,24 @@ struct BlockedCoupling {
 
 BlockedCoupling block_coupling(const Coupling &c, int rb);
 
+// Work plan of the operator kernel: the rows are cut into chunks of one or two rows
+// of one degree l (two only where the pair costs at most the mean warp load), and
+// the chunks are dealt to n_groups x warps warp lists, longest first, each to the
+// least loaded list.  CTA (tile, group) runs the `warps` lists of its group, one per
+// warp.  Chunks are stored list by list, so list b is the chunk range
+// [list_ptr[b], list_ptr[b + 1]) and the Gaunt weights of group y are the contiguous
+// range [group_goff[y], group_goff[y + 1]) of g, which the kernel stages in shared
+// memory where it fits.  Costs follow the kernel's inner loops: a row of degree l
+// costs sum_l1 (l1 + 1) (min(l, l1) + 3).
+struct CouplingPlan {
+    BlockedCoupling blocks;     // rb = 2, chunks in list order
+    int n_groups = 1, warps = 8;
+    std::vector<int> list_ptr;  // [n_groups * warps + 1]
+    std::vector<int> group_goff;  // [n_groups + 1]
+    double max_list_cost = 0, total_cost = 0;
+    int max_group_g = 0;        // doubles of the largest group's weights
+};
+
+CouplingPlan plan_coupling(const Coupling &c, int n_groups, int warps);
+
 }  // namespace cnm

@@ -42,6 +42,41 @@ __device__ void block_sum(double (&v)[NV], double *scratch /* NV * 32 */)
 
 // ------------------------------------------------------------------ radial weights
 
+__device__ void bicg_stage(Krylov *kr, int stage, const double *red);
+__device__ void wood_setup_dev(Krylov *kr, const double2 *vw, double c0, double c1);
+__device__ void wood_scalar_dev(Krylov *kr, int which, const double2 *proj);
+
+// Completion of a launch whose CTAs each left `nslots` partial sums in
+// partials[slot * nblocks + block]: every CTA calls this after its partial store; the
+// CTA that takes the last ticket (after a device-scope fence) sums the partials in a
+// fixed order, independent of which CTA finishes last, stores red[0..nslots) and runs
+// the scalar stage; after KS_INIT and KS_UPDATE it also forms the next beta unless
+// the solve is done or must restart.  The ticket is re-armed for the next launch.
+// `scratch` is 6 * 32 doubles of shared memory; blockDim.x must be a multiple of 32.
+__device__ void finish_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage,
+                             unsigned *ticket, double *scratch)
+{
+    __shared__ unsigned s_last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == (unsigned)nblocks - 1u ? 1u : 0u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+        for (int q = 0; q < nslots && q < 6; ++q) acc[q] += __ldcg(partials + (int64_t)q * nblocks + b);
+    block_sum<6>(acc, scratch);
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < nslots && q < 6; ++q) red[q] = acc[q];
+        if (kr && stage != KS_NONE) {
+            bicg_stage(kr, stage, red);
+            if ((stage == KS_INIT || stage == KS_UPDATE) && !kr->done && !kr->restart) bicg_stage(kr, KS_BETA, red);
+        }
+        *ticket = 0u;
+    }
+}
+
 // hh[l][i] = scale * (a1 F1_l(r_i) + a2 (-1)^l F2_l(r_i)) on interior nodes, zero on the
 // two boundary nodes (the reference fills radial_f1/f2 for i = 1..Nr-2 only,
 // src/CrankNicolsonModes_hamiltonian.cpp:178-185).
@@ -571,7 +606,7 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics2(Grid g, Coupling
 // is read through L1 where the stencil and the output need it.
 constexpr int TILE3 = 64;
 
-template <int S_EFF, int RB, bool DVDT>
+template <int S_EFF, int RB, bool DVDT, bool GSM>
 __device__ __forceinline__ void coupling_block3(const double *__restrict__ g, int stride, int ncols, int col0,
                                                 const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
                                                 double2 (&acc)[RB][2], double2 (&accm)[RB][2])
@@ -593,14 +628,15 @@ __device__ __forceinline__ void coupling_block3(const double *__restrict__ g, in
             double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
 #pragma unroll
             for (int s2 = 0; s2 + 1 < S_EFF; s2 += 2) {
-                const double2 gg = __ldg(reinterpret_cast<const double2 *>(gr + s2));
+                const double2 gg = GSM ? *reinterpret_cast<const double2 *>(gr + s2)
+                                       : __ldg(reinterpret_cast<const double2 *>(gr + s2));
                 a0 = fma(gg.x, h0[s2], a0);
                 a1 = fma(gg.y, h0[s2 + 1], a1);
                 b0 = fma(gg.x, h1[s2], b0);
                 b1 = fma(gg.y, h1[s2 + 1], b1);
             }
             if (S_EFF & 1) {
-                const double gl = __ldg(gr + S_EFF - 1);
+                const double gl = GSM ? gr[S_EFF - 1] : __ldg(gr + S_EFF - 1);
                 a0 = fma(gl, h0[S_EFF - 1], a0);
                 b0 = fma(gl, h1[S_EFF - 1], b0);
             }
@@ -620,10 +656,10 @@ __device__ __forceinline__ void coupling_block3(const double *__restrict__ g, in
     }
 }
 
-template <int SMAX, int RB, bool DVDT>
-__device__ __forceinline__ void coupling_chunk3(const BlockTable &bt, int l_max, int ci, int lcut, const double2 *zs,
-                                                const double *hs, const int *mode_m, int lane, double2 (&acc)[RB][2],
-                                                double2 (&accm)[RB][2])
+template <int SMAX, int RB, bool DVDT, bool GSM>
+__device__ __forceinline__ void coupling_chunk3(const BlockTable &bt, const double *gbase, int goff0, int l_max, int ci,
+                                                int lcut, const double2 *zs, const double *hs, const int *mode_m,
+                                                int lane, double2 (&acc)[RB][2], double2 (&accm)[RB][2])
 {
 #pragma unroll
     for (int rr = 0; rr < RB; ++rr) acc[rr][0] = acc[rr][1] = accm[rr][0] = accm[rr][1] = cmake(0.0, 0.0);
@@ -633,14 +669,14 @@ __device__ __forceinline__ void coupling_chunk3(const BlockTable &bt, int l_max,
         const int L0 = abs(l - l1), S = min(l, l1) + 1;
         if (lcut < L0) continue;
         const int s_eff = min(S, (lcut - L0) / 2 + 1);
-        const double *g = bt.g + bt.chunk_goff[ci * (l_max + 1) + l1];
+        const double *g = gbase + (bt.chunk_goff[ci * (l_max + 1) + l1] - goff0);
         const int stride = (S + 1) & ~1, col0 = bt.l_off[l1];
         const double *hs_l0 = hs + L0 * TILE3;
 #define CNM_CASE3(S2)                                                                                            \
     case S2:                                                                                                     \
         if (S2 <= SMAX)                                                                                          \
-            coupling_block3<(S2 <= SMAX ? S2 : 1), RB, DVDT>(g, stride, l1 + 1, col0, zs, hs_l0, mode_m, lane, \
-                                                             acc, accm);                                        \
+            coupling_block3<(S2 <= SMAX ? S2 : 1), RB, DVDT, GSM>(g, stride, l1 + 1, col0, zs, hs_l0, mode_m,   \
+                                                                  lane, acc, accm);                              \
         break;
         switch (s_eff) {
             CNM_CASE3(1) CNM_CASE3(2) CNM_CASE3(3) CNM_CASE3(4) CNM_CASE3(5) CNM_CASE3(6) CNM_CASE3(7)
@@ -653,15 +689,18 @@ __device__ __forceinline__ void coupling_chunk3(const BlockTable &bt, int l_max,
     }
 }
 
-template <int SMAX, int RB, int VP>
+template <int SMAX, int RB, int VP, bool GSM>
 __device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
-                                             const ApplyArgs &a, const double2 *zs, const double2 *ph,
-                                             const double *hs, int lane, int i0, int lcut, int ci, double (&dacc)[4])
+                                             const double *gbase, int goff0, const ApplyArgs &a, const double2 *zs,
+                                             const double2 *ph, const double *hs, int lane, int i0, int lcut, int ci,
+                                             double (&dacc)[4])
 {
     double2 acc[RB][2], accm[RB][2];
-    if (VP != V_NONE) coupling_chunk3<SMAX, RB, VP == V_DVDT>(bt, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
+    if (VP != V_NONE)
+        coupling_chunk3<SMAX, RB, VP == V_DVDT, GSM>(bt, gbase, goff0, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane,
+                                                     acc, accm);
     const int Nr = g.Nr;
-    const double alpha_d = 1.0 / (g.dr * g.dr);
+    const double alpha_d = 1.0 / (g.dr * g.dr), inv2mu = 1.0 / (2 * g.mu);
 #pragma unroll
     for (int rr = 0; rr < RB; ++rr) {
         const int j = bt.chunk_rows[ci * 2 + rr];
@@ -675,9 +714,8 @@ __device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable 
             double2 h = cmake(0.0, 0.0);
             if (a.use_h0 && interior) {
                 const int l = ct.mode_l[j];
-                const double ri = g.r[i];
-                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
-                const double off = -alpha_d / (2 * g.mu);
+                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) * g.ir2[i]) * inv2mu;
+                const double off = -alpha_d * inv2mu;
                 h = cadd(cscale(xv, diag), cscale(cadd(xr[i - 1], xr[i + 1]), off));
             }
             if (VP != V_NONE && interior) {
@@ -701,6 +739,8 @@ __device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable 
                 double2 d;
                 if (a.dot_kind[q] == 1) d = cconjmul(a.dot_ext[q][(int64_t)j * Nr + i], y);
                 else if (a.dot_kind[q] == 2) d = cconjmul(y, a.dot_ext[q][(int64_t)j * Nr + i]);
+                else if (a.dot_kind[q] == 4)
+                    d = cmake(cabs2(csub(cscale(y, a.dot_scale), a.dot_ext[q][(int64_t)j * Nr + i])), 0.0);
                 else d = cmake(cabs2(y), 0.0);
                 dacc[2 * q] += d.x;
                 dacc[2 * q + 1] += d.y;
@@ -709,8 +749,11 @@ __device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable 
     }
 }
 
-template <int SMAX, int VP>
-__global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a)
+// CTA (tile, group): the group's warp lists (ApplyPlan), one per warp; the group's
+// Gaunt weights are staged in shared memory when GSM is set.
+template <int SMAX, int VP, bool GSM>
+__global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTable ct, BlockTable bt, ApplyPlan pl,
+                                                             ApplyArgs a)
 {
     extern __shared__ double2 smem3[];
     __shared__ int s_lcut;
@@ -720,8 +763,17 @@ __global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTab
     double2 *zs = smem3;                              // n * TILE3
     double2 *ph = zs + n * TILE3;                     // n
     double *hs = reinterpret_cast<double *>(ph + n);  // max(K, 4) * TILE3
+    double *gs = hs + max(K, 4) * TILE3;              // group weights (GSM)
     constexpr bool vp = VP != V_NONE;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int grp = blockIdx.y;
+    const int goff0 = pl.group_goff[grp];
+    if (GSM && vp) {
+        const int ng2 = (pl.group_goff[grp + 1] - goff0) >> 1;
+        const double2 *src = reinterpret_cast<const double2 *>(bt.g + goff0);
+        for (int e = threadIdx.x; e < ng2; e += blockDim.x) reinterpret_cast<double2 *>(gs)[e] = src[e];
+    }
+    const double *gbase = GSM ? gs : bt.g + goff0;
     for (int k = threadIdx.x; k < n; k += blockDim.x) {
         double sn, cs;
         sincos((double)ct.mode_m[k] * a.theta, &sn, &cs);
@@ -764,9 +816,12 @@ __global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTab
     __syncthreads();
     const int lcut = vp ? s_lcut : -1;
     double dacc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int ci = blockIdx.y + gridDim.y * warp; ci < bt.n_chunks; ci += gridDim.y * nw) {
-        if (bt.chunk_nrows[ci] == 1) apply_chunk3<SMAX, 1, VP>(g, ct, bt, a, zs, ph, hs, lane, i0, lcut, ci, dacc);
-        else apply_chunk3<SMAX, 2, VP>(g, ct, bt, a, zs, ph, hs, lane, i0, lcut, ci, dacc);
+    const int list = grp * nw + warp;
+    for (int ci = pl.list_ptr[list]; ci < pl.list_ptr[list + 1]; ++ci) {
+        if (bt.chunk_nrows[ci] == 1)
+            apply_chunk3<SMAX, 1, VP, GSM>(g, ct, bt, gbase, goff0, a, zs, ph, hs, lane, i0, lcut, ci, dacc);
+        else
+            apply_chunk3<SMAX, 2, VP, GSM>(g, ct, bt, gbase, goff0, a, zs, ph, hs, lane, i0, lcut, ci, dacc);
     }
     if (a.n_dots > 0) {
         __syncthreads();
@@ -782,6 +837,11 @@ __global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTab
             double sm = 0.0;
             for (int w = 0; w < nw; ++w) sm += red[threadIdx.x * 32 + w];
             a.dot_partials[(int64_t)threadIdx.x * nblocks + blk] = sm;
+        }
+        if (a.stage >= 0) {
+            __syncthreads();
+            finish_stage(a.dot_partials, nblocks, 2 * a.n_dots, a.red, a.kr, a.stage, a.ticket,
+                         reinterpret_cast<double *>(smem3));
         }
     }
 }
@@ -812,28 +872,54 @@ cudaError_t set_operator_smem(int apply_bytes, int diag_bytes)
 cudaError_t set_apply3_smem(int bytes)
 {
     cudaError_t e = cudaSuccess;
-#define CNM_ATTR3(S)                                                                                           \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply3<S, V_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes); \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply3<S, V_POT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);  \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply3<S, V_DVDT>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+#define CNM_ATTR3V(S, V, G) \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply3<S, V, G>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+#define CNM_ATTR3(S) \
+    CNM_ATTR3V(S, V_NONE, false) CNM_ATTR3V(S, V_POT, false) CNM_ATTR3V(S, V_DVDT, false) \
+    CNM_ATTR3V(S, V_NONE, true) CNM_ATTR3V(S, V_POT, true) CNM_ATTR3V(S, V_DVDT, true)
     CNM_FOR_SMAX(CNM_ATTR3)
 #undef CNM_ATTR3
+#undef CNM_ATTR3V
     return e;
 }
 
-void launch_apply3(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
-                   const BlockTable &bt, const ApplyArgs &a)
+const void *apply3_kernel(int l_max, int vpart, bool gsm)
 {
     const int smax = smax_for(l_max);
-#define CNM_LAUNCH3(S)                                                                                     \
-    if (smax == S) {                                                                                       \
-        if (a.vpart == V_POT) k_apply3<S, V_POT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);       \
-        else if (a.vpart == V_DVDT) k_apply3<S, V_DVDT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);\
-        else k_apply3<S, V_NONE><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);                       \
-        return;                                                                                            \
+#define CNM_PICK3(S)                                                                            \
+    if (smax == S) {                                                                            \
+        if (gsm) return vpart == V_POT ? (const void *)k_apply3<S, V_POT, true>                 \
+                      : vpart == V_DVDT ? (const void *)k_apply3<S, V_DVDT, true>               \
+                                         : (const void *)k_apply3<S, V_NONE, true>;             \
+        return vpart == V_POT ? (const void *)k_apply3<S, V_POT, false>                          \
+             : vpart == V_DVDT ? (const void *)k_apply3<S, V_DVDT, false>                        \
+                                : (const void *)k_apply3<S, V_NONE, false>;                      \
+    }
+    CNM_FOR_SMAX(CNM_PICK3)
+#undef CNM_PICK3
+    return nullptr;
+}
+
+void launch_apply3(int l_max, bool gsm, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
+                   const CouplingTable &ct, const BlockTable &bt, const ApplyPlan &pl, const ApplyArgs &a)
+{
+    const int smax = smax_for(l_max);
+#define CNM_LAUNCH3G(S, G)                                                                                      \
+    if (a.vpart == V_POT) k_apply3<S, V_POT, G><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, pl, a);        \
+    else if (a.vpart == V_DVDT) k_apply3<S, V_DVDT, G><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, pl, a); \
+    else k_apply3<S, V_NONE, G><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, pl, a);
+#define CNM_LAUNCH3(S)              \
+    if (smax == S) {                \
+        if (gsm) {                  \
+            CNM_LAUNCH3G(S, true)   \
+        } else {                    \
+            CNM_LAUNCH3G(S, false)  \
+        }                           \
+        return;                     \
     }
     CNM_FOR_SMAX(CNM_LAUNCH3)
 #undef CNM_LAUNCH3
+#undef CNM_LAUNCH3G
 }
 
 void launch_apply(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
@@ -1208,7 +1294,8 @@ __global__ void __launch_bounds__(SCAN2_THREADS) k_precond_solve2(int Nr, int ch
             D[e] = dinv[base + e];
             const int64_t k = base + e;
             double2 rhsv;
-            if (in.mode == PI_P) rhsv = cadd(in.r[k], cmul(beta, csub(in.p_old[k], cmul(omega, in.v[k]))));
+            if (in.mode == PI_P)
+                rhsv = in.p_old ? cadd(in.r[k], cmul(beta, csub(in.p_old[k], cmul(omega, in.v[k])))) : in.r[k];
             else rhsv = csub(in.r[k], cmul(alpha, in.v[k]));
             Y[e] = rhsv;
             const int i = lo + e;
@@ -1431,9 +1518,10 @@ __device__ __forceinline__ Mob mob_identity()
 // for blockIdx.y >= n_modes, the second right-hand side / output pair (b2, x2), so
 // one launch can carry two independent solves.  PrecondInput fuses the BiCGSTAB
 // combinations as in k_precond_solve2.
-__global__ void __launch_bounds__(PCL_THREADS) k_precond_solve_cl(int Nr, int n_modes, int per, double2 off,
+__global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int n_modes, int per, double2 off,
                                                                    const double2 *dinv, const double2 *b, double2 *x,
-                                                                   const double2 *b2, double2 *x2, PrecondInput in)
+                                                                   const double2 *b2, double2 *x2, PrecondInput in,
+                                                                   WoodArgs wd)
 {
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
@@ -1452,21 +1540,64 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_solve_cl(int Nr, int n_
     double2 *D = smc, *Y = smc + Lc;
     const int64_t base = (int64_t)j * Nr + c0;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // staging: two elements per thread in flight (every load of a batch issues
+    // before its stores)
+    constexpr int SB = 2;
     if (in.mode == PI_PLAIN) {
-        for (int e = tid; e < len; e += T) {
-            D[e] = dinv[base + e];
-            Y[e] = bv[base + e];
+        const double2 *__restrict__ bsrc = bv + base;
+        const double2 *__restrict__ dsrc = dinv + base;
+        for (int e0 = tid; e0 < len; e0 += SB * T) {
+            double2 dv[SB], yv[SB];
+#pragma unroll
+            for (int u = 0; u < SB; ++u) {
+                const int e = e0 + u * T;
+                if (e < len) {
+                    dv[u] = dsrc[e];
+                    yv[u] = bsrc[e];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < SB; ++u) {
+                const int e = e0 + u * T;
+                if (e < len) {
+                    D[e] = dv[u];
+                    Y[e] = yv[u];
+                }
+            }
         }
     } else {
         const double2 beta = in.kr->beta, omega = in.kr->omega, alpha = in.kr->alpha;
-        for (int e = tid; e < len; e += T) {
-            D[e] = dinv[base + e];
-            const int64_t k = base + e;
-            double2 rhsv;
-            if (in.mode == PI_P) rhsv = cadd(in.r[k], cmul(beta, csub(in.p_old[k], cmul(omega, in.v[k]))));
-            else rhsv = csub(in.r[k], cmul(alpha, in.v[k]));
-            Y[e] = rhsv;
-            in.out[k] = rhsv;
+        const double2 *__restrict__ dsrc = dinv + base;
+        const double2 *__restrict__ rsrc = in.r + base;
+        // PI_P without p_old (first iteration: p_old = v = 0) is p = r
+        const bool first = in.mode == PI_P && in.p_old == nullptr;
+        const double2 *__restrict__ vsrc = first ? nullptr : in.v + base;
+        const double2 *__restrict__ psrc = (in.mode == PI_P && !first) ? in.p_old + base : nullptr;
+        double2 *__restrict__ odst = in.out + base;
+        for (int e0 = tid; e0 < len; e0 += SB * T) {
+            double2 dv[SB], rv[SB], vv[SB], pv[SB];
+#pragma unroll
+            for (int u = 0; u < SB; ++u) {
+                const int e = e0 + u * T;
+                if (e < len) {
+                    dv[u] = dsrc[e];
+                    rv[u] = rsrc[e];
+                    vv[u] = vsrc ? vsrc[e] : cmake(0.0, 0.0);
+                    pv[u] = psrc ? psrc[e] : cmake(0.0, 0.0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < SB; ++u) {
+                const int e = e0 + u * T;
+                if (e < len) {
+                    const double2 rhsv = first ? rv[u]
+                                         : psrc ? cadd(rv[u], cmul(beta, csub(pv[u], cmul(omega, vv[u]))))
+                                                : csub(rv[u], cmul(alpha, vv[u]));
+                    D[e] = dv[u];
+                    Y[e] = rhsv;
+                    odst[e] = rhsv;
+                }
+            }
         }
     }
     __syncthreads();
@@ -1490,19 +1621,37 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_solve_cl(int Nr, int n_
     if (lane == 0) excl = aff_identity();
     if (lane == 31) wagg[warp] = acc;
     __syncthreads();
-    if (tid == 0) {
-        Aff c = aff_identity();
-        for (int w = 0; w < NW; ++w) c = aff_then(c, wagg[w]);
-        cagg_f = c;
+    if (warp == 0) {
+        // CTA total: ordered scan of the warp totals in lanes 0..NW-1
+        Aff c = lane < NW ? wagg[lane] : aff_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff prev = shfl_up_aff(c, o);
+            if (lane >= o) c = aff_then(prev, c);
+        }
+        if (lane == 31) cagg_f = c;
     }
     cl.sync();
-    if (tid == 0) {
-        double2 y = cmake(0.0, 0.0);
-        for (int q = 0; q < rank; ++q) y = aff_apply(*cl.map_shared_rank(&cagg_f, q), y);
-        for (int w = 0; w < NW; ++w) {
-            win[w] = y;
-            y = aff_apply(wagg[w], y);
+    if (warp == 0) {
+        // start value of the CTA: lane q < rank holds CTA q's total; their ordered
+        // composition applied to y = 0 is its B part
+        Aff c = lane < rank ? *cl.map_shared_rank(&cagg_f, lane) : aff_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff prev = shfl_up_aff(c, o);
+            if (lane >= o) c = aff_then(prev, c);
         }
+        const double2 ycta = cmake(__shfl_sync(0xffffffffu, c.B.x, 31), __shfl_sync(0xffffffffu, c.B.y, 31));
+        // start values of the warps: exclusive scan of the warp totals
+        Aff w = lane < NW ? wagg[lane] : aff_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff prev = shfl_up_aff(w, o);
+            if (lane >= o) w = aff_then(prev, w);
+        }
+        Aff wex = shfl_up_aff(w, 1);
+        if (lane == 0) wex = aff_identity();
+        if (lane < NW) win[lane] = aff_apply(wex, ycta);
     }
     __syncthreads();
     {
@@ -1534,19 +1683,35 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_solve_cl(int Nr, int n_
     __syncthreads();  // every thread has read win[] of the forward sweep
     if (lane == 0) wagg[warp] = bcc;
     __syncthreads();
-    if (tid == 0) {
-        Aff c = aff_identity();
-        for (int w = NW - 1; w >= 0; --w) c = aff_then(c, wagg[w]);
-        cagg_b = c;
+    if (warp == 0) {
+        // CTA total of the backward maps: ordered suffix scan of the warp totals
+        Aff c = lane < NW ? wagg[lane] : aff_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff nxt = shfl_down_aff(c, o);
+            if (lane + o < 32) c = aff_then(nxt, c);
+        }
+        if (lane == 0) cagg_b = c;
     }
     cl.sync();
-    if (tid == 0) {
-        double2 xr = cmake(0.0, 0.0);
-        for (int q = cs - 1; q > rank; --q) xr = aff_apply(*cl.map_shared_rank(&cagg_b, q), xr);
-        for (int w = NW - 1; w >= 0; --w) {
-            win[w] = xr;
-            xr = aff_apply(wagg[w], xr);
+    if (warp == 0) {
+        // start value of the CTA from the CTAs after it (applied last to first)
+        Aff c = (lane > rank && lane < cs) ? *cl.map_shared_rank(&cagg_b, lane) : aff_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff nxt = shfl_down_aff(c, o);
+            if (lane + o < 32) c = aff_then(nxt, c);
         }
+        const double2 xcta = cmake(__shfl_sync(0xffffffffu, c.B.x, 0), __shfl_sync(0xffffffffu, c.B.y, 0));
+        Aff w = lane < NW ? wagg[lane] : aff_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff nxt = shfl_down_aff(w, o);
+            if (lane + o < 32) w = aff_then(nxt, w);
+        }
+        Aff wex = shfl_down_aff(w, 1);
+        if (lane == 31) wex = aff_identity();
+        if (lane < NW) win[lane] = aff_apply(wex, xcta);
     }
     // the other CTAs read cagg_b only before this arrive; the matching wait is the
     // last statement, so a CTA's shared memory outlives every remote read of it
@@ -1563,6 +1728,55 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_solve_cl(int Nr, int n_
     }
     __syncthreads();
     for (int e = tid; e < len; e += T) xv[base + e] = Y[e];
+    if (wd.mode != WD_NONE) {
+        // sink projections v_a^dag x of this CTA's nodes; the last CTA finishes the
+        // Woodbury scalars
+        __shared__ double wscr[8 * 32];
+        double acc[4] = {0, 0, 0, 0};
+        for (int a = 0; a < wd.n_sinks; ++a) {
+            const double2 *va = a == 0 ? wd.v0 : wd.v1;
+            const int lo = max((a == 0 ? wd.lo0 : wd.lo1) - c0, 0), hi = min((a == 0 ? wd.hi0 : wd.hi1) - c0, len);
+            for (int e = lo + tid; e < hi; e += T) {
+                const double2 d = cconjmul(va[base + e], Y[e]);
+                acc[2 * a] += d.x;
+                acc[2 * a + 1] += d.y;
+            }
+        }
+        block_sum<4>(acc, wscr);
+        const int nblk = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
+        const int nslots = wd.mode == WD_SETUP ? 8 : 4;
+        if (tid == 0)
+            for (int q = 0; q < nslots; ++q) {
+                // setup: slots 4 b + (2 a + re/im) hold v_a^dag W_b
+                const int own = wd.mode == WD_SETUP ? q - 4 * second : q;
+                wd.partials[(int64_t)q * nblk + blk] = (own >= 0 && own < 4) ? acc[own] : 0.0;
+            }
+        __shared__ unsigned s_last;
+        __threadfence();
+        __syncthreads();
+        if (tid == 0) s_last = atomicAdd(wd.ticket, 1u) == (unsigned)nblk - 1u ? 1u : 0u;
+        __syncthreads();
+        if (s_last) {
+            __threadfence();
+            double sm[8];
+            for (int q = 0; q < 8; ++q) sm[q] = 0.0;
+            for (int bb = tid; bb < nblk; bb += T)
+                for (int q = 0; q < nslots; ++q) sm[q] += __ldcg(wd.partials + (int64_t)q * nblk + bb);
+            block_sum<8>(sm, wscr);
+            if (tid == 0) {
+                if (wd.mode == WD_SETUP) {
+                    // vw[2 b + a] = v_a^dag W_b
+                    double2 vw[4] = {cmake(sm[0], sm[1]), cmake(sm[2], sm[3]), cmake(sm[4], sm[5]),
+                                     cmake(sm[6], sm[7])};
+                    wood_setup_dev(wd.kr, vw, wd.c0, wd.c1);
+                } else {
+                    const double2 proj[2] = {cmake(sm[0], sm[1]), cmake(sm[2], sm[3])};
+                    wood_scalar_dev(wd.kr, wd.which, proj);
+                }
+                *wd.ticket = 0u;
+            }
+        }
+    }
     cl.barrier_wait();
 }
 
@@ -1586,33 +1800,31 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
     const int c0 = rank * Lc, c1 = min(Nr, c0 + Lc), len = max(0, c1 - c0);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     double2 *A = smc;
-    // diagonal of A = 1 + i dt/2 (H0 + V + CAP), staged term by term with coalesced
-    // passes over the hh rows (as k_precond_factor2)
+    // diagonal of A = 1 + i dt/2 (H0 + V + CAP): the diagonal pair's terms go to shared
+    // memory first, then every node's loads (r, CAP, one hh row per term) are
+    // independent and issue together
+    __shared__ double tg[64];
+    __shared__ int tl[64];
+    const int pd = ct.diag_pair[j];
+    const int t0 = pd >= 0 ? ct.pair_term_ptr[pd] : 0, nt = pd >= 0 ? min(64, ct.pair_term_ptr[pd + 1] - t0) : 0;
+    if (tid < nt) {
+        tg[tid] = ct.term_g[t0 + tid];
+        tl[tid] = ct.term_l[t0 + tid];
+    }
+    __syncthreads();
     {
         const int l = ct.mode_l[j];
-        const double alpha_d = 1.0 / (g.dr * g.dr);
+        const double alpha_d = 1.0 / (g.dr * g.dr), ll = (double)(l * (l + 1)), inv2mu = 1.0 / (2 * g.mu);
+#pragma unroll 2
         for (int e = tid; e < len; e += T) {
             const int i = c0 + e;
             double hre = 0.0;
             if (i >= 1 && i <= Nr - 2) {
-                const double ri = g.r[i];
-                hre = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
+                hre = (2.0 * alpha_d + ll * g.ir2[i]) * inv2mu;
+                for (int t = 0; t < nt; ++t) hre += tg[t] * hh[(int64_t)tl[t] * Nr + i];
             }
-            A[e] = cmake(0.0, hre);
-        }
-        const int p = ct.diag_pair[j];
-        if (p >= 0)
-            for (int t = ct.pair_term_ptr[p]; t < ct.pair_term_ptr[p + 1]; ++t) {
-                const double gt = ct.term_g[t];
-                const double *row = hh + (int64_t)ct.term_l[t] * Nr + c0;
-                for (int e = tid; e < len; e += T) {
-                    const int i = c0 + e;
-                    if (i >= 1 && i <= Nr - 2) A[e].y += gt * row[e];
-                }
-            }
-        for (int e = tid; e < len; e += T) {
-            const double him = g.capw ? -g.capw[c0 + e] : 0.0;
-            A[e] = cmake(1.0 - half_dt * him, half_dt * A[e].y);
+            const double him = g.capw ? -g.capw[i] : 0.0;
+            A[e] = cmake(1.0 - half_dt * him, half_dt * hre);
         }
     }
     __syncthreads();
@@ -1635,23 +1847,44 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
     const Mob excl = shfl_up_mob(acc, 1);
     if (lane == 31) wmob[warp] = acc;
     __syncthreads();
-    if (tid == 0) {
-        Mob m = mob_identity();
-        for (int w = 0; w < NW; ++w) {
-            m = mob_mul(wmob[w], m);
-            mob_normalize(m);
+    if (warp == 0) {
+        Mob m = lane < NW ? wmob[lane] : mob_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Mob prev = shfl_up_mob(m, o);
+            if (lane >= o) {
+                m = mob_mul(m, prev);
+                mob_normalize(m);
+            }
         }
-        cmob = m;
+        if (lane == 31) cmob = m;
     }
     cl.sync();
-    if (tid == 0) {
+    if (warp == 0) {
         // node 0's map is constant (p_0 = a_0), so any finite start value is exact
-        double2 p = cmake(1.0, 0.0);
-        for (int q = 0; q < rank; ++q) p = mob_apply(*cl.map_shared_rank(&cmob, q), p);
-        for (int w = 0; w < NW; ++w) {
-            pwin[w] = p;
-            if (w + 1 < NW) p = mob_apply(wmob[w], p);
+        Mob m = lane < rank ? *cl.map_shared_rank(&cmob, lane) : mob_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Mob prev = shfl_up_mob(m, o);
+            if (lane >= o) {
+                m = mob_mul(m, prev);
+                mob_normalize(m);
+            }
         }
+        double2 pc = lane == 31 ? mob_apply(m, cmake(1.0, 0.0)) : cmake(0.0, 0.0);
+        pc = cmake(__shfl_sync(0xffffffffu, pc.x, 31), __shfl_sync(0xffffffffu, pc.y, 31));
+        Mob w = lane < NW ? wmob[lane] : mob_identity();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Mob prev = shfl_up_mob(w, o);
+            if (lane >= o) {
+                w = mob_mul(w, prev);
+                mob_normalize(w);
+            }
+        }
+        Mob wex = shfl_up_mob(w, 1);
+        if (lane == 0) wex = mob_identity();
+        if (lane < NW) pwin[lane] = mob_apply(wex, pc);
     }
     cl.barrier_arrive();
     __syncthreads();
@@ -1757,11 +1990,12 @@ __global__ void k_bicg_s(int64_t n, const Krylov *kr, const double2 *r, const do
 }
 
 // x += alpha y + omega z; r = s - omega t; per-CTA partials of |r|^2 and r0 . r.
-__global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, const Krylov *kr, double2 *x, const double2 *y,
+__global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, Krylov *kr, double2 *x, const double2 *y,
                                                               const double2 *z, double2 *r, const double2 *s,
-                                                              const double2 *t, const double2 *r0, double *partials)
+                                                              const double2 *t, const double2 *r0, double *partials,
+                                                              double *red, unsigned *ticket)
 {
-    __shared__ double scratch[3 * 32];
+    __shared__ double scratch[6 * 32];
     const double2 al = kr->alpha, w = kr->omega;
     double acc[3] = {0, 0, 0};
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -1776,6 +2010,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, const Kr
     block_sum<3>(acc, scratch);
     if (threadIdx.x == 0)
         for (int q = 0; q < 3; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = acc[q];
+    if (ticket) finish_stage(partials, gridDim.x, 3, red, kr, KS_UPDATE, ticket, scratch);
 }
 
 // Woodbury correction y = yP - sum_a W_a c_a on the vector (src/CrankNicolsonModes_matrices.cpp:146-153).
@@ -1842,9 +2077,8 @@ __global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
 
 // Woodbury set-up on the device (src/CrankNicolsonModes_matrices.cpp:133-145):
 // G = diag(1 / (dt/4 g_a)) + v_a^dag W_b from vw[2 b + a] = v_a^dag W_b, and G^{-1}.
-__global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1)
+__device__ void wood_setup_dev(Krylov *kr, const double2 *vw, double c0, double c1)
 {
-    if (threadIdx.x != 0) return;
     const int k = kr->n_sinks;
     double2 G[2][2];
     for (int a = 0; a < 2; ++a)
@@ -1869,6 +2103,11 @@ __global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1
     }
 }
 
+__global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1)
+{
+    if (threadIdx.x == 0) wood_setup_dev(kr, vw, c0, c1);
+}
+
 // b = rhs / |rhs|, x = psi / |rhs| with |rhs|^2 = red[0]; a zero right-hand side is
 // flagged (kr->zero_rhs) and leaves b = x = 0.
 __global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
@@ -1890,12 +2129,13 @@ __global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const 
 //   b = s rhs, x = s psi, r = r0 = b - A_full x = 2 s (rhs - psi)
 // because A_full + B_full = 2 I and rhs = B_full psi (src/CrankNicolsonModes.cpp:170-172,
 // _matrices.cpp:36-37); per-CTA partials of |r|^2 and |b|^2 for KS_INIT.
-__global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov *kr, const double *red,
+__global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov *kr, const double *red_in,
                                                                const double2 *rhs, const double2 *psi, double2 *b,
-                                                               double2 *x, double2 *r, double2 *r0, double *partials)
+                                                               double2 *x, double2 *r, double2 *r0, double *partials,
+                                                               double *red, unsigned *ticket)
 {
-    __shared__ double scratch[4 * 32];
-    const double nrm = sqrt(red[0]);
+    __shared__ double scratch[6 * 32];
+    const double nrm = sqrt(red_in[0]);
     const double sc = nrm > 0.0 ? 1.0 / nrm : 0.0;
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         kr->rhs_norm = nrm;
@@ -1916,6 +2156,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov 
     block_sum<4>(acc, scratch);
     if (threadIdx.x == 0)
         for (int q = 0; q < 4; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = acc[q];
+    if (ticket) finish_stage(partials, gridDim.x, 4, red, kr, KS_INIT, ticket, scratch);
 }
 
 // candidate = x |rhs|.
@@ -1928,9 +2169,8 @@ __global__ void k_scale_candidate(int64_t n, const Krylov *kr, const double2 *x,
 
 // Woodbury projections: with proj_a = v_a^dag yP (dots), c = G^{-1} proj and the sink
 // dots of the corrected vector, v_a^dag y = proj_a - sum_b (v_a^dag W_b) c_b.
-__global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj)
+__device__ void wood_scalar_dev(Krylov *kr, int which, const double2 *proj)
 {
-    if (threadIdx.x != 0) return;
     const int k = kr->n_sinks;
     double2 c[2] = {cmake(0, 0), cmake(0, 0)};
     for (int a = 0; a < k; ++a)
@@ -1941,6 +2181,11 @@ __global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj)
         for (int b = 0; b < k; ++b) d = csub(d, cmul(kr->vW[a][b], c[b]));
         kr->sdots[which][a] = d;
     }
+}
+
+__global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj)
+{
+    if (threadIdx.x == 0) wood_scalar_dev(kr, which, proj);
 }
 
 // ------------------------------------------------------------------ absorbers

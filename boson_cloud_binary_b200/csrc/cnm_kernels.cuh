@@ -43,7 +43,9 @@ struct PrecondInput {
     double2 *out;
 };
 
-enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3, KS_INIT = 4 };
+enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3, KS_INIT = 4, KS_NONE = 5 };
+// Completion tickets (one counter per kind of launch that finishes a stage).
+enum Ticket : int { TK_APPLY_T = 0, TK_UPDATE_T = 1, TK_START_T = 2, TK_WOOD_T = 3, TK_DIAG_T = 4, TK_COUNT_T = 8 };
 
 __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
                            double scale, double a1, double a2);
@@ -54,8 +56,9 @@ cudaError_t set_operator_smem(int apply_bytes, int diag_bytes);
 // Two-nodes-per-thread operator kernel on 64-node tiles with a two-row blocked table.
 constexpr int APPLY3_TILE = 64;
 cudaError_t set_apply3_smem(int bytes);
-void launch_apply3(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
-                   const BlockTable &bt, const ApplyArgs &a);
+const void *apply3_kernel(int l_max, int vpart, bool gsm);
+void launch_apply3(int l_max, bool gsm, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
+                   const CouplingTable &ct, const BlockTable &bt, const ApplyPlan &pl, const ApplyArgs &a);
 void launch_apply(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
                   const BlockTable &bt, const ApplyArgs &a);
 void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
@@ -78,8 +81,9 @@ __global__ void k_axpby(int64_t n, double2 a, const double2 *x, double2 b, const
 __global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y);
 __global__ void k_bicg_p(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *p);
 __global__ void k_bicg_s(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *s);
-__global__ void k_bicg_update(int64_t n, const Krylov *kr, double2 *x, const double2 *y, const double2 *z,
-                              double2 *r, const double2 *s, const double2 *t, const double2 *r0, double *partials);
+__global__ void k_bicg_update(int64_t n, Krylov *kr, double2 *x, const double2 *y, const double2 *z, double2 *r,
+                              const double2 *s, const double2 *t, const double2 *r0, double *partials, double *red,
+                              unsigned *ticket);
 __global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2 *yP, const double2 *W0,
                            const double2 *W1, double2 *y);
 __global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red);
@@ -87,15 +91,29 @@ __global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj);
 __global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1);
 __global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
                                 double2 *b, double2 *x);
-__global__ void k_krylov_start(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
-                               double2 *b, double2 *x, double2 *r, double2 *r0, double *partials);
+__global__ void k_krylov_start(int64_t n, Krylov *kr, const double *red_in, const double2 *rhs, const double2 *psi,
+                               double2 *b, double2 *x, double2 *r, double2 *r0, double *partials, double *red,
+                               unsigned *ticket);
 __global__ void k_scale_candidate(int64_t n, const Krylov *kr, const double2 *x, double2 *cand);
 __global__ void k_precond_solve2(int Nr, int chunk, int window, double2 off, const double2 *dinv, const double2 *b,
                                  double2 *x, PrecondInput in);
 __global__ void k_precond_factor2(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int chunk,
                                   int window, double2 *dinv, int *status);
+// Woodbury scalars finished by the cluster solve (last CTA): WD_SETUP after solving
+// W_b = P^{-1} v_b (b = 0 in the first half of the grid, 1 in the second), WD_PROJ
+// after y = P^{-1} b (c = G^{-1} v^dag y into kr->wc[which], kr->sdots[which]).
+enum WoodMode : int { WD_NONE = 0, WD_SETUP = 1, WD_PROJ = 2 };
+struct WoodArgs {
+    int mode, which, n_sinks;
+    const double2 *v0, *v1;
+    int lo0, hi0, lo1, hi1;
+    double c0, c1;       // dt/4 g_a (WD_SETUP)
+    double *partials;    // [8][grid blocks]
+    unsigned *ticket;
+    Krylov *kr;
+};
 __global__ void k_precond_solve_cl(int Nr, int n_modes, int per, double2 off, const double2 *dinv, const double2 *b,
-                                   double2 *x, const double2 *b2, double2 *x2, PrecondInput in);
+                                   double2 *x, const double2 *b2, double2 *x2, PrecondInput in, WoodArgs wd);
 __global__ void k_precond_factor_cl(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int per,
                                     double2 *dinv, int *status);
 __global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
