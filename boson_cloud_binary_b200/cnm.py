@@ -73,7 +73,18 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_get_state", "cnm_configure_isolated_black_hole", "cnm_initialize",
            "cnm_set_power_average_orbits", "cnm_build_damping_mask", "cnm_build_cap", "cnm_prepare_run",
            "cnm_refresh", "cnm_step", "cnm_should_stop", "cnm_apply", "cnm_sink_strength", "cnm_sink_active",
-           "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop")
+           "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
+           "cnm_plan_info", "cnm_measure_fp64_peak")
+
+def measure_fp64_peak():
+    """FP64 FMA throughput of the current device, TFLOP/s (cnm_measure_fp64_peak)."""
+    L = load_library()
+    v = C.c_double()
+    rc = L.cnm_measure_fp64_peak(C.byref(v))
+    if rc != CNM_OK:
+        raise CudaError(L.cnm_create_error().decode())
+    return v.value
+
 
 KERNELS = {"apply": 0, "precond_solve": 1, "precond_factor": 2, "diagnostics": 3}
 
@@ -124,6 +135,8 @@ def load_library():
     L.cnm_kernel_times.argtypes = [p, i32, dp, C.POINTER(C.c_int64)]
     L.cnm_timer_start.argtypes = [p]
     L.cnm_timer_stop.argtypes = [p, dp]
+    L.cnm_plan_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.cnm_measure_fp64_peak.argtypes = [dp]
     _lib = L
     return L
 
@@ -346,6 +359,13 @@ class CrankNicolsonModes:
 
     def timer_start(self):
         self._check(self._lib.cnm_timer_start(self._h))
+
+    def plan_info(self):
+        """Launch plan chosen for this device: {scan_per, scan_cluster, apply_groups,
+        apply_weights_in_smem} (see cnm_plan_info)."""
+        v = [C.c_int32() for _ in range(4)]
+        self._check(self._lib.cnm_plan_info(self._h, *[C.byref(x) for x in v]))
+        return dict(zip(("scan_per", "scan_cluster", "apply_groups", "apply_weights_in_smem"), (x.value for x in v)))
 
     def timer_stop(self):
         """Device milliseconds on the solver's stream since timer_start()."""

@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cmath>
 #include <complex>
 #include <cstring>
@@ -270,6 +271,7 @@ struct Solver {
     // exact cluster scans: nodes per thread (odd) and CTAs per radial block; 0 = the
     // windowed scans are used instead
     int pcl_per = 0, pcl_cs = 0;
+    bool jacobi = false;  // fallback solve: point-Jacobi preconditioner in place of the radial blocks
     DevBuf<unsigned> d_tickets;  // completion tickets (zero between launches)
     DevBuf<double> d_wpart;      // partials of the Woodbury projections
     static constexpr int RED_RHS = 16, RED_RES = 20;  // red slots: |rhs|^2, final residual^2
@@ -976,6 +978,11 @@ struct Solver {
     void factorize(double dtv)
     {
         CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
+        if (jacobi) {
+            k_jacobi_diag<<<vec_blocks, VEC_THREADS, 0, stream>>>(grid(), table(), d_hh.p, 0.5 * dtv, dinv.p);
+            launch_check();
+            return;
+        }
         if (pcl_per > 0) {
             const size_t smem = (size_t)PCL_THREADS * pcl_per * sizeof(double2);
             cudaLaunchConfig_t cfg = cluster_config(pcl_cs, n_modes, smem);
@@ -1005,6 +1012,11 @@ struct Solver {
                                                                                              nullptr, nullptr,
                                                                                              nullptr, nullptr})
     {
+        if (jacobi) {
+            k_jacobi_apply<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dinv.p, bv, xv, in);
+            launch_check();
+            return;
+        }
         if (pcl_per > 0) {
             precond_cl(bv, xv, nullptr, nullptr, dtv, in);
             return;
@@ -1067,7 +1079,11 @@ struct Solver {
     // finishes the matching scalar stage in its last CTA, so an iteration is seven
     // launches (five without sinks) and one host synchronisation (convergence and
     // restart test).  |rhs|^2 is left in red[RED_RHS] by the right-hand-side apply.
-    void solve_CN()
+    // One preconditioned BiCGSTAB attempt from the initial guess psi / |rhs|, with the
+    // radial-block preconditioner or, when `jacobi` is set, the point-Jacobi one; true
+    // when the solve was accepted (pivots finite and true residual <= accept_residual).
+    // The accepted candidate stays in x (scaled by 1 / |rhs|).
+    bool solve_attempt(int max_it, double &rhs_norm_out)
     {
         const double dtv = op.dt;
         const Absorber *sk[2];
@@ -1077,7 +1093,7 @@ struct Solver {
         std::memset(&kr, 0, sizeof(kr));
         kr.n_sinks = k;
         kr.tol = tolerance;
-        kr.max_iterations = max_iterations;
+        kr.max_iterations = max_it;
         kr.eigen_path = k == 0;
         CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
         // b = rhs / |rhs|, x = psi / |rhs|, r = r0 = b - A_full x in one pass; its last
@@ -1091,10 +1107,11 @@ struct Solver {
         CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
         sync();
         if (kr.zero_rhs) {
-            CK(cudaMemsetAsync(psi.p, 0, nN * sizeof(double2), stream));
+            CK(cudaMemsetAsync(x.p, 0, nN * sizeof(double2), stream));
             last_residual = 0.0;
             last_iterations = 0;
-            return;
+            rhs_norm_out = 0.0;
+            return true;
         }
         const bool eigen_path = k == 0;
         const double eps = std::numeric_limits<double>::epsilon();
@@ -1174,10 +1191,32 @@ struct Solver {
         int status = 0;
         std::memcpy(&status, hres + 1, sizeof(int));
         last_residual = std::isfinite(res2) ? std::sqrt(res2) / rhs_norm : std::numeric_limits<double>::infinity();
-        if (status != 0)
-            throw Error(CNM_ESOLVE, "Radial preconditioner factorization failed (zero or non-finite pivot)");
-        if (!(last_residual <= accept_residual))
-            throw Error(CNM_ESOLVE, "Crank-Nicolson solve failed the relative residual check");
+        rhs_norm_out = rhs_norm;
+        return status == 0 && last_residual <= accept_residual;
+    }
+
+    // solve_CN (src/CrankNicolsonModes_matrices.cpp:94-215): the radial-block attempt;
+    // if its factorisation fails or its result misses the 1e-9 residual, the reference
+    // retries with a full ILUT preconditioner and 5000 iterations -- here the retry is a
+    // point-Jacobi BiCGSTAB on the device with the same iteration budget.  With
+    // use_block_preconditioner off the retry path is the only one, as in the reference.
+    void solve_CN()
+    {
+        double rhs_norm = 0.0;
+        bool ok = false;
+        if (use_block) ok = solve_attempt(max_iterations, rhs_norm);
+        if (!ok) {
+            if (use_block) std::fprintf(stderr, "\nRadial preconditioner did not converge; retrying with the point-Jacobi fallback.\n");
+            jacobi = true;
+            try {
+                ok = solve_attempt(5000, rhs_norm);
+            } catch (...) {
+                jacobi = false;
+                throw;
+            }
+            jacobi = false;
+            if (!ok) throw Error(CNM_ESOLVE, "Crank-Nicolson solve failed the relative residual check");
+        }
         // psi = mask (|rhs| x)
         k_scale_mask<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, Nr, rhs_norm, mask ? d_mask.p : nullptr, x.p,
                                                               psi.p);
@@ -1189,7 +1228,7 @@ struct Solver {
     void wood_setup(const Absorber *const *sk, int k, double dtv)
     {
         const double c0 = 0.25 * dtv * sk[0]->strength, c1 = k > 1 ? 0.25 * dtv * sk[1]->strength : 1.0;
-        if (pcl_per > 0) {
+        if (pcl_per > 0 && !jacobi) {
             WoodArgs wd = wood_args(WD_SETUP, 0, sk, k);
             wd.c0 = c0;
             wd.c1 = c1;
@@ -1234,7 +1273,7 @@ struct Solver {
             precond(nullptr, out, dtv, in);
             return;
         }
-        if (pcl_per > 0) {
+        if (pcl_per > 0 && !jacobi) {
             precond_cl(nullptr, yP.p, nullptr, nullptr, dtv, in, wood_args(WD_PROJ, which, sk, k));
         } else {
             precond(nullptr, yP.p, dtv, in);
@@ -1874,6 +1913,58 @@ int cnm_timer_stop(cnm_handle *h, double *ms)
         CK(cudaEventElapsedTime(&f, s.region_a, s.region_b));
         *ms = f;
     });
+}
+
+int cnm_measure_fp64_peak(double *tflops)
+{
+    if (!tflops) return CNM_EINVAL;
+    try {
+        int dev = 0, nsm = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        double *buf = nullptr;
+        CK(cudaMalloc(&buf, sizeof(double) * 4 * nsm));
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        const int blocks = 4 * nsm, threads = 512, iters = 1 << 14;
+        cnm::k_fp64_peak<<<blocks, threads>>>(buf, 256, 1.0000001, 1e-12);  // warm-up
+        CK(cudaGetLastError());
+        float best = 1e30f;
+        for (int rep = 0; rep < 5; ++rep) {
+            CK(cudaEventRecord(e0));
+            cnm::k_fp64_peak<<<blocks, threads>>>(buf, iters, 1.0000001, 1e-12);
+            CK(cudaEventRecord(e1));
+            CK(cudaEventSynchronize(e1));
+            float ms = 0.f;
+            CK(cudaEventElapsedTime(&ms, e0, e1));
+            best = std::min(best, ms);
+        }
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        cudaFree(buf);
+        const double flops = 2.0 * 8.0 * iters * (double)blocks * threads;
+        *tflops = flops / (best * 1e-3) / 1e12;
+        return CNM_OK;
+    } catch (const cnm::Error &e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return CNM_ECUDA;
+    }
+}
+
+int cnm_plan_info(const cnm_handle *h, int32_t *scan_per, int32_t *scan_cluster, int32_t *apply_groups,
+                  int32_t *apply_weights_in_smem)
+{
+    if (!h || !h->s) return CNM_EINVAL;
+    const cnm::Solver &s = *h->s;
+    if (scan_per) *scan_per = s.pcl_per;
+    if (scan_cluster) *scan_cluster = s.pcl_cs;
+    if (apply_groups) *apply_groups = s.plan3.n_groups;
+    if (apply_weights_in_smem) *apply_weights_in_smem = s.apply3_gsm ? 1 : 0;
+    return CNM_OK;
 }
 
 }  // extern "C"

@@ -47,17 +47,18 @@ __device__ void wood_setup_dev(Krylov *kr, const double2 *vw, double c0, double 
 __device__ void wood_scalar_dev(Krylov *kr, int which, const double2 *proj);
 
 // Completion of a launch whose CTAs each left `nslots` partial sums in
-// partials[slot * nblocks + block]: every CTA calls this after its partial store; the
-// CTA that takes the last ticket (after a device-scope fence) sums the partials in a
-// fixed order, independent of which CTA finishes last, stores red[0..nslots) and runs
-// the scalar stage; after KS_INIT and KS_UPDATE it also forms the next beta unless
-// the solve is done or must restart.  The ticket is re-armed for the next launch.
-// `scratch` is 6 * 32 doubles of shared memory; blockDim.x must be a multiple of 32.
+// partials[slot * nblocks + block]: every CTA calls this after its partial store (the
+// threads that stored a partial issue __threadfence() right after it; no other
+// thread waits on a fence, so the CTA's bulk stores stay in flight); the CTA that
+// takes the last ticket sums the partials in a fixed order, independent of which CTA
+// finishes last, stores red[0..nslots) and runs the scalar stage; after KS_INIT and
+// KS_UPDATE it also forms the next beta unless the solve is done or must restart.
+// The ticket is re-armed for the next launch.  `scratch` is 6 * 32 doubles of shared
+// memory; blockDim.x must be a multiple of 32.
 __device__ void finish_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage,
                              unsigned *ticket, double *scratch)
 {
     __shared__ unsigned s_last;
-    __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == (unsigned)nblocks - 1u ? 1u : 0u;
     __syncthreads();
@@ -837,6 +838,7 @@ __global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTab
             double sm = 0.0;
             for (int w = 0; w < nw; ++w) sm += red[threadIdx.x * 32 + w];
             a.dot_partials[(int64_t)threadIdx.x * nblocks + blk] = sm;
+            if (a.stage >= 0) __threadfence();
         }
         if (a.stage >= 0) {
             __syncthreads();
@@ -1745,14 +1747,15 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         block_sum<4>(acc, wscr);
         const int nblk = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
         const int nslots = wd.mode == WD_SETUP ? 8 : 4;
-        if (tid == 0)
+        if (tid == 0) {
             for (int q = 0; q < nslots; ++q) {
                 // setup: slots 4 b + (2 a + re/im) hold v_a^dag W_b
                 const int own = wd.mode == WD_SETUP ? q - 4 * second : q;
                 wd.partials[(int64_t)q * nblk + blk] = (own >= 0 && own < 4) ? acc[own] : 0.0;
             }
+            __threadfence();
+        }
         __shared__ unsigned s_last;
-        __threadfence();
         __syncthreads();
         if (tid == 0) s_last = atomicAdd(wd.ticket, 1u) == (unsigned)nblk - 1u ? 1u : 0u;
         __syncthreads();
@@ -2008,8 +2011,10 @@ __global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, Krylov *
         acc[2] += d.y;
     }
     block_sum<3>(acc, scratch);
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
         for (int q = 0; q < 3; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = acc[q];
+        __threadfence();
+    }
     if (ticket) finish_stage(partials, gridDim.x, 3, red, kr, KS_UPDATE, ticket, scratch);
 }
 
@@ -2154,8 +2159,10 @@ __global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov 
         acc[2] += cabs2(bv);
     }
     block_sum<4>(acc, scratch);
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
         for (int q = 0; q < 4; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = acc[q];
+        __threadfence();
+    }
     if (ticket) finish_stage(partials, gridDim.x, 4, red, kr, KS_INIT, ticket, scratch);
 }
 
@@ -2447,6 +2454,65 @@ __global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, 
         for (int q = 0; q < nslots; ++q) red[q] = acc[q];
         bicg_stage(kr, stage, red);
     }
+}
+
+// ------------------------------------------------------------------ fallback preconditioner
+
+// Inverse diagonal of A = 1 + i dt/2 (H0 + V + CAP): the point-Jacobi preconditioner of
+// the fallback solve that replaces the reference's ILUT retry
+// (src/CrankNicolsonModes_matrices.cpp:175-186,203-214).
+__global__ void k_jacobi_diag(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 *dj)
+{
+    const int64_t n = (int64_t)g.n_modes * g.Nr;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(e / g.Nr), i = (int)(e % g.Nr);
+        dj[e] = crcp(a_diag(g, ct, hh, half_dt, j, i));
+    }
+}
+
+// out = diag(A)^{-1} b, with b = the PrecondInput combination formed on the fly (and
+// stored to in.out) as in the block solves.
+__global__ void k_jacobi_apply(int64_t n, const double2 *dj, const double2 *b, double2 *out, PrecondInput in)
+{
+    double2 beta = cmake(0, 0), omega = cmake(0, 0), alpha = cmake(0, 0);
+    if (in.mode != PI_PLAIN) {
+        beta = in.kr->beta;
+        omega = in.kr->omega;
+        alpha = in.kr->alpha;
+    }
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        double2 rhsv;
+        if (in.mode == PI_PLAIN) {
+            rhsv = b[e];
+        } else {
+            if (in.mode == PI_P)
+                rhsv = in.p_old ? cadd(in.r[e], cmul(beta, csub(in.p_old[e], cmul(omega, in.v[e])))) : in.r[e];
+            else
+                rhsv = csub(in.r[e], cmul(alpha, in.v[e]));
+            in.out[e] = rhsv;
+        }
+        out[e] = cmul(dj[e], rhsv);
+    }
+}
+
+// ------------------------------------------------------------------ FP64 FMA peak
+
+// Microbenchmark of the FP64 pipe: eight independent FMA chains per thread (enough
+// to cover the FMA latency with two or more warps per scheduler); the sum is stored
+// only under a condition that never holds, so the chains stay live.
+__global__ void __launch_bounds__(512) k_fp64_peak(double *out, int iters, double b, double c)
+{
+    double a[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) a[k] = 1.0 + 1e-3 * (threadIdx.x + 32 * k);
+    for (int it = 0; it < iters; ++it) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) a[k] = fma(a[k], b, c);
+    }
+    double s = 0.0;
+#pragma unroll
+    for (int k = 0; k < 8; ++k) s += a[k];
+    if (s == -1.0) out[blockIdx.x] = s;
 }
 
 }  // namespace cnm

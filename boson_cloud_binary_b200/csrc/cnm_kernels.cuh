@@ -129,4 +129,9 @@ __global__ void k_diagnostics(Grid g, CouplingTable ct, const double *hh, double
 __global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out);
 __global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage);
 
+__global__ void k_fp64_peak(double *out, int iters, double b, double c);
+
+__global__ void k_jacobi_diag(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 *dj);
+__global__ void k_jacobi_apply(int64_t n, const double2 *dj, const double2 *b, double2 *out, PrecondInput in);
+
 }  // namespace cnm

@@ -217,6 +217,16 @@ int cnm_set_profiling(cnm_handle *h, int32_t on);
 int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *launches);
 int cnm_timer_start(cnm_handle *h);
 int cnm_timer_stop(cnm_handle *h, double *ms);
+/* FP64 FMA throughput of the current device in TFLOP/s (2 flops per FMA), from a
+ * register-resident chain microbenchmark timed with device events: the denominator of
+ * the FP64 roofline of the operator kernels. */
+int cnm_measure_fp64_peak(double *tflops);
+/* Launch plan chosen at creation for this device: nodes per thread and CTAs per cluster
+ * of the exact preconditioner scans (0, 0 when the windowed scans are used), CTA groups
+ * per node tile of the operator kernel and whether a group's weights sit in shared
+ * memory (1) or are read through L1 (0). */
+int cnm_plan_info(const cnm_handle *h, int32_t *scan_per, int32_t *scan_cluster, int32_t *apply_groups,
+                  int32_t *apply_weights_in_smem);
 
 /* --- radial block solve without allocation (no counterpart in the reference) -----
  * For callers that cannot call cudaMalloc -- a host code that gives the solver a
