@@ -74,7 +74,7 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_set_power_average_orbits", "cnm_build_damping_mask", "cnm_build_cap", "cnm_prepare_run",
            "cnm_refresh", "cnm_step", "cnm_should_stop", "cnm_apply", "cnm_sink_strength", "cnm_sink_active",
            "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
-           "cnm_plan_info", "cnm_measure_fp64_peak")
+           "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel")
 
 def measure_fp64_peak():
     """FP64 FMA throughput of the current device, TFLOP/s (cnm_measure_fp64_peak)."""
@@ -137,6 +137,7 @@ def load_library():
     L.cnm_timer_stop.argtypes = [p, dp]
     L.cnm_plan_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     L.cnm_measure_fp64_peak.argtypes = [dp]
+    L.cnm_set_operator_kernel.argtypes = [p, i32]
     _lib = L
     return L
 
@@ -359,6 +360,11 @@ class CrankNicolsonModes:
 
     def timer_start(self):
         self._check(self._lib.cnm_timer_start(self._h))
+
+    def set_operator_kernel(self, specialised):
+        """Select the operator kernel specialised for l_max <= 8 (True, default) or the
+        generic plan-driven one (False)."""
+        self._check(self._lib.cnm_set_operator_kernel(self._h, int(bool(specialised))))
 
     def plan_info(self):
         """Launch plan chosen for this device: {scan_per, scan_cluster, apply_groups,

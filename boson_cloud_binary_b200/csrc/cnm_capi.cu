@@ -12,6 +12,7 @@
 #include "../../include/cnm_gpu.h"
 #include "cnm_coupling.h"
 #include "cnm_kernels.cuh"
+#include "cnm_apply5.cuh"
 
 #include <cuda_runtime.h>
 
@@ -272,6 +273,14 @@ struct Solver {
     // windowed scans are used instead
     int pcl_per = 0, pcl_cs = 0;
     bool jacobi = false;  // fallback solve: point-Jacobi preconditioner in place of the radial blocks
+    // The reference's A and B are refreshed only by initialize() and step()
+    // (update_CN_values), not by the operator rebuild of run(); a CAP built after
+    // initialize() reaches H at run() but A and B only at the next step.
+    bool ab_cap = false;
+    // operator kernel specialised for this l_max (0 groups: the generic plan-driven kernel)
+    int a5_groups = 0;
+    bool a5_enabled = true;
+    DevBuf<double> d_a5tab;
     DevBuf<unsigned> d_tickets;  // completion tickets (zero between launches)
     DevBuf<double> d_wpart;      // partials of the Woodbury projections
     static constexpr int RED_RHS = 16, RED_RES = 20;  // red slots: |rhs|^2, final residual^2
@@ -423,6 +432,11 @@ struct Solver {
         CK(cudaFuncSetAttribute(k_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
         CK(set_operator_smem((int)apply_smem, (int)diag_smem));
         plan_operator(nsm);
+        a5_groups = apply5_groups(l_max);
+        if (a5_groups > 0) {
+            upload(d_a5tab, apply5_table(l_max, cpl));
+            CK(set_apply5_smem());
+        }
         CK(cudaFuncSetAttribute(k_diagnostics, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
         CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CK(cudaFuncSetAttribute(k_precond_solve2, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
@@ -666,6 +680,7 @@ struct Solver {
         abs1.valid = abs2.valid = false;
         t_i = 0.0;
         build_time_dependent_perturbation(0.0);
+        ab_cap = op.cap;
         initialized = true;
     }
 
@@ -775,7 +790,7 @@ struct Solver {
             upload(d_glw, gw);
             gl_n = nq;
         }
-        const int threads = 128;
+        const int threads = std::max(128, (nq + 31) / 32 * 32);  // one quadrature node per thread
         k_abs_moments<<<ab.hi - ab.lo, threads, (size_t)(degree + 1) * (threads / 32) * sizeof(double), stream>>>(
             d_r.p, Nr, ab.lo, radius, width, nq, d_glx.p, d_glw.p, degree, ab.mom.p);
         launch_check();
@@ -869,8 +884,17 @@ struct Solver {
         return dim3((unsigned)((Nr + APPLY3_TILE - 1) / APPLY3_TILE), (unsigned)plan3.n_groups);
     }
 
+    bool use_apply5(const ApplyArgs &a) const { return a5_groups > 0 && a5_enabled && a.vpart == V_POT; }
+
     void launch_apply(const ApplyArgs &a)
     {
+        if (use_apply5(a)) {
+            kt_begin(TK_APPLY);
+            ::cnm::launch_apply5(l_max, stream, grid(), d_a5tab.p, a);
+            launch_check();
+            kt_end(TK_APPLY);
+            return;
+        }
         const dim3 blocks3 = apply3_grid();
         kt_begin(TK_APPLY);
         ::cnm::launch_apply3(l_max, apply3_gsm, blocks3, apply3_smem, stream, grid(), table(), btable2(), aplan(), a);
@@ -1312,6 +1336,7 @@ struct Solver {
         theta += (counter ? -1.0 : 1.0) * Omega * dt;
         phase += Omega * dt;
         build_time_dependent_perturbation(t_i);
+        ab_cap = op.cap;
         // projections of the old state on the new sinks (for the midpoint accretion rate)
         const Absorber *all[2] = {&abs1, &abs2};
         const bool have_sinks = absorption && cpl.mode00 >= 0;
@@ -1545,7 +1570,7 @@ struct Solver {
             a.alpha = cmake(1, 0);
             a.beta = cmake(0, (opc == CNM_OP_B ? -0.5 : 0.5) * op.dt);
             a.use_h0 = 1;
-            a.use_cap = 1;
+            a.use_cap = ab_cap ? 1 : 0;
             a.vpart = V_POT;
             if (opc == CNM_OP_AFULL) with_sinks(0.25 * op.dt);
             break;
@@ -1558,10 +1583,15 @@ struct Solver {
             with_sinks(-0.5);
             break;
         case CNM_OP_CAP: a.use_cap = 1; break;
-        case CNM_OP_PRECOND:
+        case CNM_OP_PRECOND: {
+            // the radial blocks of the member A (whose CAP term follows ab_cap)
+            const bool cap_now = op.cap;
+            op.cap = ab_cap;
             factorize(op.dt);
             precond(tmp.p, cand.p, op.dt);
+            op.cap = cap_now;
             break;
+        }
         default: throw Error(CNM_EINVAL, "unknown operator");
         }
         if (opc != CNM_OP_PRECOND) launch_apply(a);
@@ -1913,6 +1943,11 @@ int cnm_timer_stop(cnm_handle *h, double *ms)
         CK(cudaEventElapsedTime(&f, s.region_a, s.region_b));
         *ms = f;
     });
+}
+
+int cnm_set_operator_kernel(cnm_handle *h, int32_t specialised)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.a5_enabled = specialised != 0; });
 }
 
 int cnm_measure_fp64_peak(double *tflops)

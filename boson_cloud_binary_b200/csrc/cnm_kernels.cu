@@ -3,80 +3,18 @@
 // Every kernel here is memory-streaming or FMA work on complex128 vectors in the
 // reference's mode-major layout; see cnm_common.cuh for the data layout.
 #include "cnm_kernels.cuh"
+#include "cnm_device.cuh"
 
 #include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 namespace cnm {
 
-// ------------------------------------------------------------------ reductions
-
-__device__ __forceinline__ double warp_sum(double v)
-{
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
-// Deterministic block sum of NV doubles per thread; result valid in thread 0.
-template <int NV>
-__device__ void block_sum(double (&v)[NV], double *scratch /* NV * 32 */)
-{
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
-#pragma unroll
-    for (int q = 0; q < NV; ++q) v[q] = warp_sum(v[q]);
-    __syncthreads();
-    if (lane == 0)
-#pragma unroll
-        for (int q = 0; q < NV; ++q) scratch[q * 32 + warp] = v[q];
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int q = 0; q < NV; ++q) {
-            double s = lane < nw ? scratch[q * 32 + lane] : 0.0;
-            v[q] = warp_sum(s);
-        }
-    }
-    __syncthreads();
-}
-
 // ------------------------------------------------------------------ radial weights
 
-__device__ void bicg_stage(Krylov *kr, int stage, const double *red);
 __device__ void wood_setup_dev(Krylov *kr, const double2 *vw, double c0, double c1);
 __device__ void wood_scalar_dev(Krylov *kr, int which, const double2 *proj);
 
-// Completion of a launch whose CTAs each left `nslots` partial sums in
-// partials[slot * nblocks + block]: every CTA calls this after its partial store (the
-// threads that stored a partial issue __threadfence() right after it; no other
-// thread waits on a fence, so the CTA's bulk stores stay in flight); the CTA that
-// takes the last ticket sums the partials in a fixed order, independent of which CTA
-// finishes last, stores red[0..nslots) and runs the scalar stage; after KS_INIT and
-// KS_UPDATE it also forms the next beta unless the solve is done or must restart.
-// The ticket is re-armed for the next launch.  `scratch` is 6 * 32 doubles of shared
-// memory; blockDim.x must be a multiple of 32.
-__device__ void finish_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage,
-                             unsigned *ticket, double *scratch)
-{
-    __shared__ unsigned s_last;
-    __syncthreads();
-    if (threadIdx.x == 0) s_last = atomicAdd(ticket, 1u) == (unsigned)nblocks - 1u ? 1u : 0u;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-        for (int q = 0; q < nslots && q < 6; ++q) acc[q] += __ldcg(partials + (int64_t)q * nblocks + b);
-    block_sum<6>(acc, scratch);
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < nslots && q < 6; ++q) red[q] = acc[q];
-        if (kr && stage != KS_NONE) {
-            bicg_stage(kr, stage, red);
-            if ((stage == KS_INIT || stage == KS_UPDATE) && !kr->done && !kr->restart) bicg_stage(kr, KS_BETA, red);
-        }
-        *ticket = 0u;
-    }
-}
 
 // hh[l][i] = scale * (a1 F1_l(r_i) + a2 (-1)^l F2_l(r_i)) on interior nodes, zero on the
 // two boundary nodes (the reference fills radial_f1/f2 for i = 1..Nr-2 only,
@@ -1762,9 +1700,15 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         if (s_last) {
             __threadfence();
             double sm[8];
+#pragma unroll
             for (int q = 0; q < 8; ++q) sm[q] = 0.0;
-            for (int bb = tid; bb < nblk; bb += T)
-                for (int q = 0; q < nslots; ++q) sm[q] += __ldcg(wd.partials + (int64_t)q * nblk + bb);
+            for (int bb = tid; bb < nblk; bb += T) {
+                double v[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) v[q] = q < nslots ? __ldcg(wd.partials + (int64_t)q * nblk + bb) : 0.0;
+#pragma unroll
+                for (int q = 0; q < 8; ++q) sm[q] += v[q];
+            }
             block_sum<8>(sm, wscr);
             if (tid == 0) {
                 if (wd.mode == WD_SETUP) {
@@ -2031,49 +1975,6 @@ __global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2
     }
 }
 
-// Scalar steps of the recurrence.
-__device__ void bicg_stage(Krylov *kr, int stage, const double *red)
-{
-    switch (stage) {
-    case KS_BETA: {  // rho_old = rho; rho = r0 . r; restart check; beta
-        const double2 rho_old = kr->rho;
-        kr->rho = kr->r0r;
-        kr->restart = sqrt(cabs2(kr->rho)) < kr->restart_thr ? 1 : 0;
-        kr->rho_old = rho_old;
-        kr->beta = cmul(cdiv(kr->rho, rho_old), cdiv(kr->alpha, kr->omega));
-        break;
-    }
-    case KS_ALPHA:  // alpha = rho / (r0 . v); red = {re, im}
-        kr->alpha = cdiv(kr->rho, cmake(red[0], red[1]));
-        break;
-    case KS_OMEGA: {  // red = {ts.re, ts.im, tt}
-        const double tt = red[2];
-        kr->omega = tt > 0.0 ? cscale(cmake(red[0], red[1]), 1.0 / tt) : cmake(0.0, 0.0);
-        break;
-    }
-    case KS_UPDATE:  // red = {|r|^2, r0.r re, im}; also flags the next iteration's restart
-        kr->r2 = red[0];
-        kr->r0r = cmake(red[1], red[2]);
-        kr->iterations += 1;
-        kr->done = !(kr->r2 > kr->thr) || kr->iterations >= kr->max_iterations;
-        kr->restart = sqrt(cabs2(kr->r0r)) < kr->restart_thr ? 1 : 0;
-        break;
-    case KS_INIT: {  // red = {|r0|^2, 0, |b|^2, 0}
-        const double r0n2 = red[0], b2 = red[2];
-        kr->rho = kr->alpha = kr->omega = cmake(1.0, 0.0);
-        kr->thr = kr->tol * kr->tol * b2;
-        const double eps = 2.220446049250313e-16;
-        kr->restart_thr = kr->eigen_path ? eps * eps * r0n2 : 1e-32 * r0n2;
-        kr->r2 = r0n2;
-        kr->r0r = cmake(r0n2, 0.0);
-        kr->iterations = 0;
-        kr->done = !(r0n2 > kr->thr) || kr->max_iterations <= 0;
-        kr->restart = 0;
-        break;
-    }
-    default: break;
-    }
-}
 
 __global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
 {
@@ -2223,26 +2124,30 @@ __global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, do
     }
     const double product = 2.0 * r[i] * radius;
     const double cap = fmin(2.0, (width * width - delta * delta) / product);
+    // one quadrature node per thread (blockDim.x >= nq): its weight and u = cos(gamma)
+    // once, then the Legendre recurrence advanced degree by degree
+    const int k = threadIdx.x;
+    double weight = 0.0, u = 0.0;
+    if (k < nq) {
+        const double z = cap * gl_x[k];
+        u = 1.0 - z;
+        const double d2 = delta * delta + product * z;
+        weight = 2.0 * M_PI * cap * gl_w[k] * exp(-1.0 / (1.0 - d2 / (width * width)));
+    }
+    double prev = 1.0, cur = u;
     for (int l = 0; l <= degree; ++l) {
-        double part = 0.0;
-        for (int k = threadIdx.x; k < nq; k += blockDim.x) {
-            const double z = cap * gl_x[k];
-            const double u = 1.0 - z;
-            const double d2 = delta * delta + product * z;
-            const double weight = 2.0 * M_PI * cap * gl_w[k] * exp(-1.0 / (1.0 - d2 / (width * width)));
-            double pl;
-            if (l == 0) pl = 1.0;
-            else {
-                double prev = 1.0, cur = u;
-                for (int m = 2; m <= l; ++m) {
-                    const double next = ((2 * m - 1) * u * cur - (m - 1) * prev) / m;
-                    prev = cur;
-                    cur = next;
-                }
-                pl = cur;
-            }
-            part += weight * pl;
+        double pl;
+        if (l == 0) {
+            pl = 1.0;
+        } else if (l == 1) {
+            pl = u;
+        } else {
+            const double next = ((2 * l - 1) * u * cur - (l - 1) * prev) / l;
+            prev = cur;
+            cur = next;
+            pl = cur;
         }
+        double part = k < nq ? 0.0 + weight * pl : 0.0;
         part = warp_sum(part);
         if (lane == 0) sh[l * nw + warp] = part;
     }

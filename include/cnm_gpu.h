@@ -217,6 +217,10 @@ int cnm_set_profiling(cnm_handle *h, int32_t on);
 int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *launches);
 int cnm_timer_start(cnm_handle *h);
 int cnm_timer_stop(cnm_handle *h, double *ms);
+/* Operator kernel selection (testing and measurement): 1 (default) uses the kernel
+ * specialised at compile time for l_max <= 8 where it exists, 0 the generic
+ * plan-driven kernel. */
+int cnm_set_operator_kernel(cnm_handle *h, int32_t specialised);
 /* FP64 FMA throughput of the current device in TFLOP/s (2 flops per FMA), from a
  * register-resident chain microbenchmark timed with device events: the denominator of
  * the FP64 roofline of the operator kernels. */
