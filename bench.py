@@ -43,9 +43,10 @@ WORKLOAD = dict(workload="fp64_single_binary_evolving_orbit", Nr=20000, L=2000.0
 METRIC = "CN mode*node*steps/s"
 UNIT = "mode*node*steps/s"
 
-# DRAM traffic per launch of the dominant kernel from the ncu capture summarised in
-# profiles/ (None until a capture of the current kernels exists).
-NCU_TRAFFIC_BYTES = None
+# DRAM traffic (read + write) per launch of the dominant kernel, the operator apply,
+# from the ncu capture summarised in profiles/k_apply5_fp64_binary_n45_N20000.md:
+# dram__bytes.sum.per_second x gpu__time_duration.sum = 373.29 GB/s x 86.816 us.
+NCU_TRAFFIC_BYTES = 373.293034e9 * 86.816e-6
 
 
 def peaks():

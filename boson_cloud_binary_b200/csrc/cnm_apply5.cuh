@@ -129,12 +129,33 @@ struct A5Host {
     int rowoff(int g, int l1, int j) const { return a5f::rowoff(L, G, g, l1, j); }
 };
 
-// Host side of the specialised kernel (0 groups: l_max not specialised).
+// Arguments of the specialised diagnostics kernel (the pass of k_diagnostics2: H psi,
+// V psi, dV/dt psi and dpsi/dt on nodes <= idx_ex, reduced into per-CTA partials
+// [slot][block]: slots 0..n-1 norms, n..2n-1 energies, 2n edge energy, 2n+1 p_bin,
+// 2n+2 dV; dpsi/dt and psi around idx_ex stored for the fluxes).
+struct DiagArgs {
+    const double *hh;
+    double theta, domega;
+    const double2 *psi;
+    int idx_ex;
+    int n_sinks;
+    const double2 *sv0, *sv1, *sink_dots;
+    double sink_coef0, sink_coef1;
+    int slo0, shi0, slo1, shi1;
+    double *partials;
+    double2 *dpsi_edge, *psi_edge;
+};
+
+// Host side of the specialised kernels (0 groups: l_max not specialised).
 int apply5_groups(int l_max);
 size_t apply5_smem(int l_max);
 unsigned apply5_blocks(int l_max, int Nr);
 std::vector<double> apply5_table(int l_max, const Coupling &c);
 cudaError_t set_apply5_smem();
 void launch_apply5(int l_max, cudaStream_t st, const Grid &g, const double *gtab, const ApplyArgs &a);
+size_t diag5_smem(int l_max);
+cudaError_t set_diag5_smem();
+// launches the diagnostics pass and returns its number of CTAs (the partials' stride)
+unsigned launch_diag5(int l_max, cudaStream_t st, const Grid &g, const double *gtab, const DiagArgs &d);
 
 }  // namespace cnm

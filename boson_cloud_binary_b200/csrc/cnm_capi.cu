@@ -436,6 +436,7 @@ struct Solver {
         if (a5_groups > 0) {
             upload(d_a5tab, apply5_table(l_max, cpl));
             CK(set_apply5_smem());
+            CK(set_diag5_smem());
         }
         CK(cudaFuncSetAttribute(k_diagnostics, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
         CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
@@ -1376,14 +1377,37 @@ struct Solver {
         // diagnostics on the masked end-of-step state with the step's operators
         if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2);
         const dim3 dgrid = apply_grid();
-        const unsigned dblocks = dgrid.x * dgrid.y;
+        unsigned dblocks = dgrid.x * dgrid.y;
         kt_begin(TK_DIAG);
-        ::cnm::launch_diagnostics(
-            l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p, idx_ex, k, k > 0 ? sk[0]->v.p : nullptr,
-            k > 1 ? sk[1]->v.p : nullptr, k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p,
-            k > 0 ? -0.5 * sk[0]->strength : 0.0,
-            k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
-            k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes);
+        if (a5_groups > 0 && a5_enabled) {
+            DiagArgs da;
+            da.hh = d_hh.p;
+            da.theta = op.theta;
+            da.domega = op.domega;
+            da.psi = psi.p;
+            da.idx_ex = idx_ex;
+            da.n_sinks = k;
+            da.sv0 = k > 0 ? sk[0]->v.p : nullptr;
+            da.sv1 = k > 1 ? sk[1]->v.p : nullptr;
+            da.sink_dots = k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p;
+            da.sink_coef0 = k > 0 ? -0.5 * sk[0]->strength : 0.0;
+            da.sink_coef1 = k > 1 ? -0.5 * sk[1]->strength : 0.0;
+            da.slo0 = k > 0 ? sk[0]->lo : 0;
+            da.shi0 = k > 0 ? sk[0]->hi : 0;
+            da.slo1 = k > 1 ? sk[1]->lo : 0;
+            da.shi1 = k > 1 ? sk[1]->hi : 0;
+            da.partials = d_partials.p;
+            da.dpsi_edge = d_edge.p;
+            da.psi_edge = d_edge.p + n_modes;
+            dblocks = ::cnm::launch_diag5(l_max, stream, grid(), d_a5tab.p, da);
+        } else {
+            ::cnm::launch_diagnostics(
+                l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p,
+                idx_ex, k, k > 0 ? sk[0]->v.p : nullptr, k > 1 ? sk[1]->v.p : nullptr,
+                k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
+                k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
+                k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes);
+        }
         launch_check();
         kt_end(TK_DIAG);
         const int nslots = 2 * n_modes + 3;
