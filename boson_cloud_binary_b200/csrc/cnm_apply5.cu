@@ -141,7 +141,9 @@ struct Epi {
                     const int64_t e = (int64_t)J * Nr + i;
                     if (a.dot_kind[q] == 1) d = cconjmul(a.dot_ext[q][e], y);
                     else if (a.dot_kind[q] == 2) d = cconjmul(y, a.dot_ext[q][e]);
-                    else if (a.dot_kind[q] == 4) d = cmake(cabs2(csub(cscale(y, a.dot_scale), a.dot_ext[q][e])), 0.0);
+                    else if (a.dot_kind[q] == 4)
+                        d = cmake(cabs2(csub(cscale(y, a.scale_kr ? a.scale_kr->rhs_norm : a.dot_scale), a.dot_ext[q][e])),
+                                  0.0);
                     else d = cmake(cabs2(y), 0.0);
                     dacc[2 * q] += d.x;
                     dacc[2 * q + 1] += d.y;
@@ -338,6 +340,7 @@ __device__ __forceinline__ void diag_dispatch(int grp, const Grid &g, const doub
 template <int L>
 __global__ void __launch_bounds__(A5_THREADS) k_diag5(Grid g, const double *gtab, DiagArgs d)
 {
+    if (d.gate && gate_closed(d.gate, GATE_ACCEPTED)) return;
     constexpr int G = A5Groups<L>::value;
     using Lay = A5Layout<L, G>;
     extern __shared__ double smem5[];
@@ -415,6 +418,7 @@ __device__ __forceinline__ void dispatch(int grp, const Grid &g, const double *g
 template <int L>
 __global__ void __launch_bounds__(A5_THREADS) k_apply5(Grid g, const double *gtab, ApplyArgs a)
 {
+    if (a.gate && gate_closed(a.gate, a.gate_mode)) return;
     constexpr int G = A5Groups<L>::value;
     using Lay = A5Layout<L, G>;
     extern __shared__ double smem5[];

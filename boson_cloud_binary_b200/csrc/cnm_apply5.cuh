@@ -144,6 +144,7 @@ struct DiagArgs {
     int slo0, shi0, slo1, shi1;
     double *partials;
     double2 *dpsi_edge, *psi_edge;
+    const struct Krylov *gate;  // skip until the step's candidate is accepted (null: always run)
 };
 
 // Host side of the specialised kernels (0 groups: l_max not specialised).

@@ -72,6 +72,8 @@ struct DotSpec {
     double scale = 1.0;
     int stage = -1;
     double *red = nullptr;
+    int gate_mode = 0;         // GateMode of the launch
+    bool scale_from_kr = false;  // kind 4 scale = the solve's |rhs| (device)
 };
 
 // Rolling time average over a window of orbital phase (src/RollingPhase.cpp:24-129).
@@ -273,6 +275,8 @@ struct Solver {
     // windowed scans are used instead
     int pcl_per = 0, pcl_cs = 0;
     bool jacobi = false;  // fallback solve: point-Jacobi preconditioner in place of the radial blocks
+    int wband_lo = 0, wband_hi = 0;  // nodes where the Woodbury vectors W_a are applied
+    int iter_hint = 2;               // iterations of the previous solve (first batch size)
     // The reference's A and B are refreshed only by initialize() and step()
     // (update_CN_values), not by the operator rebuild of run(); a CAP built after
     // initialize() reaches H at run() but A and B only at the next step.
@@ -283,7 +287,8 @@ struct Solver {
     DevBuf<double> d_a5tab;
     DevBuf<unsigned> d_tickets;  // completion tickets (zero between launches)
     DevBuf<double> d_wpart;      // partials of the Woodbury projections
-    static constexpr int RED_RHS = 16, RED_RES = 20;  // red slots: |rhs|^2, final residual^2
+    // red slots past the diagnostics' 2 n + 3 sums: |rhs|^2 and the candidate's residual^2
+    int RED_RHS = 0, RED_RES = 0;
     size_t apply_smem = 0, diag_smem = 0;
     // pinned host staging
     double *h_stage = nullptr;
@@ -420,7 +425,9 @@ struct Solver {
         d_edge.alloc(4 * (size_t)n_modes);
         d_kr.alloc(1);
         d_status.alloc(1);
-        d_red.alloc(std::max(64, 2 * n_modes + 8));
+        RED_RHS = 2 * n_modes + 8;
+        RED_RES = 2 * n_modes + 12;
+        d_red.alloc(std::max(64, 2 * n_modes + 16));
         d_tickets.alloc(TK_COUNT_T);
         const int diag_blocks = 2 * ((Nr + APPLY_TILE - 1) / APPLY_TILE);  // node tiles x row split
         d_partials.alloc(std::max<size_t>({(size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks,
@@ -711,9 +718,8 @@ struct Solver {
     // hh table of the geometry frozen in `op` (set by build_time_dependent_perturbation).
     void build_hh(double *dst, double a1, double a2)
     {
-        const int64_t total = (int64_t)K * Nr;
-        k_hh_table<<<(unsigned)((total + 255) / 256), 256, 0, stream>>>(dst, d_r.p, Nr, K, op.R1, op.R2, op.q,
-                                                                        -mu * op.Mtot, a1, a2);
+        k_hh_table<<<(unsigned)((Nr + 255) / 256), 256, 0, stream>>>(dst, d_r.p, Nr, K, op.R1, op.R2, op.q,
+                                                                     -mu * op.Mtot, a1, a2);
         launch_check();
     }
 
@@ -853,11 +859,12 @@ struct Solver {
 
     int sink_slot(const Absorber *ab) const { return ab == &abs1 ? 0 : 1; }
 
-    void sink_dots(const double2 *xv, double2 *dots, const Absorber *const *sk, int k)
+    void sink_dots(const double2 *xv, double2 *dots, const Absorber *const *sk, int k, int gate_mode = GATE_NONE)
     {
-        k_sink_dots<<<1, 512, 0, stream>>>(xv, Nr, n_modes, k, k > 0 ? sk[0]->v.p : nullptr,
+        k_sink_dots<<<1, 1024, 0, stream>>>(xv, Nr, n_modes, k, k > 0 ? sk[0]->v.p : nullptr,
                                            k > 1 ? sk[1]->v.p : nullptr, k > 0 ? sk[0]->lo : 0,
-                                           k > 0 ? sk[0]->hi : 0, k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, dots);
+                                           k > 0 ? sk[0]->hi : 0, k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, dots,
+                                           gate_mode == GATE_NONE ? nullptr : d_kr.p, gate_mode);
         launch_check();
     }
 
@@ -872,6 +879,9 @@ struct Solver {
         a.domega = op.domega;
         a.stage = -1;
         a.dot_scale = 1.0;
+        a.gate = nullptr;
+        a.gate_mode = GATE_NONE;
+        a.scale_kr = nullptr;
         return a;
     }
 
@@ -949,6 +959,9 @@ struct Solver {
         a.kr = d_kr.p;
         a.ticket = ticket(TK_APPLY_T);
         a.red = ds.red ? ds.red : d_red.p;
+        a.gate = ds.gate_mode != GATE_NONE ? d_kr.p : nullptr;
+        a.gate_mode = ds.gate_mode;
+        a.scale_kr = ds.scale_from_kr ? d_kr.p : nullptr;
     }
 
     unsigned *ticket(int which) const { return d_tickets.p + which; }
@@ -1104,15 +1117,140 @@ struct Solver {
     // finishes the matching scalar stage in its last CTA, so an iteration is seven
     // launches (five without sinks) and one host synchronisation (convergence and
     // restart test).  |rhs|^2 is left in red[RED_RHS] by the right-hand-side apply.
-    // One preconditioned BiCGSTAB attempt from the initial guess psi / |rhs|, with the
-    // radial-block preconditioner or, when `jacobi` is set, the point-Jacobi one; true
-    // when the solve was accepted (pivots finite and true residual <= accept_residual).
-    // The accepted candidate stays in x (scaled by 1 / |rhs|).
-    bool solve_attempt(int max_it, double &rhs_norm_out)
+    // The diagnostics pass of the accepted end-of-step state with the step's operators
+    // (src/CrankNicolsonModes_extraction.cpp), gated on the candidate's acceptance:
+    // the sink projections of the new state, the fused pass and the sums of its slots.
+    void enqueue_diagnostics(const Absorber *const *sk, int k)
+    {
+        const Absorber *all[2] = {&abs1, &abs2};
+        const bool have_sinks = absorption && cpl.mode00 >= 0;
+        if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2, GATE_ACCEPTED);
+        const dim3 dgrid = apply_grid();
+        unsigned dblocks = dgrid.x * dgrid.y;
+        kt_begin(TK_DIAG);
+        if (a5_groups > 0 && a5_enabled) {
+            DiagArgs da;
+            da.hh = d_hh.p;
+            da.theta = op.theta;
+            da.domega = op.domega;
+            da.psi = psi.p;
+            da.idx_ex = idx_ex;
+            da.n_sinks = k;
+            da.sv0 = k > 0 ? sk[0]->v.p : nullptr;
+            da.sv1 = k > 1 ? sk[1]->v.p : nullptr;
+            da.sink_dots = k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p;
+            da.sink_coef0 = k > 0 ? -0.5 * sk[0]->strength : 0.0;
+            da.sink_coef1 = k > 1 ? -0.5 * sk[1]->strength : 0.0;
+            da.slo0 = k > 0 ? sk[0]->lo : 0;
+            da.shi0 = k > 0 ? sk[0]->hi : 0;
+            da.slo1 = k > 1 ? sk[1]->lo : 0;
+            da.shi1 = k > 1 ? sk[1]->hi : 0;
+            da.partials = d_partials.p;
+            da.dpsi_edge = d_edge.p;
+            da.psi_edge = d_edge.p + n_modes;
+            da.gate = d_kr.p;
+            dblocks = ::cnm::launch_diag5(l_max, stream, grid(), d_a5tab.p, da);
+        } else {
+            ::cnm::launch_diagnostics(
+                l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p,
+                idx_ex, k, k > 0 ? sk[0]->v.p : nullptr, k > 1 ? sk[1]->v.p : nullptr,
+                k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
+                k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
+                k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes, d_kr.p);
+        }
+        launch_check();
+        kt_end(TK_DIAG);
+        const int nslots = 2 * n_modes + 3;
+        k_sum_slots<<<nslots, 256, 0, stream>>>(d_partials.p, (int)dblocks, nslots, d_red.p, d_kr.p);
+        launch_check();
+    }
+
+    // One BiCGSTAB iteration (src/CrankNicolsonModes_matrices.cpp:47-91), every launch
+    // gated on the device (skipped once the solve is done or must restart), so several
+    // can be queued ahead of the host's convergence test.
+    void enqueue_iteration(const Absorber *const *sk, int k, double dtv, bool first)
+    {
+        Krylov *dk = d_kr.p;
+        // p = r + beta (p - omega v) formed inside the preconditioner pass; y = M p
+        precond_M(PrecondInput{PI_P, dk, rr.p, p.p, v.p, nullptr, p2.p, first ? 1 : 0, GATE_ITER}, 0, sk, k, dtv,
+                  y.p);
+        // v = A y with r0 . v reduced in the same pass; alpha = rho / r0.v
+        {
+            DotSpec ds;
+            ds.n = 1;
+            ds.kind[0] = 1;
+            ds.ext[0] = r0.p;
+            ds.stage = KS_ALPHA;
+            ds.gate_mode = GATE_ITER;
+            apply_A(y.p, v.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[0][0]), dtv, ds);
+        }
+        // s = r - alpha v formed inside the preconditioner pass; z = M s
+        precond_M(PrecondInput{PI_S, dk, rr.p, nullptr, v.p, s.p, nullptr, 0, GATE_ITER}, 1, sk, k, dtv, z.p);
+        // t = A z with t . s and |t|^2 reduced in the same pass; omega = t.s / |t|^2
+        {
+            DotSpec ds;
+            ds.n = 2;
+            ds.kind[0] = 2;
+            ds.ext[0] = s.p;
+            ds.kind[1] = 3;
+            ds.stage = KS_OMEGA;
+            ds.gate_mode = GATE_ITER;
+            apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv, ds);
+        }
+        // x += alpha y + omega z; r = s - omega t; then KS_UPDATE and the next beta
+        k_bicg_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, y.p, z.p, rr.p, s.p, t.p, r0.p,
+                                                               d_partials.p, d_red.p, ticket(TK_UPDATE_T));
+        launch_check();
+    }
+
+    // Read-backs of a step, in the pinned stage: the Krylov scalars, the diagnostics'
+    // 2 n + 3 sums, psi and dpsi/dt around the extraction node, the sink projections.
+    size_t readback_doubles() const
+    {
+        return (sizeof(Krylov) + 7) / 8 + (size_t)(2 * n_modes + 3) + 8 * (size_t)n_modes + 16;
+    }
+
+    // Launches that follow the solve, queued behind every batch of iterations and gated
+    // on the device: the true residual of the candidate once the solve is done (its
+    // last CTA decides acceptance, KS_RESID), then psi = mask (|rhs| x), the
+    // diagnostics pass of the new state and the read-backs, once accepted.
+    void enqueue_tail(const Absorber *const *sk, int k, double dtv, double *hs)
+    {
+        sink_dots(x.p, d_dots.p, sk, k, GATE_DONE);
+        {
+            DotSpec ds;
+            ds.n = 1;
+            ds.kind[0] = 4;
+            ds.ext[0] = rhs.p;
+            ds.scale_from_kr = true;
+            ds.stage = KS_RESID;
+            ds.red = d_red.p + RED_RES;
+            ds.gate_mode = GATE_DONE;
+            apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv, ds);
+        }
+        k_scale_mask<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, Nr, 0.0, mask ? d_mask.p : nullptr, x.p, psi.p,
+                                                              d_kr.p);
+        launch_check();
+        enqueue_diagnostics(sk, k);
+        const size_t kd = (sizeof(Krylov) + 7) / 8;
+        const int nslots = 2 * n_modes + 3;
+        CK(cudaMemcpyAsync(hs, d_kr.p, sizeof(Krylov), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hs + kd, d_red.p, nslots * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hs + kd + nslots, d_edge.p, 4 * n_modes * sizeof(double2), cudaMemcpyDeviceToHost,
+                           stream));
+        CK(cudaMemcpyAsync(hs + kd + nslots + 8 * n_modes, d_dots.p, 8 * sizeof(double2), cudaMemcpyDeviceToHost,
+                           stream));
+    }
+
+    // One preconditioned BiCGSTAB attempt from the initial guess psi / |rhs| with the
+    // radial-block preconditioner or, when `jacobi` is set, the point-Jacobi one.  The
+    // iterations go out in batches (as many as the previous step needed) followed by
+    // the gated tail, with one host synchronisation per batch for the convergence and
+    // restart test.  True when the candidate was accepted (pivots finite and true
+    // residual <= accept_residual); the tail's read-backs are then in hs.
+    bool solve_attempt(int max_it, const Absorber *const *sk, int k, double *hs)
     {
         const double dtv = op.dt;
-        const Absorber *sk[2];
-        const int k = active_sinks(sk);
         Krylov *dk = d_kr.p;
         Krylov kr;
         std::memset(&kr, 0, sizeof(kr));
@@ -1120,6 +1258,8 @@ struct Solver {
         kr.tol = tolerance;
         kr.max_iterations = max_it;
         kr.eigen_path = k == 0;
+        kr.accept = accept_residual;
+        kr.status = d_status.p;
         CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
         // b = rhs / |rhs|, x = psi / |rhs|, r = r0 = b - A_full x in one pass; its last
         // CTA runs KS_INIT (and the first beta) on |r0|^2 and |b|^2
@@ -1129,20 +1269,20 @@ struct Solver {
         launch_check();
         factorize(dtv);
         if (k > 0) wood_setup(sk, k, dtv);
-        CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
-        sync();
-        if (kr.zero_rhs) {
-            CK(cudaMemsetAsync(x.p, 0, nN * sizeof(double2), stream));
-            last_residual = 0.0;
-            last_iterations = 0;
-            rhs_norm_out = 0.0;
-            return true;
-        }
         const bool eigen_path = k == 0;
         const double eps = std::numeric_limits<double>::epsilon();
         int restarts = 0;
-        const double2 *p_cur = nullptr;  // no search direction yet: p = r
-        while (!kr.done) {
+        bool first = true;
+        int batch = std::max(1, std::min(4, iter_hint));
+        for (;;) {
+            for (int q = 0; q < batch; ++q) {
+                enqueue_iteration(sk, k, dtv, first);
+                first = false;
+            }
+            enqueue_tail(sk, k, dtv, hs);
+            sync();
+            std::memcpy(&kr, hs, sizeof(kr));
+            if (kr.done) break;
             if (kr.restart) {
                 // Lost biorthogonality: restart from the current residual (_matrices.cpp:69-75).
                 const double2 rho_old = kr.rho;
@@ -1162,62 +1302,12 @@ struct Solver {
                 kr.restart = 0;
                 CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
             }
-            // p = r + beta (p - omega v) formed inside the preconditioner pass; y = M p
-            double2 *p_new = p_cur == p.p ? p2.p : p.p;
-            precond_M(PrecondInput{PI_P, dk, rr.p, p_cur, v.p, p_new}, 0, sk, k, dtv, y.p);
-            p_cur = p_new;
-            // v = A y with r0 . v reduced in the same pass; alpha = rho / r0.v
-            {
-                DotSpec ds;
-                ds.n = 1;
-                ds.kind[0] = 1;
-                ds.ext[0] = r0.p;
-                ds.stage = KS_ALPHA;
-                apply_A(y.p, v.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[0][0]), dtv, ds);
-            }
-            // s = r - alpha v formed inside the preconditioner pass; z = M s
-            precond_M(PrecondInput{PI_S, dk, rr.p, nullptr, v.p, s.p}, 1, sk, k, dtv, z.p);
-            // t = A z with t . s and |t|^2 reduced in the same pass; omega = t.s / |t|^2
-            {
-                DotSpec ds;
-                ds.n = 2;
-                ds.kind[0] = 2;
-                ds.ext[0] = s.p;
-                ds.kind[1] = 3;
-                ds.stage = KS_OMEGA;
-                apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv, ds);
-            }
-            // x += alpha y + omega z; r = s - omega t; then KS_UPDATE and the next beta
-            k_bicg_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, y.p, z.p, rr.p, s.p, t.p, r0.p,
-                                                                   d_partials.p, d_red.p, ticket(TK_UPDATE_T));
-            launch_check();
-            CK(cudaMemcpyAsync(&kr, dk, sizeof(kr), cudaMemcpyDeviceToHost, stream));
-            sync();
+            batch = 2;
         }
         last_iterations = kr.iterations;
-        // candidate = |rhs| x; residual |A candidate - rhs| / |rhs| = | |rhs| (A x) - rhs | / |rhs|
-        const double rhs_norm = kr.rhs_norm;
-        sink_dots(x.p, d_dots.p, sk, k);
-        {
-            DotSpec ds;
-            ds.n = 1;
-            ds.kind[0] = 4;
-            ds.ext[0] = rhs.p;
-            ds.scale = rhs_norm;
-            ds.stage = KS_NONE;
-            ds.red = d_red.p + RED_RES;
-            apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv, ds);
-        }
-        double *hres = stage(2);
-        CK(cudaMemcpyAsync(hres, d_red.p + RED_RES, sizeof(double), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(hres + 1, d_status.p, sizeof(int), cudaMemcpyDeviceToHost, stream));
-        sync();
-        const double res2 = hres[0];
-        int status = 0;
-        std::memcpy(&status, hres + 1, sizeof(int));
-        last_residual = std::isfinite(res2) ? std::sqrt(res2) / rhs_norm : std::numeric_limits<double>::infinity();
-        rhs_norm_out = rhs_norm;
-        return status == 0 && last_residual <= accept_residual;
+        last_residual = kr.residual;
+        iter_hint = std::max(1, kr.iterations);
+        return kr.accepted != 0;
     }
 
     // solve_CN (src/CrankNicolsonModes_matrices.cpp:94-215): the radial-block attempt;
@@ -1225,16 +1315,17 @@ struct Solver {
     // retries with a full ILUT preconditioner and 5000 iterations -- here the retry is a
     // point-Jacobi BiCGSTAB on the device with the same iteration budget.  With
     // use_block_preconditioner off the retry path is the only one, as in the reference.
-    void solve_CN()
+    // On return psi holds the accepted state and hs the step's read-backs.
+    void solve_CN(const Absorber *const *sk, int k, double *hs)
     {
-        double rhs_norm = 0.0;
         bool ok = false;
-        if (use_block) ok = solve_attempt(max_iterations, rhs_norm);
+        if (use_block) ok = solve_attempt(max_iterations, sk, k, hs);
         if (!ok) {
-            if (use_block) std::fprintf(stderr, "\nRadial preconditioner did not converge; retrying with the point-Jacobi fallback.\n");
+            if (use_block)
+                std::fprintf(stderr, "\nRadial preconditioner did not converge; retrying with the point-Jacobi fallback.\n");
             jacobi = true;
             try {
-                ok = solve_attempt(5000, rhs_norm);
+                ok = solve_attempt(5000, sk, k, hs);
             } catch (...) {
                 jacobi = false;
                 throw;
@@ -1242,10 +1333,6 @@ struct Solver {
             jacobi = false;
             if (!ok) throw Error(CNM_ESOLVE, "Crank-Nicolson solve failed the relative residual check");
         }
-        // psi = mask (|rhs| x)
-        k_scale_mask<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, Nr, rhs_norm, mask ? d_mask.p : nullptr, x.p,
-                                                              psi.p);
-        launch_check();
     }
 
     // Woodbury set-up (src/CrankNicolsonModes_matrices.cpp:133-145): W_a = P^{-1} v_a and
@@ -1253,6 +1340,7 @@ struct Solver {
     void wood_setup(const Absorber *const *sk, int k, double dtv)
     {
         const double c0 = 0.25 * dtv * sk[0]->strength, c1 = k > 1 ? 0.25 * dtv * sk[1]->strength : 1.0;
+        set_wood_band(sk, k, dtv);
         if (pcl_per > 0 && !jacobi) {
             WoodArgs wd = wood_args(WD_SETUP, 0, sk, k);
             wd.c0 = c0;
@@ -1299,15 +1387,48 @@ struct Solver {
             return;
         }
         if (pcl_per > 0 && !jacobi) {
-            precond_cl(nullptr, yP.p, nullptr, nullptr, dtv, in, wood_args(WD_PROJ, which, sk, k));
+            precond_cl(nullptr, out, nullptr, nullptr, dtv, in, wood_args(WD_PROJ, which, sk, k));
         } else {
-            precond(nullptr, yP.p, dtv, in);
-            sink_dots(yP.p, d_dots.p + 4, sk, k);
+            precond(nullptr, out, dtv, in);
+            sink_dots(out, d_dots.p + 4, sk, k);
             k_wood_scalar<<<1, 32, 0, stream>>>(d_kr.p, which, d_dots.p + 4);
             launch_check();
         }
-        k_woodbury<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_kr.p, which, yP.p, W0.p, W1.p, out);
+        // out -= sum_a W_a c_a where the W_a live
+        const int64_t nb = (int64_t)(wband_hi - wband_lo) * n_modes;
+        const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nb + 255) / 256, vec_blocks));
+        k_woodbury_band<<<blocks, 256, 0, stream>>>(Nr, n_modes, wband_lo, wband_hi, d_kr.p, which, W0.p, W1.p, out);
         launch_check();
+    }
+
+    // Band of nodes outside which every W_a = P^{-1} v_a is below 1e-40 of its largest
+    // value: the entries of the inverse of a radial block decay by the contraction
+    // rho = |off| / |p+| per node (with the potential's deepest depression of the
+    // diagonal, as choose_window bounds it), so 92 / -ln(rho) nodes past the sinks'
+    // support suffice; the point-Jacobi W_a vanish outside the support itself.
+    void set_wood_band(const Absorber *const *sk, int k, double dtv)
+    {
+        int lo = Nr, hi = 0;
+        for (int a = 0; a < k; ++a) {
+            lo = std::min(lo, sk[a]->lo);
+            hi = std::max(hi, sk[a]->hi);
+        }
+        if (hi <= lo) {
+            wband_lo = wband_hi = 0;
+            return;
+        }
+        int w = 0;
+        if (!jacobi) {
+            const double kappa = std::abs(offdiag(dtv).y);
+            const double depress = std::min(0.5, 0.5 * dtv * diag_potential_bound() / (2.0 * kappa));
+            const std::complex<double> a(1.0, 2.0 * kappa * (1.0 - depress)), c(-kappa * kappa, 0.0);
+            const std::complex<double> sq = std::sqrt(a * a - 4.0 * c);
+            const double pp = std::max(std::abs((a + sq) * 0.5), std::abs((a - sq) * 0.5));
+            const double rho = kappa / pp;
+            w = rho < 1.0 ? (int)std::min<double>(Nr, std::ceil(92.2 / -std::log(rho)) + 16) : Nr;
+        }
+        wband_lo = std::max(0, lo - w);
+        wband_hi = std::min(Nr, hi + w);
     }
 
     // -------------------------------------------------------------- step
@@ -1373,51 +1494,11 @@ struct Solver {
             }
             launch_apply(a);
         }
-        solve_CN();
-        // diagnostics on the masked end-of-step state with the step's operators
-        if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2);
-        const dim3 dgrid = apply_grid();
-        unsigned dblocks = dgrid.x * dgrid.y;
-        kt_begin(TK_DIAG);
-        if (a5_groups > 0 && a5_enabled) {
-            DiagArgs da;
-            da.hh = d_hh.p;
-            da.theta = op.theta;
-            da.domega = op.domega;
-            da.psi = psi.p;
-            da.idx_ex = idx_ex;
-            da.n_sinks = k;
-            da.sv0 = k > 0 ? sk[0]->v.p : nullptr;
-            da.sv1 = k > 1 ? sk[1]->v.p : nullptr;
-            da.sink_dots = k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p;
-            da.sink_coef0 = k > 0 ? -0.5 * sk[0]->strength : 0.0;
-            da.sink_coef1 = k > 1 ? -0.5 * sk[1]->strength : 0.0;
-            da.slo0 = k > 0 ? sk[0]->lo : 0;
-            da.shi0 = k > 0 ? sk[0]->hi : 0;
-            da.slo1 = k > 1 ? sk[1]->lo : 0;
-            da.shi1 = k > 1 ? sk[1]->hi : 0;
-            da.partials = d_partials.p;
-            da.dpsi_edge = d_edge.p;
-            da.psi_edge = d_edge.p + n_modes;
-            dblocks = ::cnm::launch_diag5(l_max, stream, grid(), d_a5tab.p, da);
-        } else {
-            ::cnm::launch_diagnostics(
-                l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p,
-                idx_ex, k, k > 0 ? sk[0]->v.p : nullptr, k > 1 ? sk[1]->v.p : nullptr,
-                k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
-                k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
-                k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes);
-        }
-        launch_check();
-        kt_end(TK_DIAG);
+        double *hs = stage(readback_doubles());
+        solve_CN(sk, k, hs);
         const int nslots = 2 * n_modes + 3;
-        k_sum_slots<<<nslots, 256, 0, stream>>>(d_partials.p, (int)dblocks, nslots, d_red.p);
-        launch_check();
-        double *hs = stage(nslots + 8 * n_modes + 16);
-        CK(cudaMemcpyAsync(hs, d_red.p, nslots * sizeof(double), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(hs + nslots, d_edge.p, 4 * n_modes * sizeof(double2), cudaMemcpyDeviceToHost, stream));
-        CK(cudaMemcpyAsync(hs + nslots + 8 * n_modes, d_dots.p, 8 * sizeof(double2), cudaMemcpyDeviceToHost, stream));
-        sync();
+        const size_t kd = (sizeof(Krylov) + 7) / 8;
+        hs += kd;
         const double *redh = hs;
         const double2 *edge = reinterpret_cast<const double2 *>(hs + nslots);
         const double2 *dh = reinterpret_cast<const double2 *>(hs + nslots + 8 * n_modes);

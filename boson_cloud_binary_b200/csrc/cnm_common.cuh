@@ -136,6 +136,11 @@ struct ApplyArgs {
     struct Krylov *kr;
     unsigned *ticket;
     double *red;
+    // device-side gate of a launch queued ahead of the host's test (GateMode), and the
+    // source of dot_scale (kr->rhs_norm) when set
+    const struct Krylov *gate;
+    int gate_mode;
+    const struct Krylov *scale_kr;
 };
 
 }  // namespace cnm

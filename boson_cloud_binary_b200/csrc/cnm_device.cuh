@@ -62,6 +62,7 @@ __device__ inline void bicg_stage(Krylov *kr, int stage, const double *red)
         kr->r2 = red[0];
         kr->r0r = cmake(red[1], red[2]);
         kr->iterations += 1;
+        kr->pturn ^= 1;
         kr->done = !(kr->r2 > kr->thr) || kr->iterations >= kr->max_iterations;
         kr->restart = sqrt(cabs2(kr->r0r)) < kr->restart_thr ? 1 : 0;
         break;
@@ -78,8 +79,42 @@ __device__ inline void bicg_stage(Krylov *kr, int stage, const double *red)
         kr->restart = 0;
         break;
     }
+    case KS_RESID: {  // red = {| |rhs| A x - rhs |^2}
+        const double r2 = red[0];
+        double res;
+        if (!isfinite(r2)) res = INFINITY;
+        else if (kr->rhs_norm > 0.0) res = sqrt(r2) / kr->rhs_norm;
+        else res = r2 == 0.0 ? 0.0 : INFINITY;
+        kr->residual = res;
+        kr->accepted = (res <= kr->accept) && !(kr->status && *kr->status != 0);
+        break;
+    }
     default: break;
     }
+}
+
+__device__ __forceinline__ bool gate_closed(const Krylov *kr, int mode)
+{
+    if (!kr || mode == GATE_NONE) return false;
+    if (mode == GATE_ITER) return kr->done || kr->restart;
+    if (mode == GATE_DONE) return !kr->done;
+    return !kr->accepted;
+}
+
+// Resolve a solve's input at launch: false when the gate is closed; otherwise picks the
+// search-direction buffers of a ping-pong PI_P input.
+__device__ __forceinline__ bool resolve_input(PrecondInput &in)
+{
+    if (in.gate != GATE_NONE && gate_closed(in.kr, in.gate)) return false;
+    if (in.mode == PI_P && in.p_alt) {
+        const int turn = in.kr->pturn;
+        double2 *a = const_cast<double2 *>(in.p_old), *b = in.p_alt;
+        in.out = turn ? b : a;
+        in.p_old = in.first ? nullptr : (turn ? a : b);
+    } else if (in.mode == PI_P && in.first) {
+        in.p_old = nullptr;
+    }
+    return true;
 }
 
 // Completion of a launch whose CTAs each left `nslots` partial sums in

@@ -22,21 +22,25 @@ __device__ void wood_scalar_dev(Krylov *kr, int which, const double2 *proj);
 __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
                            double scale, double a1, double a2)
 {
-    const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (int64_t)K * Nr) return;
-    const int l = (int)(idx / Nr), i = (int)(idx % Nr);
+    // one node per thread; the radial factors r_<^l / r_>^(l+1) of both bodies
+    // (_hamiltonian.cpp:12-42) by repeated multiplication with r_< / r_> over l
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= Nr) return;
     if (i == 0 || i == Nr - 1) {
-        hh[idx] = 0.0;
+        for (int l = 0; l < K; ++l) hh[(int64_t)l * Nr + i] = 0.0;
         return;
     }
     const double ri = r[i];
-    double f1, f2;
-    if (ri >= R1) f1 = 1 / (1 + q) * pow(R1, l) / pow(ri, l + 1);
-    else f1 = 1 / (1 + q) * pow(ri, l) / pow(R1, l + 1);
-    if (ri >= R2) f2 = 1.0 * q / (1 + q) * pow(R2, l) / pow(ri, l + 1);
-    else f2 = 1.0 * q / (1 + q) * pow(ri, l) / pow(R2, l + 1);
-    const double par = (l & 1) ? -1.0 : 1.0;
-    hh[idx] = scale * (a1 * f1 + a2 * par * f2);
+    const double big1 = ri >= R1 ? ri : R1, small1 = ri >= R1 ? R1 : ri;
+    const double big2 = ri >= R2 ? ri : R2, small2 = ri >= R2 ? R2 : ri;
+    const double x1 = small1 / big1, x2 = small2 / big2;
+    double f1 = 1 / (1 + q) / big1, f2 = 1.0 * q / (1 + q) / big2;
+    for (int l = 0; l < K; ++l) {
+        const double par = (l & 1) ? -1.0 : 1.0;
+        hh[(int64_t)l * Nr + i] = scale * (a1 * f1 + a2 * par * f2);
+        f1 *= x1;
+        f2 *= x2;
+    }
 }
 
 // ------------------------------------------------------------------ operator application
@@ -454,8 +458,9 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics2(Grid g, Coupling
                                                                  const double2 *sink_dots, double sink_coef0,
                                                                  double sink_coef1, int slo0, int shi0, int slo1,
                                                                  int shi1, double *partials, double2 *dpsi_edge,
-                                                                 double2 *psi_edge)
+                                                                 double2 *psi_edge, const Krylov *gate)
 {
+    if (gate && gate_closed(gate, GATE_ACCEPTED)) return;
     extern __shared__ double2 smem2[];
     __shared__ int s_lcut;
     const int n = g.n_modes, Nr = g.Nr;
@@ -679,7 +684,9 @@ __device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable 
                 if (a.dot_kind[q] == 1) d = cconjmul(a.dot_ext[q][(int64_t)j * Nr + i], y);
                 else if (a.dot_kind[q] == 2) d = cconjmul(y, a.dot_ext[q][(int64_t)j * Nr + i]);
                 else if (a.dot_kind[q] == 4)
-                    d = cmake(cabs2(csub(cscale(y, a.dot_scale), a.dot_ext[q][(int64_t)j * Nr + i])), 0.0);
+                    d = cmake(cabs2(csub(cscale(y, a.scale_kr ? a.scale_kr->rhs_norm : a.dot_scale),
+                                         a.dot_ext[q][(int64_t)j * Nr + i])),
+                              0.0);
                 else d = cmake(cabs2(y), 0.0);
                 dacc[2 * q] += d.x;
                 dacc[2 * q + 1] += d.y;
@@ -694,6 +701,7 @@ template <int SMAX, int VP, bool GSM>
 __global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTable ct, BlockTable bt, ApplyPlan pl,
                                                              ApplyArgs a)
 {
+    if (a.gate && gate_closed(a.gate, a.gate_mode)) return;
     extern __shared__ double2 smem3[];
     __shared__ int s_lcut;
     const int n = g.n_modes, Nr = g.Nr;
@@ -881,7 +889,7 @@ void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, co
                         const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
                         const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
                         const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0, int slo1,
-                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge)
+                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge, const Krylov *gate)
 {
     const int smax = smax_for(l_max);
 #define CNM_LAUNCH(S)                                                                                        \
@@ -889,7 +897,7 @@ void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, co
         k_diagnostics2<S><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, hh, theta, domega, psi, idx_ex,    \
                                                                n_sinks, sv0, sv1, sink_dots, sink_coef0,     \
                                                                sink_coef1, slo0, shi0, slo1, shi1, partials, \
-                                                               dpsi_edge, psi_edge);                         \
+                                                               dpsi_edge, psi_edge, gate);                   \
         return;                                                                                              \
     }
     CNM_FOR_SMAX(CNM_LAUNCH)
@@ -901,21 +909,26 @@ void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, co
 // dots[s] = v_s^dagger x over the support of v_s (v_s vanishes elsewhere), one CTA,
 // fixed summation order.
 __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
-                            const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots)
+                            const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots, const Krylov *gate,
+                            int gate_mode)
 {
+    if (gate && gate_closed(gate, gate_mode)) return;
+    // warp w takes modes w, w + nwarps, ...; its lanes stride over the support nodes, so
+    // every load of a thread is independent of the others (fixed order: deterministic)
     __shared__ double scratch[4 * 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     double acc[4] = {0, 0, 0, 0};
     for (int s = 0; s < n_sinks; ++s) {
-        const double2 *v = s == 0 ? v0 : v1;
+        const double2 *__restrict__ v = s == 0 ? v0 : v1;
         const int lo = s == 0 ? lo0 : lo1, hi = s == 0 ? hi0 : hi1;
-        const int w = hi - lo;
-        if (w <= 0) continue;
-        for (int e = threadIdx.x; e < w * n_modes; e += blockDim.x) {
-            const int j = e / w, i = lo + e % w;
-            const int64_t k = (int64_t)j * Nr + i;
-            const double2 d = cconjmul(v[k], x[k]);
-            acc[2 * s] += d.x;
-            acc[2 * s + 1] += d.y;
+        for (int j = warp; j < n_modes; j += nw) {
+            const int64_t base = (int64_t)j * Nr;
+#pragma unroll 4
+            for (int i = lo + lane; i < hi; i += 32) {
+                const double2 d = cconjmul(v[base + i], x[base + i]);
+                acc[2 * s] += d.x;
+                acc[2 * s + 1] += d.y;
+            }
         }
     }
     block_sum<4>(acc, scratch);
@@ -1212,6 +1225,7 @@ __global__ void __launch_bounds__(SCAN2_THREADS) k_precond_solve2(int Nr, int ch
                                                                   const double2 *dinv, const double2 *b, double2 *x,
                                                                   PrecondInput in)
 {
+    if (!resolve_input(in)) return;
     extern __shared__ double2 sm2[];
     __shared__ Aff tf[SCAN2_THREADS];
     const int j = blockIdx.y;
@@ -1463,6 +1477,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
                                                                    const double2 *b2, double2 *x2, PrecondInput in,
                                                                    WoodArgs wd)
 {
+    if (!resolve_input(in)) return;
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double2 smc[];
@@ -1912,8 +1927,14 @@ __global__ void k_axpby(int64_t n, double2 a, const double2 *x, double2 b, const
 }
 
 // y *= mask(i) (the damping mask is one profile shared by every mode).
-__global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y)
+__global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y,
+                             const Krylov *kr)
 {
+    // with kr: s = kr->rhs_norm, and only once the candidate is accepted
+    if (kr) {
+        if (!kr->accepted) return;
+        s = kr->rhs_norm;
+    }
     for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         const double f = mask ? s * mask[e % Nr] : s;
         y[e] = cscale(x[e], f);
@@ -1942,6 +1963,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, Krylov *
                                                               const double2 *t, const double2 *r0, double *partials,
                                                               double *red, unsigned *ticket)
 {
+    if (kr->done || kr->restart) return;  // queued ahead of the convergence test
     __shared__ double scratch[6 * 32];
     const double2 al = kr->alpha, w = kr->omega;
     double acc[3] = {0, 0, 0};
@@ -1975,6 +1997,24 @@ __global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2
     }
 }
 
+
+// Woodbury correction in place on the band of nodes [lo, hi) of every mode where the
+// W_a = P^{-1} v_a can be non-negligible: y -= sum_a W_a c_a (c from kr->wc[which]).
+__global__ void k_woodbury_band(int Nr, int n_modes, int lo, int hi, const Krylov *kr, int which, const double2 *W0,
+                                const double2 *W1, double2 *y)
+{
+    if (kr->done || kr->restart) return;  // queued ahead of the convergence test
+    const double2 c0 = kr->wc[which][0], c1 = kr->wc[which][1];
+    const int k = kr->n_sinks, w = hi - lo;
+    const int64_t n = (int64_t)w * n_modes;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(e / w), i = lo + (int)(e % w);
+        const int64_t q = (int64_t)j * Nr + i;
+        double2 corr = cmul(W0[q], c0);
+        if (k > 1) corr = cadd(corr, cmul(W1[q], c1));
+        y[q] = csub(y[q], corr);
+    }
+}
 
 __global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
 {
@@ -2093,7 +2133,7 @@ __device__ void wood_scalar_dev(Krylov *kr, int which, const double2 *proj)
 
 __global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj)
 {
-    if (threadIdx.x == 0) wood_scalar_dev(kr, which, proj);
+    if (threadIdx.x == 0 && !(kr->done || kr->restart)) wood_scalar_dev(kr, which, proj);
 }
 
 // ------------------------------------------------------------------ absorbers
@@ -2335,8 +2375,9 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics(Grid g, CouplingT
 }
 
 // out[q] = sum_b partials[q][b]: one CTA per slot, coalesced loads, fixed-order tree.
-__global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out)
+__global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out, const Krylov *gate)
 {
+    if (gate && gate_closed(gate, GATE_ACCEPTED)) return;
     __shared__ double scratch[32];
     const int q = blockIdx.x;
     if (q >= nslots) return;
@@ -2379,6 +2420,7 @@ __global__ void k_jacobi_diag(Grid g, CouplingTable ct, const double *hh, double
 // stored to in.out) as in the block solves.
 __global__ void k_jacobi_apply(int64_t n, const double2 *dj, const double2 *b, double2 *out, PrecondInput in)
 {
+    if (!resolve_input(in)) return;
     double2 beta = cmake(0, 0), omega = cmake(0, 0), alpha = cmake(0, 0);
     if (in.mode != PI_PLAIN) {
         beta = in.kr->beta;

@@ -30,6 +30,11 @@ struct Krylov {
     int eigen_path;       // 1: Eigen's restart rule (no sinks), 0: the sink path's
     int zero_rhs;
     double rhs_norm;
+    int pturn;            // which of the two search-direction buffers the next PI_P solve writes
+    int accepted;         // KS_RESID: the candidate passed the residual (and pivot) check
+    double residual;      // KS_RESID: | |rhs| A x - rhs | / |rhs|
+    double accept;        // acceptance bound of the true relative residual
+    const int *status;    // pivot-failure word of the factorisation (device)
 };
 
 // Right-hand side of a preconditioner solve: b itself, or a BiCGSTAB combination
@@ -41,9 +46,20 @@ struct PrecondInput {
     const struct Krylov *kr;
     const double2 *r, *p_old, *v;
     double2 *out;
+    // PI_P with p_alt set: the search directions alternate between p_old and p_alt by
+    // kr->pturn (out = pturn ? p_alt : p_old, the previous direction the other one);
+    // `first`: no previous direction (p = r)
+    double2 *p_alt;
+    int first;
+    int gate;  // GateMode of the launch (GATE_ITER for the iteration's solves)
 };
 
-enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3, KS_INIT = 4, KS_NONE = 5 };
+// Launches queued ahead of the host's convergence test skip themselves on the device:
+// GATE_ITER while the solve is done or must restart, GATE_DONE until it is done,
+// GATE_ACCEPTED until its candidate passed the residual check.
+enum GateMode : int { GATE_NONE = 0, GATE_ITER = 1, GATE_DONE = 2, GATE_ACCEPTED = 3 };
+
+enum KrylovStage : int { KS_BETA = 0, KS_ALPHA = 1, KS_OMEGA = 2, KS_UPDATE = 3, KS_INIT = 4, KS_NONE = 5, KS_RESID = 6 };
 // Completion tickets (one counter per kind of launch that finishes a stage).
 enum Ticket : int { TK_APPLY_T = 0, TK_UPDATE_T = 1, TK_START_T = 2, TK_WOOD_T = 3, TK_DIAG_T = 4, TK_COUNT_T = 8 };
 
@@ -65,9 +81,10 @@ void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, co
                         const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
                         const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
                         const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0, int slo1,
-                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge);
+                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge, const Krylov *gate);
 __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
-                            const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots);
+                            const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots, const Krylov *gate,
+                            int gate_mode);
 __global__ void k_precond_factor(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off,
                                  int chunk, int window, double2 *dinv, int *status);
 __global__ void k_precond_factor_diag(const double2 *diag, int Nr, double2 off, int chunk, int window,
@@ -78,7 +95,8 @@ __global__ void k_dots(int64_t n, int nq, const double2 *a0, const double2 *b0, 
                        const double2 *b1, const double2 *a2, const double2 *b2, double *partials);
 __global__ void k_sum_partials(const double *partials, int nblocks, int nslots, double *out);
 __global__ void k_axpby(int64_t n, double2 a, const double2 *x, double2 b, const double2 *w, double2 *y);
-__global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y);
+__global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y,
+                             const Krylov *kr);
 __global__ void k_bicg_p(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *p);
 __global__ void k_bicg_s(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *s);
 __global__ void k_bicg_update(int64_t n, Krylov *kr, double2 *x, const double2 *y, const double2 *z, double2 *r,
@@ -126,12 +144,15 @@ __global__ void k_diagnostics(Grid g, CouplingTable ct, const double *hh, double
                               const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
                               const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0,
                               int slo1, int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge);
-__global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out);
+__global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out, const Krylov *gate);
 __global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage);
 
 __global__ void k_fp64_peak(double *out, int iters, double b, double c);
 
 __global__ void k_jacobi_diag(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 *dj);
 __global__ void k_jacobi_apply(int64_t n, const double2 *dj, const double2 *b, double2 *out, PrecondInput in);
+
+__global__ void k_woodbury_band(int Nr, int n_modes, int lo, int hi, const Krylov *kr, int which, const double2 *W0,
+                                const double2 *W1, double2 *y);
 
 }  // namespace cnm
