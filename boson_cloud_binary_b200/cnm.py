@@ -74,7 +74,8 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_set_power_average_orbits", "cnm_build_damping_mask", "cnm_build_cap", "cnm_prepare_run",
            "cnm_refresh", "cnm_step", "cnm_should_stop", "cnm_apply", "cnm_sink_strength", "cnm_sink_active",
            "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
-           "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel")
+           "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel",
+           "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy")
 
 def measure_fp64_peak():
     """FP64 FMA throughput of the current device, TFLOP/s (cnm_measure_fp64_peak)."""
@@ -138,6 +139,11 @@ def load_library():
     L.cnm_plan_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     L.cnm_measure_fp64_peak.argtypes = [dp]
     L.cnm_set_operator_kernel.argtypes = [p, i32]
+    L.cnm_batch_create.argtypes = [C.POINTER(cnm_params), i32, C.POINTER(C.c_void_p)]
+    L.cnm_batch_size.argtypes = [p, C.POINTER(i32)]
+    L.cnm_batch_handle.argtypes = [p, i32, C.POINTER(C.c_void_p)]
+    L.cnm_batch_step.argtypes = [p, i32, C.c_void_p]
+    L.cnm_batch_destroy.argtypes = [p]
     _lib = L
     return L
 
@@ -165,18 +171,23 @@ class CrankNicolsonModes:
     """B200 drop-in of the reference's CrankNicolsonModes (FP64 path)."""
 
     def __init__(self, Nx, L, dt, epsilon, l_max, mu, M_c, q, a, R, counter, absorption, save_every,
-                 ramp_periods, epsilon_smear, config_file=None):
+                 ramp_periods, epsilon_smear, config_file=None, _handle=None):
         lib = load_library()
-        prm = cnm_params(int(Nx), float(L), float(dt), float(epsilon), int(l_max), float(mu), float(M_c),
-                         float(q), float(a), float(R), int(bool(counter)), int(bool(absorption)),
-                         int(save_every), float(ramp_periods), float(epsilon_smear), 0)
-        h = C.c_void_p()
-        rc = lib.cnm_create(C.byref(prm), C.byref(h))
-        if rc != CNM_OK:
-            msg = lib.cnm_create_error().decode()
-            if rc == CNM_EINVAL:
-                raise ValueError(msg)
-            raise CudaError(msg)
+        if _handle is None:
+            prm = cnm_params(int(Nx), float(L), float(dt), float(epsilon), int(l_max), float(mu), float(M_c),
+                             float(q), float(a), float(R), int(bool(counter)), int(bool(absorption)),
+                             int(save_every), float(ramp_periods), float(epsilon_smear), 0)
+            h = C.c_void_p()
+            rc = lib.cnm_create(C.byref(prm), C.byref(h))
+            if rc != CNM_OK:
+                msg = lib.cnm_create_error().decode()
+                if rc == CNM_EINVAL:
+                    raise ValueError(msg)
+                raise CudaError(msg)
+            self.__dict__["_owned"] = True
+        else:
+            h = _handle   # a binary of a Batch: the batch owns and destroys it
+            self.__dict__["_owned"] = False
         self.__dict__["_h"] = h
         self.__dict__["_lib"] = lib
         n = C.c_int32()
@@ -193,9 +204,9 @@ class CrankNicolsonModes:
 
     def __del__(self):
         h = self.__dict__.get("_h")
-        if h:
+        if h and self.__dict__.get("_owned", True):
             self._lib.cnm_destroy(h)
-            self.__dict__["_h"] = None
+        self.__dict__["_h"] = None
 
     def _check(self, rc):
         if rc == CNM_OK:
@@ -378,3 +389,56 @@ class CrankNicolsonModes:
         ms = C.c_double()
         self._check(self._lib.cnm_timer_stop(self._h, C.byref(ms)))
         return ms.value
+
+
+class Batch:
+    """Independent binaries stepped together (cnm_batch_*): ``Batch([args0, args1, ...])``
+    with the constructor arguments of CrankNicolsonModes per binary.  ``binaries[i]`` is a
+    CrankNicolsonModes view of binary i for set-up and read-out; ``step(k)`` advances all
+    of them by one step and returns their step diagnostics (scalars only)."""
+
+    def __init__(self, arg_lists):
+        lib = load_library()
+        n = len(arg_lists)
+        prms = (cnm_params * n)()
+        for i, a in enumerate(arg_lists):
+            (Nx, L, dt, epsilon, l_max, mu, M_c, q, aa, R, counter, absorption, save_every,
+             ramp_periods, epsilon_smear) = a[:15]
+            prms[i] = cnm_params(int(Nx), float(L), float(dt), float(epsilon), int(l_max), float(mu), float(M_c),
+                                 float(q), float(aa), float(R), int(bool(counter)), int(bool(absorption)),
+                                 int(save_every), float(ramp_periods), float(epsilon_smear), 0)
+        b = C.c_void_p()
+        rc = lib.cnm_batch_create(prms, n, C.byref(b))
+        if rc != CNM_OK:
+            msg = lib.cnm_create_error().decode()
+            raise ValueError(msg) if rc == CNM_EINVAL else CudaError(msg)
+        self._lib, self._b = lib, b
+        self.binaries = []
+        for i, a in enumerate(arg_lists):
+            h = C.c_void_p()
+            lib.cnm_batch_handle(b, i, C.byref(h))
+            self.binaries.append(CrankNicolsonModes(*a[:15], _handle=h))
+
+    def step(self, step_id):
+        n = len(self.binaries)
+        diags = (cnm_diag * n)()
+        rc = self._lib.cnm_batch_step(self._b, int(step_id), C.cast(diags, C.c_void_p))
+        if rc != CNM_OK:
+            raise SolveError(f"batch step {step_id} failed (status {rc})")
+        out = []
+        for i, c in enumerate(self.binaries):
+            d = diags[i]
+            out.append({f: getattr(d, f) for f, _ in cnm_diag._fields_})
+            t = c.__dict__["t"]
+            while len(t) <= step_id:
+                t.append(0.0)
+            t[step_id] = d.t
+        return out
+
+    def __del__(self):
+        b = getattr(self, "_b", None)
+        if b:
+            for c in self.binaries:
+                c.__dict__["_h"] = None
+            self._lib.cnm_batch_destroy(b)
+            self._b = None

@@ -277,6 +277,7 @@ struct Solver {
     bool jacobi = false;  // fallback solve: point-Jacobi preconditioner in place of the radial blocks
     int wband_lo = 0, wband_hi = 0;  // nodes where the Woodbury vectors W_a are applied
     int iter_hint = 2;               // iterations of the previous solve (first batch size)
+    Krylov h_kr_init;                // host source of the Krylov struct's asynchronous upload
     // The reference's A and B are refreshed only by initialize() and step()
     // (update_CN_values), not by the operator rebuild of run(); a CAP built after
     // initialize() reaches H at run() but A and B only at the next step.
@@ -1246,9 +1247,16 @@ struct Solver {
     // radial-block preconditioner or, when `jacobi` is set, the point-Jacobi one.  The
     // iterations go out in batches (as many as the previous step needed) followed by
     // the gated tail, with one host synchronisation per batch for the convergence and
-    // restart test.  True when the candidate was accepted (pivots finite and true
-    // residual <= accept_residual); the tail's read-backs are then in hs.
-    bool solve_attempt(int max_it, const Absorber *const *sk, int k, double *hs)
+    // restart test.  begin_attempt queues the set-up and the first batch; finish_attempt
+    // waits, queues further batches (and restarts) until the solve is done, and tells
+    // whether the candidate was accepted (pivots finite and true residual <=
+    // accept_residual); the tail's read-backs are then in hs.
+    struct AttemptState {
+        int restarts = 0;
+        int max_it = 0;
+    } att;
+
+    void begin_attempt(int max_it, const Absorber *const *sk, int k, double *hs)
     {
         const double dtv = op.dt;
         Krylov *dk = d_kr.p;
@@ -1260,7 +1268,8 @@ struct Solver {
         kr.eigen_path = k == 0;
         kr.accept = accept_residual;
         kr.status = d_status.p;
-        CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
+        h_kr_init = kr;
+        CK(cudaMemcpyAsync(dk, &h_kr_init, sizeof(kr), cudaMemcpyHostToDevice, stream));
         // b = rhs / |rhs|, x = psi / |rhs|, r = r0 = b - A_full x in one pass; its last
         // CTA runs KS_INIT (and the first beta) on |r0|^2 and |b|^2
         k_krylov_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, d_red.p + RED_RHS, rhs.p, psi.p, b.p, x.p,
@@ -1269,17 +1278,21 @@ struct Solver {
         launch_check();
         factorize(dtv);
         if (k > 0) wood_setup(sk, k, dtv);
+        att = AttemptState();
+        att.max_it = max_it;
+        const int batch = std::max(1, std::min(4, iter_hint));
+        for (int q = 0; q < batch; ++q) enqueue_iteration(sk, k, dtv, q == 0);
+        enqueue_tail(sk, k, dtv, hs);
+    }
+
+    bool finish_attempt(const Absorber *const *sk, int k, double *hs)
+    {
+        const double dtv = op.dt;
+        Krylov *dk = d_kr.p;
+        Krylov kr;
         const bool eigen_path = k == 0;
         const double eps = std::numeric_limits<double>::epsilon();
-        int restarts = 0;
-        bool first = true;
-        int batch = std::max(1, std::min(4, iter_hint));
         for (;;) {
-            for (int q = 0; q < batch; ++q) {
-                enqueue_iteration(sk, k, dtv, first);
-                first = false;
-            }
-            enqueue_tail(sk, k, dtv, hs);
             sync();
             std::memcpy(&kr, hs, sizeof(kr));
             if (kr.done) break;
@@ -1296,13 +1309,15 @@ struct Solver {
                 kr.rho = cmake(nr2, 0.0);
                 if (eigen_path) {
                     kr.restart_thr = eps * eps * nr2;
-                    if (restarts++ == 0) kr.iterations = 0;
+                    if (att.restarts++ == 0) kr.iterations = 0;
                 }
                 kr.beta = cmul(cdiv(kr.rho, rho_old), cdiv(kr.alpha, kr.omega));
                 kr.restart = 0;
-                CK(cudaMemcpyAsync(dk, &kr, sizeof(kr), cudaMemcpyHostToDevice, stream));
+                h_kr_init = kr;
+                CK(cudaMemcpyAsync(dk, &h_kr_init, sizeof(kr), cudaMemcpyHostToDevice, stream));
             }
-            batch = 2;
+            for (int q = 0; q < 2; ++q) enqueue_iteration(sk, k, dtv, false);
+            enqueue_tail(sk, k, dtv, hs);
         }
         last_iterations = kr.iterations;
         last_residual = kr.residual;
@@ -1315,24 +1330,32 @@ struct Solver {
     // retries with a full ILUT preconditioner and 5000 iterations -- here the retry is a
     // point-Jacobi BiCGSTAB on the device with the same iteration budget.  With
     // use_block_preconditioner off the retry path is the only one, as in the reference.
-    // On return psi holds the accepted state and hs the step's read-backs.
-    void solve_CN(const Absorber *const *sk, int k, double *hs)
+    // begin_solve queues the first attempt; finish_solve completes it (and the retry)
+    // and leaves psi holding the accepted state and hs the step's read-backs.
+    void begin_solve(const Absorber *const *sk, int k, double *hs)
+    {
+        jacobi = !use_block;
+        begin_attempt(use_block ? max_iterations : 5000, sk, k, hs);
+    }
+
+    void finish_solve(const Absorber *const *sk, int k, double *hs)
     {
         bool ok = false;
-        if (use_block) ok = solve_attempt(max_iterations, sk, k, hs);
-        if (!ok) {
-            if (use_block)
-                std::fprintf(stderr, "\nRadial preconditioner did not converge; retrying with the point-Jacobi fallback.\n");
-            jacobi = true;
-            try {
-                ok = solve_attempt(5000, sk, k, hs);
-            } catch (...) {
-                jacobi = false;
-                throw;
+        try {
+            ok = finish_attempt(sk, k, hs);
+            if (!ok && !jacobi) {
+                std::fprintf(stderr,
+                             "\nRadial preconditioner did not converge; retrying with the point-Jacobi fallback.\n");
+                jacobi = true;
+                begin_attempt(5000, sk, k, hs);
+                ok = finish_attempt(sk, k, hs);
             }
+        } catch (...) {
             jacobi = false;
-            if (!ok) throw Error(CNM_ESOLVE, "Crank-Nicolson solve failed the relative residual check");
+            throw;
         }
+        jacobi = false;
+        if (!ok) throw Error(CNM_ESOLVE, "Crank-Nicolson solve failed the relative residual check");
     }
 
     // Woodbury set-up (src/CrankNicolsonModes_matrices.cpp:133-145): W_a = P^{-1} v_a and
@@ -1449,11 +1472,26 @@ struct Solver {
         sync();
     }
 
+    // step (src/CrankNicolsonModes.cpp:145-234) in two halves: step_begin queues the
+    // operator rebuild, the right-hand side and the first batch of the solve (with its
+    // gated tail) without waiting; step_end waits, completes the solve and runs the
+    // host side (orbit, diagnostics).  step() is both; batches of binaries call all the
+    // begins before the ends so that their launches share the device.
+    double step_start_t = 0.0;
+    double *step_hs = nullptr;
+
     void step(int step_id, cnm_diag *dg, double *ef, double *fl, double *nm, double *en)
     {
+        step_begin(step_id);
+        step_end(step_id, dg, ef, fl, nm, en);
+    }
+
+    void step_begin(int step_id)
+    {
+        (void)step_id;
         if (!initialized) throw Error(CNM_ELOGIC, "initialize() must be called before step()");
         if (idx_ex < 1) throw Error(CNM_ELOGIC, "run() (cnm_prepare_run) must set the extraction radius first");
-        const double step_start = t_i;
+        step_start_t = t_i;
         t_i += dt;
         theta += (counter ? -1.0 : 1.0) * Omega * dt;
         phase += Omega * dt;
@@ -1494,8 +1532,19 @@ struct Solver {
             }
             launch_apply(a);
         }
-        double *hs = stage(readback_doubles());
-        solve_CN(sk, k, hs);
+        step_hs = stage(readback_doubles());
+        begin_solve(sk, k, step_hs);
+    }
+
+    void step_end(int step_id, cnm_diag *dg, double *ef, double *fl, double *nm, double *en)
+    {
+        const double step_start = step_start_t;
+        const Absorber *all[2] = {&abs1, &abs2};
+        const bool have_sinks = absorption && cpl.mode00 >= 0;
+        const Absorber *sk[2];
+        const int k = active_sinks(sk);
+        double *hs = step_hs;
+        finish_solve(sk, k, hs);
         const int nslots = 2 * n_modes + 3;
         const size_t kd = (sizeof(Krylov) + 7) / 8;
         hs += kd;
@@ -2048,6 +2097,71 @@ int cnm_timer_stop(cnm_handle *h, double *ms)
         CK(cudaEventElapsedTime(&f, s.region_a, s.region_b));
         *ms = f;
     });
+}
+
+struct cnm_batch {
+    std::vector<cnm_handle *> hs;
+};
+
+int cnm_batch_create(const cnm_params *params, int32_t count, cnm_batch **out)
+{
+    if (!params || !out || count < 1) {
+        g_create_error = "cnm_batch_create: need params[count >= 1] and an output pointer";
+        return CNM_EINVAL;
+    }
+    cnm_batch *b = new cnm_batch();
+    for (int32_t i = 0; i < count; ++i) {
+        cnm_handle *h = nullptr;
+        const int rc = cnm_create(&params[i], &h);
+        if (rc != CNM_OK) {
+            for (cnm_handle *q : b->hs) cnm_destroy(q);
+            delete b;
+            g_create_error = "binary " + std::to_string(i) + ": " + g_create_error;
+            return rc;
+        }
+        b->hs.push_back(h);
+    }
+    *out = b;
+    return CNM_OK;
+}
+
+int cnm_batch_size(const cnm_batch *b, int32_t *count)
+{
+    if (!b || !count) return CNM_EINVAL;
+    *count = (int32_t)b->hs.size();
+    return CNM_OK;
+}
+
+int cnm_batch_handle(cnm_batch *b, int32_t index, cnm_handle **h)
+{
+    if (!b || !h || index < 0 || index >= (int32_t)b->hs.size()) return CNM_EINVAL;
+    *h = b->hs[(size_t)index];
+    return CNM_OK;
+}
+
+int cnm_batch_step(cnm_batch *b, int32_t step_id, cnm_diag *diags)
+{
+    if (!b) return CNM_EINVAL;
+    const size_t n = b->hs.size();
+    std::vector<int> rc(n, CNM_OK);
+    for (size_t i = 0; i < n; ++i)
+        rc[i] = guarded(b->hs[i], [&](cnm::Solver &s) { s.step_begin(step_id); });
+    for (size_t i = 0; i < n; ++i)
+        if (rc[i] == CNM_OK)
+            rc[i] = guarded(b->hs[i], [&](cnm::Solver &s) {
+                s.step_end(step_id, diags ? &diags[i] : nullptr, nullptr, nullptr, nullptr, nullptr);
+            });
+    for (size_t i = 0; i < n; ++i)
+        if (rc[i] != CNM_OK) return rc[i];
+    return CNM_OK;
+}
+
+int cnm_batch_destroy(cnm_batch *b)
+{
+    if (!b) return CNM_EINVAL;
+    for (cnm_handle *h : b->hs) cnm_destroy(h);
+    delete b;
+    return CNM_OK;
 }
 
 int cnm_set_operator_kernel(cnm_handle *h, int32_t specialised)

@@ -175,6 +175,23 @@ int cnm_step(cnm_handle *h, int32_t step_id, cnm_diag *diag, double *energy_flux
  * on an evolving binary orbit. */
 int cnm_should_stop(const cnm_handle *h, int32_t *stop);
 
+/* --- batched sweep (independent binaries) ------------------------------------------
+ * A batch owns one handle per binary, each with its own stream.  cnm_batch_step
+ * advances every binary by one step: it queues the device work of all binaries
+ * before it waits on any, so binaries too small to fill the device run side by side.
+ * The per-binary handles are set up and read through the single-binary calls
+ * (cnm_set_initial_state_full, cnm_initialize, cnm_prepare_run, cnm_get_state, ...). */
+typedef struct cnm_batch cnm_batch;
+/* params[count]: one binary each.  On failure no batch is created. */
+int cnm_batch_create(const cnm_params *params, int32_t count, cnm_batch **out);
+int cnm_batch_size(const cnm_batch *b, int32_t *count);
+int cnm_batch_handle(cnm_batch *b, int32_t index, cnm_handle **h);
+/* diags[count] may be NULL; the per-mode diagnostics of a binary are not returned here
+ * (step it alone with cnm_step for those).  Every binary's step is completed even when
+ * another one fails; the first failure's status is returned. */
+int cnm_batch_step(cnm_batch *b, int32_t step_id, cnm_diag *diags);
+int cnm_batch_destroy(cnm_batch *b);
+
 /* --- checkpoints --------------------------------------------------------------- */
 
 /* save_checkpoint (src/CrankNicolsonModes_restart.cpp:139-177): the exact bytes of
