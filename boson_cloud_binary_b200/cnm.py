@@ -75,7 +75,25 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_refresh", "cnm_step", "cnm_should_stop", "cnm_apply", "cnm_sink_strength", "cnm_sink_active",
            "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
            "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel",
-           "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy")
+           "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy",
+           "cnm_displaced_100_state")
+
+def displaced_100_state(r, modes, mu, x_bh):
+    """displaced_100_state (src/DisplacedAtom.cpp:12-76) on the device: the mode projection
+    of a hydrogenic 1s state centred at x_bh on the x axis, complex n_modes x Nr."""
+    L = load_library()
+    r = np.ascontiguousarray(np.asarray(r, float))
+    l = np.array([a for a, _ in modes], np.int32)
+    m = np.array([b for _, b in modes], np.int32)
+    out = np.zeros(2 * len(r) * len(modes))
+    rc = L.cnm_displaced_100_state(_dptr(r), len(r), l.ctypes.data_as(C.POINTER(C.c_int32)),
+                                   m.ctypes.data_as(C.POINTER(C.c_int32)), len(modes), float(mu), float(x_bh),
+                                   _dptr(out))
+    if rc != CNM_OK:
+        msg = L.cnm_create_error().decode()
+        raise ValueError(msg) if rc == CNM_EINVAL else CudaError(msg)
+    return out.view(np.complex128)
+
 
 def measure_fp64_peak():
     """FP64 FMA throughput of the current device, TFLOP/s (cnm_measure_fp64_peak)."""
@@ -144,6 +162,7 @@ def load_library():
     L.cnm_batch_handle.argtypes = [p, i32, C.POINTER(C.c_void_p)]
     L.cnm_batch_step.argtypes = [p, i32, C.c_void_p]
     L.cnm_batch_destroy.argtypes = [p]
+    L.cnm_displaced_100_state.argtypes = [dp, i32, C.POINTER(i32), C.POINTER(i32), i32, C.c_double, C.c_double, dp]
     _lib = L
     return L
 

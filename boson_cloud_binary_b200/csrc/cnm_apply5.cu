@@ -341,7 +341,7 @@ template <int L>
 __global__ void __launch_bounds__(A5_THREADS) k_diag5(Grid g, const double *gtab, DiagArgs d)
 {
     if (d.gate && gate_closed(d.gate, GATE_ACCEPTED)) return;
-    constexpr int G = A5Groups<L>::value;
+    constexpr int G = D5Groups<L>::value;
     using Lay = A5Layout<L, G>;
     extern __shared__ double smem5[];
     double *gs = smem5;
@@ -441,6 +441,17 @@ int apply5_groups(int l_max)
     }
 }
 
+int diag5_groups(int l_max)
+{
+    switch (l_max) {
+#define CNM_D5G(L) \
+    case L: return D5Groups<L>::value;
+        CNM_D5G(1) CNM_D5G(2) CNM_D5G(3) CNM_D5G(4) CNM_D5G(5) CNM_D5G(6) CNM_D5G(7) CNM_D5G(8)
+#undef CNM_D5G
+    default: return 0;
+    }
+}
+
 size_t apply5_smem(int l_max)
 {
     switch (l_max) {
@@ -452,9 +463,8 @@ size_t apply5_smem(int l_max)
     }
 }
 
-std::vector<double> apply5_table(int l_max, const Coupling &c)
+std::vector<double> apply5_table(int l_max, int G, const Coupling &c)
 {
-    const int G = apply5_groups(l_max);
     std::vector<double> t;
     if (G == 0) return t;
     const int n = c.n_modes, Lm = c.l_max;
@@ -510,7 +520,15 @@ void launch_apply5(int l_max, cudaStream_t st, const Grid &g, const double *gtab
 size_t diag5_smem(int l_max)
 {
     const int n = (l_max + 1) * (l_max + 2) / 2;
-    return apply5_smem(l_max) + (size_t)(2 * n + 3) * (A5_THREADS / 32) * sizeof(double);
+    size_t g = 0;
+    switch (l_max) {
+#define CNM_D5S(L) \
+    case L: g = (size_t)A5Layout<L, D5Groups<L>::value>::gsize_max(); break;
+        CNM_D5S(1) CNM_D5S(2) CNM_D5S(3) CNM_D5S(4) CNM_D5S(5) CNM_D5S(6) CNM_D5S(7) CNM_D5S(8)
+#undef CNM_D5S
+    default: return 0;
+    }
+    return g * sizeof(double) + (size_t)n * sizeof(double2) + (size_t)(2 * n + 3) * (A5_THREADS / 32) * sizeof(double);
 }
 
 cudaError_t set_diag5_smem()
@@ -526,7 +544,7 @@ cudaError_t set_diag5_smem()
 unsigned launch_diag5(int l_max, cudaStream_t st, const Grid &g, const double *gtab, const DiagArgs &d)
 {
     const int nodes = d.idx_ex + 1;
-    const dim3 blocks((unsigned)((nodes + A5_THREADS - 1) / A5_THREADS), (unsigned)apply5_groups(l_max));
+    const dim3 blocks((unsigned)((nodes + A5_THREADS - 1) / A5_THREADS), (unsigned)diag5_groups(l_max));
     const size_t smem = diag5_smem(l_max);
     switch (l_max) {
 #define CNM_D5L(L) \

@@ -91,6 +91,11 @@ __host__ __device__ constexpr int rowoff(int L, int G, int g, int l1, int j)
 // 20000-node grid fills one wave.
 template <int L>
 struct A5Groups {
+    static constexpr int value = L <= 2 ? 1 : (L <= 4 ? 2 : (L <= 6 ? 4 : 9));
+};
+// The diagnostics pass keeps a second accumulator per row, so it takes fewer groups.
+template <int L>
+struct D5Groups {
     static constexpr int value = L <= 2 ? 1 : (L <= 4 ? 2 : (L <= 6 ? 4 : 7));
 };
 
@@ -151,7 +156,9 @@ struct DiagArgs {
 int apply5_groups(int l_max);
 size_t apply5_smem(int l_max);
 unsigned apply5_blocks(int l_max, int Nr);
-std::vector<double> apply5_table(int l_max, const Coupling &c);
+int diag5_groups(int l_max);
+// the weight table of a layout with G row groups (apply5_groups or diag5_groups)
+std::vector<double> apply5_table(int l_max, int G, const Coupling &c);
 cudaError_t set_apply5_smem();
 void launch_apply5(int l_max, cudaStream_t st, const Grid &g, const double *gtab, const ApplyArgs &a);
 size_t diag5_smem(int l_max);

@@ -285,7 +285,7 @@ struct Solver {
     // operator kernel specialised for this l_max (0 groups: the generic plan-driven kernel)
     int a5_groups = 0;
     bool a5_enabled = true;
-    DevBuf<double> d_a5tab;
+    DevBuf<double> d_a5tab, d_d5tab;  // weights of the specialised operator and diagnostics layouts
     DevBuf<unsigned> d_tickets;  // completion tickets (zero between launches)
     DevBuf<double> d_wpart;      // partials of the Woodbury projections
     // red slots past the diagnostics' 2 n + 3 sums: |rhs|^2 and the candidate's residual^2
@@ -442,7 +442,8 @@ struct Solver {
         plan_operator(nsm);
         a5_groups = apply5_groups(l_max);
         if (a5_groups > 0) {
-            upload(d_a5tab, apply5_table(l_max, cpl));
+            upload(d_a5tab, apply5_table(l_max, apply5_groups(l_max), cpl));
+            upload(d_d5tab, apply5_table(l_max, diag5_groups(l_max), cpl));
             CK(set_apply5_smem());
             CK(set_diag5_smem());
         }
@@ -1150,7 +1151,7 @@ struct Solver {
             da.dpsi_edge = d_edge.p;
             da.psi_edge = d_edge.p + n_modes;
             da.gate = d_kr.p;
-            dblocks = ::cnm::launch_diag5(l_max, stream, grid(), d_a5tab.p, da);
+            dblocks = ::cnm::launch_diag5(l_max, stream, grid(), d_d5tab.p, da);
         } else {
             ::cnm::launch_diagnostics(
                 l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p,
@@ -2097,6 +2098,61 @@ int cnm_timer_stop(cnm_handle *h, double *ms)
         CK(cudaEventElapsedTime(&f, s.region_a, s.region_b));
         *ms = f;
     });
+}
+
+int cnm_displaced_100_state(const double *r, int32_t Nr, const int32_t *l, const int32_t *m, int32_t n_modes,
+                            double mu, double x_bh, double *state)
+{
+    try {
+        if (!r || !l || !m || !state || !std::isfinite(mu) || mu <= 0 || !std::isfinite(x_bh) || Nr < 3 || n_modes < 1)
+            throw cnm::Error(CNM_EINVAL, "Invalid displaced 100 state parameters");
+        for (int i = 0; i < Nr; ++i)
+            if (!std::isfinite(r[i]) || r[0] < 0)
+                throw cnm::Error(CNM_EINVAL, "Radial coordinates must be finite and nonnegative");
+        for (int i = 1; i < Nr; ++i)
+            if (r[i] <= r[i - 1]) throw cnm::Error(CNM_EINVAL, "Radial coordinates must increase");
+        int lmax = 0;
+        for (int j = 0; j < n_modes; ++j) {
+            if (l[j] < 0 || std::abs(m[j]) > l[j]) throw cnm::Error(CNM_EINVAL, "Invalid spherical harmonic mode");
+            lmax = std::max(lmax, (int)l[j]);
+        }
+        const double a0 = 1.0 / (mu * mu), distance = std::abs(x_bh);
+        const double amplitude = 1.0 / std::sqrt(M_PI * a0 * a0 * a0);
+        const int nq = std::max(128, 2 * lmax + 32);
+        std::vector<double> gx, gw;
+        cnm::gauss_legendre01(nq, gx, gw);
+        cnm::DevBuf<double> d_r, d_gx, d_gw, d_mom;
+        d_r.alloc(Nr);
+        d_gx.alloc(nq);
+        d_gw.alloc(nq);
+        d_mom.alloc((size_t)(lmax + 1) * Nr);
+        CK(cudaMemcpy(d_r.p, r, Nr * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_gx.p, gx.data(), nq * sizeof(double), cudaMemcpyHostToDevice));
+        CK(cudaMemcpy(d_gw.p, gw.data(), nq * sizeof(double), cudaMemcpyHostToDevice));
+        const int threads = (nq + 31) / 32 * 32;
+        const size_t smem = (size_t)(lmax + 1) * (threads / 32) * sizeof(double);
+        cnm::k_displaced_100<<<Nr - 2, threads, smem>>>(d_r.p, Nr, lmax, a0, distance, amplitude, nq, d_gx.p, d_gw.p,
+                                                        d_mom.p);
+        CK(cudaGetLastError());
+        std::vector<double> mom((size_t)(lmax + 1) * Nr);
+        CK(cudaMemcpy(mom.data(), d_mom.p, mom.size() * sizeof(double), cudaMemcpyDeviceToHost));
+        std::fill(state, state + 2 * (int64_t)Nr * n_modes, 0.0);
+        for (int j = 0; j < n_modes; ++j) {
+            // Y*_lm(pi/2, phi_BH) with phi_BH = 0 or pi (real, exact parity)
+            double y = cnm::sph_plm_equator(l[j], std::abs(m[j]));
+            if (m[j] < 0 && (std::abs(m[j]) & 1)) y = -y;
+            if (x_bh < 0 && (std::abs(m[j]) & 1)) y = -y;
+            for (int i = 1; i < Nr - 1; ++i)
+                state[2 * ((int64_t)j * Nr + i)] = r[i] * mom[(size_t)l[j] * Nr + i] * y;
+        }
+        return CNM_OK;
+    } catch (const cnm::Error &e) {
+        g_create_error = e.what();
+        return e.code;
+    } catch (const std::exception &e) {
+        g_create_error = e.what();
+        return CNM_ECUDA;
+    }
 }
 
 struct cnm_batch {

@@ -2402,6 +2402,60 @@ __global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, 
     }
 }
 
+// ------------------------------------------------------------------ initial states
+
+// Legendre moments of a hydrogenic 1s density centred at distance `distance` from the
+// origin (src/DisplacedAtom.cpp:45-70): one CTA per interior node, one Gauss-Legendre
+// node of the body-centred distance s per thread (blockDim.x >= nq), the Legendre
+// recurrence advanced degree by degree, fixed-order sums.  mom: (lmax + 1) x Nr.
+__global__ void k_displaced_100(const double *r, int Nr, int lmax, double a0, double distance, double amplitude,
+                                int nq, const double *gl_x, const double *gl_w, double *mom)
+{
+    extern __shared__ double shd[];  // (lmax + 1) * nwarps
+    const int i = blockIdx.x + 1;
+    if (i > Nr - 2) return;
+    const double ri = r[i];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    if (distance == 0.0) {
+        if (threadIdx.x == 0) {
+            mom[i] = 4.0 * M_PI * amplitude * exp(-ri / a0);
+            for (int l = 1; l <= lmax; ++l) mom[(int64_t)l * Nr + i] = 0.0;
+        }
+        return;
+    }
+    const double low = fabs(ri - distance), high = fmin(ri + distance, low + 40.0 * a0);
+    const int k = threadIdx.x;
+    double weight = 0.0, u = 0.0;
+    if (k < nq) {
+        const double sv = low + (high - low) * gl_x[k];
+        u = fmin(1.0, fmax(-1.0, (ri * ri + distance * distance - sv * sv) / (2.0 * ri * distance)));
+        weight = 2.0 * M_PI * (high - low) * gl_w[k] * sv / (ri * distance) * amplitude * exp(-sv / a0);
+    }
+    double prev = 1.0, cur = u;
+    for (int l = 0; l <= lmax; ++l) {
+        double pl;
+        if (l == 0) {
+            pl = 1.0;
+        } else if (l == 1) {
+            pl = u;
+        } else {
+            const double next = ((2 * l - 1) * u * cur - (l - 1) * prev) / l;
+            prev = cur;
+            cur = next;
+            pl = cur;
+        }
+        double part = k < nq ? weight * pl : 0.0;
+        part = warp_sum(part);
+        if (lane == 0) shd[l * nw + warp] = part;
+    }
+    __syncthreads();
+    for (int l = threadIdx.x; l <= lmax; l += blockDim.x) {
+        double sm = 0.0;
+        for (int w = 0; w < nw; ++w) sm += shd[l * nw + w];
+        mom[(int64_t)l * Nr + i] = sm;
+    }
+}
+
 // ------------------------------------------------------------------ fallback preconditioner
 
 // Inverse diagonal of A = 1 + i dt/2 (H0 + V + CAP): the point-Jacobi preconditioner of

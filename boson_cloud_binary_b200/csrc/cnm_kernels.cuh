@@ -155,4 +155,7 @@ __global__ void k_jacobi_apply(int64_t n, const double2 *dj, const double2 *b, d
 __global__ void k_woodbury_band(int Nr, int n_modes, int lo, int hi, const Krylov *kr, int which, const double2 *W0,
                                 const double2 *W1, double2 *y);
 
+__global__ void k_displaced_100(const double *r, int Nr, int lmax, double a0, double distance, double amplitude,
+                                int nq, const double *gl_x, const double *gl_w, double *mom);
+
 }  // namespace cnm

@@ -634,3 +634,18 @@ std::vector<dcomplex> load_initial_modes_binary(const std::string &filename, con
     }
     return psi;
 }
+
+std::vector<dcomplex> displaced_100_state(const std::vector<double> &r, const std::vector<mode> &modes, double mu,
+                                          double x_bh)
+{
+    std::vector<int32_t> l(modes.size()), m(modes.size());
+    for (size_t j = 0; j < modes.size(); ++j) {
+        l[j] = modes[j].l;
+        m[j] = modes[j].m;
+    }
+    std::vector<dcomplex> psi(r.size() * modes.size());
+    const int rc = cnm_displaced_100_state(r.data(), (int32_t)r.size(), l.data(), m.data(), (int32_t)modes.size(), mu,
+                                           x_bh, reinterpret_cast<double *>(psi.data()));
+    if (rc != CNM_OK) raise(rc, cnm_create_error());
+    return psi;
+}

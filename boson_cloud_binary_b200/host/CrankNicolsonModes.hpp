@@ -124,3 +124,8 @@ std::string create_output_folder();
 /// load_initial_modes_binary (src/InitialData.cpp:7-79): MODESBIN reader; stored modes
 /// not in `modes` are ignored, missing ones are zero.
 std::vector<dcomplex> load_initial_modes_binary(const std::string &filename, const std::vector<mode> &modes);
+
+/// displaced_100_state (src/DisplacedAtom.cpp:12-76), computed on the device: the mode
+/// projection of a hydrogenic 1s state centred at x_bh on the x axis.
+std::vector<dcomplex> displaced_100_state(const std::vector<double> &r, const std::vector<mode> &modes, double mu,
+                                          double x_bh);

@@ -175,6 +175,14 @@ int cnm_step(cnm_handle *h, int32_t step_id, cnm_diag *diag, double *energy_flux
  * on an evolving binary orbit. */
 int cnm_should_stop(const cnm_handle *h, int32_t *stop);
 
+/* --- initial states ----------------------------------------------------------------
+ * displaced_100_state (src/DisplacedAtom.cpp:12-76) on the device: the mode projection
+ * of a hydrogenic 1s state of reduced mass mu centred at x_bh on the x axis, on the
+ * radial nodes r[Nr] and modes (l[j], m[j]); state: interleaved complex, n_modes x Nr
+ * (host buffer).  CNM_EINVAL for the reference's invalid_argument cases. */
+int cnm_displaced_100_state(const double *r, int32_t Nr, const int32_t *l, const int32_t *m, int32_t n_modes,
+                            double mu, double x_bh, double *state);
+
 /* --- batched sweep (independent binaries) ------------------------------------------
  * A batch owns one handle per binary, each with its own stream.  cnm_batch_step
  * advances every binary by one step: it queues the device work of all binaries

@@ -1521,4 +1521,67 @@ void orc_gauss_legendre(int n, double a, double b, double *x, double *w)
     std::copy(wv.begin(), wv.end(), w);
 }
 
+// displaced_100_state (src/DisplacedAtom.cpp:12-76): the mode projection of a
+// hydrogenic 1s state centred at x_bh on the x axis.  For every interior node the
+// Legendre moments of the displaced density about the origin, by Gauss-Legendre
+// quadrature in the body-centred distance s (tail beyond 40 a0 dropped), times r and
+// Y*_lm(pi/2, phi_BH).  out: interleaved complex, n_modes x Nr.
+int orc_displaced_100_state(const double *r, int Nr, const int *l, const int *m, int n_modes, double mu, double x_bh,
+                            double *out)
+{
+    return guarded([&] {
+        if (!std::isfinite(mu) || mu <= 0 || !std::isfinite(x_bh) || Nr < 3 || n_modes < 1)
+            throw std::invalid_argument("Invalid displaced 100 state parameters");
+        for (int i = 0; i < Nr; ++i)
+            if (!std::isfinite(r[i]) || r[0] < 0) throw std::invalid_argument("Radial coordinates must be finite and nonnegative");
+        for (int i = 1; i < Nr; ++i)
+            if (r[i] <= r[i - 1]) throw std::invalid_argument("Radial coordinates must increase");
+        int lmax = 0;
+        for (int j = 0; j < n_modes; ++j) {
+            if (l[j] < 0 || std::abs(m[j]) > l[j]) throw std::invalid_argument("Invalid spherical harmonic mode");
+            lmax = std::max(lmax, l[j]);
+        }
+        const double a0 = 1.0 / (mu * mu), distance = std::abs(x_bh);
+        const double amplitude = 1.0 / std::sqrt(M_PI * a0 * a0 * a0);
+        const int nq = std::max(128, 2 * lmax + 32);
+        std::vector<double> nodes, weights;
+        gauss_legendre(nq, 0.0, 1.0, nodes, weights);
+        std::vector<double> direction(n_modes);
+        for (int j = 0; j < n_modes; ++j) {
+            double y = sph_plm_equator(l[j], std::abs(m[j]));
+            if (m[j] < 0 && (std::abs(m[j]) & 1)) y = -y;
+            if (x_bh < 0 && (std::abs(m[j]) & 1)) y = -y;
+            direction[j] = y;
+        }
+        std::fill(out, out + 2 * (int64_t)Nr * n_modes, 0.0);
+#pragma omp parallel for schedule(static)
+        for (int i = 1; i < Nr - 1; ++i) {
+            std::vector<double> mom(lmax + 1, 0.0);
+            if (distance == 0.0) {
+                mom[0] = 4 * M_PI * amplitude * std::exp(-r[i] / a0);
+            } else {
+                const double low = std::abs(r[i] - distance);
+                const double high = std::min(r[i] + distance, low + 40 * a0);
+                for (int k = 0; k < nq; ++k) {
+                    const double sv = low + (high - low) * nodes[k];
+                    const double u =
+                        std::clamp((r[i] * r[i] + distance * distance - sv * sv) / (2 * r[i] * distance), -1.0, 1.0);
+                    const double wgt =
+                        2 * M_PI * (high - low) * weights[k] * sv / (r[i] * distance) * amplitude * std::exp(-sv / a0);
+                    double prev = 1.0, cur = u;
+                    mom[0] += wgt;
+                    if (lmax > 0) mom[1] += wgt * cur;
+                    for (int q = 2; q <= lmax; ++q) {
+                        const double next = ((2 * q - 1) * u * cur - (q - 1) * prev) / q;
+                        mom[q] += wgt * next;
+                        prev = cur;
+                        cur = next;
+                    }
+                }
+            }
+            for (int j = 0; j < n_modes; ++j) out[2 * ((int64_t)j * Nr + i)] = r[i] * mom[l[j]] * direction[j];
+        }
+    });
+}
+
 }  // extern "C"

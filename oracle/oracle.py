@@ -284,3 +284,18 @@ class OracleCNM:
         lib().orc_coupling_terms(self._h, rows.ctypes.data_as(ip), cols.ctypes.data_as(ip),
                                  ls.ctypes.data_as(ip), _dptr(ang))
         return rows, cols, ls, ang
+
+
+def displaced_100_state(r, modes, mu, x_bh):
+    """displaced_100_state (src/DisplacedAtom.cpp:12-76) on the CPU: the mode projection
+    of a hydrogenic 1s state centred at x_bh on the x axis (complex, n_modes x Nr)."""
+    r = np.ascontiguousarray(np.asarray(r, float))
+    l = np.array([a for a, _ in modes], np.int32)
+    m = np.array([b for _, b in modes], np.int32)
+    out = np.zeros(2 * len(r) * len(modes))
+    ip = C.POINTER(C.c_int)
+    rc = lib().orc_displaced_100_state(_dptr(r), len(r), l.ctypes.data_as(ip), m.ctypes.data_as(ip), len(modes),
+                                       C.c_double(mu), C.c_double(x_bh), _dptr(out))
+    if rc != 0:
+        raise ValueError(lib().orc_last_error().decode())
+    return out.view(np.complex128)

@@ -240,6 +240,18 @@ int main(int argc, char **argv)
         require(threw, "resume without any snapshot did not fail");
     }
     modesbin_reader(work);
+    {  // displaced_100_state: the centred state is the analytic 1s radial function
+        std::vector<double> r(257);
+        for (int i = 0; i < 257; ++i) r[i] = 40.0 * i / 256;
+        std::vector<mode> modes;
+        for (int l = 0; l <= 4; ++l)
+            for (int m = -l; m <= l; m += 2) modes.push_back({l, m});
+        const std::vector<dcomplex> psi = displaced_100_state(r, modes, 0.5, 0.0);
+        double worst = 0.0;
+        for (int i = 1; i < 256; ++i)
+            worst = std::max(worst, std::abs(psi[i] - 2 * r[i] * std::exp(-r[i] / 4.0) / 8.0));
+        require(worst < 1e-13, "displaced_100_state: centred state differs from 2 r e^{-r/a0} / a0^{3/2}");
+    }
     std::printf(failures ? "host_check: %d failure(s)\n" : "host_check: OK\n", failures);
     return failures ? 1 : 0;
 }
