@@ -2272,8 +2272,9 @@ int cnm_plan_info(const cnm_handle *h, int32_t *scan_per, int32_t *scan_cluster,
     const cnm::Solver &s = *h->s;
     if (scan_per) *scan_per = s.pcl_per;
     if (scan_cluster) *scan_cluster = s.pcl_cs;
-    if (apply_groups) *apply_groups = s.plan3.n_groups;
-    if (apply_weights_in_smem) *apply_weights_in_smem = s.apply3_gsm ? 1 : 0;
+    const bool a5 = s.a5_groups > 0 && s.a5_enabled;
+    if (apply_groups) *apply_groups = a5 ? s.a5_groups : s.plan3.n_groups;
+    if (apply_weights_in_smem) *apply_weights_in_smem = a5 || s.apply3_gsm ? 1 : 0;
     return CNM_OK;
 }
 

@@ -251,9 +251,10 @@ int cnm_set_operator_kernel(cnm_handle *h, int32_t specialised);
  * the FP64 roofline of the operator kernels. */
 int cnm_measure_fp64_peak(double *tflops);
 /* Launch plan chosen at creation for this device: nodes per thread and CTAs per cluster
- * of the exact preconditioner scans (0, 0 when the windowed scans are used), CTA groups
- * per node tile of the operator kernel and whether a group's weights sit in shared
- * memory (1) or are read through L1 (0). */
+ * of the exact preconditioner scans (0, 0 when the windowed scans are used), row groups
+ * of the operator kernel in use (the kernel specialised for l_max <= 8 when it is
+ * enabled, else CTA groups per node tile of the generic kernel) and whether a group's
+ * weights sit in shared memory (1) or are read through L1 (0). */
 int cnm_plan_info(const cnm_handle *h, int32_t *scan_per, int32_t *scan_cluster, int32_t *apply_groups,
                   int32_t *apply_weights_in_smem);
 
