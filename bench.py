@@ -45,8 +45,9 @@ UNIT = "mode*node*steps/s"
 
 # DRAM traffic (read + write) per launch of the dominant kernel, the operator apply,
 # from the ncu capture summarised in profiles/k_apply5_fp64_binary_n45_N20000.md:
-# dram__bytes.sum.per_second x gpu__time_duration.sum = 373.29 GB/s x 86.816 us.
-NCU_TRAFFIC_BYTES = 373.293034e9 * 86.816e-6
+# dram__bytes.sum.per_second x gpu__time_duration.sum = 242.04 GB/s x 73.952 us (below the
+# algorithmic bytes: the input vector, written by the launch before, is read from L2).
+NCU_TRAFFIC_BYTES = 242.035482e9 * 73.952e-6
 
 
 def peaks():
