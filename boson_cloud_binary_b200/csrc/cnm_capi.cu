@@ -263,7 +263,7 @@ struct Solver {
     DevBuf<int> d2_chunk_l, d2_chunk_nrows, d2_chunk_rows, d2_chunk_goff, d2_l_off;
     DevBuf<double> d2_block_g;
     size_t apply3_smem = 0;
-    DevBuf<double2> psi, rhs, b, x, rr, r0, p, p2, v, s, t, y, z, yP, W0, W1, tmp, cand, dinv;
+    DevBuf<double2> psi, rhs, x, rr, r0, p, p2, v, s, t, y, z, yP, W0, W1, tmp, cand, dinv;
     DevBuf<double2> d_dots;   // [0..1] psi, [2..3] psi_last, [4..5] scratch, [6..7] G set-up
     DevBuf<double2> d_edge;   // dpsi at idx_ex (n) + psi at idx_ex-1..idx_ex+1 (3n)
     DevBuf<Krylov> d_kr;
@@ -419,7 +419,7 @@ struct Solver {
         }
         d_hh.alloc((size_t)K * Nr);
         d_hh_aux.alloc((size_t)K * Nr);
-        for (DevBuf<double2> *bptr : {&psi, &rhs, &b, &x, &rr, &r0, &p, &p2, &v, &s, &t, &y, &z, &yP, &W0, &W1, &tmp,
+        for (DevBuf<double2> *bptr : {&psi, &rhs, &x, &rr, &r0, &p, &p2, &v, &s, &t, &y, &z, &yP, &W0, &W1, &tmp,
                                       &cand, &dinv})
             bptr->alloc(nN);
         d_dots.alloc(8);
@@ -449,6 +449,8 @@ struct Solver {
         }
         CK(cudaFuncSetAttribute(k_diagnostics, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
         CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+        CK(cudaFuncSetAttribute(k_wood_setup_band, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)(2 * WOOD_BAND_MAX * sizeof(double2))));
         CK(cudaFuncSetAttribute(k_precond_solve2, cudaFuncAttributeMaxDynamicSharedMemorySize, 210 * 1024));
         CK(cudaFuncSetAttribute(k_precond_factor2, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
         plan_cluster_scans();
@@ -1271,11 +1273,10 @@ struct Solver {
         kr.status = d_status.p;
         h_kr_init = kr;
         CK(cudaMemcpyAsync(dk, &h_kr_init, sizeof(kr), cudaMemcpyHostToDevice, stream));
-        // b = rhs / |rhs|, x = psi / |rhs|, r = r0 = b - A_full x in one pass; its last
-        // CTA runs KS_INIT (and the first beta) on |r0|^2 and |b|^2
-        k_krylov_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, d_red.p + RED_RHS, rhs.p, psi.p, b.p, x.p,
-                                                                rr.p, r0.p, d_partials.p, d_red.p + 8,
-                                                                ticket(TK_START_T));
+        // with b = rhs / |rhs| (never stored): x = psi / |rhs|, r = r0 = b - A_full x in one
+        // pass; its last CTA runs KS_INIT (and the first beta) on |r0|^2 and |b|^2
+        k_krylov_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, d_red.p + RED_RHS, rhs.p, psi.p, x.p, rr.p,
+                                                                r0.p, d_partials.p, d_red.p + 8, ticket(TK_START_T));
         launch_check();
         factorize(dtv);
         if (k > 0) wood_setup(sk, k, dtv);
@@ -1302,7 +1303,8 @@ struct Solver {
                 const double2 rho_old = kr.rho;
                 sink_dots(x.p, d_dots.p, sk, k);
                 apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv);
-                axpby(cmake(1, 0), b.p, cmake(-1, 0), tmp.p, rr.p);
+                // r = rhs / |rhs| - A_full x
+                axpby(cmake(kr.rhs_norm > 0.0 ? 1.0 / kr.rhs_norm : 0.0, 0.0), rhs.p, cmake(-1, 0), tmp.p, rr.p);
                 CK(cudaMemcpyAsync(r0.p, rr.p, nN * sizeof(double2), cudaMemcpyDeviceToDevice, stream));
                 dots(1, rr.p, rr.p);
                 const double nr2 = read_red(0);
@@ -1365,6 +1367,29 @@ struct Solver {
     {
         const double c0 = 0.25 * dtv * sk[0]->strength, c1 = k > 1 ? 0.25 * dtv * sk[1]->strength : 1.0;
         set_wood_band(sk, k, dtv);
+        if (pcl_per > 0 && !jacobi && wband_hi - wband_lo <= WOOD_BAND_MAX) {
+            // W_a only on the band, one warp per (radial block, sink)
+            WoodBand wb;
+            wb.n_sinks = k;
+            wb.v0 = sk[0]->v.p;
+            wb.v1 = k > 1 ? sk[1]->v.p : nullptr;
+            wb.W0 = W0.p;
+            wb.W1 = W1.p;
+            wb.slo0 = sk[0]->lo;
+            wb.shi0 = sk[0]->hi;
+            wb.slo1 = k > 1 ? sk[1]->lo : 0;
+            wb.shi1 = k > 1 ? sk[1]->hi : 0;
+            wb.c0 = c0;
+            wb.c1 = c1;
+            wb.partials = d_wpart.p;
+            wb.ticket = ticket(TK_WOOD_T);
+            wb.kr = d_kr.p;
+            const size_t smem = (size_t)2 * (wband_hi - wband_lo) * sizeof(double2);
+            k_wood_setup_band<<<n_modes * k, WSB_THREADS, smem, stream>>>(Nr, n_modes, wband_lo, wband_hi,
+                                                                          offdiag(dtv), dinv.p, wb);
+            launch_check();
+            return;
+        }
         if (pcl_per > 0 && !jacobi) {
             WoodArgs wd = wood_args(WD_SETUP, 0, sk, k);
             wd.c0 = c0;
@@ -1424,6 +1449,10 @@ struct Solver {
         k_woodbury_band<<<blocks, 256, 0, stream>>>(Nr, n_modes, wband_lo, wband_hi, d_kr.p, which, W0.p, W1.p, out);
         launch_check();
     }
+
+    // Widest band the CTA-per-block Woodbury set-up takes (its shared memory holds the
+    // band's pivots and values); wider bands use the cluster solve.
+    static constexpr int WOOD_BAND_MAX = 4096;
 
     // Band of nodes outside which every W_a = P^{-1} v_a is below 1e-40 of its largest
     // value: the entries of the inverse of a radial block decay by the contraction

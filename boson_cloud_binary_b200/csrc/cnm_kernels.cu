@@ -913,22 +913,27 @@ __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, 
                             int gate_mode)
 {
     if (gate && gate_closed(gate, gate_mode)) return;
-    // warp w takes modes w, w + nwarps, ...; its lanes stride over the support nodes, so
-    // every load of a thread is independent of the others (fixed order: deterministic)
+    // the (sink, mode, support node) terms are dealt to the threads in a fixed order, a
+    // few per thread with independent loads (deterministic: fixed per-thread order, then
+    // a fixed block reduction)
     __shared__ double scratch[4 * 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const int n0 = n_sinks > 0 ? max(0, hi0 - lo0) : 0, n1 = n_sinks > 1 ? max(0, hi1 - lo1) : 0;
+    const int64_t tot0 = (int64_t)n0 * n_modes, tot = tot0 + (int64_t)n1 * n_modes;
     double acc[4] = {0, 0, 0, 0};
-    for (int s = 0; s < n_sinks; ++s) {
-        const double2 *__restrict__ v = s == 0 ? v0 : v1;
-        const int lo = s == 0 ? lo0 : lo1, hi = s == 0 ? hi0 : hi1;
-        for (int j = warp; j < n_modes; j += nw) {
-            const int64_t base = (int64_t)j * Nr;
 #pragma unroll 4
-            for (int i = lo + lane; i < hi; i += 32) {
-                const double2 d = cconjmul(v[base + i], x[base + i]);
-                acc[2 * s] += d.x;
-                acc[2 * s + 1] += d.y;
-            }
+    for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+        const bool first = e < tot0;
+        const int64_t f = first ? e : e - tot0;
+        const int w = first ? n0 : n1;
+        const int j = (int)(f / w), i = (first ? lo0 : lo1) + (int)(f - (int64_t)j * w);
+        const int64_t q = (int64_t)j * Nr + i;
+        const double2 d = cconjmul((first ? v0 : v1)[q], x[q]);
+        if (first) {
+            acc[0] += d.x;
+            acc[1] += d.y;
+        } else {
+            acc[2] += d.x;
+            acc[3] += d.y;
         }
     }
     block_sum<4>(acc, scratch);
@@ -1482,7 +1487,6 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double2 smc[];
     __shared__ Aff wagg[PCL_THREADS / 32];
-    __shared__ double2 win[PCL_THREADS / 32];
     __shared__ Aff cagg_f, cagg_b;
     const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
     const int second = blockIdx.y >= (unsigned)n_modes;
@@ -1587,7 +1591,10 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         if (lane == 31) cagg_f = c;
     }
     cl.sync();
-    if (warp == 0) {
+    // Every warp derives its own start value (the same scans in each warp): a single
+    // warp doing this while the others wait at a barrier ran about six times slower.
+    double2 ywarp;
+    {
         // start value of the CTA: lane q < rank holds CTA q's total; their ordered
         // composition applied to y = 0 is its B part
         Aff c = lane < rank ? *cl.map_shared_rank(&cagg_f, lane) : aff_identity();
@@ -1597,7 +1604,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
             if (lane >= o) c = aff_then(prev, c);
         }
         const double2 ycta = cmake(__shfl_sync(0xffffffffu, c.B.x, 31), __shfl_sync(0xffffffffu, c.B.y, 31));
-        // start values of the warps: exclusive scan of the warp totals
+        // start values of the warps: exclusive scan of the warp totals; lane w holds warp w's
         Aff w = lane < NW ? wagg[lane] : aff_identity();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1606,11 +1613,11 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         }
         Aff wex = shfl_up_aff(w, 1);
         if (lane == 0) wex = aff_identity();
-        if (lane < NW) win[lane] = aff_apply(wex, ycta);
+        const double2 ys = aff_apply(wex, ycta);
+        ywarp = cmake(__shfl_sync(0xffffffffu, ys.x, warp), __shfl_sync(0xffffffffu, ys.y, warp));
     }
-    __syncthreads();
     {
-        double2 y = aff_apply(excl, win[warp]);
+        double2 y = aff_apply(excl, ywarp);
         for (int e = s0; e < s1; ++e) {
             const int i = c0 + e;
             const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
@@ -1635,7 +1642,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     }
     Aff bexcl = shfl_down_aff(bcc, 1);
     if (lane == 31) bexcl = aff_identity();
-    __syncthreads();  // every thread has read win[] of the forward sweep
+    __syncthreads();  // every thread has read wagg[] of the forward sweep
     if (lane == 0) wagg[warp] = bcc;
     __syncthreads();
     if (warp == 0) {
@@ -1649,7 +1656,8 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         if (lane == 0) cagg_b = c;
     }
     cl.sync();
-    if (warp == 0) {
+    double2 xwarp;
+    {
         // start value of the CTA from the CTAs after it (applied last to first)
         Aff c = (lane > rank && lane < cs) ? *cl.map_shared_rank(&cagg_b, lane) : aff_identity();
 #pragma unroll
@@ -1666,14 +1674,14 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         }
         Aff wex = shfl_down_aff(w, 1);
         if (lane == 31) wex = aff_identity();
-        if (lane < NW) win[lane] = aff_apply(wex, xcta);
+        const double2 xs = aff_apply(wex, xcta);
+        xwarp = cmake(__shfl_sync(0xffffffffu, xs.x, warp), __shfl_sync(0xffffffffu, xs.y, warp));
     }
     // the other CTAs read cagg_b only before this arrive; the matching wait is the
     // last statement, so a CTA's shared memory outlives every remote read of it
     cl.barrier_arrive();
-    __syncthreads();
     {
-        double2 xr = aff_apply(bexcl, win[warp]);
+        double2 xr = aff_apply(bexcl, xwarp);
         for (int e = s1 - 1; e >= s0; --e) {
             const int i = c0 + e;
             const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
@@ -1742,6 +1750,189 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     cl.barrier_wait();
 }
 
+// Woodbury set-up (src/CrankNicolsonModes_matrices.cpp:133-145) on the band [blo, bhi)
+// outside which every W_a = P^{-1} v_a is below 1e-40 of its largest value: one CTA per
+// (radial block j, sink a) stages the band's pivots and v_a in shared memory and runs the
+// block's forward and backward Thomas sweeps over it as affine scans (thread: its run of
+// nodes, an odd count so 16-byte shared accesses do not conflict; warp: shuffles; CTA:
+// every warp composes the warp totals before it).  Left of the band y vanishes exactly
+// (v_a does), right of it x is taken as zero; the pivots are the full block's, so the band
+// values are those of the full solve.  Each CTA reduces v_b^dag W_a over the sinks'
+// supports into partials[slot][j] (slot 4 a + 2 b + re/im); the last CTA sums them over j
+// in order and forms G = diag(1 / (dt/4 g)) + v^dag W and its inverse.
+__global__ void __launch_bounds__(WSB_THREADS) k_wood_setup_band(int Nr, int n_modes, int blo, int bhi, double2 off,
+                                                                 const double2 *dinv, WoodBand wb)
+{
+    extern __shared__ double2 wsb[];
+    __shared__ Aff wagg[WSB_THREADS / 32];
+    __shared__ double wscr[4 * 32];
+    constexpr int T = WSB_THREADS, NW = WSB_THREADS / 32;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int j = blockIdx.x / wb.n_sinks, a = blockIdx.x - j * wb.n_sinks;
+    const int Lb = bhi - blo;
+    double2 *D = wsb, *Y = wsb + Lb;
+    const int64_t base = (int64_t)j * Nr + blo;
+    {
+        const double2 *__restrict__ v = (a == 0 ? wb.v0 : wb.v1) + base;
+        const double2 *__restrict__ d = dinv + base;
+        for (int e0 = tid; e0 < Lb; e0 += 4 * T) {
+            double2 dv[4], vv[4];
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + T * u;
+                if (e < Lb) {
+                    dv[u] = d[e];
+                    vv[u] = v[e];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+                const int e = e0 + T * u;
+                if (e < Lb) {
+                    D[e] = dv[u];
+                    Y[e] = vv[u];
+                }
+            }
+        }
+    }
+    __syncthreads();
+    const int cnt = ((Lb + T - 1) / T) | 1;
+    const int s0 = min(Lb, tid * cnt), s1 = min(Lb, s0 + cnt);
+    // forward: y_i = d_i (v_i - l y_{i-1}), y = 0 left of the band
+    Aff acc = aff_identity();
+    for (int e = s0; e < s1; ++e) {
+        const int i = blo + e;
+        const double2 di = D[e];
+        const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0.0, 0.0);
+        const Aff m{cmake(-(l.x * di.x - l.y * di.y), -(l.x * di.y + l.y * di.x)), cmul(di, Y[e])};
+        acc = aff_then(acc, m);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Aff prev = shfl_up_aff(acc, o);
+        if (lane >= o) acc = aff_then(prev, acc);
+    }
+    Aff excl = shfl_up_aff(acc, 1);
+    if (lane == 0) excl = aff_identity();
+    if (lane == 31) wagg[warp] = acc;
+    __syncthreads();
+    double2 y;
+    {
+        // start of this warp: the warp totals before it, applied to y = 0
+        Aff w = lane < NW ? wagg[lane] : aff_identity();
+#pragma unroll
+        for (int o = 1; o < NW; o <<= 1) {
+            const Aff prev = shfl_up_aff(w, o);
+            if (lane >= o) w = aff_then(prev, w);
+        }
+        const Aff wex = shfl_up_aff(w, 1);
+        const double2 ys = lane == 0 ? cmake(0.0, 0.0) : wex.B;
+        y = aff_apply(excl, cmake(__shfl_sync(0xffffffffu, ys.x, warp), __shfl_sync(0xffffffffu, ys.y, warp)));
+    }
+    for (int e = s0; e < s1; ++e) {
+        const int i = blo + e;
+        const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0.0, 0.0);
+        y = cmul(D[e], csub(Y[e], cmul(l, y)));
+        Y[e] = y;
+    }
+    // backward: x_i = y_i - u d_i x_{i+1}, x = 0 right of the band
+    Aff bcc = aff_identity();
+    for (int e = s1 - 1; e >= s0; --e) {
+        const int i = blo + e;
+        const double2 di = D[e];
+        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0.0, 0.0);
+        const Aff m{cmake(-(u.x * di.x - u.y * di.y), -(u.x * di.y + u.y * di.x)), Y[e]};
+        bcc = aff_then(bcc, m);
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Aff nxt = shfl_down_aff(bcc, o);
+        if (lane + o < 32) bcc = aff_then(nxt, bcc);
+    }
+    Aff bexcl = shfl_down_aff(bcc, 1);
+    if (lane == 31) bexcl = aff_identity();
+    __syncthreads();  // every warp has read wagg[] of the forward sweep
+    if (lane == 0) wagg[warp] = bcc;
+    __syncthreads();
+    double2 x;
+    {
+        // start of this warp: the warp totals after it (applied last to first), x = 0 past the band
+        Aff w = lane < NW ? wagg[lane] : aff_identity();
+#pragma unroll
+        for (int o = 1; o < NW; o <<= 1) {
+            const Aff nxt = shfl_down_aff(w, o);
+            if (lane + o < 32) w = aff_then(nxt, w);
+        }
+        const Aff wex = shfl_down_aff(w, 1);
+        const double2 xs = lane >= NW - 1 ? cmake(0.0, 0.0) : wex.B;
+        x = aff_apply(bexcl, cmake(__shfl_sync(0xffffffffu, xs.x, warp), __shfl_sync(0xffffffffu, xs.y, warp)));
+    }
+    for (int e = s1 - 1; e >= s0; --e) {
+        const int i = blo + e;
+        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0.0, 0.0);
+        x = csub(Y[e], cmul(cmul(u, D[e]), x));
+        Y[e] = x;
+    }
+    __syncthreads();
+    // W_a on the band and the projections v_b^dag W_a (b = 0, 1) over the supports
+    double pr[4] = {0.0, 0.0, 0.0, 0.0};
+    {
+        double2 *__restrict__ W = (a == 0 ? wb.W0 : wb.W1) + base;
+        for (int e = tid; e < Lb; e += T) {
+            const double2 xv = Y[e];
+            W[e] = xv;
+            const int i = blo + e;
+            if (i >= wb.slo0 && i < wb.shi0) {
+                const double2 q = cconjmul(wb.v0[base + e], xv);
+                pr[0] += q.x;
+                pr[1] += q.y;
+            }
+            if (wb.n_sinks > 1 && i >= wb.slo1 && i < wb.shi1) {
+                const double2 q = cconjmul(wb.v1[base + e], xv);
+                pr[2] += q.x;
+                pr[3] += q.y;
+            }
+        }
+    }
+    block_sum<4>(pr, wscr);
+    if (tid == 0) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) wb.partials[(int64_t)(4 * a + q) * n_modes + j] = pr[q];
+        __threadfence();
+    }
+    __shared__ unsigned s_last;
+    __syncthreads();
+    if (tid == 0) s_last = atomicAdd(wb.ticket, 1u) == gridDim.x - 1u ? 1u : 0u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    // the partials of up to T / 8 blocks at a time are loaded together, then slot q's are
+    // added in block order by thread q
+    __shared__ double fin[8][WSB_THREADS / 8];
+    const int nq = 4 * wb.n_sinks, per = T / 8;
+    double sm = 0.0;
+    for (int j0 = 0; j0 < n_modes; j0 += per) {
+        {
+            const int q = tid / per, jj = j0 + tid % per;
+            if (q < nq && jj < n_modes) fin[q][tid % per] = __ldcg(wb.partials + (int64_t)q * n_modes + jj);
+        }
+        __syncthreads();
+        if (tid < nq)
+            for (int u = 0; u < per && j0 + u < n_modes; ++u) sm += fin[tid][u];
+        __syncthreads();
+    }
+    __shared__ double sums[8];
+    if (tid < 8) sums[tid] = (tid < nq && (tid & 3) < 2 * wb.n_sinks) ? sm : 0.0;
+    __syncthreads();
+    if (tid == 0) {
+        // vw[2 a + b] = v_b^dag W_a
+        const double2 vw[4] = {cmake(sums[0], sums[1]), cmake(sums[2], sums[3]), cmake(sums[4], sums[5]),
+                               cmake(sums[6], sums[7])};
+        wood_setup_dev(wb.kr, vw, wb.c0, wb.c1);
+        *wb.ticket = 0u;
+    }
+}
+
 // Inverse Thomas pivots d_i = 1 / p_i, exact: the pivot recurrence p_i = a_i - c / p_{i-1}
 // is a chain of Moebius maps composed by the cluster scan above (2x2 complex matrices,
 // rescaled by powers of two as they grow).  Grid (cluster size, modes).
@@ -1753,7 +1944,6 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double2 smc[];
     __shared__ Mob wmob[PCL_THREADS / 32];
-    __shared__ double2 pwin[PCL_THREADS / 32];
     __shared__ Mob cmob;
     const int rank = (int)cl.block_rank();
     const int Nr = g.Nr, j = blockIdx.y;
@@ -1822,7 +2012,9 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
         if (lane == 31) cmob = m;
     }
     cl.sync();
-    if (warp == 0) {
+    // every warp derives its own start pivot (see the solve: a lone warp here is slow)
+    double2 p;
+    {
         // node 0's map is constant (p_0 = a_0), so any finite start value is exact
         Mob m = lane < rank ? *cl.map_shared_rank(&cmob, lane) : mob_identity();
 #pragma unroll
@@ -1846,11 +2038,10 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
         }
         Mob wex = shfl_up_mob(w, 1);
         if (lane == 0) wex = mob_identity();
-        if (lane < NW) pwin[lane] = mob_apply(wex, pc);
+        const double2 ps = mob_apply(wex, pc);
+        p = cmake(__shfl_sync(0xffffffffu, ps.x, warp), __shfl_sync(0xffffffffu, ps.y, warp));
     }
     cl.barrier_arrive();
-    __syncthreads();
-    double2 p = pwin[warp];
     if (lane > 0) p = mob_apply(excl, p);
     int bad = 0;
     double2 dprev = crcp(p);
@@ -2076,9 +2267,9 @@ __global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const 
 // because A_full + B_full = 2 I and rhs = B_full psi (src/CrankNicolsonModes.cpp:170-172,
 // _matrices.cpp:36-37); per-CTA partials of |r|^2 and |b|^2 for KS_INIT.
 __global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov *kr, const double *red_in,
-                                                               const double2 *rhs, const double2 *psi, double2 *b,
-                                                               double2 *x, double2 *r, double2 *r0, double *partials,
-                                                               double *red, unsigned *ticket)
+                                                               const double2 *rhs, const double2 *psi, double2 *x,
+                                                               double2 *r, double2 *r0, double *partials, double *red,
+                                                               unsigned *ticket)
 {
     __shared__ double scratch[6 * 32];
     const double nrm = sqrt(red_in[0]);
@@ -2092,7 +2283,6 @@ __global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov 
         const double2 hv = rhs[e], pv = psi[e];
         const double2 bv = cscale(hv, sc);
         const double2 rv = cscale(csub(hv, pv), 2.0 * sc);
-        b[e] = bv;
         x[e] = cscale(pv, sc);
         r[e] = rv;
         r0[e] = rv;

@@ -110,8 +110,7 @@ __global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1
 __global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
                                 double2 *b, double2 *x);
 __global__ void k_krylov_start(int64_t n, Krylov *kr, const double *red_in, const double2 *rhs, const double2 *psi,
-                               double2 *b, double2 *x, double2 *r, double2 *r0, double *partials, double *red,
-                               unsigned *ticket);
+                               double2 *x, double2 *r, double2 *r0, double *partials, double *red, unsigned *ticket);
 __global__ void k_scale_candidate(int64_t n, const Krylov *kr, const double2 *x, double2 *cand);
 __global__ void k_precond_solve2(int Nr, int chunk, int window, double2 off, const double2 *dinv, const double2 *b,
                                  double2 *x, PrecondInput in);
@@ -132,6 +131,22 @@ struct WoodArgs {
 };
 __global__ void k_precond_solve_cl(int Nr, int n_modes, int per, double2 off, const double2 *dinv, const double2 *b,
                                    double2 *x, const double2 *b2, double2 *x2, PrecondInput in, WoodArgs wd);
+// Woodbury set-up restricted to the band of nodes where W_a = P^{-1} v_a is not
+// negligible (one CTA of WSB_THREADS per radial block and sink, 32 bytes of dynamic
+// shared memory per band node); see k_wood_setup_band.
+struct WoodBand {
+    int n_sinks;
+    const double2 *v0, *v1;  // sink projectors (zero outside their supports)
+    double2 *W0, *W1;        // W_a on the band (not written elsewhere)
+    int slo0, shi0, slo1, shi1;
+    double c0, c1;           // dt/4 g_a
+    double *partials;        // [8][n_modes]
+    unsigned *ticket;
+    Krylov *kr;
+};
+constexpr int WSB_THREADS = 512;
+__global__ void k_wood_setup_band(int Nr, int n_modes, int blo, int bhi, double2 off, const double2 *dinv,
+                                  WoodBand wb);
 __global__ void k_precond_factor_cl(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int per,
                                     double2 *dinv, int *status);
 __global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
