@@ -757,10 +757,11 @@ struct Solver {
         op.sink_active = sink_active;
     }
 
-    // src/CrankNicolsonModes_absorption.cpp:12-81
-    void update_absorption_profile(Absorber &ab, double radius, double width)
+    // src/CrankNicolsonModes_absorption.cpp:12-81: the support of a changed profile; true
+    // when its moments must be computed (launch_moments)
+    bool prepare_profile(Absorber &ab, double radius, double width)
     {
-        if (ab.valid && ab.radius == radius && ab.width == width) return;
+        if (ab.valid && ab.radius == radius && ab.width == width) return false;
         const int old_lo = ab.lo, old_hi = ab.hi;
         ab.radius = radius;
         ab.width = width;
@@ -791,9 +792,8 @@ struct Solver {
             ab.wlo = old_lo;
             ab.whi = old_hi;
         }
-        if (ab.hi <= ab.lo) return;
-        const int degree = 2 * l_max;
-        const int nq = std::max(128, degree + 16);
+        if (ab.hi <= ab.lo) return false;
+        const int nq = abs_nodes();
         if (gl_n != nq) {
             std::vector<double> gx, gw;
             gauss_legendre01(nq, gx, gw);
@@ -801,38 +801,76 @@ struct Solver {
             upload(d_glw, gw);
             gl_n = nq;
         }
-        const int threads = std::max(128, (nq + 31) / 32 * 32);  // one quadrature node per thread
-        k_abs_moments<<<ab.hi - ab.lo, threads, (size_t)(degree + 1) * (threads / 32) * sizeof(double), stream>>>(
-            d_r.p, Nr, ab.lo, radius, width, nq, d_glx.p, d_glw.p, degree, ab.mom.p);
-        launch_check();
-        k_abs_normalize<<<1, 256, 0, stream>>>(d_r.p, Nr, ab.lo, ab.hi, dr, degree, ab.mom.p);
+        return true;
+    }
+
+    // Gauss-Legendre nodes of the angular quadrature and the moment kernels' CTA size
+    // (one quadrature node per thread)
+    int abs_nodes() const { return std::max(128, 2 * l_max + 16); }
+    int abs_threads() const { return std::max(128, (abs_nodes() + 31) / 32 * 32); }
+
+    static void add_absorber(AbsorberPair &ap, Absorber &ab, bool secondary)
+    {
+        const int c = ap.count++;
+        ap.lo[c] = ab.lo;
+        ap.hi[c] = ab.hi;
+        ap.wlo[c] = ab.wlo;
+        ap.whi[c] = ab.whi;
+        ap.radius[c] = ab.radius;
+        ap.width[c] = ab.width;
+        ap.mom[c] = ab.mom.p;
+        ap.v[c] = ab.v.p;
+        ap.secondary[c] = secondary ? 1 : 0;
+    }
+
+    // moments of the changed profiles, one launch
+    void launch_moments(bool m1, bool m2)
+    {
+        AbsorberPair ap;
+        std::memset(&ap, 0, sizeof(ap));
+        if (m1) add_absorber(ap, abs1, false);
+        if (m2) add_absorber(ap, abs2, true);
+        if (ap.count == 0) return;
+        const int degree = 2 * l_max, threads = abs_threads();
+        const unsigned blocks = (unsigned)((ap.hi[0] - ap.lo[0]) + (ap.count > 1 ? ap.hi[1] - ap.lo[1] : 0));
+        k_abs_moments<<<blocks, threads, (size_t)(degree + 1) * (threads / 32) * sizeof(double), stream>>>(
+            d_r.p, Nr, abs_nodes(), d_glx.p, d_glw.p, degree, ap);
         launch_check();
     }
 
-    void build_projector(Absorber &ab, bool secondary)
+    // both projectors, one launch; nodes of a previous support are rewritten (as zero)
+    void build_projectors()
     {
-        const int lo = ab.wlo, hi = ab.whi;
-        if (hi <= lo) return;
-        // nodes outside the current support are written as zero (the kernel tests the geometry)
-        const int w = hi - lo;
-        const int blocks = std::max(1, std::min(1024, (w * n_modes + 255) / 256));
-        if (ab.hi > ab.lo) {
-            k_swave_projector<<<blocks, 256, 0, stream>>>(d_r.p, Nr, n_modes, lo, hi, ab.mom.p, d_ang00.p,
-                                                           d_mode_l.p, d_mode_m.p, theta, secondary ? 1 : 0, ab.v.p);
-        } else {
-            for (int j = 0; j < n_modes; ++j)
-                CK(cudaMemsetAsync(ab.v.p + (int64_t)j * Nr + lo, 0, (size_t)w * sizeof(double2), stream));
+        AbsorberPair ap;
+        std::memset(&ap, 0, sizeof(ap));
+        int64_t work = 0;
+        for (int a = 0; a < 2; ++a) {
+            Absorber &ab = a == 0 ? abs1 : abs2;
+            const int lo = ab.wlo, hi = ab.whi;
+            if (hi <= lo) continue;
+            if (ab.hi > ab.lo) {
+                add_absorber(ap, ab, a == 1);
+                work += (int64_t)(hi - lo) * n_modes;
+            } else {
+                for (int j = 0; j < n_modes; ++j)
+                    CK(cudaMemsetAsync(ab.v.p + (int64_t)j * Nr + lo, 0, (size_t)(hi - lo) * sizeof(double2), stream));
+            }
+            ab.wlo = ab.lo;
+            ab.whi = ab.hi;
         }
+        if (ap.count == 0) return;
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(1024, (work + 255) / 256));
+        k_swave_projector<<<blocks, 256, 0, stream>>>(d_r.p, Nr, n_modes, dr, d_ang00.p, d_mode_l.p, d_mode_m.p, theta,
+                                                       ap);
         launch_check();
-        ab.wlo = ab.lo;
-        ab.whi = ab.hi;
     }
 
     // src/CrankNicolsonModes_absorption.cpp:153-182
     void build_spherical_absorption()
     {
-        update_absorption_profile(abs1, R1, epsilon_smear * M1);
-        update_absorption_profile(abs2, R2, epsilon_smear * M2);
+        const bool m1 = prepare_profile(abs1, R1, epsilon_smear * M1);
+        const bool m2 = prepare_profile(abs2, R2, epsilon_smear * M2);
+        launch_moments(m1, m2);
         double ramp = 1.0;
         if (!isolated && t_i < ramp_end_time()) {
             ramp = 0.0;
@@ -842,10 +880,7 @@ struct Solver {
         }
         const double Ah1 = 16.0 * M_PI * M1 * M1 * ramp;
         const double Ah2 = 16.0 * M_PI * M2 * M2 * ramp;
-        if (cpl.mode00 >= 0) {
-            build_projector(abs1, false);
-            build_projector(abs2, true);
-        }
+        if (cpl.mode00 >= 0) build_projectors();
         abs1.strength = Ah1 * dr;
         abs2.strength = Ah2 * dr;
     }

@@ -2332,11 +2332,11 @@ __global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj)
 // radial node per CTA (src/CrankNicolsonModes_absorption.cpp:35-70): Gauss-Legendre
 // quadrature over the angular cap z = 1 - cos(gamma) in [0, cap], one quadrature node
 // per thread, Legendre recurrence to degree 2 l_max.
-__global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
-                              const double *gl_x, const double *gl_w, int degree, double *mom)
+// Legendre moments of an absorber profile at node i into mom[l][i], l <= degree
+// (src/CrankNicolsonModes_absorption.cpp:12-81), unnormalised; sh: (degree + 1) x warps doubles.
+__device__ void abs_moments_node(const double *r, int Nr, int i, double radius, double width, int nq,
+                                 const double *gl_x, const double *gl_w, int degree, double *mom, double *sh)
 {
-    extern __shared__ double sh[];  // (degree + 1) * nwarps
-    const int i = lo + blockIdx.x;
     if (i < 1 || i > Nr - 2) return;
     const double delta = r[i] - radius;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
@@ -2389,46 +2389,58 @@ __global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, do
     }
 }
 
-// Discrete volume normalisation sum_i dr r_i^2 K_0(r_i) = 1 (_absorption.cpp:71-80), one CTA.
-__global__ void k_abs_normalize(const double *r, int Nr, int lo, int hi, double dr, int degree, double *mom)
+// Moments of one or two absorbers in one launch: CTA b < hi[0] - lo[0] takes node lo[0] + b
+// of the first entry, the others the nodes of the second.  The moments stay unnormalised;
+// the projector kernel divides by the profile's norm.
+__global__ void k_abs_moments(const double *r, int Nr, int nq, const double *gl_x, const double *gl_w, int degree,
+                              AbsorberPair ap)
 {
-    __shared__ double scratch[32];
-    __shared__ double norm_s;
-    double acc[1] = {0.0};
-    for (int i = lo + threadIdx.x; i < hi; i += blockDim.x)
-        if (i >= 1 && i <= Nr - 2) acc[0] += dr * r[i] * r[i] * mom[i];
-    block_sum<1>(acc, scratch);
-    if (threadIdx.x == 0) norm_s = acc[0];
-    __syncthreads();
-    const double norm = norm_s;
-    if (norm > 0.0)
-        for (int e = threadIdx.x; e < (degree + 1) * (hi - lo); e += blockDim.x) {
-            const int l = e / (hi - lo), i = lo + e % (hi - lo);
-            mom[(int64_t)l * Nr + i] /= norm;
-        }
+    extern __shared__ double sh[];  // (degree + 1) * nwarps
+    const int n0 = ap.hi[0] - ap.lo[0];
+    const int a = (int)blockIdx.x < n0 ? 0 : 1;
+    abs_moments_node(r, Nr, ap.lo[a] + (int)blockIdx.x - (a == 0 ? 0 : n0), ap.radius[a], ap.width[a], nq, gl_x,
+                     gl_w, degree, ap.mom[a], sh);
 }
 
-// v[j, i] = r_i sqrt(4 pi) parity_j kappa_j(r_i), kappa_j = mom_{l_j}(r_i) ang_j e^{-i m_j theta}
-// (_absorption.cpp:127-151; the only Gaunt term of the pair (j, (0,0)) has l* = l_j and
-// m* = -m_j).  Writes the support [lo, hi) of every mode.
-__global__ void k_swave_projector(const double *r, int Nr, int n_modes, int lo, int hi, const double *mom,
-                                  const double *ang00, const int *mode_l, const int *mode_m, double theta,
-                                  int secondary, double2 *v)
+// s-wave projectors of one or two absorbers (src/CrankNicolsonModes_absorption.cpp:
+// 153-182): every CTA first forms each profile's norm sum_support dr r^2 mom_0 (the same
+// fixed-order sum in every CTA), then the threads write v_a on [wlo_a, whi_a), zero
+// outside the support [lo_a, hi_a); blockDim.x = 256.
+__global__ void __launch_bounds__(256) k_swave_projector(const double *r, int Nr, int n_modes, double dr,
+                                                         const double *ang00, const int *mode_l, const int *mode_m,
+                                                         double theta, AbsorberPair ap)
 {
-    const int w = hi - lo;
-    for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < w * n_modes; e += gridDim.x * blockDim.x) {
-        const int j = e / w, i = lo + e % w;
+    __shared__ double scratch[32];
+    __shared__ double norm_s[2];
+    for (int a = 0; a < ap.count; ++a) {
+        double acc[1] = {0.0};
+        for (int i = ap.lo[a] + threadIdx.x; i < ap.hi[a]; i += blockDim.x)
+            if (i >= 1 && i <= Nr - 2) acc[0] += dr * r[i] * r[i] * ap.mom[a][i];
+        block_sum<1>(acc, scratch);
+        if (threadIdx.x == 0) norm_s[a] = acc[0];
+    }
+    __syncthreads();
+    const int w0 = ap.whi[0] - ap.wlo[0];
+    const int64_t t0 = (int64_t)w0 * n_modes;
+    const int64_t tot = t0 + (ap.count > 1 ? (int64_t)(ap.whi[1] - ap.wlo[1]) * n_modes : 0);
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < tot; e += (int64_t)gridDim.x * blockDim.x) {
+        const int a = e < t0 ? 0 : 1;
+        const int64_t f = a == 0 ? e : e - t0;
+        const int w = ap.whi[a] - ap.wlo[a];
+        const int j = (int)(f / w), i = ap.wlo[a] + (int)(f - (int64_t)j * w);
         double2 val = cmake(0.0, 0.0);
-        if (i >= 1 && i <= Nr - 2 && ang00[j] != 0.0) {
+        if (i >= 1 && i <= Nr - 2 && ang00[j] != 0.0 && i >= ap.lo[a] && i < ap.hi[a]) {
             const int ms = -mode_m[j];
             double sn, cs;
             sincos((double)ms * theta, &sn, &cs);
-            const double parity = (secondary && (ms & 1)) ? -1.0 : 1.0;
-            const double m = mom[(int64_t)mode_l[j] * Nr + i];
+            const double parity = (ap.secondary[a] && (ms & 1)) ? -1.0 : 1.0;
+            const double norm = norm_s[a];
+            double m = ap.mom[a][(int64_t)mode_l[j] * Nr + i];
+            if (norm > 0.0) m /= norm;
             const double2 kappa = cscale(cmake(cs, sn), m * ang00[j]);
             val = cscale(kappa, r[i] * sqrt(4.0 * M_PI) * parity);
         }
-        v[(int64_t)j * Nr + i] = val;
+        ap.v[a][(int64_t)j * Nr + i] = val;
     }
 }
 

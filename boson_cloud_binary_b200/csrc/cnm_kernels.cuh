@@ -149,12 +149,20 @@ __global__ void k_wood_setup_band(int Nr, int n_modes, int blo, int bhi, double2
                                   WoodBand wb);
 __global__ void k_precond_factor_cl(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int per,
                                     double2 *dinv, int *status);
-__global__ void k_abs_moments(const double *r, int Nr, int lo, double radius, double width, int nq,
-                              const double *gl_x, const double *gl_w, int degree, double *mom);
-__global__ void k_abs_normalize(const double *r, int Nr, int lo, int hi, double dr, int degree, double *mom);
-__global__ void k_swave_projector(const double *r, int Nr, int n_modes, int lo, int hi, const double *mom,
-                                  const double *ang00, const int *mode_l, const int *mode_m, double theta,
-                                  int secondary, double2 *v);
+// One or two absorbers: support [lo, hi), projector range [wlo, whi) (the support and
+// the previous one), moments and projector buffers, the parity flag of the second body.
+struct AbsorberPair {
+    int count;
+    int lo[2], hi[2], wlo[2], whi[2];
+    double radius[2], width[2];
+    double *mom[2];
+    double2 *v[2];
+    int secondary[2];
+};
+__global__ void k_abs_moments(const double *r, int Nr, int nq, const double *gl_x, const double *gl_w, int degree,
+                              AbsorberPair ap);
+__global__ void k_swave_projector(const double *r, int Nr, int n_modes, double dr, const double *ang00,
+                                  const int *mode_l, const int *mode_m, double theta, AbsorberPair ap);
 __global__ void k_diagnostics(Grid g, CouplingTable ct, const double *hh, double theta, double domega,
                               const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
                               const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0,
