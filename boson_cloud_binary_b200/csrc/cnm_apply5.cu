@@ -340,6 +340,7 @@ __device__ __forceinline__ void diag_dispatch(int grp, const Grid &g, const doub
 template <int L>
 __global__ void __launch_bounds__(A5_THREADS) k_diag5(Grid g, const double *gtab, DiagArgs d)
 {
+    pdl_wait();
     if (d.gate && gate_closed(d.gate, GATE_ACCEPTED)) return;
     constexpr int G = D5Groups<L>::value;
     using Lay = A5Layout<L, G>;
@@ -418,6 +419,7 @@ __device__ __forceinline__ void dispatch(int grp, const Grid &g, const double *g
 template <int L>
 __global__ void __launch_bounds__(A5_THREADS) k_apply5(Grid g, const double *gtab, ApplyArgs a)
 {
+    pdl_wait();
     if (a.gate && gate_closed(a.gate, a.gate_mode)) return;
     constexpr int G = A5Groups<L>::value;
     using Lay = A5Layout<L, G>;
@@ -510,7 +512,7 @@ void launch_apply5(int l_max, cudaStream_t st, const Grid &g, const double *gtab
     const size_t smem = apply5_smem(l_max);
     switch (l_max) {
 #define CNM_A5L(L) \
-    case L: k_apply5<L><<<blocks, A5_THREADS, smem, st>>>(g, gtab, a); break;
+    case L: (void)launch_pdl(k_apply5<L>, blocks, dim3(A5_THREADS), smem, st, g, gtab, a); break;
         CNM_A5L(1) CNM_A5L(2) CNM_A5L(3) CNM_A5L(4) CNM_A5L(5) CNM_A5L(6) CNM_A5L(7) CNM_A5L(8)
 #undef CNM_A5L
     default: break;
@@ -548,7 +550,7 @@ unsigned launch_diag5(int l_max, cudaStream_t st, const Grid &g, const double *g
     const size_t smem = diag5_smem(l_max);
     switch (l_max) {
 #define CNM_D5L(L) \
-    case L: k_diag5<L><<<blocks, A5_THREADS, smem, st>>>(g, gtab, d); break;
+    case L: (void)launch_pdl(k_diag5<L>, blocks, dim3(A5_THREADS), smem, st, g, gtab, d); break;
         CNM_D5L(1) CNM_D5L(2) CNM_D5L(3) CNM_D5L(4) CNM_D5L(5) CNM_D5L(6) CNM_D5L(7) CNM_D5L(8)
 #undef CNM_D5L
     default: return 0;

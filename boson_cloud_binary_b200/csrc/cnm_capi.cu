@@ -568,6 +568,14 @@ struct Solver {
         return cfg;
     }
 
+    // programmatic stream serialization (see launch_pdl)
+    static void pdl_attr(cudaLaunchAttribute &at)
+    {
+        std::memset(&at, 0, sizeof(at));
+        at.id = cudaLaunchAttributeProgrammaticStreamSerialization;
+        at.val.programmaticStreamSerializationAllowed = 1;
+    }
+
     static void cluster_attr(cudaLaunchAttribute &at, int cs)
     {
         std::memset(&at, 0, sizeof(at));
@@ -722,8 +730,8 @@ struct Solver {
     // hh table of the geometry frozen in `op` (set by build_time_dependent_perturbation).
     void build_hh(double *dst, double a1, double a2)
     {
-        k_hh_table<<<(unsigned)((Nr + 255) / 256), 256, 0, stream>>>(dst, d_r.p, Nr, K, op.R1, op.R2, op.q,
-                                                                     -mu * op.Mtot, a1, a2);
+        CK(launch_pdl(k_hh_table, (unsigned)((Nr + 255) / 256), 256, 0, stream, dst, d_r.p, Nr, K, op.R1, op.R2, op.q,
+                                                                     -mu * op.Mtot, a1, a2));
         launch_check();
     }
 
@@ -833,8 +841,8 @@ struct Solver {
         if (ap.count == 0) return;
         const int degree = 2 * l_max, threads = abs_threads();
         const unsigned blocks = (unsigned)((ap.hi[0] - ap.lo[0]) + (ap.count > 1 ? ap.hi[1] - ap.lo[1] : 0));
-        k_abs_moments<<<blocks, threads, (size_t)(degree + 1) * (threads / 32) * sizeof(double), stream>>>(
-            d_r.p, Nr, abs_nodes(), d_glx.p, d_glw.p, degree, ap);
+        CK(launch_pdl(k_abs_moments, blocks, threads, (size_t)(degree + 1) * (threads / 32) * sizeof(double), stream, 
+            d_r.p, Nr, abs_nodes(), d_glx.p, d_glw.p, degree, ap));
         launch_check();
     }
 
@@ -860,8 +868,8 @@ struct Solver {
         }
         if (ap.count == 0) return;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(1024, (work + 255) / 256));
-        k_swave_projector<<<blocks, 256, 0, stream>>>(d_r.p, Nr, n_modes, dr, d_ang00.p, d_mode_l.p, d_mode_m.p, theta,
-                                                       ap);
+        CK(launch_pdl(k_swave_projector, blocks, 256, 0, stream, d_r.p, Nr, n_modes, dr, d_ang00.p, d_mode_l.p, d_mode_m.p, theta,
+                                                       ap));
         launch_check();
     }
 
@@ -900,10 +908,10 @@ struct Solver {
 
     void sink_dots(const double2 *xv, double2 *dots, const Absorber *const *sk, int k, int gate_mode = GATE_NONE)
     {
-        k_sink_dots<<<1, 1024, 0, stream>>>(xv, Nr, n_modes, k, k > 0 ? sk[0]->v.p : nullptr,
+        CK(launch_pdl(k_sink_dots, 1, 1024, 0, stream, xv, Nr, n_modes, k, k > 0 ? sk[0]->v.p : nullptr,
                                            k > 1 ? sk[1]->v.p : nullptr, k > 0 ? sk[0]->lo : 0,
                                            k > 0 ? sk[0]->hi : 0, k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, dots,
-                                           gate_mode == GATE_NONE ? nullptr : d_kr.p, gate_mode);
+                                           gate_mode == GATE_NONE ? nullptr : d_kr.p, gate_mode));
         launch_check();
     }
 
@@ -1063,9 +1071,11 @@ struct Solver {
         if (pcl_per > 0) {
             const size_t smem = (size_t)PCL_THREADS * pcl_per * sizeof(double2);
             cudaLaunchConfig_t cfg = cluster_config(pcl_cs, n_modes, smem);
-            cudaLaunchAttribute at;
-            cluster_attr(at, pcl_cs);
-            cfg.attrs = &at;
+            cudaLaunchAttribute at[2];
+            cluster_attr(at[0], pcl_cs);
+            pdl_attr(at[1]);
+            cfg.attrs = at;
+            cfg.numAttrs = 2;
             kt_begin(TK_PFACTOR);
             CK(cudaLaunchKernelEx(&cfg, k_precond_factor_cl, grid(), table(), (const double *)d_hh.p, 0.5 * dtv,
                                   offdiag(dtv), pcl_per, dinv.p, d_status.p));
@@ -1114,9 +1124,11 @@ struct Solver {
     {
         const size_t smem = (size_t)2 * PCL_THREADS * pcl_per * sizeof(double2);
         cudaLaunchConfig_t cfg = cluster_config(pcl_cs, b2 ? 2 * n_modes : n_modes, smem);
-        cudaLaunchAttribute at;
-        cluster_attr(at, pcl_cs);
-        cfg.attrs = &at;
+        cudaLaunchAttribute at[2];
+        cluster_attr(at[0], pcl_cs);
+        pdl_attr(at[1]);
+        cfg.attrs = at;
+        cfg.numAttrs = 2;
         kt_begin(TK_PSOLVE);
         CK(cudaLaunchKernelEx(&cfg, k_precond_solve_cl, Nr, n_modes, pcl_per, offdiag(dtv), (const double2 *)dinv.p,
                               bv, xv, b2, x2, in, wd));
@@ -1200,7 +1212,7 @@ struct Solver {
         launch_check();
         kt_end(TK_DIAG);
         const int nslots = 2 * n_modes + 3;
-        k_sum_slots<<<nslots, 256, 0, stream>>>(d_partials.p, (int)dblocks, nslots, d_red.p, d_kr.p);
+        CK(launch_pdl(k_sum_slots, nslots, 256, 0, stream, d_partials.p, (int)dblocks, nslots, d_red.p, d_kr.p));
         launch_check();
     }
 
@@ -1237,8 +1249,8 @@ struct Solver {
             apply_A(z.p, t.p, sk, k, reinterpret_cast<const double2 *>(&dk->sdots[1][0]), dtv, ds);
         }
         // x += alpha y + omega z; r = s - omega t; then KS_UPDATE and the next beta
-        k_bicg_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, x.p, y.p, z.p, rr.p, s.p, t.p, r0.p,
-                                                               d_partials.p, d_red.p, ticket(TK_UPDATE_T));
+        CK(launch_pdl(k_bicg_update, vec_blocks, VEC_THREADS, 0, stream, nN, dk, x.p, y.p, z.p, rr.p, s.p, t.p, r0.p,
+                                                               d_partials.p, d_red.p, ticket(TK_UPDATE_T)));
         launch_check();
     }
 
@@ -1267,8 +1279,8 @@ struct Solver {
             ds.gate_mode = GATE_DONE;
             apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv, ds);
         }
-        k_scale_mask<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, Nr, 0.0, mask ? d_mask.p : nullptr, x.p, psi.p,
-                                                              d_kr.p);
+        CK(launch_pdl(k_scale_mask, vec_blocks, VEC_THREADS, 0, stream, nN, Nr, 0.0, mask ? d_mask.p : nullptr, x.p, psi.p,
+                                                              d_kr.p));
         launch_check();
         enqueue_diagnostics(sk, k);
         const size_t kd = (sizeof(Krylov) + 7) / 8;
@@ -1310,8 +1322,8 @@ struct Solver {
         CK(cudaMemcpyAsync(dk, &h_kr_init, sizeof(kr), cudaMemcpyHostToDevice, stream));
         // with b = rhs / |rhs| (never stored): x = psi / |rhs|, r = r0 = b - A_full x in one
         // pass; its last CTA runs KS_INIT (and the first beta) on |r0|^2 and |b|^2
-        k_krylov_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dk, d_red.p + RED_RHS, rhs.p, psi.p, x.p, rr.p,
-                                                                r0.p, d_partials.p, d_red.p + 8, ticket(TK_START_T));
+        CK(launch_pdl(k_krylov_start, vec_blocks, VEC_THREADS, 0, stream, nN, dk, d_red.p + RED_RHS, rhs.p, psi.p, x.p, rr.p,
+                                                                r0.p, d_partials.p, d_red.p + 8, ticket(TK_START_T)));
         launch_check();
         factorize(dtv);
         if (k > 0) wood_setup(sk, k, dtv);
@@ -1420,8 +1432,8 @@ struct Solver {
             wb.ticket = ticket(TK_WOOD_T);
             wb.kr = d_kr.p;
             const size_t smem = (size_t)2 * (wband_hi - wband_lo) * sizeof(double2);
-            k_wood_setup_band<<<n_modes * k, WSB_THREADS, smem, stream>>>(Nr, n_modes, wband_lo, wband_hi,
-                                                                          offdiag(dtv), dinv.p, wb);
+            CK(launch_pdl(k_wood_setup_band, n_modes * k, WSB_THREADS, smem, stream, Nr, n_modes, wband_lo, wband_hi,
+                                                                          offdiag(dtv), dinv.p, wb));
             launch_check();
             return;
         }
@@ -1481,7 +1493,7 @@ struct Solver {
         // out -= sum_a W_a c_a where the W_a live
         const int64_t nb = (int64_t)(wband_hi - wband_lo) * n_modes;
         const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nb + 255) / 256, vec_blocks));
-        k_woodbury_band<<<blocks, 256, 0, stream>>>(Nr, n_modes, wband_lo, wband_hi, d_kr.p, which, W0.p, W1.p, out);
+        CK(launch_pdl(k_woodbury_band, blocks, 256, 0, stream, Nr, n_modes, wband_lo, wband_hi, d_kr.p, which, W0.p, W1.p, out));
         launch_check();
     }
 

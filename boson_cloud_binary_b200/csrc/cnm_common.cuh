@@ -24,6 +24,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <utility>
 
 namespace cnm {
 
@@ -142,5 +143,28 @@ struct ApplyArgs {
     int gate_mode;
     const struct Krylov *scale_kr;
 };
+
+#ifdef __CUDACC__
+// Launch with programmatic stream serialization: the kernel may be scheduled while the
+// kernel ahead of it on the stream is still running, so its launch overlaps that kernel's
+// tail.  Every kernel launched this way calls pdl_wait() (cnm_device.cuh) before its first
+// access to global memory.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                              Args &&...args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+#endif
 
 }  // namespace cnm

@@ -9,6 +9,12 @@ namespace cnm {
 
 // ------------------------------------------------------------------ reductions
 
+// Programmatic dependent launch: a kernel launched with programmatic stream serialization
+// may be scheduled before the kernel ahead of it on the stream has finished; it waits here,
+// before its first access to global memory, until that kernel has completed and its
+// writes are visible.  A no-op for an ordinary launch.
+__device__ __forceinline__ void pdl_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 __device__ __forceinline__ double warp_sum(double v)
 {
 #pragma unroll

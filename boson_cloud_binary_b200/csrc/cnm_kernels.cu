@@ -22,6 +22,7 @@ __device__ void wood_scalar_dev(Krylov *kr, int which, const double2 *proj);
 __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
                            double scale, double a1, double a2)
 {
+    pdl_wait();
     // one node per thread; the radial factors r_<^l / r_>^(l+1) of both bodies
     // (_hamiltonian.cpp:12-42) by repeated multiplication with r_< / r_> over l
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -912,6 +913,7 @@ __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, 
                             const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots, const Krylov *gate,
                             int gate_mode)
 {
+    pdl_wait();
     if (gate && gate_closed(gate, gate_mode)) return;
     // the (sink, mode, support node) terms are dealt to the threads in a fixed order, a
     // few per thread with independent loads (deterministic: fixed per-thread order, then
@@ -1482,6 +1484,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
                                                                    const double2 *b2, double2 *x2, PrecondInput in,
                                                                    WoodArgs wd)
 {
+    pdl_wait();
     if (!resolve_input(in)) return;
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
@@ -1763,6 +1766,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
 __global__ void __launch_bounds__(WSB_THREADS) k_wood_setup_band(int Nr, int n_modes, int blo, int bhi, double2 off,
                                                                  const double2 *dinv, WoodBand wb)
 {
+    pdl_wait();
     extern __shared__ double2 wsb[];
     __shared__ Aff wagg[WSB_THREADS / 32];
     __shared__ double wscr[4 * 32];
@@ -1940,6 +1944,7 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
                                                                     double half_dt, double2 off, int per,
                                                                     double2 *dinv, int *status)
 {
+    pdl_wait();
     namespace cg = cooperative_groups;
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double2 smc[];
@@ -2121,6 +2126,7 @@ __global__ void k_axpby(int64_t n, double2 a, const double2 *x, double2 b, const
 __global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y,
                              const Krylov *kr)
 {
+    pdl_wait();
     // with kr: s = kr->rhs_norm, and only once the candidate is accepted
     if (kr) {
         if (!kr->accepted) return;
@@ -2154,6 +2160,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, Krylov *
                                                               const double2 *t, const double2 *r0, double *partials,
                                                               double *red, unsigned *ticket)
 {
+    pdl_wait();
     if (kr->done || kr->restart) return;  // queued ahead of the convergence test
     __shared__ double scratch[6 * 32];
     const double2 al = kr->alpha, w = kr->omega;
@@ -2194,6 +2201,7 @@ __global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2
 __global__ void k_woodbury_band(int Nr, int n_modes, int lo, int hi, const Krylov *kr, int which, const double2 *W0,
                                 const double2 *W1, double2 *y)
 {
+    pdl_wait();
     if (kr->done || kr->restart) return;  // queued ahead of the convergence test
     const double2 c0 = kr->wc[which][0], c1 = kr->wc[which][1];
     const int k = kr->n_sinks, w = hi - lo;
@@ -2271,6 +2279,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov 
                                                                double2 *r, double2 *r0, double *partials, double *red,
                                                                unsigned *ticket)
 {
+    pdl_wait();
     __shared__ double scratch[6 * 32];
     const double nrm = sqrt(red_in[0]);
     const double sc = nrm > 0.0 ? 1.0 / nrm : 0.0;
@@ -2395,6 +2404,7 @@ __device__ void abs_moments_node(const double *r, int Nr, int i, double radius, 
 __global__ void k_abs_moments(const double *r, int Nr, int nq, const double *gl_x, const double *gl_w, int degree,
                               AbsorberPair ap)
 {
+    pdl_wait();
     extern __shared__ double sh[];  // (degree + 1) * nwarps
     const int n0 = ap.hi[0] - ap.lo[0];
     const int a = (int)blockIdx.x < n0 ? 0 : 1;
@@ -2410,6 +2420,7 @@ __global__ void __launch_bounds__(256) k_swave_projector(const double *r, int Nr
                                                          const double *ang00, const int *mode_l, const int *mode_m,
                                                          double theta, AbsorberPair ap)
 {
+    pdl_wait();
     __shared__ double scratch[32];
     __shared__ double norm_s[2];
     for (int a = 0; a < ap.count; ++a) {
@@ -2579,6 +2590,7 @@ __global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics(Grid g, CouplingT
 // out[q] = sum_b partials[q][b]: one CTA per slot, coalesced loads, fixed-order tree.
 __global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out, const Krylov *gate)
 {
+    pdl_wait();
     if (gate && gate_closed(gate, GATE_ACCEPTED)) return;
     __shared__ double scratch[32];
     const int q = blockIdx.x;
