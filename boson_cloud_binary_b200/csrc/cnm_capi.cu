@@ -1123,6 +1123,7 @@ struct Solver {
                                            nullptr})
     {
         const size_t smem = (size_t)2 * PCL_THREADS * pcl_per * sizeof(double2);
+        in.fault = d_status.p;
         cudaLaunchConfig_t cfg = cluster_config(pcl_cs, b2 ? 2 * n_modes : n_modes, smem);
         cudaLaunchAttribute at[2];
         cluster_attr(at[0], pcl_cs);

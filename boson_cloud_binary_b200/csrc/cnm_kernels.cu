@@ -1474,6 +1474,32 @@ __device__ __forceinline__ Mob mob_identity()
     return m;
 }
 
+// Bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned) from global to
+// this CTA's shared memory, completing on the mbarrier at shared address `bar`.
+__device__ __forceinline__ void bulk_load_s(void *dst, const void *src, unsigned bytes, unsigned bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     (unsigned)__cvta_generic_to_shared(dst)),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+// Wait for phase `parity` of the mbarrier at `bar`, giving up after a bounded number of
+// polls (each try_wait suspends for a hardware-chosen interval); false if it gave up.
+__device__ __forceinline__ bool mbar_wait_parity(unsigned bar, unsigned parity)
+{
+    for (int it = 0; it < (1 << 22); ++it) {
+        unsigned done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 // x = P^{-1} b for every radial block, exact (see the scan scheme above).  Grid
 // (cluster size, blocks): blockIdx.y selects the mode j = blockIdx.y % n_modes and,
 // for blockIdx.y >= n_modes, the second right-hand side / output pair (b2, x2), so
@@ -1504,46 +1530,44 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     // staging: two elements per thread in flight (every load of a batch issues
     // before its stores)
-    constexpr int SB = 2;
-    if (in.mode == PI_PLAIN) {
-        const double2 *__restrict__ bsrc = bv + base;
-        const double2 *__restrict__ dsrc = dinv + base;
-        for (int e0 = tid; e0 < len; e0 += SB * T) {
-            double2 dv[SB], yv[SB];
-#pragma unroll
-            for (int u = 0; u < SB; ++u) {
-                const int e = e0 + u * T;
-                if (e < len) {
-                    dv[u] = dsrc[e];
-                    yv[u] = bsrc[e];
-                }
-            }
-#pragma unroll
-            for (int u = 0; u < SB; ++u) {
-                const int e = e0 + u * T;
-                if (e < len) {
-                    D[e] = dv[u];
-                    Y[e] = yv[u];
-                }
-            }
+    // staging: the pivots and b (or r) arrive by bulk copies into shared memory that
+    // complete on an mbarrier; the threads load the other inputs of a BiCGSTAB combination
+    __shared__ __align__(8) unsigned long long stage_bar;
+    const unsigned bar = (unsigned)__cvta_generic_to_shared(&stage_bar);
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    if (len > 0) {
+        if (tid == 0) {
+            const unsigned bytes = (unsigned)len * (unsigned)sizeof(double2);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(2u * bytes)
+                         : "memory");
+            bulk_load_s(D, dinv + base, bytes, bar);
+            bulk_load_s(Y, (in.mode == PI_PLAIN ? bv : in.r) + base, bytes, bar);
         }
-    } else {
+        if (!mbar_wait_parity(bar, 0u)) {
+            // the copies did not complete in time: flag the solve as failed (the attempt
+            // is then not accepted) and wait once more for them before going on
+            if (tid == 0 && in.fault) atomicOr(in.fault, 2);
+            mbar_wait_parity(bar, 0u);
+        }
+    }
+    if (in.mode != PI_PLAIN) {
         const double2 beta = in.kr->beta, omega = in.kr->omega, alpha = in.kr->alpha;
-        const double2 *__restrict__ dsrc = dinv + base;
-        const double2 *__restrict__ rsrc = in.r + base;
         // PI_P without p_old (first iteration: p_old = v = 0) is p = r
         const bool first = in.mode == PI_P && in.p_old == nullptr;
         const double2 *__restrict__ vsrc = first ? nullptr : in.v + base;
         const double2 *__restrict__ psrc = (in.mode == PI_P && !first) ? in.p_old + base : nullptr;
         double2 *__restrict__ odst = in.out + base;
+        constexpr int SB = 4;
         for (int e0 = tid; e0 < len; e0 += SB * T) {
-            double2 dv[SB], rv[SB], vv[SB], pv[SB];
+            double2 vv[SB], pv[SB];
 #pragma unroll
             for (int u = 0; u < SB; ++u) {
                 const int e = e0 + u * T;
                 if (e < len) {
-                    dv[u] = dsrc[e];
-                    rv[u] = rsrc[e];
                     vv[u] = vsrc ? vsrc[e] : cmake(0.0, 0.0);
                     pv[u] = psrc ? psrc[e] : cmake(0.0, 0.0);
                 }
@@ -1552,10 +1576,10 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
             for (int u = 0; u < SB; ++u) {
                 const int e = e0 + u * T;
                 if (e < len) {
-                    const double2 rhsv = first ? rv[u]
-                                         : psrc ? cadd(rv[u], cmul(beta, csub(pv[u], cmul(omega, vv[u]))))
-                                                : csub(rv[u], cmul(alpha, vv[u]));
-                    D[e] = dv[u];
+                    const double2 rv = Y[e];
+                    const double2 rhsv = first ? rv
+                                         : psrc ? cadd(rv, cmul(beta, csub(pv[u], cmul(omega, vv[u]))))
+                                                : csub(rv, cmul(alpha, vv[u]));
                     Y[e] = rhsv;
                     odst[e] = rhsv;
                 }

@@ -52,6 +52,7 @@ struct PrecondInput {
     double2 *p_alt;
     int first;
     int gate;  // GateMode of the launch (GATE_ITER for the iteration's solves)
+    int *fault = nullptr;  // set (bit 1) when a staging copy did not complete in time
 };
 
 // Launches queued ahead of the host's convergence test skip themselves on the device:
