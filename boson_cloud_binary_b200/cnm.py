@@ -76,7 +76,7 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
            "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel",
            "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy",
-           "cnm_displaced_100_state")
+           "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info")
 
 def displaced_100_state(r, modes, mu, x_bh):
     """displaced_100_state (src/DisplacedAtom.cpp:12-76) on the device: the mode projection
@@ -104,6 +104,8 @@ def measure_fp64_peak():
         raise CudaError(L.cnm_create_error().decode())
     return v.value
 
+
+PRECISIONS = {"fp64": 0, "mixed": 1}
 
 KERNELS = {"apply": 0, "precond_solve": 1, "precond_factor": 2, "diagnostics": 3}
 
@@ -143,6 +145,8 @@ def load_library():
     L.cnm_step.argtypes = [p, i32, C.POINTER(cnm_diag), dp, dp, dp, dp]
     L.cnm_should_stop.argtypes = [p, C.POINTER(i32)]
     L.cnm_apply.argtypes = [p, i32, dp, dp]
+    L.cnm_apply_lowp.argtypes = [p, i32, dp, dp]
+    L.cnm_mixed_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), dp]
     L.cnm_sink_strength.argtypes = [p, i32, dp]
     L.cnm_sink_active.argtypes = [p, C.POINTER(i32)]
     L.cnm_sink_vector.argtypes = [p, i32, dp]
@@ -187,15 +191,20 @@ class Diag(dict):
 
 
 class CrankNicolsonModes:
-    """B200 drop-in of the reference's CrankNicolsonModes (FP64 path)."""
+    """B200 drop-in of the reference's CrankNicolsonModes.
+
+    ``precision="fp64"`` (default) is the complex128 drop-in; ``precision="mixed"`` solves
+    each step by defect correction with complex64 inner iterations on the tensor-core
+    coupling apply and fp64 residuals, stopping at the relative residual ``tolerance``."""
 
     def __init__(self, Nx, L, dt, epsilon, l_max, mu, M_c, q, a, R, counter, absorption, save_every,
-                 ramp_periods, epsilon_smear, config_file=None, _handle=None):
+                 ramp_periods, epsilon_smear, config_file=None, _handle=None, precision="fp64"):
         lib = load_library()
         if _handle is None:
             prm = cnm_params(int(Nx), float(L), float(dt), float(epsilon), int(l_max), float(mu), float(M_c),
                              float(q), float(a), float(R), int(bool(counter)), int(bool(absorption)),
-                             int(save_every), float(ramp_periods), float(epsilon_smear), 0)
+                             int(save_every), float(ramp_periods), float(epsilon_smear),
+                             PRECISIONS[precision])
             h = C.c_void_p()
             rc = lib.cnm_create(C.byref(prm), C.byref(h))
             if rc != CNM_OK:
@@ -342,6 +351,19 @@ class CrankNicolsonModes:
         y = np.zeros(2 * self.size)
         self._check(self._lib.cnm_apply(self._h, OPS[op], _dptr(x.view(np.float64)), _dptr(y)))
         return y.view(np.complex128).copy()
+
+    def apply_lowp(self, op, x):
+        """The mixed path's complex64 tensor-core operator (op in H, V, A, A_full)."""
+        x = np.ascontiguousarray(np.asarray(x, np.complex128))
+        y = np.zeros(2 * self.size)
+        self._check(self._lib.cnm_apply_lowp(self._h, OPS[op], _dptr(x.view(np.float64)), _dptr(y)))
+        return y.view(np.complex128).copy()
+
+    def mixed_info(self):
+        """(passes, fp64 operator applications, final relative residual) of the last mixed step."""
+        p, f, r = C.c_int32(), C.c_int32(), C.c_double()
+        self._check(self._lib.cnm_mixed_info(self._h, C.byref(p), C.byref(f), C.byref(r)))
+        return p.value, f.value, r.value
 
     def apply_sink(self, x):
         return self.apply("sink", x)

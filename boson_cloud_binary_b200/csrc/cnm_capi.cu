@@ -13,6 +13,7 @@
 #include "cnm_coupling.h"
 #include "cnm_kernels.cuh"
 #include "cnm_apply5.cuh"
+#include "cnm_mixed.cuh"
 
 #include <cuda_runtime.h>
 
@@ -294,6 +295,22 @@ struct Solver {
     // pinned host staging
     double *h_stage = nullptr;
     size_t h_stage_n = 0;
+    // mixed precision (CNM_MIXED): tensor-core Gaunt image and plan, complex64 work
+    // vectors, fp32 pivots, the fp64 residual and the inner scalars
+    bool mixed = false;
+    TcGaunt tg;
+    TcPlan tcp;
+    DevBuf<uint8_t> d_tcblob;
+    DevBuf<int> d_tc_loff, d_tc_lbytes, d_tc_slices, d_tc_lnblk;
+    DevBuf<float2> m_r, m_y, m_v, m_s, m_z, m_t, m_d, m_xa, dinv32;
+    DevBuf<double2> m_r64, m_dots;  // m_dots: [0..1] sink projections, [2..3] corrected ones
+    DevBuf<MixScalars> d_msc;
+    DevBuf<double> m_part;
+    int ps_per = 0, ps_cs = 0;      // fp32 cluster solve: nodes per thread, CTAs per cluster
+    int mx_passes = 0, mx_fp64 = 0; // counters of the last mixed step
+    double mx_residual = 0.0;
+    double mixed_tol = 1e-12;       // fp64 relative residual the mixed solve stops at
+    int mixed_max_passes = 8;
     // profiling
     bool profiling = false;
     KernelTimer ktime[TK_COUNT];
@@ -345,7 +362,8 @@ struct Solver {
     {
         if (Nr < 3 || l_max < 0 || L <= 0.0 || dt <= 0.0 || save_every <= 0)
             throw Error(CNM_EINVAL, "Require Nr >= 3, l_max >= 0, and positive L, dt, save_every");
-        if (pr.precision != CNM_FP64) throw Error(CNM_EINVAL, "unknown precision");
+        if (pr.precision != CNM_FP64 && pr.precision != CNM_MIXED) throw Error(CNM_EINVAL, "unknown precision");
+        mixed = pr.precision == CNM_MIXED;
         Omega = 0.0;
         Omega_0 = std::sqrt((1.0 + q) / std::pow(R, 3));
         P = initial_period;
@@ -455,6 +473,43 @@ struct Solver {
         CK(cudaFuncSetAttribute(k_precond_factor2, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024));
         plan_cluster_scans();
         d_wpart.alloc((size_t)8 * std::max(1, pcl_cs) * 2 * n_modes);
+        if (mixed) setup_mixed(nsm);
+    }
+
+    // Tensor-core image of the Gaunt matrices, the tensor-core apply's plan, the fp32
+    // cluster solve's plan and the complex64 work vectors of the mixed solve.
+    void setup_mixed(int nsm)
+    {
+        if (pcl_per <= 0) throw Error(CNM_EINVAL, "The mixed solve needs the cluster preconditioner scans");
+        tg = build_tc_gaunt(cpl);
+        int amax = 0;
+        for (int b : tg.l_bytes) amax = std::max(amax, b);
+        if (!tc_plan(n_modes, Nr, amax, nsm, tcp))
+            throw Error(CNM_EINVAL, "The mixed solve supports at most 128 modes (l_max <= 14)");
+        std::vector<uint8_t> bytes(tg.blob.size() * 2);
+        std::memcpy(bytes.data(), tg.blob.data(), bytes.size());
+        upload(d_tcblob, bytes);
+        upload(d_tc_loff, tg.l_off);
+        upload(d_tc_lbytes, tg.l_bytes);
+        upload(d_tc_slices, tg.slices);
+        upload(d_tc_lnblk, tg.l_nblk);
+        CK(tc_prepare(tcp));
+        for (DevBuf<float2> *b : {&m_r, &m_y, &m_v, &m_s, &m_z, &m_t, &m_d, &m_xa, &dinv32}) b->alloc(nN);
+        m_r64.alloc(nN);
+        m_dots.alloc(8);
+        d_msc.alloc(1);
+        m_part.alloc((size_t)8 * std::max(vec_blocks, tcp.grid));
+        // fp32 cluster solve: the fp64 solve's CTAs per cluster, nodes per thread from it
+        ps_cs = pcl_cs;
+        ps_per = pcl_per;
+        int optin = 0, dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+        cudaFuncAttributes fa;
+        CK(cudaFuncGetAttributes(&fa, k_psolve32_cl));
+        CK(cudaFuncSetAttribute(k_psolve32_cl, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                optin - (int)fa.sharedSizeBytes));
+        if (ps_cs > 8) CK(cudaFuncSetAttribute(k_psolve32_cl, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     }
 
     // Work plan of the operator kernel: for 1..8 CTA groups per 64-node tile, the LPT
@@ -1172,11 +1227,12 @@ struct Solver {
     // The diagnostics pass of the accepted end-of-step state with the step's operators
     // (src/CrankNicolsonModes_extraction.cpp), gated on the candidate's acceptance:
     // the sink projections of the new state, the fused pass and the sums of its slots.
-    void enqueue_diagnostics(const Absorber *const *sk, int k)
+    void enqueue_diagnostics(const Absorber *const *sk, int k, const double2 *state = nullptr)
     {
+        const double2 *st = state ? state : psi.p;
         const Absorber *all[2] = {&abs1, &abs2};
         const bool have_sinks = absorption && cpl.mode00 >= 0;
-        if (have_sinks) sink_dots(psi.p, d_dots.p + 4, all, 2, GATE_ACCEPTED);
+        if (have_sinks) sink_dots(st, d_dots.p + 4, all, 2, GATE_ACCEPTED);
         const dim3 dgrid = apply_grid();
         unsigned dblocks = dgrid.x * dgrid.y;
         kt_begin(TK_DIAG);
@@ -1185,7 +1241,7 @@ struct Solver {
             da.hh = d_hh.p;
             da.theta = op.theta;
             da.domega = op.domega;
-            da.psi = psi.p;
+            da.psi = st;
             da.idx_ex = idx_ex;
             da.n_sinks = k;
             da.sv0 = k > 0 ? sk[0]->v.p : nullptr;
@@ -1204,7 +1260,7 @@ struct Solver {
             dblocks = ::cnm::launch_diag5(l_max, stream, grid(), d_d5tab.p, da);
         } else {
             ::cnm::launch_diagnostics(
-                l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, psi.p,
+                l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, st,
                 idx_ex, k, k > 0 ? sk[0]->v.p : nullptr, k > 1 ? sk[1]->v.p : nullptr,
                 k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
                 k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
@@ -1259,7 +1315,321 @@ struct Solver {
     // 2 n + 3 sums, psi and dpsi/dt around the extraction node, the sink projections.
     size_t readback_doubles() const
     {
-        return (sizeof(Krylov) + 7) / 8 + (size_t)(2 * n_modes + 3) + 8 * (size_t)n_modes + 16;
+        return (sizeof(Krylov) + 7) / 8 + (size_t)(2 * n_modes + 3) + 8 * (size_t)n_modes + 16 +
+               (sizeof(MixScalars) + 7) / 8;
+    }
+
+    // -------------------------------------------------------------- mixed precision
+
+    TcTable tc_table() const
+    {
+        TcTable t;
+        t.blob = d_tcblob.p;
+        t.l_off = d_tc_loff.p;
+        t.l_bytes = d_tc_lbytes.p;
+        t.slices = d_tc_slices.p;
+        t.l_nblk = d_tc_lnblk.p;
+        return t;
+    }
+
+    // y = A_full x on complex64 vectors (tensor-core coupling): alpha = 1, beta = i dt/2,
+    // the sinks with their projections at `dots`; up to three fused reductions.
+    TcArgs tc_a_args(const float2 *xv, float2 *yv, const Absorber *const *sk, int k, const double2 *dots, double dtv)
+    {
+        TcArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.x = xv;
+        a.y = yv;
+        a.alpha = make_float2(1.f, 0.f);
+        a.beta = make_float2(0.f, (float)(0.5 * dtv));
+        a.use_h0 = 1;
+        a.use_cap = 1;
+        a.use_v = 1;
+        a.hh = d_hh.p;
+        a.theta = (float)op.theta;
+        a.n_sinks = k;
+        a.sink_dots = dots;
+        for (int i = 0; i < k; ++i) {
+            a.sink_v[i] = sk[i]->v.p;
+            a.sink_coef[i] = (float)(0.25 * dtv * sk[i]->strength);
+            a.sink_lo[i] = sk[i]->lo;
+            a.sink_hi[i] = sk[i]->hi;
+        }
+        a.partials = m_part.p;
+        a.status = d_status.p;
+        return a;
+    }
+
+    void launch_tc(const TcArgs &a)
+    {
+        kt_begin(TK_APPLY);
+        CK(launch_tc_apply(tcp, stream, grid(), d_mode_l.p, d_mode_m.p, K, tc_table(), a));
+        kt_end(TK_APPLY);
+    }
+
+    void mx_finish(int nblocks, int nslots, int stage)
+    {
+        k_mx_finish<<<1, 256, 0, stream>>>(m_part.p, nblocks, nslots, d_msc.p, stage);
+        launch_check();
+    }
+
+    // out = P32^{-1} in (mode 0) or, mode 1, s = r - alpha v formed and stored, out = P32^{-1} s
+    void psolve32(int mode, const float2 *in, float2 *out)
+    {
+        Ps32Args a;
+        std::memset(&a, 0, sizeof(a));
+        a.mode = mode;
+        a.b = in;
+        a.r = m_r.p;
+        a.v = m_v.p;
+        a.s_out = m_s.p;
+        a.sc = d_msc.p;
+        a.status = d_status.p;
+        cudaLaunchConfig_t cfg;
+        std::memset(&cfg, 0, sizeof(cfg));
+        cfg.gridDim = dim3((unsigned)ps_cs, (unsigned)n_modes, 1);
+        cfg.blockDim = dim3(PS32_THREADS, 1, 1);
+        cfg.dynamicSmemBytes = (size_t)2 * PS32_THREADS * ps_per * sizeof(float2);
+        cfg.stream = stream;
+        cudaLaunchAttribute at[1];
+        cluster_attr(at[0], ps_cs);
+        cfg.attrs = at;
+        cfg.numAttrs = 1;
+        const double2 o = offdiag(op.dt);
+        kt_begin(TK_PSOLVE);
+        CK(cudaLaunchKernelEx(&cfg, k_psolve32_cl, Nr, ps_per, make_float2((float)o.x, (float)o.y),
+                              (const float2 *)dinv32.p, out, a));
+        kt_end(TK_PSOLVE);
+    }
+
+    // One defect-correction pass on the current residual m_r (complex64): one
+    // right-preconditioned BiCGSTAB iteration from d = 0 (_matrices.cpp:47-91 with
+    // r0 = r, rho = |r|^2, p = r): y = M r, v = A y, alpha = rho / r.v, s = r - alpha v,
+    // z = M s, t = A z, omega = t.s / |t|^2, d = alpha y + omega z; x += d in fp64.
+    void mixed_pass(const Absorber *const *sk, int k, double dtv)
+    {
+        psolve32(0, m_r.p, m_y.p);
+        wood32(sk, k, m_y.p);
+        {
+            TcArgs a = tc_a_args(m_y.p, m_v.p, sk, k, m_dots.p + 2, dtv);
+            a.n_dots = 1;
+            a.dot_kind[0] = 1;
+            a.dot_ext[0] = m_r.p;
+            launch_tc(a);
+            mx_finish(tcp.grid, 2, MX_ALPHA);
+        }
+        psolve32(1, nullptr, m_z.p);
+        wood32(sk, k, m_z.p);
+        {
+            TcArgs a = tc_a_args(m_z.p, m_t.p, sk, k, m_dots.p + 2, dtv);
+            a.n_dots = 2;
+            a.dot_kind[0] = 2;
+            a.dot_ext[0] = m_s.p;
+            a.dot_kind[1] = 3;
+            launch_tc(a);
+            mx_finish(tcp.grid, 4, MX_OMEGA);
+        }
+        k_mx_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, x.p, m_y.p, m_z.p, m_d.p, m_part.p);
+        launch_check();
+        mx_finish(vec_blocks, 1, MX_D2);
+        ++mx_passes;
+    }
+
+    // fp64 residual of x: r64 = rhs - A_full x (fp64 operator), r = r64 in complex64.
+    void mixed_resid64(const Absorber *const *sk, int k, double dtv, double2 *diff = nullptr)
+    {
+        sink_dots(x.p, d_dots.p, sk, k);
+        apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv);
+        k_mx_resid<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, tmp.p, m_r64.p, diff, m_r.p, m_part.p);
+        launch_check();
+        mx_finish(vec_blocks, 1, MX_R64);
+        ++mx_fp64;
+    }
+
+    // Residual of x = x_prev + d from the tensor-core operator: |r64 - A_full d|^2, where
+    // r64 is the fp64 residual of x_prev (valid when |d| is small, see mixed_check_bound).
+    void mixed_resid_tc(const Absorber *const *sk, int k, double dtv)
+    {
+        if (k > 0) {
+            k_sink_dots32<<<1, 1024, 0, stream>>>(m_d.p, Nr, n_modes, k, sk[0]->v.p, k > 1 ? sk[1]->v.p : nullptr,
+                                                 sk[0]->lo, sk[0]->hi, k > 1 ? sk[1]->lo : 0,
+                                                 k > 1 ? sk[1]->hi : 0, m_dots.p + 4);
+            launch_check();
+        }
+        TcArgs a = tc_a_args(m_d.p, m_t.p, sk, k, m_dots.p + 4, dtv);
+        a.n_dots = 1;
+        a.dot_kind[0] = 4;
+        a.dot_ext64 = m_r64.p;
+        launch_tc(a);
+        mx_finish(tcp.grid, 2, MX_TCRES);
+    }
+
+    // Bound of the error of the tensor-core residual: the coupling of A_full d is formed
+    // from bf16 operands (relative rounding 2^-8 per product, fp32 sums), so
+    //   |err| <= (dt/2) 2^-7 sum_l* |G_l*|_F max|h_l*| |d|  (2^-7: rounding and sums),
+    // with max|h_l*| <= mu (M1+M2) (1/((1+q) R1) + |w| q/((1+q) R2)); the stencil, CAP and
+    // sinks are combined in fp64 from fp32 inputs (relative 2^-23 of |A d|).
+    double mixed_check_bound(double d_norm, double dtv) const
+    {
+        const double h = mu * op.Mtot * (1.0 / ((1 + op.q) * std::max(op.R1, dr)) +
+                                         std::abs(op.w) * op.q / ((1 + op.q) * std::max(op.R2, dr)));
+        const double kin = 4.0 / (2.0 * mu * dr * dr);
+        return (0.5 * dtv * std::ldexp(tg.fro_sum * h, -7) + std::ldexp(1.0 + 0.5 * dtv * kin, -22)) * d_norm;
+    }
+
+    // Calibration of the tensor-core residual check on the pass just verified in fp64:
+    // |(r_before - r_after) - A_tc d|^2 with d the pass's correction (m_d) and the fp64
+    // change of the residual in cand.
+    void mixed_calibrate(const Absorber *const *sk, int k, double dtv)
+    {
+        if (k > 0) {
+            k_sink_dots32<<<1, 1024, 0, stream>>>(m_d.p, Nr, n_modes, k, sk[0]->v.p, k > 1 ? sk[1]->v.p : nullptr,
+                                                 sk[0]->lo, sk[0]->hi, k > 1 ? sk[1]->lo : 0,
+                                                 k > 1 ? sk[1]->hi : 0, m_dots.p + 4);
+            launch_check();
+        }
+        TcArgs a = tc_a_args(m_d.p, m_t.p, sk, k, m_dots.p + 4, dtv);
+        a.n_dots = 1;
+        a.dot_kind[0] = 4;
+        a.dot_ext64 = cand.p;
+        launch_tc(a);
+        mx_finish(tcp.grid, 2, MX_ECAL);
+    }
+
+    // psi candidate = mask x into cand, the diagnostics pass on it, the read-backs (the
+    // Krylov struct's slot, the diagnostics sums, the edge values, the sink projections,
+    // then the inner scalars).
+    void mixed_tail(const Absorber *const *sk, int k, double *hs)
+    {
+        CK(launch_pdl(k_scale_mask, vec_blocks, VEC_THREADS, 0, stream, nN, Nr, 1.0, mask ? d_mask.p : nullptr,
+                      (const double2 *)x.p, cand.p, (const Krylov *)nullptr));
+        launch_check();
+        enqueue_diagnostics(sk, k, cand.p);
+        const size_t kd = (sizeof(Krylov) + 7) / 8;
+        const int nslots = 2 * n_modes + 3;
+        CK(cudaMemcpyAsync(hs, d_kr.p, sizeof(Krylov), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hs + kd, d_red.p, nslots * sizeof(double), cudaMemcpyDeviceToHost, stream));
+        CK(cudaMemcpyAsync(hs + kd + nslots, d_edge.p, 4 * n_modes * sizeof(double2), cudaMemcpyDeviceToHost,
+                           stream));
+        CK(cudaMemcpyAsync(hs + kd + nslots + 8 * n_modes, d_dots.p, 8 * sizeof(double2), cudaMemcpyDeviceToHost,
+                           stream));
+        CK(cudaMemcpyAsync(hs + kd + nslots + 8 * n_modes + 16, d_msc.p, sizeof(MixScalars), cudaMemcpyDeviceToHost,
+                           stream));
+    }
+
+    MixScalars mixed_scalars(const double *hs) const
+    {
+        MixScalars m;
+        const size_t kd = (sizeof(Krylov) + 7) / 8;
+        std::memcpy(&m, hs + kd + (2 * n_modes + 3) + 8 * n_modes + 16, sizeof(m));
+        return m;
+    }
+
+    // The mixed solve of one step, queued without waiting: rhs is in place (fp64 rhs
+    // apply); pivots (fp64, then fp32 copies), Woodbury set-up, r0 = 2 (rhs - psi), pass 1,
+    // the fp64 residual and the calibration of the tensor-core check, pass 2, the
+    // tensor-core residual check, and the tail.
+    void begin_mixed(const Absorber *const *sk, int k, double *hs)
+    {
+        const double dtv = op.dt;
+        mx_passes = 0;
+        mx_fp64 = 1;  // the right-hand side
+        Krylov kr;
+        std::memset(&kr, 0, sizeof(kr));
+        kr.n_sinks = k;
+        kr.accepted = 1;  // gates of the diagnostics pass: the host decides acceptance
+        kr.rhs_norm = 1.0;
+        kr.status = d_status.p;
+        h_kr_init = kr;
+        CK(cudaMemcpyAsync(d_kr.p, &h_kr_init, sizeof(kr), cudaMemcpyHostToDevice, stream));
+        jacobi = false;
+        factorize(dtv);
+        k_to_f32<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dinv.p, dinv32.p);
+        launch_check();
+        if (k > 0) wood_setup(sk, k, dtv);
+        k_mx_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, psi.p, x.p, m_r64.p, m_r.p, m_part.p);
+        launch_check();
+        mx_finish(vec_blocks, 2, MX_B2R0);
+        mixed_pass(sk, k, dtv);
+        mixed_resid64(sk, k, dtv, cand.p);
+        mixed_calibrate(sk, k, dtv);
+        mixed_pass(sk, k, dtv);
+        mixed_resid_tc(sk, k, dtv);
+        mixed_tail(sk, k, hs);
+    }
+
+    // Waits for the queued mixed solve and decides: accepted when the tensor-core residual
+    // plus four times its calibrated error is within `tolerance`; when only the error
+    // estimate is too large, an fp64 residual decides; otherwise further passes (fp64
+    // residual, pass, tensor-core check) up to mixed_max_passes.  A solve that still misses
+    // `tolerance` is accepted at accept_residual, else the step is redone by the fp64 solve.
+    void finish_mixed(const Absorber *const *sk, int k, double *hs)
+    {
+        const double dtv = op.dt;
+        for (;;) {
+            sync();
+            int st = 0;
+            CK(cudaMemcpy(&st, d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+            const MixScalars m = mixed_scalars(hs);
+            const double bn = std::sqrt(std::max(m.b2, 1e-300));
+            const double res_tc = std::sqrt(m.tc_res2) / bn;
+            const double ratio = m.d2_cal > 0.0 ? std::sqrt(m.e2_cal / m.d2_cal) : 0.0;
+            const double est = 4.0 * ratio * std::sqrt(m.d2) / bn;
+            const bool finite = std::isfinite(res_tc) && std::isfinite(est) && st == 0;
+            bool ok = finite && res_tc + est <= tolerance;
+            double res = res_tc + est;
+            if (finite && !ok && res_tc <= tolerance) {
+                // the estimate alone is too large: the fp64 residual decides
+                mixed_resid64(sk, k, dtv);
+                MixScalars m2;
+                CK(cudaMemcpyAsync(&m2, d_msc.p, sizeof(m2), cudaMemcpyDeviceToHost, stream));
+                sync();
+                res = std::sqrt(m2.r64) / bn;
+                ok = std::isfinite(res) && res <= tolerance;
+                if (!ok) {
+                    // continue from this fp64 residual
+                    if (mx_passes >= mixed_max_passes) break;
+                    mixed_pass(sk, k, dtv);
+                    mixed_resid_tc(sk, k, dtv);
+                    mixed_tail(sk, k, hs);
+                    continue;
+                }
+            }
+            if (ok) {
+                std::swap(psi.p, cand.p);
+                last_iterations = mx_passes;
+                last_residual = res;
+                mx_residual = res;
+                return;
+            }
+            if (!finite || mx_passes >= mixed_max_passes) break;
+            mixed_resid64(sk, k, dtv, cand.p);
+            mixed_calibrate(sk, k, dtv);
+            mixed_pass(sk, k, dtv);
+            mixed_resid_tc(sk, k, dtv);
+            mixed_tail(sk, k, hs);
+        }
+        // not converged in low precision: the fp64 solve from the step's psi and rhs
+        std::fprintf(stderr, "\nMixed solve did not reach the tolerance; redoing the step with the fp64 solve.\n");
+        begin_solve(sk, k, hs);
+        finish_solve(sk, k, hs);
+        mx_residual = last_residual;
+    }
+
+    // Woodbury correction of a preconditioner output y; the corrected sink projections
+    // land in m_dots[2..3]
+    void wood32(const Absorber *const *sk, int k, float2 *yv)
+    {
+        if (k == 0) return;
+        k_sink_dots32<<<1, 1024, 0, stream>>>(yv, Nr, n_modes, k, sk[0]->v.p, k > 1 ? sk[1]->v.p : nullptr,
+                                             sk[0]->lo, sk[0]->hi, k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0,
+                                             m_dots.p);
+        launch_check();
+        const int64_t nb = (int64_t)std::max(1, wband_hi - wband_lo) * n_modes;
+        const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nb + 255) / 256, vec_blocks));
+        k_wood32<<<blocks, 256, 0, stream>>>(Nr, n_modes, wband_lo, wband_hi, d_kr.p, m_dots.p, W0.p, W1.p, yv,
+                                            m_dots.p + 2);
+        launch_check();
     }
 
     // Launches that follow the solve, queued behind every batch of iterations and gated
@@ -1611,7 +1981,8 @@ struct Solver {
             launch_apply(a);
         }
         step_hs = stage(readback_doubles());
-        begin_solve(sk, k, step_hs);
+        if (mixed && use_block) begin_mixed(sk, k, step_hs);
+        else begin_solve(sk, k, step_hs);
     }
 
     void step_end(int step_id, cnm_diag *dg, double *ef, double *fl, double *nm, double *en)
@@ -1622,7 +1993,8 @@ struct Solver {
         const Absorber *sk[2];
         const int k = active_sinks(sk);
         double *hs = step_hs;
-        finish_solve(sk, k, hs);
+        if (mixed && use_block) finish_mixed(sk, k, hs);
+        else finish_solve(sk, k, hs);
         const int nslots = 2 * n_modes + 3;
         const size_t kd = (sizeof(Krylov) + 7) / 8;
         hs += kd;
@@ -1829,6 +2201,49 @@ struct Solver {
         if (opc != CNM_OP_PRECOND) launch_apply(a);
         CK(cudaMemcpyAsync(yh, cand.p, nN * sizeof(double2), cudaMemcpyDeviceToHost, stream));
         sync();
+    }
+
+    // cnm_apply_lowp: the mixed path's complex64 tensor-core operator on a host vector.
+    void apply_lowp(int opc, const double *xh, double *yh)
+    {
+        if (!mixed) throw Error(CNM_ELOGIC, "the low-precision operator exists only on a CNM_MIXED handle");
+        if (!op.built) throw Error(CNM_ELOGIC, "operators exist only after initialize()");
+        CK(cudaMemcpyAsync(tmp.p, xh, nN * sizeof(double2), cudaMemcpyHostToDevice, stream));
+        k_to_f32<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, tmp.p, m_xa.p);
+        launch_check();
+        const Absorber *sk[2];
+        int k = 0;
+        TcArgs a = tc_a_args(m_xa.p, m_t.p, sk, 0, nullptr, op.dt);
+        switch (opc) {
+        case CNM_OP_H: a.alpha = make_float2(0.f, 0.f); a.beta = make_float2(1.f, 0.f); break;
+        case CNM_OP_V: a.alpha = make_float2(0.f, 0.f); a.beta = make_float2(1.f, 0.f); a.use_h0 = 0; a.use_cap = 0; break;
+        case CNM_OP_A: a.use_cap = ab_cap ? 1 : 0; break;
+        case CNM_OP_AFULL:
+            a.use_cap = ab_cap ? 1 : 0;
+            k = active_sinks(sk);
+            if (k > 0) {
+                k_sink_dots32<<<1, 1024, 0, stream>>>(m_xa.p, Nr, n_modes, k, sk[0]->v.p,
+                                                     k > 1 ? sk[1]->v.p : nullptr, sk[0]->lo, sk[0]->hi,
+                                                     k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, m_dots.p + 6);
+                launch_check();
+            }
+            {
+                TcArgs b = tc_a_args(m_xa.p, m_t.p, sk, k, m_dots.p + 6, op.dt);
+                b.use_cap = a.use_cap;
+                a = b;
+            }
+            break;
+        default: throw Error(CNM_EINVAL, "operator not available in low precision");
+        }
+        CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
+        launch_tc(a);
+        k_to_f64<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, m_t.p, cand.p);
+        launch_check();
+        CK(cudaMemcpyAsync(yh, cand.p, nN * sizeof(double2), cudaMemcpyDeviceToHost, stream));
+        sync();
+        int st = 0;
+        CK(cudaMemcpy(&st, d_status.p, sizeof(int), cudaMemcpyDeviceToHost));
+        if (st) throw Error(CNM_EDEVICE, "tensor-core apply: a pipeline wait gave up");
     }
 
     double sink_strength(int body)
@@ -2079,6 +2494,20 @@ int cnm_should_stop(const cnm_handle *h, int32_t *stop)
 int cnm_apply(cnm_handle *h, int32_t op, const double *x, double *y)
 {
     return guarded(h, [&](cnm::Solver &s) { s.apply_op(op, x, y); });
+}
+
+int cnm_apply_lowp(cnm_handle *h, int32_t op, const double *x, double *y)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.apply_lowp(op, x, y); });
+}
+
+int cnm_mixed_info(const cnm_handle *h, int32_t *passes, int32_t *fp64_applies, double *residual)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) {
+        if (passes) *passes = s.mx_passes;
+        if (fp64_applies) *fp64_applies = s.mx_fp64;
+        if (residual) *residual = s.mx_residual;
+    });
 }
 
 int cnm_sink_strength(const cnm_handle *h, int32_t body, double *out)

@@ -1,0 +1,942 @@
+// cnm_mixed.cu -- kernels of the mixed-precision CN solve (see cnm_mixed.cuh): the
+// tcgen05 tensor-core operator apply, the fp32 cluster radial-block solve and the
+// vector kernels of the defect correction.
+#include <cooperative_groups.h>
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "cnm_coupling.h"
+#include "cnm_device.cuh"
+#include "cnm_mixed.cuh"
+
+namespace cnm {
+
+// ==================================================================== host: Gaunt image
+
+static uint16_t bf16_bits(double v)
+{
+    const float f = (float)v;
+    uint32_t u;
+    std::memcpy(&u, &f, 4);
+    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);  // inf / nan (not produced)
+    u += 0x7fffu + ((u >> 16) & 1u);                                    // round to nearest even
+    return (uint16_t)(u >> 16);
+}
+
+TcGaunt build_tc_gaunt(const Coupling &c)
+{
+    TcGaunt t;
+    const int n = c.n_modes;
+    t.n_modes = n;
+    t.kp = (n + 15) / 16 * 16;
+    t.K = 2 * c.l_max + 1;
+    const int nsl = t.kp / 16;
+    std::vector<double> G((size_t)t.K * n * n, 0.0);
+    for (int j = 0; j < n; ++j)
+        for (int p = c.pair_row_ptr[j]; p < c.pair_row_ptr[j + 1]; ++p) {
+            const int k = c.pair_col[p];
+            for (int e = c.pair_term_ptr[p]; e < c.pair_term_ptr[p + 1]; ++e)
+                G[((size_t)c.term_l[e] * n + j) * n + k] += c.term_g[e];
+        }
+    t.l_off.assign(t.K, 0);
+    t.l_bytes.assign(t.K, 0);
+    t.l_nblk.assign(t.K, 0);
+    t.slices.assign((size_t)t.K * 16, -1);
+    for (int l = 0; l < t.K; ++l) {
+        double fro = 0.0;
+        t.l_off[l] = (int)(t.blob.size() * sizeof(uint16_t));
+        for (int s = 0; s < nsl; ++s) {
+            bool nz = false;
+            for (int j = 0; j < n && !nz; ++j)
+                for (int k = 16 * s; k < std::min(n, 16 * s + 16); ++k)
+                    if (G[((size_t)l * n + j) * n + k] != 0.0) {
+                        nz = true;
+                        break;
+                    }
+            if (!nz) continue;
+            const size_t at = t.blob.size();
+            t.blob.resize(at + 2048, 0);  // 4096 bytes
+            for (int j = 0; j < n; ++j)
+                for (int k = 16 * s; k < std::min(n, 16 * s + 16); ++k) {
+                    const double g = G[((size_t)l * n + j) * n + k];
+                    fro += g * g;
+                    const int kk = k - 16 * s;
+                    const size_t byte = (size_t)(kk / 8) * 2048 + (size_t)(j / 8) * 128 + (size_t)(j % 8) * 16 +
+                                        (size_t)(kk % 8) * 2;
+                    t.blob[at + byte / 2] = bf16_bits(g);
+                }
+            t.slices[(size_t)l * 16 + t.l_nblk[l]] = s;
+            t.l_nblk[l] += 1;
+        }
+        t.l_bytes[l] = t.l_nblk[l] * 4096;
+        t.fro_sum += std::sqrt(fro);
+    }
+    return t;
+}
+
+// ==================================================================== device helpers
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+
+// Bounded wait on phase `parity`.  Once any wait of the CTA has given up (*abort set),
+// later waits return at once, so a failed launch ends quickly; `force` waits (bounded)
+// even then -- the drains of copies and MMAs in flight before the CTA exits.
+__device__ __forceinline__ void mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort, bool force = false)
+{
+    for (int it = 0; it < (1 << 22); ++it) {
+        if (mbar_try(bar, parity)) return;
+        if (!force && *abort) return;
+    }
+    *abort = 1;
+}
+
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor, K-major, no swizzle: start address, leading (K)
+// byte offset, stride (M/N) byte offset, descriptor version 1.
+__device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t sbo)
+{
+    return (uint64_t)((addr >> 4) & 0x3fffu) | ((uint64_t)((lbo >> 4) & 0x3fffu) << 16) |
+           ((uint64_t)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
+}
+
+// Instruction descriptor of kind::f16: bf16 A and B, fp32 D, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
+{
+    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+}
+
+__device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(dtmem),
+        "l"(ad), "l"(bd), "r"(idesc), "r"(acc)
+        : "memory");
+}
+
+__device__ __forceinline__ void tc_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+// 16 consecutive fp32 columns of this warp's 32 TMEM lanes.
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+}
+
+__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+
+__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+// ==================================================================== tensor-core apply
+
+constexpr int TC_WORKERS = 256;           // B-operand producers and epilogue (warps 0-7)
+constexpr int TC_THREADS = TC_WORKERS + 32;  // + the copy / MMA warp (warp 8)
+constexpr int TC_ASTAGES = 3, TC_BSTAGES = 2;
+constexpr float TC_HCUT = 1e-9f;          // multipoles below this fraction of the monopole are skipped
+
+struct TcShared {
+    unsigned long long afull[TC_ASTAGES], afree[TC_ASTAGES], bfull[TC_BSTAGES], bfree[TC_BSTAGES];
+    unsigned long long accfull, accfree, tinfo, drain;
+    uint32_t tmem_base;
+    int lcut[2];
+    int lcut_red;
+    int abort;
+    int l_off[64], l_bytes[64], l_nblk[64];
+};
+
+// Bulk copy of multipole lv's Gaunt blocks into the A stage of use v (v % 3).
+__device__ __forceinline__ void tc_issue_a(TcShared &sh, uint8_t *Ast, int a_stage, const uint8_t *blob, int v, int lv)
+{
+    const int s = v % TC_ASTAGES;
+    const uint32_t bar = smem_addr(&sh.afull[s]);
+    if (sh.l_bytes[lv] == 0) {  // no non-zero block: complete the phase without a copy
+        mbar_arrive(bar);
+        return;
+    }
+    mbar_expect_tx(bar, (uint32_t)sh.l_bytes[lv]);
+    bulk_g2s(smem_addr(Ast + (size_t)s * a_stage), blob + sh.l_off[lv], (uint32_t)sh.l_bytes[lv], bar);
+}
+
+// Grid: persistent CTAs, tile t = blockIdx.x + q gridDim.x.  Worker thread w owns node
+// c = w % NT of the tile and the KPT columns k = (w / NT) KPT .. of B.
+template <int KPT, int NT>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int a_stage)
+{
+    constexpr int TPN = TC_WORKERS / NT;       // worker threads per node
+    constexpr int KP = TPN * KPT;              // padded columns k
+    constexpr int LBO_B = 32 * NT;             // bytes between 8-column groups of k in B
+    constexpr int B_STAGE = KP * 4 * NT;       // bytes of one B stage
+    constexpr int NCOL = 2 * NT;               // accumulator columns (Re | Im)
+    constexpr uint32_t IDESC = idesc_bf16(128, NCOL);
+    extern __shared__ __align__(128) uint8_t tc_smem[];
+    __shared__ TcShared sh;
+    const int n = g.n_modes, Nr = g.Nr;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    uint8_t *Ast = tc_smem;                                        // TC_ASTAGES x a_stage
+    uint8_t *Bst = Ast + (size_t)TC_ASTAGES * a_stage;             // TC_BSTAGES x B_STAGE
+    float *hs = reinterpret_cast<float *>(Bst + (size_t)TC_BSTAGES * B_STAGE);  // K x NT
+    float2 *ph = reinterpret_cast<float2 *>(hs + (size_t)K * NT);  // KP phases e^{i m_k theta}
+    volatile int *abort = &sh.abort;
+
+    if (tid == 0) {
+        for (int s = 0; s < TC_ASTAGES; ++s) {
+            mbar_init(smem_addr(&sh.afull[s]), 1);
+            mbar_init(smem_addr(&sh.afree[s]), 1);
+        }
+        for (int s = 0; s < TC_BSTAGES; ++s) {
+            mbar_init(smem_addr(&sh.bfull[s]), TC_WORKERS);
+            mbar_init(smem_addr(&sh.bfree[s]), 1);
+        }
+        mbar_init(smem_addr(&sh.accfull), 1);
+        mbar_init(smem_addr(&sh.accfree), TC_WORKERS);
+        mbar_init(smem_addr(&sh.tinfo), 1);
+        mbar_init(smem_addr(&sh.drain), 1);
+        sh.abort = 0;
+        sh.lcut_red = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    for (int l = tid; l < K; l += TC_THREADS) {
+        sh.l_off[l] = tt.l_off[l];
+        sh.l_bytes[l] = tt.l_bytes[l];
+        sh.l_nblk[l] = tt.l_nblk[l];
+    }
+    for (int k = tid; k < KP; k += TC_THREADS) {
+        float s = 0.f, c = 0.f;
+        if (k < n) sincosf((float)mode_m[k] * a.theta, &s, &c);
+        ph[k] = k < n ? make_float2(c, s) : make_float2(0.f, 0.f);
+    }
+    if (warp == 8) {
+        // TMEM accumulator: NCOL fp32 columns x 128 lanes
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&sh.tmem_base)),
+                     "r"((uint32_t)NCOL)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+        tc_fence_before();
+    }
+    __syncthreads();
+    tc_fence_after();
+    const uint32_t tmem = sh.tmem_base;
+
+    if (warp == 8) {
+        // ---------------------------------------------------------- copies and MMAs
+        if (lane == 0) {
+            int u = 0;  // multipole uses issued so far (all tiles)
+            int copies = 0;
+            int it = 0;
+            const int first = blockIdx.x;
+            if (first < tiles) {
+                tc_issue_a(sh, Ast, a_stage, tt.blob, 0, 0);
+                tc_issue_a(sh, Ast, a_stage, tt.blob, 1, 1);
+                copies = 2;
+            }
+            for (int tile = first; tile < tiles; tile += gridDim.x, ++it) {
+                mbar_wait(smem_addr(&sh.tinfo), it & 1, abort);
+                const int lc = sh.lcut[it & 1];
+                const bool more = tile + (int)gridDim.x < tiles;
+                if (it > 0) mbar_wait(smem_addr(&sh.accfree), (it - 1) & 1, abort);
+                tc_fence_after();
+                bool firstmma = true;
+                for (int l = 0; l <= lc; ++l, ++u) {
+                    const int sa = u % TC_ASTAGES, sb = u % TC_BSTAGES;
+                    mbar_wait(smem_addr(&sh.afull[sa]), (u / TC_ASTAGES) & 1, abort);
+                    mbar_wait(smem_addr(&sh.bfull[sb]), (u / TC_BSTAGES) & 1, abort);
+                    tc_fence_after();
+                    const uint32_t abase = smem_addr(Ast + (size_t)sa * a_stage);
+                    const uint32_t bbase = smem_addr(Bst + (size_t)sb * B_STAGE);
+                    const int nb = sh.l_nblk[l];
+                    for (int q = 0; q < nb; ++q) {
+                        const int s16 = tt.slices[l * 16 + q];
+                        const uint64_t ad = sdesc(abase + (uint32_t)q * 4096u, 2048u, 128u);
+                        const uint64_t bd = sdesc(bbase + (uint32_t)s16 * 2u * LBO_B, (uint32_t)LBO_B, 128u);
+                        tc_mma(tmem, ad, bd, IDESC, firstmma ? 0u : 1u);
+                        firstmma = false;
+                    }
+                    tc_commit(smem_addr(&sh.afree[sa]));
+                    tc_commit(smem_addr(&sh.bfree[sb]));
+                    // refill: use u + 2 goes into the stage of use u - 1
+                    int lnext = -1;
+                    if (l + 2 <= lc) lnext = l + 2;
+                    else if (more) lnext = l + 2 - (lc + 1);
+                    if (lnext >= 0) {
+                        if (u >= 1) mbar_wait(smem_addr(&sh.afree[(u - 1) % TC_ASTAGES]), ((u - 1) / TC_ASTAGES) & 1, abort);
+                        tc_issue_a(sh, Ast, a_stage, tt.blob, u + 2, lnext);
+                        ++copies;
+                    }
+                }
+                tc_commit(smem_addr(&sh.accfull));
+            }
+            // drain: every MMA issued has completed, every copy issued has landed
+            tc_commit(smem_addr(&sh.drain));
+            mbar_wait(smem_addr(&sh.drain), 0, abort, true);
+            for (int v = u; v < copies; ++v)
+                mbar_wait(smem_addr(&sh.afull[v % TC_ASTAGES]), (v / TC_ASTAGES) & 1, abort, true);
+        }
+        __syncwarp();
+    } else {
+        // ---------------------------------------------------------- workers
+        const int c = tid % NT, kq = tid / NT;
+        const double alpha_d = 1.0 / (g.dr * g.dr), inv2mu = 1.0 / (2.0 * g.mu);
+        const double offd = -alpha_d * inv2mu;
+        const int q4 = warp & 3, half = warp >> 2;
+        const int j = 32 * q4 + lane;  // epilogue row
+        const bool jv = j < n;
+        const int lj = jv ? mode_l[j] : 0;
+        const float2 phj = jv ? ph[j] : make_float2(1.f, 0.f);
+        double dacc[6] = {0, 0, 0, 0, 0, 0};
+        int u = 0, it = 0;
+        for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+            const int i0 = tile * NT;
+            const int i = i0 + c;
+            // z_k(r_c) = e^{i m_k theta} x_k(r_c) for this thread's columns
+            float2 z[KPT];
+#pragma unroll
+            for (int e = 0; e < KPT; ++e) {
+                const int k = kq * KPT + e;
+                float2 xv = make_float2(0.f, 0.f);
+                if (k < n && i < Nr) xv = a.x[(int64_t)k * Nr + i];
+                const float2 p = ph[k < KP ? k : 0];
+                z[e] = make_float2(p.x * xv.x - p.y * xv.y, p.x * xv.y + p.y * xv.x);
+            }
+            // radial weights of the tile and the multipole cut
+            if (kq == 0) {
+                int lcl = 0;
+                double h0 = 0.0;
+                for (int l = 0; l < K; ++l) {
+                    double h = 0.0;
+                    if (a.use_v && i >= 1 && i <= Nr - 2) h = a.hh[(int64_t)l * Nr + i];
+                    if (l == 0) h0 = fabs(h);
+                    else if (fabs(h) > (double)TC_HCUT * h0) lcl = l;
+                    hs[l * NT + c] = (float)h;
+                }
+                if (lcl > 0) atomicMax(&sh.lcut_red, lcl);
+            }
+            workers_sync();
+            const int lc = max(1, sh.lcut_red);
+            workers_sync();
+            if (tid == 0) {
+                sh.lcut[it & 1] = lc;
+                sh.lcut_red = 0;
+                mbar_arrive(smem_addr(&sh.tinfo));
+            }
+            // B operand, one multipole per stage
+            for (int l = 0; l <= lc; ++l, ++u) {
+                const int sb = u % TC_BSTAGES;
+                if (u >= TC_BSTAGES) mbar_wait(smem_addr(&sh.bfree[sb]), ((u / TC_BSTAGES) - 1) & 1, abort);
+                uint8_t *B = Bst + (size_t)sb * B_STAGE;
+                const float h = hs[l * NT + c];
+#pragma unroll
+                for (int gq = 0; gq < KPT / 8; ++gq) {
+                    const int kg = kq * (KPT / 8) + gq;
+                    uint4 re, im;
+                    re.x = pack_bf16(h * z[8 * gq + 0].x, h * z[8 * gq + 1].x);
+                    re.y = pack_bf16(h * z[8 * gq + 2].x, h * z[8 * gq + 3].x);
+                    re.z = pack_bf16(h * z[8 * gq + 4].x, h * z[8 * gq + 5].x);
+                    re.w = pack_bf16(h * z[8 * gq + 6].x, h * z[8 * gq + 7].x);
+                    im.x = pack_bf16(h * z[8 * gq + 0].y, h * z[8 * gq + 1].y);
+                    im.y = pack_bf16(h * z[8 * gq + 2].y, h * z[8 * gq + 3].y);
+                    im.z = pack_bf16(h * z[8 * gq + 4].y, h * z[8 * gq + 5].y);
+                    im.w = pack_bf16(h * z[8 * gq + 6].y, h * z[8 * gq + 7].y);
+                    const int cim = NT + c;
+                    *reinterpret_cast<uint4 *>(B + (size_t)kg * LBO_B + (c >> 3) * 128 + (c & 7) * 16) = re;
+                    *reinterpret_cast<uint4 *>(B + (size_t)kg * LBO_B + (cim >> 3) * 128 + (cim & 7) * 16) = im;
+                }
+                fence_proxy_async();
+                mbar_arrive(smem_addr(&sh.bfull[sb]));
+            }
+            // epilogue: row j, nodes [half NT/2, (half + 1) NT/2) of the tile
+            mbar_wait(smem_addr(&sh.accfull), it & 1, abort);
+            tc_fence_after();
+            const uint32_t trow = tmem + ((uint32_t)(32 * q4) << 16);
+            for (int cb = half * (NT / 2); cb < (half + 1) * (NT / 2); cb += 16) {
+                float wr[16], wi[16];
+                tmem_ld16(trow + (uint32_t)cb, wr);
+                tmem_ld16(trow + (uint32_t)(NT + cb), wi);
+                if (!jv) continue;
+                const float2 *xr = a.x + (int64_t)j * Nr;
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    const int ii = i0 + cb + e;
+                    if (ii >= Nr) continue;
+                    const bool interior = ii >= 1 && ii <= Nr - 2;
+                    const float2 xf = xr[ii];
+                    const double xr_ = xf.x, xi_ = xf.y;
+                    double hr = 0.0, hi = 0.0;
+                    if (interior) {
+                        if (a.use_h0) {
+                            const float2 xm = xr[ii - 1], xp = xr[ii + 1];
+                            const double diag = (2.0 * alpha_d + (double)(lj * (lj + 1)) * g.ir2[ii]) * inv2mu;
+                            hr = diag * xr_ + offd * ((double)xm.x + (double)xp.x);
+                            hi = diag * xi_ + offd * ((double)xm.y + (double)xp.y);
+                        }
+                        if (a.use_v) {
+                            // conj(ph_j) w
+                            const double pr = phj.x, pim = phj.y;
+                            hr += pr * (double)wr[e] + pim * (double)wi[e];
+                            hi += pr * (double)wi[e] - pim * (double)wr[e];
+                        }
+                    }
+                    if (a.use_cap && g.capw) {
+                        const double cw = g.capw[ii];
+                        hr += cw * xi_;
+                        hi -= cw * xr_;
+                    }
+                    double yr = (double)a.alpha.x * xr_ - (double)a.alpha.y * xi_ + (double)a.beta.x * hr -
+                                (double)a.beta.y * hi;
+                    double yi = (double)a.alpha.x * xi_ + (double)a.alpha.y * xr_ + (double)a.beta.x * hi +
+                                (double)a.beta.y * hr;
+#pragma unroll
+                    for (int s2 = 0; s2 < 2; ++s2)
+                        if (s2 < a.n_sinks && ii >= a.sink_lo[s2] && ii < a.sink_hi[s2]) {
+                            const double2 dd = a.sink_dots[s2];
+                            const double2 vv = a.sink_v[s2][(int64_t)j * Nr + ii];
+                            const double cr = a.sink_coef[s2] * dd.x, ci = a.sink_coef[s2] * dd.y;
+                            yr += cr * vv.x - ci * vv.y;
+                            yi += cr * vv.y + ci * vv.x;
+                        }
+                    const float2 yo = make_float2((float)yr, (float)yi);
+                    a.y[(int64_t)j * Nr + ii] = yo;
+                    const double yrf = yo.x, yif = yo.y;
+#pragma unroll
+                    for (int q = 0; q < 3; ++q) {
+                        if (q >= a.n_dots) break;
+                        double dr_ = 0.0, di_ = 0.0;
+                        const int kd = a.dot_kind[q];
+                        if (kd == 1 || kd == 2) {
+                            const float2 ef = a.dot_ext[q][(int64_t)j * Nr + ii];
+                            const double er = ef.x, ei = ef.y;
+                            if (kd == 1) {  // conj(e) y
+                                dr_ = er * yrf + ei * yif;
+                                di_ = er * yif - ei * yrf;
+                            } else {        // conj(y) e
+                                dr_ = yrf * er + yif * ei;
+                                di_ = yrf * ei - yif * er;
+                            }
+                        } else if (kd == 3) {
+                            dr_ = yrf * yrf + yif * yif;
+                        } else {            // |e64 - y|^2 with the unrounded y
+                            const double2 e64 = a.dot_ext64[(int64_t)j * Nr + ii];
+                            const double ddr = e64.x - yr, ddi = e64.y - yi;
+                            dr_ = ddr * ddr + ddi * ddi;
+                        }
+                        dacc[2 * q] += dr_;
+                        dacc[2 * q + 1] += di_;
+                    }
+                }
+            }
+            tc_fence_before();
+            mbar_arrive(smem_addr(&sh.accfree));
+        }
+        // per-CTA partials of the fused reductions (fixed order: warps, then lanes)
+        if (a.n_dots > 0) {
+            double *red = reinterpret_cast<double *>(hs);  // the h tile is no longer read
+            workers_sync();
+#pragma unroll
+            for (int q = 0; q < 6; ++q) dacc[q] = warp_sum(dacc[q]);
+            if (lane == 0)
+#pragma unroll
+                for (int q = 0; q < 6; ++q) red[q * 8 + warp] = dacc[q];
+            workers_sync();
+            if (tid < 2 * a.n_dots) {
+                double s = 0.0;
+                for (int w = 0; w < 8; ++w) s += red[tid * 8 + w];
+                a.partials[(int64_t)tid * gridDim.x + blockIdx.x] = s;
+            }
+        }
+    }
+    __syncthreads();
+    if (tid == 0 && sh.abort && a.status) atomicOr(a.status, 16);
+    if (warp == 8) {
+        tc_fence_after();
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)NCOL)
+                     : "memory");
+    }
+}
+
+// Plans: (columns k per worker thread, nodes per tile).  The worker thread holds its
+// z values in registers, so KPT stays at or below 48.
+#define CNM_TC_PLANS(X) X(8, 128) X(16, 128) X(24, 128) X(32, 128) X(40, 128) X(48, 128)
+
+bool tc_plan(int n_modes, int Nr, int a_stage_bytes, int n_sm, TcPlan &p)
+{
+    const int kp = (n_modes + 15) / 16 * 16;
+    if (n_modes > 128) return false;
+    p.nt = 128;
+    p.kpt = std::max(8, (kp / 2 + 7) / 8 * 8);
+    if (p.kpt * 2 < kp || p.kpt > 48) return false;
+    const int KP = 2 * p.kpt;
+    p.a_stage = (a_stage_bytes + 127) / 128 * 128;
+    const int K = 64;  // upper bound of the multipole count used for the h tile
+    p.smem = (size_t)TC_ASTAGES * p.a_stage + (size_t)TC_BSTAGES * KP * 4 * p.nt + (size_t)K * p.nt * 4 +
+             (size_t)KP * 8 + 128;
+    // at least 120 KiB, so that one CTA (and its 2 NT TMEM columns) is resident per SM and
+    // no tcgen05.alloc has to wait for another CTA's columns
+    p.smem = std::max<size_t>(p.smem, 120 * 1024);
+    p.tiles = (Nr + p.nt - 1) / p.nt;
+    p.grid = std::min(p.tiles, n_sm);
+    return p.smem <= 220 * 1024;
+}
+
+cudaError_t tc_prepare(const TcPlan &p)
+{
+    cudaError_t e = cudaSuccess;
+#define CNM_TC_ATTR(KPT_, NT_) \
+    if (p.kpt == KPT_ && p.nt == NT_) \
+        e = cudaFuncSetAttribute(k_tc_apply<KPT_, NT_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    CNM_TC_PLANS(CNM_TC_ATTR)
+#undef CNM_TC_ATTR
+    return e;
+}
+
+cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, const int *mode_l, const int *mode_m,
+                            int K, const TcTable &tt, const TcArgs &a)
+{
+#define CNM_TC_LAUNCH(KPT_, NT_)                                                                             \
+    if (p.kpt == KPT_ && p.nt == NT_) {                                                                      \
+        k_tc_apply<KPT_, NT_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage); \
+        return cudaGetLastError();                                                                           \
+    }
+    CNM_TC_PLANS(CNM_TC_LAUNCH)
+#undef CNM_TC_LAUNCH
+    return cudaErrorInvalidConfiguration;
+}
+
+// ==================================================================== fp32 radial solve
+
+struct Aff32 {
+    float2 A, B;  // y -> A y + B
+};
+
+__device__ __forceinline__ float2 fmul2(float2 a, float2 b) { return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); }
+__device__ __forceinline__ float2 fadd2(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 fsub2(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+__device__ __forceinline__ Aff32 aff32_id() { return Aff32{make_float2(1.f, 0.f), make_float2(0.f, 0.f)}; }
+// first f, then g
+__device__ __forceinline__ Aff32 aff32_then(const Aff32 &f, const Aff32 &g)
+{
+    return Aff32{fmul2(g.A, f.A), fadd2(fmul2(g.A, f.B), g.B)};
+}
+__device__ __forceinline__ float2 aff32_apply(const Aff32 &m, float2 y) { return fadd2(fmul2(m.A, y), m.B); }
+__device__ __forceinline__ Aff32 shfl_aff32(const Aff32 &a, int src_delta, bool up)
+{
+    Aff32 r;
+    if (up) {
+        r.A.x = __shfl_up_sync(0xffffffffu, a.A.x, src_delta);
+        r.A.y = __shfl_up_sync(0xffffffffu, a.A.y, src_delta);
+        r.B.x = __shfl_up_sync(0xffffffffu, a.B.x, src_delta);
+        r.B.y = __shfl_up_sync(0xffffffffu, a.B.y, src_delta);
+    } else {
+        r.A.x = __shfl_down_sync(0xffffffffu, a.A.x, src_delta);
+        r.A.y = __shfl_down_sync(0xffffffffu, a.A.y, src_delta);
+        r.B.x = __shfl_down_sync(0xffffffffu, a.B.x, src_delta);
+        r.B.y = __shfl_down_sync(0xffffffffu, a.B.y, src_delta);
+    }
+    return r;
+}
+
+// x = P^{-1} rhs for radial block j = blockIdx.y, exactly (forward and backward Thomas
+// sweeps as affine-map scans: thread -> warp shuffles -> CTA -> cluster through
+// distributed shared memory; the same scheme as the fp64 cluster solve, in fp32).
+__global__ void __launch_bounds__(PS32_THREADS) k_psolve32_cl(int Nr, int per, float2 off, const float2 *dinv,
+                                                              float2 *x, Ps32Args in)
+{
+    namespace cg = cooperative_groups;
+    cg::cluster_group cl = cg::this_cluster();
+    extern __shared__ float2 ps32[];
+    __shared__ Aff32 wagg[PS32_THREADS / 32];
+    __shared__ Aff32 cagg_f, cagg_b;
+    constexpr int T = PS32_THREADS, NW = PS32_THREADS / 32;
+    const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
+    const int j = blockIdx.y;
+    const int Lc = T * per;
+    const int c0 = rank * Lc, c1 = min(Nr, c0 + Lc), len = max(0, c1 - c0);
+    float2 *D = ps32, *Y = ps32 + Lc;
+    const int64_t base = (int64_t)j * Nr + c0;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    if (in.mode == 0) {
+        for (int e = tid; e < len; e += T) {
+            D[e] = dinv[base + e];
+            Y[e] = in.b[base + e];
+        }
+    } else {
+        const float2 al = make_float2((float)in.sc->alpha.x, (float)in.sc->alpha.y);
+        for (int e = tid; e < len; e += T) {
+            D[e] = dinv[base + e];
+            const float2 s = fsub2(in.r[base + e], fmul2(al, in.v[base + e]));
+            Y[e] = s;
+            in.s_out[base + e] = s;
+        }
+    }
+    __syncthreads();
+    const int s0 = tid * per, s1 = min(len, s0 + per);
+    // forward: y_i = d_i (b_i - l_i y_{i-1})
+    Aff32 acc = aff32_id();
+    for (int e = s0; e < s1; ++e) {
+        const int i = c0 + e;
+        const float2 d = D[e];
+        const float2 l = (i >= 1 && i <= Nr - 2) ? off : make_float2(0.f, 0.f);
+        const float2 ld = fmul2(l, d);
+        acc = aff32_then(acc, Aff32{make_float2(-ld.x, -ld.y), fmul2(d, Y[e])});
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Aff32 prev = shfl_aff32(acc, o, true);
+        if (lane >= o) acc = aff32_then(prev, acc);
+    }
+    Aff32 excl = shfl_aff32(acc, 1, true);
+    if (lane == 0) excl = aff32_id();
+    if (lane == 31) wagg[warp] = acc;
+    __syncthreads();
+    if (warp == 0) {
+        Aff32 cc = lane < NW ? wagg[lane] : aff32_id();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff32 prev = shfl_aff32(cc, o, true);
+            if (lane >= o) cc = aff32_then(prev, cc);
+        }
+        if (lane == 31) cagg_f = cc;
+    }
+    cl.sync();
+    float2 ywarp;
+    {
+        Aff32 cc = lane < rank ? *cl.map_shared_rank(&cagg_f, lane) : aff32_id();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff32 prev = shfl_aff32(cc, o, true);
+            if (lane >= o) cc = aff32_then(prev, cc);
+        }
+        const float2 ycta = make_float2(__shfl_sync(0xffffffffu, cc.B.x, 31), __shfl_sync(0xffffffffu, cc.B.y, 31));
+        Aff32 w = lane < NW ? wagg[lane] : aff32_id();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff32 prev = shfl_aff32(w, o, true);
+            if (lane >= o) w = aff32_then(prev, w);
+        }
+        Aff32 wex = shfl_aff32(w, 1, true);
+        if (lane == 0) wex = aff32_id();
+        const float2 ys = aff32_apply(wex, ycta);
+        ywarp = make_float2(__shfl_sync(0xffffffffu, ys.x, warp), __shfl_sync(0xffffffffu, ys.y, warp));
+    }
+    {
+        float2 y = aff32_apply(excl, ywarp);
+        for (int e = s0; e < s1; ++e) {
+            const int i = c0 + e;
+            const float2 l = (i >= 1 && i <= Nr - 2) ? off : make_float2(0.f, 0.f);
+            y = fmul2(D[e], fsub2(Y[e], fmul2(l, y)));
+            Y[e] = y;
+        }
+    }
+    // backward: x_i = y_i - u_i d_i x_{i+1}
+    Aff32 bcc = aff32_id();
+    for (int e = s1 - 1; e >= s0; --e) {
+        const int i = c0 + e;
+        const float2 ud = fmul2((i >= 1 && i <= Nr - 2) ? off : make_float2(0.f, 0.f), D[e]);
+        bcc = aff32_then(bcc, Aff32{make_float2(-ud.x, -ud.y), Y[e]});
+    }
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const Aff32 nxt = shfl_aff32(bcc, o, false);
+        if (lane + o < 32) bcc = aff32_then(nxt, bcc);
+    }
+    Aff32 bexcl = shfl_aff32(bcc, 1, false);
+    if (lane == 31) bexcl = aff32_id();
+    __syncthreads();
+    if (lane == 0) wagg[warp] = bcc;
+    __syncthreads();
+    if (warp == 0) {
+        Aff32 cc = lane < NW ? wagg[lane] : aff32_id();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff32 nxt = shfl_aff32(cc, o, false);
+            if (lane + o < 32) cc = aff32_then(nxt, cc);
+        }
+        if (lane == 0) cagg_b = cc;
+    }
+    cl.sync();
+    float2 xwarp;
+    {
+        Aff32 cc = (lane > rank && lane < cs) ? *cl.map_shared_rank(&cagg_b, lane) : aff32_id();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff32 nxt = shfl_aff32(cc, o, false);
+            if (lane + o < 32) cc = aff32_then(nxt, cc);
+        }
+        const float2 xcta = make_float2(__shfl_sync(0xffffffffu, cc.B.x, 0), __shfl_sync(0xffffffffu, cc.B.y, 0));
+        Aff32 w = lane < NW ? wagg[lane] : aff32_id();
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const Aff32 nxt = shfl_aff32(w, o, false);
+            if (lane + o < 32) w = aff32_then(nxt, w);
+        }
+        Aff32 wex = shfl_aff32(w, 1, false);
+        if (lane == 31) wex = aff32_id();
+        const float2 xs = aff32_apply(wex, xcta);
+        xwarp = make_float2(__shfl_sync(0xffffffffu, xs.x, warp), __shfl_sync(0xffffffffu, xs.y, warp));
+    }
+    // remote reads of cagg_b happen before this arrive; the wait is the last statement
+    cl.barrier_arrive();
+    {
+        float2 xr = aff32_apply(bexcl, xwarp);
+        for (int e = s1 - 1; e >= s0; --e) {
+            const int i = c0 + e;
+            const float2 ud = fmul2((i >= 1 && i <= Nr - 2) ? off : make_float2(0.f, 0.f), D[e]);
+            xr = fsub2(Y[e], fmul2(ud, xr));
+            Y[e] = xr;
+        }
+    }
+    __syncthreads();
+    for (int e = tid; e < len; e += T) x[base + e] = Y[e];
+    cl.barrier_wait();
+}
+
+// ==================================================================== vector kernels
+
+template <int NV>
+__device__ __forceinline__ void partials_out(double (&v)[NV], double *partials)
+{
+    __shared__ double scr[NV * 32];
+    block_sum<NV>(v, scr);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = v[q];
+}
+
+// x = psi, r = b - A_full psi = 2 (b - psi) (A_full psi = 2 psi - b by construction of b);
+// partials: |r|^2, |b|^2.
+__global__ void __launch_bounds__(VEC_THREADS) k_mx_start(int64_t n, const double2 *b, const double2 *psi,
+                                                          double2 *x, double2 *r64, float2 *r32, double *partials)
+{
+    double acc[2] = {0.0, 0.0};
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const double2 bv = b[e], pv = psi[e];
+        x[e] = pv;
+        const double rr = 2.0 * (bv.x - pv.x), ri = 2.0 * (bv.y - pv.y);
+        r64[e] = make_double2(rr, ri);
+        r32[e] = make_float2((float)rr, (float)ri);
+        acc[0] += rr * rr + ri * ri;
+        acc[1] += bv.x * bv.x + bv.y * bv.y;
+    }
+    partials_out<2>(acc, partials);
+}
+
+// r64 = b - A_full x, r32 = r64; with diff set, diff = r64_before - r64_after (the change
+// the last correction made, against which its tensor-core image is calibrated); partial
+// |r64|^2.
+__global__ void __launch_bounds__(VEC_THREADS) k_mx_resid(int64_t n, const double2 *b, const double2 *ax,
+                                                          double2 *r64, double2 *diff, float2 *r32, double *partials)
+{
+    double acc[1] = {0.0};
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const double2 bv = b[e], av = ax[e];
+        const double rr = bv.x - av.x, ri = bv.y - av.y;
+        if (diff) {
+            const double2 old = r64[e];
+            diff[e] = make_double2(old.x - rr, old.y - ri);
+        }
+        r64[e] = make_double2(rr, ri);
+        r32[e] = make_float2((float)rr, (float)ri);
+        acc[0] += rr * rr + ri * ri;
+    }
+    partials_out<1>(acc, partials);
+}
+
+// d = alpha y + omega z (fp64 from fp32 operands), x += d, d32 = d; partial |d|^2.
+__global__ void __launch_bounds__(VEC_THREADS) k_mx_update(int64_t n, const MixScalars *sc, double2 *x,
+                                                           const float2 *y, const float2 *z, float2 *d,
+                                                           double *partials)
+{
+    const double2 al = sc->alpha, om = sc->omega;
+    double acc[1] = {0.0};
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const float2 yv = y[e], zv = z[e];
+        const double dr = al.x * yv.x - al.y * yv.y + om.x * zv.x - om.y * zv.y;
+        const double di = al.x * yv.y + al.y * yv.x + om.x * zv.y + om.y * zv.x;
+        double2 xv = x[e];
+        xv.x += dr;
+        xv.y += di;
+        x[e] = xv;
+        d[e] = make_float2((float)dr, (float)di);
+        acc[0] += dr * dr + di * di;
+    }
+    partials_out<1>(acc, partials);
+}
+
+// Sum the partials in a fixed order and run one scalar step of the inner iteration.
+__global__ void k_mx_finish(const double *partials, int nblocks, int nslots, MixScalars *sc, int stage)
+{
+    __shared__ double scr[6 * 32];
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < 6; ++q)
+            if (q < nslots) acc[q] += partials[(int64_t)q * nblocks + b];
+    block_sum<6>(acc, scr);
+    if (threadIdx.x != 0) return;
+    switch (stage) {
+    case MX_B2R0:
+        sc->rr = acc[0];
+        sc->r64 = acc[0];
+        sc->b2 = acc[1];
+        break;
+    case MX_R64:
+        sc->rr = acc[0];
+        sc->r64 = acc[0];
+        break;
+    case MX_ALPHA: {
+        sc->rv = make_double2(acc[0], acc[1]);
+        const double2 rv = sc->rv;
+        const double den = rv.x * rv.x + rv.y * rv.y;
+        // alpha = rr / rv
+        sc->alpha = den > 0.0 ? make_double2(sc->rr * rv.x / den, -sc->rr * rv.y / den) : make_double2(0.0, 0.0);
+        break;
+    }
+    case MX_OMEGA:
+        sc->ts = make_double2(acc[0], acc[1]);
+        sc->tt = acc[2];
+        sc->omega = acc[2] > 0.0 ? make_double2(acc[0] / acc[2], acc[1] / acc[2]) : make_double2(0.0, 0.0);
+        break;
+    case MX_D2: sc->d2 = acc[0]; break;
+    case MX_TCRES: sc->tc_res2 = acc[0]; break;
+    case MX_ECAL:
+        sc->e2_cal = acc[0];
+        sc->d2_cal = sc->d2;
+        break;
+    default: break;
+    }
+}
+
+__global__ void k_to_f64(int64_t n, const float2 *a, double2 *b)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const float2 v = a[e];
+        b[e] = make_double2(v.x, v.y);
+    }
+}
+
+__global__ void k_to_f32(int64_t n, const double2 *a, float2 *b)
+{
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const double2 v = a[e];
+        b[e] = make_float2((float)v.x, (float)v.y);
+    }
+}
+
+// dots[s] = v_s^dag x over the support of v_s (fp64 sums, one CTA, fixed order: the
+// (sink, mode, node) terms are dealt to the threads, then a fixed block reduction).
+__global__ void k_sink_dots32(const float2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
+                              const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots)
+{
+    __shared__ double scr[4 * 32];
+    const int n0 = n_sinks > 0 ? max(0, hi0 - lo0) : 0, n1 = n_sinks > 1 ? max(0, hi1 - lo1) : 0;
+    const int64_t tot0 = (int64_t)n0 * n_modes, tot = tot0 + (int64_t)n1 * n_modes;
+    double acc[4] = {0, 0, 0, 0};
+    for (int64_t e = threadIdx.x; e < tot; e += blockDim.x) {
+        const bool first = e < tot0;
+        const int64_t f = first ? e : e - tot0;
+        const int w = first ? n0 : n1;
+        const int j = (int)(f / w), i = (first ? lo0 : lo1) + (int)(f - (int64_t)j * w);
+        const int64_t q = (int64_t)j * Nr + i;
+        const double2 v = (first ? v0 : v1)[q];
+        const float2 xv = x[q];
+        const double dr = v.x * xv.x + v.y * xv.y, di = v.x * xv.y - v.y * xv.x;
+        if (first) {
+            acc[0] += dr;
+            acc[1] += di;
+        } else {
+            acc[2] += dr;
+            acc[3] += di;
+        }
+    }
+    block_sum<4>(acc, scr);
+    if (threadIdx.x == 0) {
+        dots[0] = make_double2(acc[0], acc[1]);
+        dots[1] = make_double2(acc[2], acc[3]);
+    }
+}
+
+// Woodbury correction of a preconditioner output (src/CrankNicolsonModes_matrices.cpp:146-153)
+// in the inner iterations: c = G^{-1} proj (proj = v^dag y, G^{-1} and v_a^dag W_b from the
+// step's fp64 set-up), y -= sum_a W_a c_a on the band [lo, hi) where the W_a live, and
+// dots_out = v^dag y of the corrected y = proj - (v^dag W) c.
+__global__ void k_wood32(int Nr, int n_modes, int lo, int hi, const Krylov *kr, const double2 *proj,
+                         const double2 *W0, const double2 *W1, float2 *y, double2 *dots_out)
+{
+    const int k = kr->n_sinks;
+    double2 c[2] = {make_double2(0, 0), make_double2(0, 0)};
+    for (int a = 0; a < k; ++a)
+        for (int b = 0; b < k; ++b) c[a] = cadd(c[a], cmul(kr->Gi[a][b], proj[b]));
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        for (int a = 0; a < 2; ++a) {
+            double2 d = a < k ? proj[a] : make_double2(0, 0);
+            for (int b = 0; b < k && a < k; ++b) d = csub(d, cmul(kr->vW[a][b], c[b]));
+            dots_out[a] = d;
+        }
+    }
+    const int w = hi - lo;
+    const int64_t n = (int64_t)w * n_modes;
+    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const int j = (int)(e / w), i = lo + (int)(e % w);
+        const int64_t q = (int64_t)j * Nr + i;
+        double2 corr = cmul(W0[q], c[0]);
+        if (k > 1) corr = cadd(corr, cmul(W1[q], c[1]));
+        const float2 yv = y[q];
+        y[q] = make_float2((float)((double)yv.x - corr.x), (float)((double)yv.y - corr.y));
+    }
+}
+
+}  // namespace cnm

@@ -39,7 +39,10 @@ enum cnm_status {
 };
 
 enum cnm_precision {
-    CNM_FP64 = 0      /* complex128 everywhere: the drop-in path */
+    CNM_FP64 = 0,     /* complex128 everywhere: the drop-in path */
+    CNM_MIXED = 1     /* complex64 inner iterations on a tensor-core coupling apply, fp64
+                         residuals, refinement, dots, diagnostics and orbit (no counterpart
+                         in the reference, which is fp64 only) */
 };
 
 /* Operators for cnm_apply (all of size Nr*n_modes). */
@@ -226,6 +229,14 @@ int cnm_replay_power_average(cnm_handle *h, const double *times, const double *p
  * the operators of the current time (H, V, dVdt, A, B, apply_sink and
  * schrodinger_rhs of include/CrankNicolsonModes.hpp:197-213). */
 int cnm_apply(cnm_handle *h, int32_t op, const double *x, double *y);
+/* The low-precision operator of the mixed path (CNM_MIXED handles only): y = op x with
+ * x rounded to complex64 and the coupling on the tensor cores (bf16 operands, fp32
+ * accumulation), for op in {CNM_OP_H, CNM_OP_V, CNM_OP_A, CNM_OP_AFULL}; the result is
+ * widened to complex128.  No counterpart in the reference (used by the parity tests). */
+int cnm_apply_lowp(cnm_handle *h, int32_t op, const double *x, double *y);
+/* Counters of the mixed solve's last step: defect-correction passes, fp64 operator
+ * applications, and the final relative residual (fp64 or from the tensor-core check). */
+int cnm_mixed_info(const cnm_handle *h, int32_t *passes, int32_t *fp64_applies, double *residual);
 /* sink_strength(body) (_absorption.cpp:119-125). */
 int cnm_sink_strength(const cnm_handle *h, int32_t body, double *out);
 /* absorption_sink_active(). */
