@@ -76,7 +76,7 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
            "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel",
            "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy",
-           "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info")
+           "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info", "cnm_mixed_trace")
 
 def displaced_100_state(r, modes, mu, x_bh):
     """displaced_100_state (src/DisplacedAtom.cpp:12-76) on the device: the mode projection
@@ -147,6 +147,7 @@ def load_library():
     L.cnm_apply.argtypes = [p, i32, dp, dp]
     L.cnm_apply_lowp.argtypes = [p, i32, dp, dp]
     L.cnm_mixed_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), dp]
+    L.cnm_mixed_trace.argtypes = [p, dp]
     L.cnm_sink_strength.argtypes = [p, i32, dp]
     L.cnm_sink_active.argtypes = [p, C.POINTER(i32)]
     L.cnm_sink_vector.argtypes = [p, i32, dp]
@@ -364,6 +365,12 @@ class CrankNicolsonModes:
         p, f, r = C.c_int32(), C.c_int32(), C.c_double()
         self._check(self._lib.cnm_mixed_info(self._h, C.byref(p), C.byref(f), C.byref(r)))
         return p.value, f.value, r.value
+
+    def mixed_trace(self):
+        """Last residual check of the mixed solve (see cnm_mixed_trace)."""
+        out = np.zeros(6)
+        self._check(self._lib.cnm_mixed_trace(self._h, _dptr(out)))
+        return dict(zip(("res_tc", "est", "res64", "d_cal", "d_last", "ratio"), out.tolist()))
 
     def apply_sink(self, x):
         return self.apply("sink", x)

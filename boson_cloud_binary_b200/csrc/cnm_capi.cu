@@ -309,6 +309,7 @@ struct Solver {
     int ps_per = 0, ps_cs = 0;      // fp32 cluster solve: nodes per thread, CTAs per cluster
     int mx_passes = 0, mx_fp64 = 0; // counters of the last mixed step
     double mx_residual = 0.0;
+    double mx_trace[6] = {0, 0, 0, 0, 0, 0};  // last check: see cnm_mixed_trace
     double mixed_tol = 1e-12;       // fp64 relative residual the mixed solve stops at
     int mixed_max_passes = 8;
     // profiling
@@ -484,8 +485,8 @@ struct Solver {
         tg = build_tc_gaunt(cpl);
         int amax = 0;
         for (int b : tg.l_bytes) amax = std::max(amax, b);
-        if (!tc_plan(n_modes, Nr, amax, nsm, tcp))
-            throw Error(CNM_EINVAL, "The mixed solve supports at most 128 modes (l_max <= 14)");
+        if (!tc_plan(n_modes, K, Nr, amax, nsm, tcp))
+            throw Error(CNM_EINVAL, "The mixed solve supports at most 112 modes (l_max <= 13)");
         std::vector<uint8_t> bytes(tg.blob.size() * 2);
         std::memcpy(bytes.data(), tg.blob.data(), bytes.size());
         upload(d_tcblob, bytes);
@@ -1329,6 +1330,7 @@ struct Solver {
         t.l_bytes = d_tc_lbytes.p;
         t.slices = d_tc_slices.p;
         t.l_nblk = d_tc_lnblk.p;
+        t.g_exp = tg.g_exp;
         return t;
     }
 
@@ -1464,19 +1466,6 @@ struct Solver {
         mx_finish(tcp.grid, 2, MX_TCRES);
     }
 
-    // Bound of the error of the tensor-core residual: the coupling of A_full d is formed
-    // from bf16 operands (relative rounding 2^-8 per product, fp32 sums), so
-    //   |err| <= (dt/2) 2^-7 sum_l* |G_l*|_F max|h_l*| |d|  (2^-7: rounding and sums),
-    // with max|h_l*| <= mu (M1+M2) (1/((1+q) R1) + |w| q/((1+q) R2)); the stencil, CAP and
-    // sinks are combined in fp64 from fp32 inputs (relative 2^-23 of |A d|).
-    double mixed_check_bound(double d_norm, double dtv) const
-    {
-        const double h = mu * op.Mtot * (1.0 / ((1 + op.q) * std::max(op.R1, dr)) +
-                                         std::abs(op.w) * op.q / ((1 + op.q) * std::max(op.R2, dr)));
-        const double kin = 4.0 / (2.0 * mu * dr * dr);
-        return (0.5 * dtv * std::ldexp(tg.fro_sum * h, -7) + std::ldexp(1.0 + 0.5 * dtv * kin, -22)) * d_norm;
-    }
-
     // Calibration of the tensor-core residual check on the pass just verified in fp64:
     // |(r_before - r_after) - A_tc d|^2 with d the pass's correction (m_d) and the fp64
     // change of the residual in cand.
@@ -1576,6 +1565,12 @@ struct Solver {
             const double ratio = m.d2_cal > 0.0 ? std::sqrt(m.e2_cal / m.d2_cal) : 0.0;
             const double est = 4.0 * ratio * std::sqrt(m.d2) / bn;
             const bool finite = std::isfinite(res_tc) && std::isfinite(est) && st == 0;
+            mx_trace[0] = res_tc;
+            mx_trace[1] = est;
+            mx_trace[2] = std::sqrt(m.r64) / bn;
+            mx_trace[3] = std::sqrt(m.d2_cal) / bn;
+            mx_trace[4] = std::sqrt(m.d2) / bn;
+            mx_trace[5] = ratio;
             bool ok = finite && res_tc + est <= tolerance;
             double res = res_tc + est;
             if (finite && !ok && res_tc <= tolerance) {
@@ -2507,6 +2502,13 @@ int cnm_mixed_info(const cnm_handle *h, int32_t *passes, int32_t *fp64_applies, 
         if (passes) *passes = s.mx_passes;
         if (fp64_applies) *fp64_applies = s.mx_fp64;
         if (residual) *residual = s.mx_residual;
+    });
+}
+
+int cnm_mixed_trace(const cnm_handle *h, double *out)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) {
+        for (int q = 0; q < 6; ++q) out[q] = s.mx_trace[q];
     });
 }
 

@@ -2,7 +2,7 @@
 // tcgen05 tensor-core operator apply, the fp32 cluster radial-block solve and the
 // vector kernels of the defect correction.
 #include <cooperative_groups.h>
-#include <cuda_bf16.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <cmath>
@@ -17,14 +17,12 @@ namespace cnm {
 
 // ==================================================================== host: Gaunt image
 
-static uint16_t bf16_bits(double v)
+static uint16_t f16_bits(double v)
 {
-    const float f = (float)v;
-    uint32_t u;
-    std::memcpy(&u, &f, 4);
-    if ((u & 0x7f800000u) == 0x7f800000u) return (uint16_t)(u >> 16);  // inf / nan (not produced)
-    u += 0x7fffu + ((u >> 16) & 1u);                                    // round to nearest even
-    return (uint16_t)(u >> 16);
+    const __half h = __float2half_rn((float)v);
+    uint16_t u;
+    std::memcpy(&u, &h, 2);
+    return u;
 }
 
 TcGaunt build_tc_gaunt(const Coupling &c)
@@ -42,6 +40,12 @@ TcGaunt build_tc_gaunt(const Coupling &c)
             for (int e = c.pair_term_ptr[p]; e < c.pair_term_ptr[p + 1]; ++e)
                 G[((size_t)c.term_l[e] * n + j) * n + k] += c.term_g[e];
         }
+    // a power-of-two scale that puts the largest |G| just below 2^14, well inside fp16
+    double gmax = 0.0;
+    for (double v : G) gmax = std::max(gmax, std::abs(v));
+    int e2 = 0;
+    std::frexp(gmax > 0.0 ? gmax : 1.0, &e2);  // gmax < 2^e2
+    t.g_exp = 14 - e2;
     t.l_off.assign(t.K, 0);
     t.l_bytes.assign(t.K, 0);
     t.l_nblk.assign(t.K, 0);
@@ -59,20 +63,20 @@ TcGaunt build_tc_gaunt(const Coupling &c)
                     }
             if (!nz) continue;
             const size_t at = t.blob.size();
-            t.blob.resize(at + 2048, 0);  // 4096 bytes
+            t.blob.resize(at + (size_t)16 * t.kp, 0);  // 32 kp bytes
             for (int j = 0; j < n; ++j)
                 for (int k = 16 * s; k < std::min(n, 16 * s + 16); ++k) {
                     const double g = G[((size_t)l * n + j) * n + k];
                     fro += g * g;
                     const int kk = k - 16 * s;
-                    const size_t byte = (size_t)(kk / 8) * 2048 + (size_t)(j / 8) * 128 + (size_t)(j % 8) * 16 +
+                    const size_t byte = (size_t)(kk / 8) * 16 * t.kp + (size_t)(j / 8) * 128 + (size_t)(j % 8) * 16 +
                                         (size_t)(kk % 8) * 2;
-                    t.blob[at + byte / 2] = bf16_bits(g);
+                    t.blob[at + byte / 2] = f16_bits(std::ldexp(g, t.g_exp));
                 }
             t.slices[(size_t)l * 16 + t.l_nblk[l]] = s;
             t.l_nblk[l] += 1;
         }
-        t.l_bytes[l] = t.l_nblk[l] * 4096;
+        t.l_bytes[l] = t.l_nblk[l] * 32 * t.kp;
         t.fro_sum += std::sqrt(fro);
     }
     return t;
@@ -139,10 +143,10 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t addr, uint32_t lbo, uint32_t 
            ((uint64_t)((sbo >> 4) & 0x3fffu) << 32) | (1ull << 46);
 }
 
-// Instruction descriptor of kind::f16: bf16 A and B, fp32 D, both K-major, M x N.
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N)
+// Instruction descriptor of kind::f16: fp16 A and B, fp32 D, both K-major, M x N.
+__host__ __device__ constexpr uint32_t idesc_f16(int M, int N)
 {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+    return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 __device__ __forceinline__ void tc_mma(uint32_t dtmem, uint64_t ad, uint64_t bd, uint32_t idesc, uint32_t acc)
@@ -176,79 +180,94 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 
 __device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
 
-__device__ __forceinline__ uint32_t pack_bf16(float lo, float hi)
+__device__ __forceinline__ uint32_t pack_f16(float lo, float hi)
 {
-    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    const __half2 v = __floats2half2_rn(lo, hi);
     return *reinterpret_cast<const uint32_t *>(&v);
 }
 
 // ==================================================================== tensor-core apply
 
-constexpr int TC_WORKERS = 256;           // B-operand producers and epilogue (warps 0-7)
+constexpr int TC_WORKERS = 256;              // operand producers and epilogue (warps 0-7)
 constexpr int TC_THREADS = TC_WORKERS + 32;  // + the copy / MMA warp (warp 8)
 constexpr int TC_ASTAGES = 3, TC_BSTAGES = 2;
-constexpr float TC_HCUT = 1e-9f;          // multipoles below this fraction of the monopole are skipped
+constexpr int TC_NT = 128;                   // nodes per tile: 2 x 64-node halves, one MMA M-tile each
+constexpr float TC_HCUT = 1e-9f;             // multipoles below this fraction of the monopole are skipped
 
 struct TcShared {
-    unsigned long long afull[TC_ASTAGES], afree[TC_ASTAGES], bfull[TC_BSTAGES], bfree[TC_BSTAGES];
+    unsigned long long gfull[TC_ASTAGES], gfree[TC_ASTAGES], zfull[TC_BSTAGES], zfree[TC_BSTAGES];
     unsigned long long accfull, accfree, tinfo, drain;
     uint32_t tmem_base;
     int lcut[2];
     int lcut_red;
+    int pmax_bits;      // largest |h z| of the tile (float bits, non-negative)
     int abort;
     int l_off[64], l_bytes[64], l_nblk[64];
 };
 
-// Bulk copy of multipole lv's Gaunt blocks into the A stage of use v (v % 3).
-__device__ __forceinline__ void tc_issue_a(TcShared &sh, uint8_t *Ast, int a_stage, const uint8_t *blob, int v, int lv)
+// Bulk copy of multipole lv's Gaunt blocks into the G stage of use v (v % 3).
+__device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_stage, const uint8_t *blob, int v, int lv)
 {
     const int s = v % TC_ASTAGES;
-    const uint32_t bar = smem_addr(&sh.afull[s]);
+    const uint32_t bar = smem_addr(&sh.gfull[s]);
     if (sh.l_bytes[lv] == 0) {  // no non-zero block: complete the phase without a copy
         mbar_arrive(bar);
         return;
     }
     mbar_expect_tx(bar, (uint32_t)sh.l_bytes[lv]);
-    bulk_g2s(smem_addr(Ast + (size_t)s * a_stage), blob + sh.l_off[lv], (uint32_t)sh.l_bytes[lv], bar);
+    bulk_g2s(smem_addr(Gst + (size_t)s * g_stage), blob + sh.l_off[lv], (uint32_t)sh.l_bytes[lv], bar);
 }
 
-// Grid: persistent CTAs, tile t = blockIdx.x + q gridDim.x.  Worker thread w owns node
-// c = w % NT of the tile and the KPT columns k = (w / NT) KPT .. of B.
-template <int KPT, int NT>
+// y = alpha x + beta (H0 x + V x + CAP x) + sinks on complex64 vectors, the coupling on the
+// tensor cores.  A tile is TC_NT nodes; its 2 TC_NT rows m = 2 node + (0: Re, 1: Im) form
+// the MMA's A operand Z_l*[m, k] = h_l*(r_node) z_k(r_node)_(Re|Im) (two M-tiles of 128
+// rows), the Gaunt matrix G_l* is the B operand (N = KP rows j, K-major), and
+// D[m, j] = sum_l* sum_k Z_l*[m, k] G_l*[j, k] accumulates in TMEM (M-tile t at columns
+// [t KP, (t + 1) KP)).  Worker thread w produces row m = w of the A operand; in the
+// epilogue warp w reads TMEM lanes 32 (w % 4) .. of M-tile w / 4, i.e. 16 consecutive
+// nodes, Re and Im in adjacent lanes, so every global access of a warp is one 128-byte
+// line per mode.  Warp 8 copies G stages and issues the MMAs (one thread).  Grid:
+// persistent CTAs, tile t = blockIdx.x + q gridDim.x.
+template <int KP>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int a_stage)
+    k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int g_stage)
 {
-    constexpr int TPN = TC_WORKERS / NT;       // worker threads per node
-    constexpr int KP = TPN * KPT;              // padded columns k
-    constexpr int LBO_B = 32 * NT;             // bytes between 8-column groups of k in B
-    constexpr int B_STAGE = KP * 4 * NT;       // bytes of one B stage
-    constexpr int NCOL = 2 * NT;               // accumulator columns (Re | Im)
-    constexpr uint32_t IDESC = idesc_bf16(128, NCOL);
+    constexpr int LBO_Z = 32 * 128;            // bytes between 8-column groups of k in a Z stage
+    constexpr int Z_STAGE = KP * 2 * TC_NT * 2;  // bytes of one Z stage (2 NT rows x KP fp16)
+    constexpr int G_LBO = KP * 16;             // bytes between the two 8-column halves of a G block
+    constexpr int G_BLK = KP * 32;             // bytes of one G block (KP rows x 16 columns)
+    constexpr uint32_t IDESC = idesc_f16(128, KP);
+    constexpr uint32_t NCOLS = 2 * KP <= 32 ? 32 : 2 * KP <= 64 ? 64 : 2 * KP <= 128 ? 128 : 256;
     extern __shared__ __align__(128) uint8_t tc_smem[];
     __shared__ TcShared sh;
     const int n = g.n_modes, Nr = g.Nr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    uint8_t *Ast = tc_smem;                                        // TC_ASTAGES x a_stage
-    uint8_t *Bst = Ast + (size_t)TC_ASTAGES * a_stage;             // TC_BSTAGES x B_STAGE
-    float *hs = reinterpret_cast<float *>(Bst + (size_t)TC_BSTAGES * B_STAGE);  // K x NT
-    float2 *ph = reinterpret_cast<float2 *>(hs + (size_t)K * NT);  // KP phases e^{i m_k theta}
+    uint8_t *Gst = tc_smem;                                              // TC_ASTAGES x g_stage
+    uint8_t *Zst = Gst + (size_t)TC_ASTAGES * g_stage;                   // TC_BSTAGES x Z_STAGE
+    float *hs = reinterpret_cast<float *>(Zst + (size_t)TC_BSTAGES * Z_STAGE);  // K x TC_NT
+    float2 *ph = reinterpret_cast<float2 *>(hs + (size_t)K * TC_NT);    // KP phases e^{i m_k theta}
+    float *cent = reinterpret_cast<float *>(ph + KP);                   // KP: l (l + 1) / (2 mu)
+    float *ir2s = cent + KP;                                             // TC_NT: 1 / r^2 of the tile
+    float *caps = ir2s + TC_NT;                                          // TC_NT: CAP weights of the tile
+    float *hmx = caps + TC_NT;                                           // TC_NT: max_l* |h_l*| per node
     volatile int *abort = &sh.abort;
 
     if (tid == 0) {
         for (int s = 0; s < TC_ASTAGES; ++s) {
-            mbar_init(smem_addr(&sh.afull[s]), 1);
-            mbar_init(smem_addr(&sh.afree[s]), 1);
+            mbar_init(smem_addr(&sh.gfull[s]), 1);
+            mbar_init(smem_addr(&sh.gfree[s]), 1);
         }
         for (int s = 0; s < TC_BSTAGES; ++s) {
-            mbar_init(smem_addr(&sh.bfull[s]), TC_WORKERS);
-            mbar_init(smem_addr(&sh.bfree[s]), 1);
+            mbar_init(smem_addr(&sh.zfull[s]), TC_WORKERS / 32);
+            mbar_init(smem_addr(&sh.zfree[s]), 1);
         }
         mbar_init(smem_addr(&sh.accfull), 1);
-        mbar_init(smem_addr(&sh.accfree), TC_WORKERS);
+        mbar_init(smem_addr(&sh.accfree), TC_WORKERS / 32);
         mbar_init(smem_addr(&sh.tinfo), 1);
         mbar_init(smem_addr(&sh.drain), 1);
         sh.abort = 0;
         sh.lcut_red = 0;
+        sh.pmax_bits = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int l = tid; l < K; l += TC_THREADS) {
@@ -260,11 +279,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         float s = 0.f, c = 0.f;
         if (k < n) sincosf((float)mode_m[k] * a.theta, &s, &c);
         ph[k] = k < n ? make_float2(c, s) : make_float2(0.f, 0.f);
+        const int l = k < n ? mode_l[k] : 0;
+        cent[k] = (float)((double)(l * (l + 1)) / (2.0 * g.mu));
     }
     if (warp == 8) {
-        // TMEM accumulator: NCOL fp32 columns x 128 lanes
+        // TMEM accumulators: 2 M-tiles x KP fp32 columns x 128 lanes
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&sh.tmem_base)),
-                     "r"((uint32_t)NCOL)
+                     "r"(NCOLS)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
         tc_fence_before();
@@ -276,13 +297,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (warp == 8) {
         // ---------------------------------------------------------- copies and MMAs
         if (lane == 0) {
-            int u = 0;  // multipole uses issued so far (all tiles)
+            int u = 0;       // multipole uses issued so far (all tiles)
             int copies = 0;
             int it = 0;
             const int first = blockIdx.x;
             if (first < tiles) {
-                tc_issue_a(sh, Ast, a_stage, tt.blob, 0, 0);
-                tc_issue_a(sh, Ast, a_stage, tt.blob, 1, 1);
+                tc_issue_g(sh, Gst, g_stage, tt.blob, 0, 0);
+                tc_issue_g(sh, Gst, g_stage, tt.blob, 1, 1);
                 copies = 2;
             }
             for (int tile = first; tile < tiles; tile += gridDim.x, ++it) {
@@ -293,29 +314,33 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tc_fence_after();
                 bool firstmma = true;
                 for (int l = 0; l <= lc; ++l, ++u) {
-                    const int sa = u % TC_ASTAGES, sb = u % TC_BSTAGES;
-                    mbar_wait(smem_addr(&sh.afull[sa]), (u / TC_ASTAGES) & 1, abort);
-                    mbar_wait(smem_addr(&sh.bfull[sb]), (u / TC_BSTAGES) & 1, abort);
+                    const int sg = u % TC_ASTAGES, sz = u % TC_BSTAGES;
+                    mbar_wait(smem_addr(&sh.gfull[sg]), (u / TC_ASTAGES) & 1, abort);
+                    mbar_wait(smem_addr(&sh.zfull[sz]), (u / TC_BSTAGES) & 1, abort);
                     tc_fence_after();
-                    const uint32_t abase = smem_addr(Ast + (size_t)sa * a_stage);
-                    const uint32_t bbase = smem_addr(Bst + (size_t)sb * B_STAGE);
+                    const uint32_t gbase = smem_addr(Gst + (size_t)sg * g_stage);
+                    const uint32_t zbase = smem_addr(Zst + (size_t)sz * Z_STAGE);
                     const int nb = sh.l_nblk[l];
                     for (int q = 0; q < nb; ++q) {
                         const int s16 = tt.slices[l * 16 + q];
-                        const uint64_t ad = sdesc(abase + (uint32_t)q * 4096u, 2048u, 128u);
-                        const uint64_t bd = sdesc(bbase + (uint32_t)s16 * 2u * LBO_B, (uint32_t)LBO_B, 128u);
-                        tc_mma(tmem, ad, bd, IDESC, firstmma ? 0u : 1u);
+                        const uint64_t bd = sdesc(gbase + (uint32_t)(q * G_BLK), (uint32_t)G_LBO, 128u);
+#pragma unroll
+                        for (int mt = 0; mt < 2; ++mt) {
+                            const uint64_t ad = sdesc(zbase + (uint32_t)(s16 * 2 * LBO_Z + mt * 2048), (uint32_t)LBO_Z, 128u);
+                            tc_mma(tmem + (uint32_t)(mt * KP), ad, bd, IDESC, firstmma ? 0u : 1u);
+                        }
                         firstmma = false;
                     }
-                    tc_commit(smem_addr(&sh.afree[sa]));
-                    tc_commit(smem_addr(&sh.bfree[sb]));
-                    // refill: use u + 2 goes into the stage of use u - 1
+                    tc_commit(smem_addr(&sh.gfree[sg]));
+                    tc_commit(smem_addr(&sh.zfree[sz]));
+                    // refill: use u + 2 goes into the G stage of use u - 1
                     int lnext = -1;
                     if (l + 2 <= lc) lnext = l + 2;
                     else if (more) lnext = l + 2 - (lc + 1);
                     if (lnext >= 0) {
-                        if (u >= 1) mbar_wait(smem_addr(&sh.afree[(u - 1) % TC_ASTAGES]), ((u - 1) / TC_ASTAGES) & 1, abort);
-                        tc_issue_a(sh, Ast, a_stage, tt.blob, u + 2, lnext);
+                        if (u >= 1)
+                            mbar_wait(smem_addr(&sh.gfree[(u - 1) % TC_ASTAGES]), ((u - 1) / TC_ASTAGES) & 1, abort);
+                        tc_issue_g(sh, Gst, g_stage, tt.blob, u + 2, lnext);
                         ++copies;
                     }
                 }
@@ -325,162 +350,218 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             tc_commit(smem_addr(&sh.drain));
             mbar_wait(smem_addr(&sh.drain), 0, abort, true);
             for (int v = u; v < copies; ++v)
-                mbar_wait(smem_addr(&sh.afull[v % TC_ASTAGES]), (v / TC_ASTAGES) & 1, abort, true);
+                mbar_wait(smem_addr(&sh.gfull[v % TC_ASTAGES]), (v / TC_ASTAGES) & 1, abort, true);
         }
         __syncwarp();
     } else {
         // ---------------------------------------------------------- workers
-        const int c = tid % NT, kq = tid / NT;
-        const double alpha_d = 1.0 / (g.dr * g.dr), inv2mu = 1.0 / (2.0 * g.mu);
-        const double offd = -alpha_d * inv2mu;
-        const int q4 = warp & 3, half = warp >> 2;
-        const int j = 32 * q4 + lane;  // epilogue row
-        const bool jv = j < n;
-        const int lj = jv ? mode_l[j] : 0;
-        const float2 phj = jv ? ph[j] : make_float2(1.f, 0.f);
+        const int m = tid, zc_node = m >> 1, zc_comp = m & 1;  // operand row of this thread
+        const float ad = (float)(1.0 / (2.0 * g.mu * g.dr * g.dr));
+        const int mt = warp >> 2, q4 = warp & 3;               // epilogue: M-tile, lane quarter
+        const float2 al = a.alpha, be = a.beta;
         double dacc[6] = {0, 0, 0, 0, 0, 0};
+        // the launch's one complex64 reduction operand (kinds 1, 2) and complex128 one (kind 4)
+        const float2 *__restrict__ ext32 = nullptr;
+        const double2 *__restrict__ ext64 = nullptr;
+        for (int d = 0; d < a.n_dots && d < 3; ++d) {
+            if (a.dot_kind[d] == 1 || a.dot_kind[d] == 2) ext32 = a.dot_ext[d];
+            if (a.dot_kind[d] == 4) ext64 = a.dot_ext64;
+        }
+        const float2 *__restrict__ xg = a.x;
         int u = 0, it = 0;
         for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
-            const int i0 = tile * NT;
-            const int i = i0 + c;
-            // z_k(r_c) = e^{i m_k theta} x_k(r_c) for this thread's columns
-            float2 z[KPT];
+            const int i0 = tile * TC_NT;
+            // z_k of this row's node and component (e^{i m_k theta} x_k)
+            float zc[KP];
+            {
+                const int i = i0 + zc_node;
 #pragma unroll
-            for (int e = 0; e < KPT; ++e) {
-                const int k = kq * KPT + e;
-                float2 xv = make_float2(0.f, 0.f);
-                if (k < n && i < Nr) xv = a.x[(int64_t)k * Nr + i];
-                const float2 p = ph[k < KP ? k : 0];
-                z[e] = make_float2(p.x * xv.x - p.y * xv.y, p.x * xv.y + p.y * xv.x);
+                for (int k = 0; k < KP; ++k) {
+                    float2 xv = make_float2(0.f, 0.f);
+                    if (k < n && i < Nr) xv = __ldg(xg + (int64_t)k * Nr + i);
+                    const float2 p = ph[k];
+                    zc[k] = zc_comp ? p.x * xv.y + p.y * xv.x : p.x * xv.x - p.y * xv.y;
+                }
             }
-            // radial weights of the tile and the multipole cut
-            if (kq == 0) {
+            // radial weights, 1/r^2 and CAP of the tile's nodes and the multipole cut (the
+            // barrier first: every worker has finished the previous epilogue)
+            workers_sync();
+            if (tid < TC_NT) {
+                const int i = i0 + tid;
                 int lcl = 0;
                 double h0 = 0.0;
+                float hm = 0.f;
                 for (int l = 0; l < K; ++l) {
                     double h = 0.0;
                     if (a.use_v && i >= 1 && i <= Nr - 2) h = a.hh[(int64_t)l * Nr + i];
                     if (l == 0) h0 = fabs(h);
                     else if (fabs(h) > (double)TC_HCUT * h0) lcl = l;
-                    hs[l * NT + c] = (float)h;
+                    hs[l * TC_NT + tid] = (float)h;
+                    hm = fmaxf(hm, fabsf((float)h));
                 }
                 if (lcl > 0) atomicMax(&sh.lcut_red, lcl);
+                hmx[tid] = hm;
+                ir2s[tid] = i < Nr ? (float)g.ir2[i] : 0.f;
+                caps[tid] = (g.capw && i < Nr) ? (float)g.capw[i] : 0.f;
+            }
+            workers_sync();
+            {
+                // the tile's operand scale: S = 2^se with max |S h z| < 2^14 (fp16 range)
+                float zm = 0.f;
+#pragma unroll
+                for (int k = 0; k < KP; ++k) zm = fmaxf(zm, fabsf(zc[k]));
+                atomicMax(&sh.pmax_bits, __float_as_int(zm * hmx[zc_node]));
             }
             workers_sync();
             const int lc = max(1, sh.lcut_red);
+            int se = 0;
+            {
+                const float pm = __int_as_float(sh.pmax_bits);
+                int e2 = 0;
+                frexpf(pm > 0.f ? pm : 1.f, &e2);  // pm < 2^e2
+                // clamped so that 2^se and 2^-(se + g_exp) are normal floats; a tile of values
+                // below 2^-86 only loses scale, not range
+                se = min(100, max(-100, 14 - e2));
+                const float sz = ldexpf(1.f, se);
+#pragma unroll
+                for (int k = 0; k < KP; ++k) zc[k] *= sz;
+            }
+            const float wscale = ldexpf(1.f, -(se + tt.g_exp));  // undoes both operand scales
             workers_sync();
             if (tid == 0) {
                 sh.lcut[it & 1] = lc;
                 sh.lcut_red = 0;
+                sh.pmax_bits = 0;
                 mbar_arrive(smem_addr(&sh.tinfo));
             }
-            // B operand, one multipole per stage
+            // A operand rows, one multipole per stage
             for (int l = 0; l <= lc; ++l, ++u) {
-                const int sb = u % TC_BSTAGES;
-                if (u >= TC_BSTAGES) mbar_wait(smem_addr(&sh.bfree[sb]), ((u / TC_BSTAGES) - 1) & 1, abort);
-                uint8_t *B = Bst + (size_t)sb * B_STAGE;
-                const float h = hs[l * NT + c];
+                const int sz = u % TC_BSTAGES;
+                if (u >= TC_BSTAGES) mbar_wait(smem_addr(&sh.zfree[sz]), ((u / TC_BSTAGES) - 1) & 1, abort);
+                uint8_t *Z = Zst + (size_t)sz * Z_STAGE + (m >> 3) * 128 + (m & 7) * 16;
+                const float h = hs[l * TC_NT + zc_node];
 #pragma unroll
-                for (int gq = 0; gq < KPT / 8; ++gq) {
-                    const int kg = kq * (KPT / 8) + gq;
-                    uint4 re, im;
-                    re.x = pack_bf16(h * z[8 * gq + 0].x, h * z[8 * gq + 1].x);
-                    re.y = pack_bf16(h * z[8 * gq + 2].x, h * z[8 * gq + 3].x);
-                    re.z = pack_bf16(h * z[8 * gq + 4].x, h * z[8 * gq + 5].x);
-                    re.w = pack_bf16(h * z[8 * gq + 6].x, h * z[8 * gq + 7].x);
-                    im.x = pack_bf16(h * z[8 * gq + 0].y, h * z[8 * gq + 1].y);
-                    im.y = pack_bf16(h * z[8 * gq + 2].y, h * z[8 * gq + 3].y);
-                    im.z = pack_bf16(h * z[8 * gq + 4].y, h * z[8 * gq + 5].y);
-                    im.w = pack_bf16(h * z[8 * gq + 6].y, h * z[8 * gq + 7].y);
-                    const int cim = NT + c;
-                    *reinterpret_cast<uint4 *>(B + (size_t)kg * LBO_B + (c >> 3) * 128 + (c & 7) * 16) = re;
-                    *reinterpret_cast<uint4 *>(B + (size_t)kg * LBO_B + (cim >> 3) * 128 + (cim & 7) * 16) = im;
+                for (int gq = 0; gq < KP / 8; ++gq) {
+                    uint4 v;
+                    v.x = pack_f16(h * zc[8 * gq + 0], h * zc[8 * gq + 1]);
+                    v.y = pack_f16(h * zc[8 * gq + 2], h * zc[8 * gq + 3]);
+                    v.z = pack_f16(h * zc[8 * gq + 4], h * zc[8 * gq + 5]);
+                    v.w = pack_f16(h * zc[8 * gq + 6], h * zc[8 * gq + 7]);
+                    *reinterpret_cast<uint4 *>(Z + (size_t)gq * LBO_Z) = v;
                 }
                 fence_proxy_async();
-                mbar_arrive(smem_addr(&sh.bfull[sb]));
+                __syncwarp();
+                if (lane == 0) mbar_arrive(smem_addr(&sh.zfull[sz]));
             }
-            // epilogue: row j, nodes [half NT/2, (half + 1) NT/2) of the tile
+            // epilogue, phase 1: the accumulators to shared memory, W[j][m] (the Z stages are
+            // idle until this thread's next operand rows)
             mbar_wait(smem_addr(&sh.accfull), it & 1, abort);
             tc_fence_after();
-            const uint32_t trow = tmem + ((uint32_t)(32 * q4) << 16);
-            for (int cb = half * (NT / 2); cb < (half + 1) * (NT / 2); cb += 16) {
-                float wr[16], wi[16];
-                tmem_ld16(trow + (uint32_t)cb, wr);
-                tmem_ld16(trow + (uint32_t)(NT + cb), wi);
-                if (!jv) continue;
-                const float2 *xr = a.x + (int64_t)j * Nr;
+            float *W = reinterpret_cast<float *>(Zst);
+            {
+                const uint32_t taddr = tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(mt * KP);
+                const int mrow = 128 * mt + 32 * q4 + lane;
+#pragma unroll 1
+                for (int jc = 0; jc < KP; jc += 16) {
+                    float wv[16];
+                    tmem_ld16(taddr + (uint32_t)jc, wv);
 #pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    const int ii = i0 + cb + e;
-                    if (ii >= Nr) continue;
-                    const bool interior = ii >= 1 && ii <= Nr - 2;
-                    const float2 xf = xr[ii];
-                    const double xr_ = xf.x, xi_ = xf.y;
-                    double hr = 0.0, hi = 0.0;
-                    if (interior) {
-                        if (a.use_h0) {
-                            const float2 xm = xr[ii - 1], xp = xr[ii + 1];
-                            const double diag = (2.0 * alpha_d + (double)(lj * (lj + 1)) * g.ir2[ii]) * inv2mu;
-                            hr = diag * xr_ + offd * ((double)xm.x + (double)xp.x);
-                            hi = diag * xi_ + offd * ((double)xm.y + (double)xp.y);
-                        }
-                        if (a.use_v) {
-                            // conj(ph_j) w
-                            const double pr = phj.x, pim = phj.y;
-                            hr += pr * (double)wr[e] + pim * (double)wi[e];
-                            hi += pr * (double)wi[e] - pim * (double)wr[e];
-                        }
-                    }
-                    if (a.use_cap && g.capw) {
-                        const double cw = g.capw[ii];
-                        hr += cw * xi_;
-                        hi -= cw * xr_;
-                    }
-                    double yr = (double)a.alpha.x * xr_ - (double)a.alpha.y * xi_ + (double)a.beta.x * hr -
-                                (double)a.beta.y * hi;
-                    double yi = (double)a.alpha.x * xi_ + (double)a.alpha.y * xr_ + (double)a.beta.x * hi +
-                                (double)a.beta.y * hr;
-#pragma unroll
-                    for (int s2 = 0; s2 < 2; ++s2)
-                        if (s2 < a.n_sinks && ii >= a.sink_lo[s2] && ii < a.sink_hi[s2]) {
-                            const double2 dd = a.sink_dots[s2];
-                            const double2 vv = a.sink_v[s2][(int64_t)j * Nr + ii];
-                            const double cr = a.sink_coef[s2] * dd.x, ci = a.sink_coef[s2] * dd.y;
-                            yr += cr * vv.x - ci * vv.y;
-                            yi += cr * vv.y + ci * vv.x;
-                        }
-                    const float2 yo = make_float2((float)yr, (float)yi);
-                    a.y[(int64_t)j * Nr + ii] = yo;
-                    const double yrf = yo.x, yif = yo.y;
-#pragma unroll
-                    for (int q = 0; q < 3; ++q) {
-                        if (q >= a.n_dots) break;
-                        double dr_ = 0.0, di_ = 0.0;
-                        const int kd = a.dot_kind[q];
-                        if (kd == 1 || kd == 2) {
-                            const float2 ef = a.dot_ext[q][(int64_t)j * Nr + ii];
-                            const double er = ef.x, ei = ef.y;
-                            if (kd == 1) {  // conj(e) y
-                                dr_ = er * yrf + ei * yif;
-                                di_ = er * yif - ei * yrf;
-                            } else {        // conj(y) e
-                                dr_ = yrf * er + yif * ei;
-                                di_ = yrf * ei - yif * er;
-                            }
-                        } else if (kd == 3) {
-                            dr_ = yrf * yrf + yif * yif;
-                        } else {            // |e64 - y|^2 with the unrounded y
-                            const double2 e64 = a.dot_ext64[(int64_t)j * Nr + ii];
-                            const double ddr = e64.x - yr, ddi = e64.y - yi;
-                            dr_ = ddr * ddr + ddi * ddi;
-                        }
-                        dacc[2 * q] += dr_;
-                        dacc[2 * q + 1] += di_;
-                    }
+                    for (int q = 0; q < 16; ++q) W[(jc + q) * (2 * TC_NT) + mrow] = wv[q];
                 }
             }
             tc_fence_before();
-            mbar_arrive(smem_addr(&sh.accfree));
+            __syncwarp();
+            if (lane == 0) mbar_arrive(smem_addr(&sh.accfree));
+            workers_sync();
+            // phase 2: one complex output per (mode j, node) and thread, consecutive threads
+            // on consecutive nodes of one mode (coalesced loads and stores)
+            {
+                const int tile_nodes = min(TC_NT, Nr - i0);
+                constexpr int EB = 4;  // elements in flight per thread
+#pragma unroll 1
+                for (int e0 = tid; e0 < n * TC_NT; e0 += EB * TC_WORKERS) {
+                    float2 x0[EB], xm[EB], xp[EB], w[EB];
+#pragma unroll
+                    for (int q = 0; q < EB; ++q) {
+                        const int e = e0 + q * TC_WORKERS;
+                        const int j = e / TC_NT, c = e - j * TC_NT;
+                        const bool ok = e < n * TC_NT && c < tile_nodes;
+                        const int i = i0 + c;
+                        const int64_t o = (int64_t)j * Nr + i;
+                        const float2 zero = make_float2(0.f, 0.f);
+                        x0[q] = ok ? __ldg(xg + o) : zero;
+                        xm[q] = (ok && i >= 1) ? __ldg(xg + o - 1) : zero;
+                        xp[q] = (ok && i + 1 < Nr) ? __ldg(xg + o + 1) : zero;
+                        w[q] = ok ? *reinterpret_cast<const float2 *>(W + j * (2 * TC_NT) + 2 * c) : zero;
+                    }
+#pragma unroll
+                    for (int q = 0; q < EB; ++q) {
+                        const int e = e0 + q * TC_WORKERS;
+                        const int j = e / TC_NT, c = e - j * TC_NT;
+                        if (!(e < n * TC_NT && c < tile_nodes)) continue;
+                        const int i = i0 + c;
+                        const int64_t o = (int64_t)j * Nr + i;
+                        const float wr_ = w[q].x * wscale, wi_ = w[q].y * wscale;
+                        float hr = 0.f, hi = 0.f;
+                        if (i >= 1 && i <= Nr - 2) {
+                            if (a.use_h0) {
+                                // H0 x = ad ((x - x_-) + (x - x_+)) + l (l + 1) / (2 mu r^2) x: the
+                                // differences of neighbours are exact for a smooth x
+                                const float cen = cent[j] * ir2s[c];
+                                hr = ad * ((x0[q].x - xm[q].x) + (x0[q].x - xp[q].x)) + cen * x0[q].x;
+                                hi = ad * ((x0[q].y - xm[q].y) + (x0[q].y - xp[q].y)) + cen * x0[q].y;
+                            }
+                            if (a.use_v) {  // conj(ph_j) w
+                                const float2 p = ph[j];
+                                hr += p.x * wr_ + p.y * wi_;
+                                hi += p.x * wi_ - p.y * wr_;
+                            }
+                        }
+                        if (a.use_cap) {
+                            const float cw = caps[c];
+                            hr += cw * x0[q].y;
+                            hi -= cw * x0[q].x;
+                        }
+                        float yr = al.x * x0[q].x - al.y * x0[q].y + be.x * hr - be.y * hi;
+                        float yi = al.x * x0[q].y + al.y * x0[q].x + be.x * hi + be.y * hr;
+#pragma unroll
+                        for (int s2 = 0; s2 < 2; ++s2)
+                            if (s2 < a.n_sinks && i >= a.sink_lo[s2] && i < a.sink_hi[s2]) {
+                                const double2 dd = a.sink_dots[s2];
+                                const double2 vv = a.sink_v[s2][o];
+                                const double cr = a.sink_coef[s2] * dd.x, ci = a.sink_coef[s2] * dd.y;
+                                yr += (float)(cr * vv.x - ci * vv.y);
+                                yi += (float)(cr * vv.y + ci * vv.x);
+                            }
+                        a.y[o] = make_float2(yr, yi);
+                        const double yrd = yr, yid = yi;
+#pragma unroll
+                        for (int d = 0; d < 3; ++d) {
+                            if (d >= a.n_dots) break;
+                            double dr_ = 0.0, di_ = 0.0;
+                            const int kd = a.dot_kind[d];
+                            if (kd == 1 || kd == 2) {
+                                const float2 ev = __ldg(ext32 + o);
+                                if (kd == 1) {  // conj(e) y
+                                    dr_ = (double)ev.x * yrd + (double)ev.y * yid;
+                                    di_ = (double)ev.x * yid - (double)ev.y * yrd;
+                                } else {        // conj(y) e
+                                    dr_ = yrd * (double)ev.x + yid * (double)ev.y;
+                                    di_ = yrd * (double)ev.y - yid * (double)ev.x;
+                                }
+                            } else if (kd == 3) {
+                                dr_ = yrd * yrd + yid * yid;
+                            } else {            // |e64 - y|^2
+                                const double2 e64 = __ldg(ext64 + o);
+                                const double ddr = e64.x - yrd, ddi = e64.y - yid;
+                                dr_ = ddr * ddr + ddi * ddi;
+                            }
+                            dacc[2 * d] += dr_;
+                            dacc[2 * d + 1] += di_;
+                        }
+                    }
+                }
+            }
         }
         // per-CTA partials of the fused reductions (fixed order: warps, then lanes)
         if (a.n_dots > 0) {
@@ -503,41 +584,34 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     if (tid == 0 && sh.abort && a.status) atomicOr(a.status, 16);
     if (warp == 8) {
         tc_fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)NCOL)
-                     : "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS) : "memory");
     }
 }
 
-// Plans: (columns k per worker thread, nodes per tile).  The worker thread holds its
-// z values in registers, so KPT stays at or below 48.
-#define CNM_TC_PLANS(X) X(8, 128) X(16, 128) X(24, 128) X(32, 128) X(40, 128) X(48, 128)
+// Kernels by padded mode count KP (the worker thread keeps KP z values in registers).
+#define CNM_TC_PLANS(X) X(16) X(32) X(48) X(64) X(80) X(96) X(112)
 
-bool tc_plan(int n_modes, int Nr, int a_stage_bytes, int n_sm, TcPlan &p)
+bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
 {
-    const int kp = (n_modes + 15) / 16 * 16;
-    if (n_modes > 128) return false;
-    p.nt = 128;
-    p.kpt = std::max(8, (kp / 2 + 7) / 8 * 8);
-    if (p.kpt * 2 < kp || p.kpt > 48) return false;
-    const int KP = 2 * p.kpt;
-    p.a_stage = (a_stage_bytes + 127) / 128 * 128;
-    const int K = 64;  // upper bound of the multipole count used for the h tile
-    p.smem = (size_t)TC_ASTAGES * p.a_stage + (size_t)TC_BSTAGES * KP * 4 * p.nt + (size_t)K * p.nt * 4 +
-             (size_t)KP * 8 + 128;
-    // at least 120 KiB, so that one CTA (and its 2 NT TMEM columns) is resident per SM and
-    // no tcgen05.alloc has to wait for another CTA's columns
+    p.kp = (n_modes + 15) / 16 * 16;
+    p.nt = TC_NT;
+    if (p.kp > 112 || K > 64) return false;
+    p.a_stage = (g_stage_bytes + 127) / 128 * 128;
+    p.smem = (size_t)TC_ASTAGES * p.a_stage + (size_t)TC_BSTAGES * p.kp * 2 * TC_NT * 2 + (size_t)K * TC_NT * 4 +
+             (size_t)p.kp * 12 + (size_t)3 * TC_NT * 4 + 128;
+    // at least 120 KiB, so that one CTA (and its TMEM columns) is resident per SM and no
+    // tcgen05.alloc has to wait for another CTA's columns
     p.smem = std::max<size_t>(p.smem, 120 * 1024);
-    p.tiles = (Nr + p.nt - 1) / p.nt;
+    p.tiles = (Nr + TC_NT - 1) / TC_NT;
     p.grid = std::min(p.tiles, n_sm);
-    return p.smem <= 220 * 1024;
+    return p.smem <= 225 * 1024;
 }
 
 cudaError_t tc_prepare(const TcPlan &p)
 {
     cudaError_t e = cudaSuccess;
-#define CNM_TC_ATTR(KPT_, NT_) \
-    if (p.kpt == KPT_ && p.nt == NT_) \
-        e = cudaFuncSetAttribute(k_tc_apply<KPT_, NT_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+#define CNM_TC_ATTR(KP_) \
+    if (p.kp == KP_) e = cudaFuncSetAttribute(k_tc_apply<KP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
     CNM_TC_PLANS(CNM_TC_ATTR)
 #undef CNM_TC_ATTR
     return e;
@@ -546,10 +620,10 @@ cudaError_t tc_prepare(const TcPlan &p)
 cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, const int *mode_l, const int *mode_m,
                             int K, const TcTable &tt, const TcArgs &a)
 {
-#define CNM_TC_LAUNCH(KPT_, NT_)                                                                             \
-    if (p.kpt == KPT_ && p.nt == NT_) {                                                                      \
-        k_tc_apply<KPT_, NT_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage); \
-        return cudaGetLastError();                                                                           \
+#define CNM_TC_LAUNCH(KP_)                                                                                      \
+    if (p.kp == KP_) {                                                                                          \
+        k_tc_apply<KP_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage);   \
+        return cudaGetLastError();                                                                              \
     }
     CNM_TC_PLANS(CNM_TC_LAUNCH)
 #undef CNM_TC_LAUNCH
@@ -804,13 +878,16 @@ __global__ void __launch_bounds__(VEC_THREADS) k_mx_update(int64_t n, const MixS
     double acc[1] = {0.0};
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         const float2 yv = y[e], zv = z[e];
-        const double dr = al.x * yv.x - al.y * yv.y + om.x * zv.x - om.y * zv.y;
-        const double di = al.x * yv.y + al.y * yv.x + om.x * zv.y + om.y * zv.x;
+        // the correction is rounded to complex64 first and x takes exactly that value, so a
+        // later A d of the tensor-core check applies the operator to the vector x received
+        const float2 df = make_float2((float)(al.x * yv.x - al.y * yv.y + om.x * zv.x - om.y * zv.y),
+                                      (float)(al.x * yv.y + al.y * yv.x + om.x * zv.y + om.y * zv.x));
+        const double dr = df.x, di = df.y;
         double2 xv = x[e];
         xv.x += dr;
         xv.y += di;
         x[e] = xv;
-        d[e] = make_float2((float)dr, (float)di);
+        d[e] = df;
         acc[0] += dr * dr + di * di;
     }
     partials_out<1>(acc, partials);

@@ -1,5 +1,5 @@
 // cnm_mixed.cuh -- the mixed-precision Crank-Nicolson solve: complex64 work vectors, a
-// tensor-core coupling apply (tcgen05, bf16 operands, fp32 accumulators in TMEM), an
+// tensor-core coupling apply (tcgen05, fp16 operands, fp32 accumulators in TMEM), an
 // fp32 radial-block preconditioner, and fp64 residuals, dots and refinement.
 //
 // The CN system A_full x = b (src/CrankNicolsonModes_matrices.cpp:94-215) is solved by
@@ -14,13 +14,14 @@
 //
 // Tensor-core coupling.  At node r the potential block is D(theta) Ahat(r) D^dag with
 // Ahat(r) = sum_l* h_l*(r) G_l*, G_l* the real Gaunt matrix of multipole l* (rows j,
-// columns k).  For a tile of NT nodes the kernel forms, per l*, the bf16 operand
-//   B_l*[k, c] = h_l*(r_c) z_k(r_c)   (columns c = Re parts, then Im parts)
-// and accumulates  W += G_l* B_l*  into one fp32 TMEM accumulator (M = 128 rows,
-// N = 2 NT columns, K = 16 per instruction); G_l* arrives in shared memory by bulk
-// copy from a pre-formatted bf16 image.  Multipoles whose radial weight is below 1e-9
-// of the monopole at every node of the tile are skipped, and so are 16-column slices
-// of G_l* that are zero.
+// columns k).  For a tile of 128 nodes the kernel forms, per l*, the fp16 operand
+//   Z_l*[m, k] = h_l*(r_node) z_k(r_node)_(Re|Im),   m = 2 node + (0 | 1),
+// and accumulates  D[m, j] += sum_k Z_l*[m, k] G_l*[j, k]  in fp32 TMEM accumulators
+// (two M-tiles of 128 rows, N = the padded mode count, K = 16 per instruction); G_l*
+// arrives in shared memory by bulk copy from a pre-formatted fp16 image (scaled by a power
+// of two, as the operand is per tile, to sit near the top of the fp16 range).  Multipoles
+// whose radial weight is below 1e-9 of the monopole at every node of the tile are
+// skipped, and so are 16-column slices of G_l* that are zero.
 #pragma once
 
 #include <cstdint>
@@ -31,16 +32,17 @@
 namespace cnm {
 
 // Shared-memory image of the Gaunt matrices for the tensor-core apply (host built).
-// Per multipole l* the blob holds its non-zero K slices (16 columns k each) as
-// 4096-byte blocks in the canonical K-major, no-swizzle layout of tcgen05:
-//   byte (k % 16 / 8) * 2048 + (j / 8) * 128 + (j % 8) * 16 + (k % 8) * 2,  j < 128.
+// Per multipole l* the blob holds its non-zero K slices (16 columns k each) as blocks of
+// 32 kp bytes in the canonical K-major, no-swizzle layout of tcgen05 (kp = padded modes):
+//   byte (k % 16 / 8) * 16 kp + (j / 8) * 128 + (j % 8) * 16 + (k % 8) * 2,  j < kp.
 struct TcGaunt {
     int n_modes = 0, kp = 0, K = 0;           // rows, padded columns (multiple of 16), multipoles
-    std::vector<uint16_t> blob;               // bf16 bits, all multipoles back to back
+    std::vector<uint16_t> blob;               // fp16 bits, all multipoles back to back
     std::vector<int> l_off, l_bytes;          // [K] byte offset / size of each multipole's blob
     std::vector<int> slices;                  // [K * 16]: K-slice index of each block (-1 pads)
     std::vector<int> l_nblk;                  // [K] blocks per multipole
     double fro_sum = 0.0;                     // sum_l* |G_l*|_F (error bound of the apply)
+    int g_exp = 0;                            // the blob holds G 2^g_exp (fp16)
 };
 TcGaunt build_tc_gaunt(const struct Coupling &c);
 
@@ -48,6 +50,7 @@ TcGaunt build_tc_gaunt(const struct Coupling &c);
 struct TcTable {
     const uint8_t *blob;
     const int *l_off, *l_bytes, *slices, *l_nblk;
+    int g_exp;
 };
 
 // Arguments of one tensor-core operator application on complex64 vectors:
@@ -76,12 +79,12 @@ struct TcArgs {
 
 // Host entry points (cnm_mixed.cu).
 struct TcPlan {
-    int kpt = 0, nt = 0;      // columns k per worker thread, nodes per tile
+    int kp = 0, nt = 0;       // padded mode count, nodes per tile
     int tiles = 0, grid = 0;
     size_t smem = 0;
-    int a_stage = 0;          // bytes of one A stage (largest multipole blob)
+    int a_stage = 0;          // bytes of one Gaunt stage (largest multipole blob)
 };
-bool tc_plan(int n_modes, int Nr, int a_stage_bytes, int n_sm, TcPlan &p);
+bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p);
 cudaError_t tc_prepare(const TcPlan &p);
 cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, const int *mode_l, const int *mode_m,
                             int K, const TcTable &tt, const TcArgs &a);

@@ -237,6 +237,11 @@ int cnm_apply_lowp(cnm_handle *h, int32_t op, const double *x, double *y);
 /* Counters of the mixed solve's last step: defect-correction passes, fp64 operator
  * applications, and the final relative residual (fp64 or from the tensor-core check). */
 int cnm_mixed_info(const cnm_handle *h, int32_t *passes, int32_t *fp64_applies, double *residual);
+/* The last residual check of the mixed solve, six doubles relative to |rhs|: the
+ * tensor-core residual, its error estimate, the last fp64 residual, the calibration
+ * correction's norm, the last correction's norm, and the calibrated error ratio
+ * |A_fp64 d - A_tc d| / |d|.  Measurement hook (no counterpart in the reference). */
+int cnm_mixed_trace(const cnm_handle *h, double *out);
 /* sink_strength(body) (_absorption.cpp:119-125). */
 int cnm_sink_strength(const cnm_handle *h, int32_t body, double *out);
 /* absorption_sink_active(). */

@@ -1,11 +1,11 @@
 """Mixed-precision path: the tensor-core coupling apply and the defect-correction solve.
 
-The low-precision operator (complex64 state, bf16 Gaunt and radial-weight products on
+The low-precision operator (complex64 state, fp16 Gaunt and radial-weight products on
 the tensor cores, fp32 accumulation) is checked three ways: against a numpy emulation of
-the same rounding (bf16 operands, exact products, fp32-level sums) to 2e-5 of the
-operator's norm, against the fp64 operator of the same handle (the bf16 error budget,
-2e-2 of |V x|, 1e-4 of |A x|), and the mixed step against the fp64 step and the CPU
-oracle.  Tolerances are relative 2-norms.
+the same rounding (fp16 significands, exact products, fp32-level sums) to 2e-5 of the
+operator's norm, against the fp64 operator of the same handle (the fp16 error budget,
+3e-3 of |V x|, 2e-5 of |A x|), and the mixed step against the fp64 step.  Tolerances
+are relative 2-norms.
 """
 import math
 
@@ -15,11 +15,11 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def bf16(a):
-    a = np.asarray(a, np.float32)
-    u = a.view(np.uint32).astype(np.uint64)
-    u = ((u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000).astype(np.uint32)
-    return u.view(np.float32)
+def f16(a):
+    """Round to the fp16 significand (11 bits) with an unbounded exponent: the kernel scales
+    both operands by powers of two into fp16's range, so only the significand rounds."""
+    m, e = np.frexp(np.asarray(a, np.float64))
+    return np.ldexp(np.rint(m * 2048.0) / 2048.0, e)
 
 
 def make(precision, l_max=12, N=2000, L=200.0, mu=0.25, q=0.5, R=50.0, dt=0.5, absorption=True, t_factor=3.0):
@@ -40,10 +40,12 @@ def make(precision, l_max=12, N=2000, L=200.0, mu=0.25, q=0.5, R=50.0, dt=0.5, a
 
 
 def emulate_v(cn, x):
-    """bf16 emulation of the tensor-core coupling V x (the handle's current operator)."""
+    """fp16 emulation of the tensor-core coupling V x (the handle's current operator)."""
     from oracle import oracle as O
     n, N = cn.n_modes, cn.Nr
     orc = O.OracleCNM(N, cn.L, cn.dt, 0.0, cn.l_max, cn.mu, 0.01, cn.q, 0.0, cn.R, False, False, 10 ** 9, 2.0, 2.0)
+    orc.set_initial_state_full(np.zeros(n * N, complex))
+    orc.initialize()   # builds the coupling cache
     rows, cols, ls, ang = orc.coupling_terms()
     K = 2 * cn.l_max + 1
     G = np.zeros((K, n, n))
@@ -66,7 +68,7 @@ def emulate_v(cn, x):
     h2 = np.concatenate([hh, hh], axis=1).astype(np.float32)
     acc = np.zeros((n, 2 * N), np.float64)
     for l in range(K):
-        acc += bf16(G[l]).astype(np.float64) @ bf16(h2[l][None, :] * Zr).astype(np.float64)
+        acc += f16(G[l]) @ f16(h2[l][None, :] * Zr)
     w = acc[:, :N] + 1j * acc[:, N:]
     return (np.conj(ph)[:, None].astype(np.complex128) * w).reshape(-1)
 
@@ -85,10 +87,10 @@ def test_tc_apply_against_emulation_and_fp64(l_max):
     v64 = cn.apply("V", x)
     v_em = emulate_v(cn, x)
     assert rel(v_tc, v_em) < 2e-5
-    assert rel(v_tc, v64) < 2e-2
+    assert rel(v_tc, v64) < 3e-3
     a_tc = cn.apply_lowp("A", x)
     a64 = cn.apply("A", x)
-    assert rel(a_tc, a64) < 1e-4
+    assert rel(a_tc, a64) < 2e-5
     h_tc = cn.apply_lowp("H", x)
     h64 = cn.apply("H", x)
     assert rel(h_tc, h64) < 1e-3
@@ -100,11 +102,13 @@ def test_tc_apply_sinks_match_fp64():
     x = cn.psi
     a_tc = cn.apply_lowp("A_full", x)
     a64 = cn.apply("A_full", x)
-    assert rel(a_tc, a64) < 1e-4
-    # the sink part alone: A_full - A
+    assert rel(a_tc, a64) < 2e-5
+    # the sink part alone, A_full - A (both outputs are rounded to complex64 at the scale
+    # of |A x|, so the difference is compared on that scale)
     d_tc = a_tc - cn.apply_lowp("A", x)
     d64 = a64 - cn.apply("A", x)
-    assert rel(d_tc, d64) < 1e-5
+    assert np.linalg.norm(d64) > 0.0
+    assert np.linalg.norm(d_tc - d64) < 1e-6 * np.linalg.norm(a64)
 
 
 @pytest.mark.parametrize("l_max,N,L", [(8, 2000, 200.0), (12, 2000, 200.0)])
@@ -121,7 +125,7 @@ def test_mixed_steps_match_fp64(l_max, N, L):
         db = b.step(k)
         passes, fp64_applies, res = a.mixed_info()
         assert res <= 1e-12
-        assert 1 <= passes <= 4
+        assert passes == 2, (k, a.mixed_trace())
     pa, pb = a.psi, b.psi
     assert rel(pa, pb) < 1e-10
     ma = a.mu * a.dr * np.sum(np.abs(pa) ** 2)
