@@ -302,7 +302,7 @@ struct Solver {
     TcPlan tcp;
     DevBuf<uint8_t> d_tcblob;
     DevBuf<int> d_tc_loff, d_tc_lbytes, d_tc_slices, d_tc_lnblk;
-    DevBuf<float2> m_r, m_y, m_v, m_s, m_z, m_t, m_d, m_xa, dinv32;
+    DevBuf<float2> m_r, m_y, m_v, m_s, m_z, m_t, m_d, m_xa, dinv32, m_r1, m_q;
     DevBuf<double2> m_r64, m_dots;  // m_dots: [0..1] sink projections, [2..3] corrected ones
     DevBuf<MixScalars> d_msc;
     DevBuf<double> m_part;
@@ -495,7 +495,7 @@ struct Solver {
         upload(d_tc_slices, tg.slices);
         upload(d_tc_lnblk, tg.l_nblk);
         CK(tc_prepare(tcp));
-        for (DevBuf<float2> *b : {&m_r, &m_y, &m_v, &m_s, &m_z, &m_t, &m_d, &m_xa, &dinv32}) b->alloc(nN);
+        for (DevBuf<float2> *b : {&m_r, &m_y, &m_v, &m_s, &m_z, &m_t, &m_d, &m_xa, &dinv32, &m_r1, &m_q}) b->alloc(nN);
         m_r64.alloc(nN);
         m_dots.alloc(8);
         d_msc.alloc(1);
@@ -1375,16 +1375,18 @@ struct Solver {
         launch_check();
     }
 
-    // out = P32^{-1} in (mode 0) or, mode 1, s = r - alpha v formed and stored, out = P32^{-1} s
-    void psolve32(int mode, const float2 *in, float2 *out)
+    // out = P32^{-1} in (mode 0); mode 1: s = r - alpha v formed and stored to s_out,
+    // out = P32^{-1} s; mode 2: out = P32^{-1} (r + beta (r0 - omega v)) with r0 = m_r
+    void psolve32(int mode, const float2 *in, float2 *out, const float2 *r = nullptr, float2 *s_out = nullptr)
     {
         Ps32Args a;
         std::memset(&a, 0, sizeof(a));
         a.mode = mode;
         a.b = in;
-        a.r = m_r.p;
+        a.r = r ? r : m_r.p;
         a.v = m_v.p;
-        a.s_out = m_s.p;
+        a.r0 = m_r.p;
+        a.s_out = s_out ? s_out : m_s.p;
         a.sc = d_msc.p;
         a.status = d_status.p;
         cudaLaunchConfig_t cfg;
@@ -1404,36 +1406,50 @@ struct Solver {
         kt_end(TK_PSOLVE);
     }
 
-    // One defect-correction pass on the current residual m_r (complex64): one
-    // right-preconditioned BiCGSTAB iteration from d = 0 (_matrices.cpp:47-91 with
-    // r0 = r, rho = |r|^2, p = r): y = M r, v = A y, alpha = rho / r.v, s = r - alpha v,
-    // z = M s, t = A z, omega = t.s / |t|^2, d = alpha y + omega z; x += d in fp64.
-    void mixed_pass(const Absorber *const *sk, int k, double dtv)
+    // One defect-correction pass on the current residual m_r (complex64): `iters`
+    // right-preconditioned BiCGSTAB iterations from d = 0 (_matrices.cpp:47-91 with the
+    // shadow residual r0 = r, rho0 = |r|^2, p = r):
+    //   y = M p, v = A y, alpha = rho / r0.v, s = r - alpha v, z = M s, t = A z,
+    //   omega = t.s / |t|^2, d += alpha y + omega z,
+    // then r1 = s - omega t, rho1 = r0.r1, beta = (rho1 / rho0)(alpha / omega) and
+    // p = r1 + beta (r0 - omega v) for the second iteration; x += d (exactly) at the end.
+    void mixed_pass(const Absorber *const *sk, int k, double dtv, int iters)
     {
-        psolve32(0, m_r.p, m_y.p);
-        wood32(sk, k, m_y.p);
-        {
-            TcArgs a = tc_a_args(m_y.p, m_v.p, sk, k, m_dots.p + 2, dtv);
-            a.n_dots = 1;
-            a.dot_kind[0] = 1;
-            a.dot_ext[0] = m_r.p;
-            launch_tc(a);
-            mx_finish(tcp.grid, 2, MX_ALPHA);
+        for (int q = 0; q < iters; ++q) {
+            const bool first = q == 0, last = q + 1 == iters;
+            if (first) psolve32(0, m_r.p, m_y.p);
+            else psolve32(2, nullptr, m_y.p, m_r1.p);
+            wood32(sk, k, m_y.p);
+            {
+                TcArgs a = tc_a_args(m_y.p, m_v.p, sk, k, m_dots.p + 2, dtv);
+                a.n_dots = 1;
+                a.dot_kind[0] = 1;
+                a.dot_ext[0] = m_r.p;  // r0
+                launch_tc(a);
+                mx_finish(tcp.grid, 2, first ? MX_ALPHA : MX_ALPHA2);
+            }
+            psolve32(1, nullptr, m_z.p, first ? m_r.p : m_r1.p, first ? m_s.p : m_q.p);
+            wood32(sk, k, m_z.p);
+            {
+                TcArgs a = tc_a_args(m_z.p, m_t.p, sk, k, m_dots.p + 2, dtv);
+                a.n_dots = 2;
+                a.dot_kind[0] = 2;
+                a.dot_ext[0] = first ? m_s.p : m_q.p;
+                a.dot_kind[1] = 3;
+                launch_tc(a);
+                mx_finish(tcp.grid, 4, MX_OMEGA);
+            }
+            k_mx_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, x.p, m_y.p, m_z.p, m_d.p, first ? 1 : 0,
+                                                                last ? 1 : 0, m_part.p);
+            launch_check();
+            if (last) {
+                mx_finish(vec_blocks, 1, MX_D2);
+            } else {
+                k_mx_next<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, m_s.p, m_t.p, m_r.p, m_r1.p, m_part.p);
+                launch_check();
+                mx_finish(vec_blocks, 2, MX_BETA);
+            }
         }
-        psolve32(1, nullptr, m_z.p);
-        wood32(sk, k, m_z.p);
-        {
-            TcArgs a = tc_a_args(m_z.p, m_t.p, sk, k, m_dots.p + 2, dtv);
-            a.n_dots = 2;
-            a.dot_kind[0] = 2;
-            a.dot_ext[0] = m_s.p;
-            a.dot_kind[1] = 3;
-            launch_tc(a);
-            mx_finish(tcp.grid, 4, MX_OMEGA);
-        }
-        k_mx_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, x.p, m_y.p, m_z.p, m_d.p, m_part.p);
-        launch_check();
-        mx_finish(vec_blocks, 1, MX_D2);
         ++mx_passes;
     }
 
@@ -1539,10 +1555,10 @@ struct Solver {
         k_mx_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, psi.p, x.p, m_r64.p, m_r.p, m_part.p);
         launch_check();
         mx_finish(vec_blocks, 2, MX_B2R0);
-        mixed_pass(sk, k, dtv);
+        mixed_pass(sk, k, dtv, 1);
         mixed_resid64(sk, k, dtv, cand.p);
         mixed_calibrate(sk, k, dtv);
-        mixed_pass(sk, k, dtv);
+        mixed_pass(sk, k, dtv, 2);
         mixed_resid_tc(sk, k, dtv);
         mixed_tail(sk, k, hs);
     }
@@ -1584,7 +1600,7 @@ struct Solver {
                 if (!ok) {
                     // continue from this fp64 residual
                     if (mx_passes >= mixed_max_passes) break;
-                    mixed_pass(sk, k, dtv);
+                    mixed_pass(sk, k, dtv, 2);
                     mixed_resid_tc(sk, k, dtv);
                     mixed_tail(sk, k, hs);
                     continue;
@@ -1600,7 +1616,7 @@ struct Solver {
             if (!finite || mx_passes >= mixed_max_passes) break;
             mixed_resid64(sk, k, dtv, cand.p);
             mixed_calibrate(sk, k, dtv);
-            mixed_pass(sk, k, dtv);
+            mixed_pass(sk, k, dtv, 2);
             mixed_resid_tc(sk, k, dtv);
             mixed_tail(sk, k, hs);
         }

@@ -687,6 +687,13 @@ __global__ void __launch_bounds__(PS32_THREADS) k_psolve32_cl(int Nr, int per, f
             D[e] = dinv[base + e];
             Y[e] = in.b[base + e];
         }
+    } else if (in.mode == 2) {
+        const float2 be = make_float2((float)in.sc->beta.x, (float)in.sc->beta.y);
+        const float2 om = make_float2((float)in.sc->omega.x, (float)in.sc->omega.y);
+        for (int e = tid; e < len; e += T) {
+            D[e] = dinv[base + e];
+            Y[e] = fadd2(in.r[base + e], fmul2(be, fsub2(in.r0[base + e], fmul2(om, in.v[base + e]))));
+        }
     } else {
         const float2 al = make_float2((float)in.sc->alpha.x, (float)in.sc->alpha.y);
         for (int e = tid; e < len; e += T) {
@@ -869,28 +876,55 @@ __global__ void __launch_bounds__(VEC_THREADS) k_mx_resid(int64_t n, const doubl
     partials_out<1>(acc, partials);
 }
 
-// d = alpha y + omega z (fp64 from fp32 operands), x += d, d32 = d; partial |d|^2.
+// The pass's correction d (complex64): d = alpha y + omega z (first iteration) or
+// d += alpha y + omega z, formed in fp64 and rounded once; with `apply`, x += d, so x
+// receives exactly the complex64 vector a later tensor-core check applies the operator to.
+// Partial |d|^2.
 __global__ void __launch_bounds__(VEC_THREADS) k_mx_update(int64_t n, const MixScalars *sc, double2 *x,
-                                                           const float2 *y, const float2 *z, float2 *d,
-                                                           double *partials)
+                                                           const float2 *y, const float2 *z, float2 *d, int first,
+                                                           int apply, double *partials)
 {
     const double2 al = sc->alpha, om = sc->omega;
     double acc[1] = {0.0};
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
         const float2 yv = y[e], zv = z[e];
-        // the correction is rounded to complex64 first and x takes exactly that value, so a
-        // later A d of the tensor-core check applies the operator to the vector x received
-        const float2 df = make_float2((float)(al.x * yv.x - al.y * yv.y + om.x * zv.x - om.y * zv.y),
-                                      (float)(al.x * yv.y + al.y * yv.x + om.x * zv.y + om.y * zv.x));
-        const double dr = df.x, di = df.y;
-        double2 xv = x[e];
-        xv.x += dr;
-        xv.y += di;
-        x[e] = xv;
+        double dr = al.x * yv.x - al.y * yv.y + om.x * zv.x - om.y * zv.y;
+        double di = al.x * yv.y + al.y * yv.x + om.x * zv.y + om.y * zv.x;
+        if (!first) {
+            const float2 dv = d[e];
+            dr += dv.x;
+            di += dv.y;
+        }
+        const float2 df = make_float2((float)dr, (float)di);
         d[e] = df;
-        acc[0] += dr * dr + di * di;
+        if (apply) {
+            double2 xv = x[e];
+            xv.x += (double)df.x;
+            xv.y += (double)df.y;
+            x[e] = xv;
+        }
+        acc[0] += (double)df.x * df.x + (double)df.y * df.y;
     }
     partials_out<1>(acc, partials);
+}
+
+// Inner residual after an iteration, r1 = s - omega t, and the partial conj(r0) . r1 of the
+// next iteration's rho.
+__global__ void __launch_bounds__(VEC_THREADS) k_mx_next(int64_t n, const MixScalars *sc, const float2 *s,
+                                                         const float2 *t, const float2 *r0, float2 *r1,
+                                                         double *partials)
+{
+    const double2 om = sc->omega;
+    const float2 omf = make_float2((float)om.x, (float)om.y);
+    double acc[2] = {0.0, 0.0};
+    for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
+        const float2 sv = s[e], tv = t[e], rv = r0[e];
+        const float2 r = make_float2(sv.x - (omf.x * tv.x - omf.y * tv.y), sv.y - (omf.x * tv.y + omf.y * tv.x));
+        r1[e] = r;
+        acc[0] += (double)rv.x * r.x + (double)rv.y * r.y;
+        acc[1] += (double)rv.x * r.y - (double)rv.y * r.x;
+    }
+    partials_out<2>(acc, partials);
 }
 
 // Sum the partials in a fixed order and run one scalar step of the inner iteration.
@@ -920,6 +954,26 @@ __global__ void k_mx_finish(const double *partials, int nblocks, int nslots, Mix
         const double den = rv.x * rv.x + rv.y * rv.y;
         // alpha = rr / rv
         sc->alpha = den > 0.0 ? make_double2(sc->rr * rv.x / den, -sc->rr * rv.y / den) : make_double2(0.0, 0.0);
+        break;
+    }
+    case MX_BETA: {  // rho1 = r0 . r1, beta = (rho1 / rho0) (alpha / omega), rho0 = |r0|^2
+        const double2 rho1 = make_double2(acc[0], acc[1]);
+        sc->rho1 = rho1;
+        const double2 al = sc->alpha, om = sc->omega;
+        const double omn = om.x * om.x + om.y * om.y;
+        // alpha / omega
+        const double2 ao = omn > 0.0 ? make_double2((al.x * om.x + al.y * om.y) / omn, (al.y * om.x - al.x * om.y) / omn)
+                                     : make_double2(0.0, 0.0);
+        const double r0n = sc->rr > 0.0 ? 1.0 / sc->rr : 0.0;
+        sc->beta = make_double2(r0n * (rho1.x * ao.x - rho1.y * ao.y), r0n * (rho1.x * ao.y + rho1.y * ao.x));
+        break;
+    }
+    case MX_ALPHA2: {  // alpha = rho1 / (r0 . v)
+        sc->rv = make_double2(acc[0], acc[1]);
+        const double2 rv = sc->rv, rho = sc->rho1;
+        const double den = rv.x * rv.x + rv.y * rv.y;
+        sc->alpha = den > 0.0 ? make_double2((rho.x * rv.x + rho.y * rv.y) / den, (rho.y * rv.x - rho.x * rv.y) / den)
+                              : make_double2(0.0, 0.0);
         break;
     }
     case MX_OMEGA:

@@ -97,6 +97,8 @@ struct MixScalars {
     double2 ts;           // conj(t) . s
     double tt;            // |t|^2
     double2 omega;        // ts / tt
+    double2 rho1;         // conj(r0) . r1 of the second inner iteration
+    double2 beta;         // (rho1 / rho0) (alpha / omega)
     double r64;           // |r|^2 of the fp64 residual
     double b2;            // |b|^2
     double d2;            // |d|^2 of the last correction
@@ -108,10 +110,11 @@ struct MixScalars {
 
 // fp32 radial-block solve over thread-block clusters (one cluster per mode):
 //   mode 0: x = P^{-1} b;  mode 1: s = r - alpha v (alpha from sc) is formed, stored to
-//   s_out and solved.
+//   s_out and solved;  mode 2: p = r + beta (r0 - omega v) (the second iteration's search
+//   direction, with the first one's p = r0) is formed and solved.
 struct Ps32Args {
     int mode;
-    const float2 *b, *r, *v;
+    const float2 *b, *r, *v, *r0;
     float2 *s_out;
     const MixScalars *sc;
     int *status;
@@ -125,7 +128,9 @@ __global__ void k_mx_start(int64_t n, const double2 *b, const double2 *psi, doub
 __global__ void k_mx_resid(int64_t n, const double2 *b, const double2 *ax, double2 *r64, double2 *diff, float2 *r32,
                            double *partials);
 __global__ void k_mx_update(int64_t n, const MixScalars *sc, double2 *x, const float2 *y, const float2 *z, float2 *d,
-                            double *partials);
+                            int first, int apply, double *partials);
+__global__ void k_mx_next(int64_t n, const MixScalars *sc, const float2 *s, const float2 *t, const float2 *r0,
+                          float2 *r1, double *partials);
 __global__ void k_mx_finish(const double *partials, int nblocks, int nslots, MixScalars *sc, int stage);
 __global__ void k_to_f32(int64_t n, const double2 *a, float2 *b);
 __global__ void k_to_f64(int64_t n, const float2 *a, double2 *b);
@@ -134,6 +139,6 @@ __global__ void k_sink_dots32(const float2 *x, int Nr, int n_modes, int n_sinks,
 __global__ void k_wood32(int Nr, int n_modes, int lo, int hi, const Krylov *kr, const double2 *proj,
                          const double2 *W0, const double2 *W1, float2 *y, double2 *dots_out);
 
-enum MixStage : int { MX_RR = 0, MX_ALPHA = 1, MX_OMEGA = 2, MX_R64 = 3, MX_D2 = 4, MX_TCRES = 5, MX_B2R0 = 6, MX_ECAL = 7 };
+enum MixStage : int { MX_RR = 0, MX_ALPHA = 1, MX_OMEGA = 2, MX_R64 = 3, MX_D2 = 4, MX_TCRES = 5, MX_B2R0 = 6, MX_ECAL = 7, MX_BETA = 8, MX_ALPHA2 = 9 };
 
 }  // namespace cnm

@@ -29,57 +29,120 @@ namespace {
     throw std::runtime_error(msg);
 }
 
-// Byte offsets just past each '\n' of a file; a trailing partial line is not counted
-// (src/CrankNicolsonModes_restart.cpp:39-58).
-std::vector<std::uintmax_t> line_ends(const std::string &path)
+// A file's bytes, or nothing when it cannot be opened.
+bool slurp(const std::string &path, std::string &out)
 {
-    std::ifstream in(path, std::ios::binary);
-    if (!in) throw std::runtime_error("Cannot open " + path);
-    std::vector<std::uintmax_t> ends;
-    std::vector<char> buf(1 << 20);
-    std::uintmax_t off = 0;
-    while (in) {
-        in.read(buf.data(), (std::streamsize)buf.size());
-        const std::streamsize got = in.gcount();
-        for (std::streamsize i = 0; i < got; ++i)
-            if (buf[(size_t)i] == '\n') ends.push_back(off + (std::uintmax_t)i + 1);
-        off += (std::uintmax_t)got;
-    }
-    return ends;
-}
-
-// First n_rows values of a one-column diagnostic file (_restart.cpp:61-76).
-std::vector<double> read_column(const std::string &path, int n_rows)
-{
-    std::ifstream in(path);
-    if (!in) throw std::runtime_error("Cannot open " + path);
-    std::vector<double> v;
-    v.reserve((size_t)std::max(n_rows, 0));
-    std::string line;
-    while ((int)v.size() < n_rows && std::getline(in, line)) v.push_back(std::strtod(line.c_str(), nullptr));
-    if ((int)v.size() != n_rows) throw std::runtime_error("Too few rows in " + path);
-    return v;
-}
-
-// A text snapshot "re im" per line, exactly `size` rows (_restart.cpp:78-104).
-bool load_snapshot(const std::string &path, std::vector<dcomplex> &state, size_t size)
-{
-    std::ifstream in(path);
+    std::ifstream in(path, std::ios::binary | std::ios::ate);
     if (!in) return false;
-    std::vector<dcomplex> values(size);
-    std::string line;
-    size_t k = 0;
-    while (std::getline(in, line)) {
-        if (line.empty()) continue;
-        if (k == size) return false;
-        char *end = nullptr, *end_im = nullptr;
-        const double re = std::strtod(line.c_str(), &end);
-        const double im = std::strtod(end, &end_im);
-        if (end == line.c_str() || end_im == end) return false;
-        values[k++] = dcomplex(re, im);
+    const std::streamoff n = in.tellg();
+    out.assign(n > 0 ? (size_t)n : 0, '\0');
+    in.seekg(0);
+    if (n > 0) in.read(&out[0], n);
+    return (bool)in || n == 0;
+}
+
+// What a run folder holds, read in one pass per file: for every diagnostic file its text
+// and the byte offset just past each complete row (a row is complete once its '\n' is
+// written), and the steps of the state snapshots psi/snapshot_NNNNNN.txt, newest first.
+// A resume restarts from the newest snapshot whose diagnostic rows are complete in every
+// file (src/CrankNicolsonModes_restart.cpp:288-399 defines that behaviour).
+struct RunIndex {
+    struct File {
+        std::string name, text;
+        std::vector<size_t> row_end;
+    };
+    std::vector<File> files;
+    std::vector<int> snapshots;
+
+    size_t complete_rows() const
+    {
+        size_t n = std::numeric_limits<size_t>::max();
+        for (const File &f : files) n = std::min(n, f.row_end.size());
+        return files.empty() ? 0 : n;
     }
-    if (k != size) return false;
+
+    const File &file(const std::string &name) const
+    {
+        for (const File &f : files)
+            if (f.name == name) return f;
+        throw std::runtime_error("Diagnostic file " + name + " is not part of the run index");
+    }
+
+    // First value of row k of a diagnostic file.
+    double value(const std::string &name, size_t k) const
+    {
+        const File &f = file(name);
+        if (k >= f.row_end.size()) throw std::runtime_error("Row " + std::to_string(k) + " missing from " + name);
+        return std::strtod(f.text.c_str() + (k == 0 ? 0 : f.row_end[k - 1]), nullptr);
+    }
+};
+
+RunIndex index_run(const std::string &folder, const std::vector<std::string> &names)
+{
+    RunIndex ix;
+    for (const std::string &name : names) {
+        RunIndex::File f;
+        f.name = name;
+        if (!slurp(folder + "/" + name, f.text)) throw std::runtime_error("Cannot read " + folder + "/" + name);
+        for (size_t i = 0; i < f.text.size(); ++i)
+            if (f.text[i] == '\n') f.row_end.push_back(i + 1);
+        ix.files.push_back(std::move(f));
+    }
+    // snapshot_ + digits + .txt
+    const std::string head = "snapshot_", tail = ".txt";
+    for (const auto &entry : fs::directory_iterator(folder + "/psi")) {
+        const std::string nm = entry.path().filename().string();
+        if (nm.size() <= head.size() + tail.size() || nm.compare(0, head.size(), head) != 0 ||
+            nm.compare(nm.size() - tail.size(), tail.size(), tail) != 0)
+            continue;
+        const std::string digits = nm.substr(head.size(), nm.size() - head.size() - tail.size());
+        if (!std::all_of(digits.begin(), digits.end(), [](char ch) { return ch >= '0' && ch <= '9'; })) continue;
+        ix.snapshots.push_back(std::stoi(digits));
+    }
+    std::sort(ix.snapshots.begin(), ix.snapshots.end(), std::greater<int>());
+    return ix;
+}
+
+// A text snapshot: one "re im" pair per non-empty line, exactly `size` of them; anything
+// else (a short, over-long or garbled file) is not a usable snapshot.
+bool parse_snapshot(const std::string &path, size_t size, std::vector<dcomplex> &state)
+{
+    std::string text;
+    if (!slurp(path, text)) return false;
+    std::vector<dcomplex> values;
+    values.reserve(size);
+    size_t pos = 0;
+    while (pos < text.size()) {
+        size_t eol = text.find('\n', pos);
+        if (eol == std::string::npos) eol = text.size();
+        if (eol > pos) {
+            const std::string line = text.substr(pos, eol - pos);
+            const char *p0 = line.c_str();
+            char *p1 = nullptr, *p2 = nullptr;
+            const double re = std::strtod(p0, &p1);
+            const double im = std::strtod(p1, &p2);
+            if (p1 == p0 || p2 == p1 || values.size() == size) return false;
+            values.emplace_back(re, im);
+        }
+        pos = eol + 1;
+    }
+    if (values.size() != size) return false;
     state.swap(values);
+    return true;
+}
+
+// The (l, m) list of a run's modes.txt ("l,m" per line); false when there is no file.
+bool read_mode_list(const std::string &path, std::vector<mode> &out)
+{
+    std::string text;
+    if (!slurp(path, text)) return false;
+    std::istringstream in(text);
+    std::string line;
+    while (std::getline(in, line)) {
+        const size_t comma = line.find(',');
+        if (line.empty() || comma == std::string::npos) continue;
+        out.push_back(mode{std::stoi(line.substr(0, comma)), std::stoi(line.substr(comma + 1))});
+    }
     return true;
 }
 
@@ -467,132 +530,115 @@ bool CrankNicolsonModes::load_checkpoint(int step_id)
     return true;
 }
 
-// src/CrankNicolsonModes_restart.cpp:235-286: the evolving scalars from the diagnostic
-// rows 0..step_id-1 (12 significant digits: accurate, not bitwise).
+std::vector<std::string> CrankNicolsonModes_diagnostic_names(
+    const std::vector<std::pair<std::ofstream *, std::string>> &files)
+{
+    std::vector<std::string> names;
+    for (const auto &f : files) names.push_back(f.second);
+    return names;
+}
+
+// Without a checkpoint for the restart step, the evolving scalars come from the
+// diagnostic rows 0 .. step_id-1 (row k is written by step k+1; 12 significant digits, so
+// the restart is close, not bitwise): the orbit of the last row, and the rolling average of
+// p_bin replayed over the phases the rows imply.  The rules -- phase advancing with the
+// previous row's Omega from t = 0 (Omega = 0 during a start-up ramp, Omega_0 otherwise),
+// P and dt following Omega once an evolving orbit is past its ramp -- are those of
+// src/CrankNicolsonModes_restart.cpp:236-286.
 void CrankNicolsonModes::reconstruct_state_from_diagnostics(int step_id)
 {
-    const std::string f = output_folder_ + "/";
-    const std::vector<double> times = read_column(f + "t.txt", step_id);
-    const std::vector<double> Rs = read_column(f + "R_orb.txt", step_id);
-    const std::vector<double> thetas = read_column(f + "theta_orb.txt", step_id);
-    const std::vector<double> Omegas = read_column(f + "Omega_orb.txt", step_id);
-    const std::vector<double> M1s = read_column(f + "M_1.txt", step_id);
-    const std::vector<double> qs = read_column(f + "q.txt", step_id);
-    const std::vector<double> p_bins = read_column(f + "p_bin.txt", step_id);
-    const std::vector<double> p_insts = read_column(f + "p_bin_inst.txt", step_id);
-    double Omega_prev = isolated_ ? 0.0 : (ramp_end_time() > 0.0 ? 0.0 : Omega_0);
-    double t_prev = 0.0;
-    std::vector<double> phases((size_t)step_id);
-    double ph = 0.0;
-    for (int k = 0; k < step_id; ++k) {
-        ph += Omega_prev * (times[k] - t_prev);
-        phases[(size_t)k] = ph;
-        Omega_prev = Omegas[k];
-        t_prev = times[k];
+    const RunIndex ix = index_run(output_folder_, CrankNicolsonModes_diagnostic_names(diagnostic_files()));
+    const size_t n = (size_t)step_id;
+    if (ix.complete_rows() < n) throw std::runtime_error("The diagnostics end before step " + std::to_string(step_id));
+    std::vector<double> times(n), phases(n), p_inst(n);
+    double omega_before = isolated_ || ramp_end_time() > 0.0 ? 0.0 : Omega_0;
+    double t_before = 0.0, ph = 0.0;
+    for (size_t k = 0; k < n; ++k) {
+        times[k] = ix.value("t.txt", k);
+        p_inst[k] = ix.value("p_bin_inst.txt", k);
+        ph += omega_before * (times[k] - t_before);
+        phases[k] = ph;
+        omega_before = ix.value("Omega_orb.txt", k);
+        t_before = times[k];
     }
     phase = ph;
-    if (isolated_) check(cnm_replay_power_average(h_, nullptr, nullptr, nullptr, 0));
-    else check(cnm_replay_power_average(h_, times.data(), phases.data(), p_insts.data(), step_id));
-    if (step_id == 0) {
-        push();
-        return;
-    }
-    const int last = step_id - 1;
-    t_i_ = times[last];
-    R = Rs[last];
-    theta = thetas[last];
-    M1 = M1s[last];
-    q = qs[last];
-    M2 = q * M1;
-    R1 = M2 / (M1 + M2) * R;
-    R2 = M1 / (M1 + M2) * R;
-    Omega = Omegas[last];
-    p_bin_ = p_bins[last];
-    if (!isolated_ && evolve_orbit && t_i_ > ramp_end_time()) {
-        P = 2.0 * M_PI / Omega;
-        dt = P / steps_per_period;
+    check(cnm_replay_power_average(h_, isolated_ ? nullptr : times.data(), isolated_ ? nullptr : phases.data(),
+                                   isolated_ ? nullptr : p_inst.data(), isolated_ ? 0 : step_id));
+    if (n > 0) {
+        const size_t last = n - 1;
+        t_i_ = times[last];
+        R = ix.value("R_orb.txt", last);
+        theta = ix.value("theta_orb.txt", last);
+        M1 = ix.value("M_1.txt", last);
+        q = ix.value("q.txt", last);
+        Omega = ix.value("Omega_orb.txt", last);
+        p_bin_ = ix.value("p_bin.txt", last);
+        M2 = q * M1;
+        R1 = M2 / (M1 + M2) * R;
+        R2 = M1 / (M1 + M2) * R;
+        if (!isolated_ && evolve_orbit && t_i_ > ramp_end_time()) {
+            P = 2.0 * M_PI / Omega;
+            dt = P / steps_per_period;
+        }
     }
     push();
 }
 
-// src/CrankNicolsonModes_restart.cpp:288-399.
+// resume (behaviour of src/CrankNicolsonModes_restart.cpp:288-399): the run folder is
+// indexed once; the restart step is the newest snapshot that parses completely and whose
+// diagnostic rows are complete in every file; the state comes from that snapshot, the
+// scalars from checkpoint.bin when it holds that step (bitwise) or else from the
+// diagnostics; every diagnostic file is cut back to the restart step's rows and the run
+// continues by appending.
 void CrankNicolsonModes::resume(const std::string &folder, int n_steps, double r_ex)
 {
-    if (verbose) std::cout << "Resuming simulation in " << folder << std::endl;
+    if (verbose) std::cout << "Resuming the run in " << folder << std::endl;
     push();
     set_extraction_radius(r_ex, n_steps);
     pull();
     output_folder_ = folder;
-    {
-        std::ifstream modes_in(folder + "/modes.txt");
-        std::string line;
-        int count = 0;
-        while (std::getline(modes_in, line)) {
-            if (line.empty()) continue;
-            int l = 0, m = 0;
-            char comma = 0;
-            std::istringstream row(line);
-            row >> l >> comma >> m;
-            if (count >= n_modes || modes[count].l != l || modes[count].m != m)
-                throw std::runtime_error("modes.txt does not match the modes built from config.toml");
-            ++count;
-        }
-        if (modes_in.is_open() && count != n_modes)
-            throw std::runtime_error("modes.txt does not match the modes built from config.toml");
-    }
-    size_t complete_rows = std::numeric_limits<size_t>::max();
-    std::vector<std::vector<std::uintmax_t>> ends;
-    for (auto &[stream, name] : diagnostic_files()) {
-        ends.push_back(line_ends(folder + "/" + name));
-        complete_rows = std::min(complete_rows, ends.back().size());
-    }
-    std::vector<int> steps;
-    const std::regex pattern(R"(snapshot_(\d+)\.txt)");
-    for (const auto &entry : fs::directory_iterator(folder + "/psi")) {
-        std::smatch m;
-        const std::string name = entry.path().filename().string();
-        if (std::regex_match(name, m, pattern)) steps.push_back(std::stoi(m[1].str()));
-    }
-    std::sort(steps.rbegin(), steps.rend());
+    std::vector<mode> stored;
+    if (read_mode_list(folder + "/modes.txt", stored) && stored != modes)
+        throw std::runtime_error("The mode list of " + folder + "/modes.txt differs from this configuration's");
+    const RunIndex ix = index_run(folder, CrankNicolsonModes_diagnostic_names(diagnostic_files()));
+    const size_t rows = ix.complete_rows();
     int start = -1;
     std::vector<dcomplex> state;
-    for (const int c : steps) {
-        if ((size_t)c > complete_rows) continue;
+    for (const int s : ix.snapshots) {
+        if ((size_t)s > rows) continue;  // its diagnostic rows were not all written
         std::ostringstream path;
-        path << folder << "/psi/snapshot_" << std::setw(6) << std::setfill('0') << c << ".txt";
-        if (load_snapshot(path.str(), state, (size_t)Nr * n_modes)) {
-            start = c;
+        path << folder << "/psi/snapshot_" << std::setw(6) << std::setfill('0') << s << ".txt";
+        if (parse_snapshot(path.str(), (size_t)Nr * n_modes, state)) {
+            start = s;
             break;
         }
-        if (verbose) std::cout << "Skipping incomplete snapshot " << path.str() << std::endl;
+        if (verbose) std::cout << "Snapshot " << path.str() << " is incomplete; trying an earlier one" << std::endl;
     }
-    if (start < 0) throw std::runtime_error("No usable snapshot found in " + folder + "/psi");
-    if (verbose) std::cout << "Restarting from snapshot " << start << std::endl;
+    if (start < 0) throw std::runtime_error("No complete snapshot to resume from in " + folder + "/psi");
+    if (verbose) std::cout << "Restart step: " << start << std::endl;
     check(cnm_set_state(h_, reinterpret_cast<const double *>(state.data()), (int64_t)state.size()));
     if (!load_checkpoint(start)) {
-        if (verbose) std::cout << "No checkpoint for this snapshot: rebuilding the orbit state from the diagnostics."
-                               << std::endl;
+        if (verbose) std::cout << "checkpoint.bin does not hold this step: orbit state from the diagnostics" << std::endl;
         reconstruct_state_from_diagnostics(start);
         sync_state();
     }
-    int fi = 0;
     for (auto &[stream, name] : diagnostic_files()) {
-        const auto &fe = ends[(size_t)fi++];
-        const std::uintmax_t keep = start == 0 ? 0 : fe[(size_t)(start - 1)];
         if (stream->is_open()) stream->close();
-        fs::resize_file(folder + "/" + name, keep);
+        const RunIndex::File &f = ix.file(name);
+        fs::resize_file(folder + "/" + name, start == 0 ? 0 : f.row_end[(size_t)start - 1]);
     }
     open_diagnostics(std::ios::out | std::ios::app);
     t.assign((size_t)n_steps, 0.0);
     if (start < n_steps) t[(size_t)start] = t_i_;
-    // H(t_n) with the restored orbit; keep the stored Omega (the refresh recomputes it)
-    const double restored_Omega = Omega;
+    // rebuild H(t_start) from the restored orbit; the refresh derives Omega from R and the
+    // masses, while the next step must start from the stored Omega
+    const double stored_Omega = Omega;
     check(cnm_refresh(h_, t_i_));
     pull();
-    Omega = restored_Omega;
+    Omega = stored_Omega;
     push();
     if (start + 1 >= n_steps) {
-        if (verbose) std::cout << "The run had already reached its last step (" << n_steps - 1 << ")." << std::endl;
+        if (verbose) std::cout << "Nothing to do: the run already reached step " << n_steps - 1 << std::endl;
         return;
     }
     evolve(start + 1, n_steps);
