@@ -1,24 +1,29 @@
 #!/usr/bin/env python
-"""Benchmark of the Crank-Nicolson step: mode*node*steps/s on one binary.
+"""Benchmark of the Crank-Nicolson step: mode*node*steps/s, mixed precision against FP64.
 
-Workload (the single-GPU configuration the headline metric is quoted on): the
-plain FP64 drop-in on one binary with an evolving orbit -- 2p hydrogenic cloud
-(n=2, l=1, m=1) on the primary, mu=0.25, q=0.5, R=50, back-reaction + GW decay +
-accretion on, s-wave absorption on; l_max=8 (45 modes); N=20000, L=2000,
-r_ex=1500; dt=0.5 (steps_per_period = P0/0.5); complex128 throughout.  Keys the
-configuration does not name take the reference's minimal-example values:
-ramp_periods=2, epsilon=0, epsilon_smear=2, M_c=0.01, damping mask 0.85/1/6.
-The timed steps start one initial period after the start-up ramp, where the
-absorbers, the back-reaction and the orbit evolution are all at full strength.
-The initial state is synthetic (analytic 2p state projected on the modes).
+Default workload (the headline: the mixed-precision solver against the plain FP64 path on
+the same binary): 2p hydrogenic cloud (n=2, l=1, m=1) on the primary, mu=0.25, q=0.5,
+R=50, back-reaction + GW decay + accretion + s-wave absorption on; l_max=12 (91 modes);
+N=40000, L=4000, r_ex=1500; dt=0.5 (steps_per_period = P0/0.5); both arms stop at the
+fp64 relative residual 1e-12.  The mixed arm solves each step by defect correction
+(complex64 inner iterations on the tensor-core coupling apply, fp64 residuals, dots,
+diagnostics and orbit); the FP64 arm is the complex128 drop-in.  `value` is the mixed
+arm; the FP64 arm, their ratio and the difference of the two solutions after the run are
+reported beside it.  Other workloads (--config): c2 (the FP64 drop-in on 45 modes x
+20000 nodes, the configuration the FP64 path was first measured on), c1 (15 modes x 3000
+nodes, fixed orbit).  Keys the configurations do not name take the reference's minimal-
+example values: ramp_periods=2, epsilon=0, epsilon_smear=2, M_c=0.01, mask 0.85/1/6.  The
+timed steps start one initial period after the start-up ramp (absorbers, back-reaction
+and orbit evolution at full strength).  Synthetic input: the analytic 2p state projected
+on the modes.
 
 Arms:
   (default)          the CUDA path through the Python binding of the C ABI;
   --impl reference   the reference's CPU algorithm on the host cores: the oracle
-                     restatement (oracle/, C++17 + OpenMP), the reference itself
-                     being unbuildable here (Eigen 3 and GSL absent).
-Under torchrun each rank advances its own replica (no collective on the data
-path; "replicas only"), timings are maxed over ranks.
+                     restatement (oracle/, C++17 + OpenMP), the reference itself being
+                     unbuildable here (Eigen 3 and GSL absent).
+Under torchrun each rank advances its own replica (no collective on the data path;
+"replicas only"); timings are maxed over ranks.
 """
 from __future__ import annotations
 
@@ -36,18 +41,25 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-WORKLOAD = dict(workload="fp64_single_binary_evolving_orbit", Nr=20000, L=2000.0, l_max=8, n_modes=45, mu=0.25,
-                q=0.5, R=50.0, dt=0.5, r_ex=1500.0, counter=False, absorption=True, evolve_orbit=True,
-                M_c=0.01, epsilon=0.0, epsilon_smear=2.0, ramp_periods=2.0, mask=[0.85, 1.0, 6],
-                state="2p hydrogenic (2,1,1) on the primary", precision="fp64")
+BASE = dict(mu=0.25, q=0.5, R=50.0, dt=0.5, counter=False, absorption=True, evolve_orbit=True, M_c=0.01,
+            epsilon=0.0, epsilon_smear=2.0, ramp_periods=2.0, mask=[0.85, 1.0, 6],
+            state="2p hydrogenic (2,1,1) on the primary")
+WORKLOADS = {
+    "c3": dict(BASE, workload="mixed_vs_fp64_single_binary_l12_N40000", Nr=40000, L=4000.0, l_max=12, n_modes=91,
+               r_ex=1500.0, precision="mixed", tolerance=1e-12),
+    "c2": dict(BASE, workload="fp64_single_binary_evolving_orbit", Nr=20000, L=2000.0, l_max=8, n_modes=45,
+               r_ex=1500.0, precision="fp64", tolerance=1e-10),
+    "c1": dict(BASE, workload="fp64_single_binary_fixed_orbit_l4_N3000", Nr=3000, L=300.0, l_max=4, n_modes=15,
+               mu=0.2, q=0.1, R=30.0, dt=1.0, r_ex=250.0, evolve_orbit=False, precision="fp64", tolerance=1e-10),
+}
 METRIC = "CN mode*node*steps/s"
 UNIT = "mode*node*steps/s"
 
-# DRAM traffic (read + write) per launch of the dominant kernel, the operator apply,
-# from the ncu capture summarised in profiles/k_apply5_fp64_binary_n45_N20000.md:
-# dram__bytes.sum.per_second x gpu__time_duration.sum = 242.04 GB/s x 73.952 us (below the
-# algorithmic bytes: the input vector, written by the launch before, is read from L2).
-NCU_TRAFFIC_BYTES = 242.035482e9 * 73.952e-6
+# DRAM traffic (read + write) per launch of each measured kernel class, from the ncu
+# captures summarised in profiles/ (bytes per launch on the named workload).
+NCU_TRAFFIC = {
+    ("c2", "apply"): 242.035482e9 * 73.952e-6,   # profiles/k_apply5_fp64_binary_n45_N20000.md
+}
 
 
 def peaks():
@@ -67,7 +79,7 @@ def dist_env():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled while the timed region runs."""
+    """nvidia-smi clocks and throttle reasons sampled while the measured steps run."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -81,7 +93,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -120,15 +132,21 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_solver(cls, w, psi0=None):
+def initial_state(w):
+    from boson_cloud_binary_b200.initial_state import hydrogenic_on_primary
+    r = np.linspace(w["epsilon"], w["epsilon"] + w["L"], w["Nr"])
+    modes = [(l, m) for l in range(w["l_max"] + 1) for m in range(-l, l + 1) if (l - m) % 2 == 0]
+    return hydrogenic_on_primary(r, modes, w["mu"], w["q"], w["R"])
+
+
+def make_solver(cls, w, psi0, precision=None):
+    kw = {} if precision is None else {"precision": precision}
     cn = cls(w["Nr"], w["L"], w["dt"], w["epsilon"], w["l_max"], w["mu"], w["M_c"], w["q"], 0.0, w["R"],
-             w["counter"], w["absorption"], 10 ** 9, w["ramp_periods"], w["epsilon_smear"])
-    if psi0 is None:
-        from boson_cloud_binary_b200.initial_state import hydrogenic_on_primary
-        psi0 = hydrogenic_on_primary(cn.r, cn.modes, w["mu"], w["q"], w["R"])
+             w["counter"], w["absorption"], 10 ** 9, w["ramp_periods"], w["epsilon_smear"], **kw)
     cn.set_initial_state_full(psi0)
     cn.evolve_orbit = w["evolve_orbit"]
     cn.steps_per_period = cn.P / w["dt"]
+    cn.tolerance = w["tolerance"]
     cn.initialize()
     cn.build_damping_mask(*w["mask"])
     cn.run(10 ** 9, w["r_ex"])
@@ -136,19 +154,55 @@ def make_solver(cls, w, psi0=None):
     t_start = (w["ramp_periods"] + 1.0) * cn.P
     cn.t_i = t_start
     cn.refresh(t_start)
-    return cn, psi0
+    return cn
 
 
-def algorithmic(kernel, w, n_terms):
+def hh_table(w, cn):
+    """Radial multipole weights h_l*(r_i) of the current orbit (the kernels' hh table)."""
+    K = 2 * w["l_max"] + 1
+    r = cn.r
+    R1, R2, q, Mt = cn.R1, cn.R2, cn.q, cn.M1 + cn.M2
+    hh = np.zeros((K, len(r)))
+    for l in range(K):
+        f1 = 1 / (1 + q) * np.minimum(r, R1) ** l / np.maximum(r, R1) ** (l + 1)
+        f2 = q / (1 + q) * np.minimum(r, R2) ** l / np.maximum(r, R2) ** (l + 1)
+        hh[l] = -w["mu"] * Mt * (f1 + (-1) ** l * f2)
+    hh[:, 0] = hh[:, -1] = 0.0
+    return hh
+
+
+def tc_mma_flops(w, cn):
+    """Tensor-core flops one tensor-core apply issues: per 128-node tile, multipoles up to the
+    tile's cut (the last one above 1e-9 of the monopole at some node), one M=128, N=KP,
+    K=16 MMA per non-zero Gaunt slice and 64-node half tile."""
+    kp, nblk = cn.tc_blocks()
+    hh = hh_table(w, cn)
+    N = w["Nr"]
+    total = 0
+    for i0 in range(0, N, 128):
+        h = np.abs(hh[:, i0:i0 + 128])
+        h0 = h[0]
+        keep = (h[1:] > 1e-9 * h0[None, :]).any(axis=1)
+        lc = max(1, int(np.max(np.nonzero(keep)[0]) + 1) if keep.any() else 1)
+        total += int(np.sum(nblk[:lc + 1])) * 2
+    return total * 2 * 128 * kp * 16
+
+
+def algorithmic(kernel, w, n_terms, cn=None):
     """Algorithmic bytes and flops of one launch of a hot kernel on the workload."""
     n, N = w["n_modes"], w["Nr"]
     K = 2 * w["l_max"] + 1
-    c128 = 16
+    c128, c64 = 16, 8
     if kernel == "apply":
-        # x in, y out, hh table; per interior node T FMAs for Ahat + n^2 complex*real MACs + stencil
+        # x in, y out, hh table; per interior node 2T FMA flops for Ahat + n^2 complex*real MACs + stencil
         return 2 * c128 * n * N + 8 * K * N, (N - 2) * (2 * n_terms + 4 * n * n) + 30 * n * N
+    if kernel == "tc_apply":
+        # x in, y out (complex64), hh table, one fused reduction operand; tensor flops issued
+        return 3 * c64 * n * N + 8 * K * N, tc_mma_flops(w, cn)
     if kernel == "precond_solve":
         return 3 * c128 * n * N, 16 * n * N      # b and inverse pivots in, x out
+    if kernel == "precond_solve32":
+        return 3 * c64 * n * N, 16 * n * N
     if kernel == "precond_factor":
         return c128 * n * N + 8 * K * N, 20 * n * N
     if kernel == "diagnostics":
@@ -157,13 +211,16 @@ def algorithmic(kernel, w, n_terms):
 
 
 def cpu_oracle_sample(w, psi0, target_s=20.0, max_steps=10, threads=0):
-    """Time the CPU oracle on a bounded sample of the same workload."""
+    """Time the CPU oracle on a bounded sample of the same workload (fp64, the reference's
+    algorithm; the workload's tolerance)."""
     from oracle import oracle as O
     O.build()
     cores = O.set_threads(threads if threads > 0 else (os.cpu_count() or 1))
-    cn, _ = make_solver(O.OracleCNM, w, psi0)
     t0 = time.perf_counter()
-    cn.step(1)   # warm-up step (first-touch of the assembled operators)
+    cn = make_solver(O.OracleCNM, w, psi0)
+    setup = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    cn.step(1)   # warm-up step (first touch of the assembled operators)
     first = time.perf_counter() - t0
     steps = int(max(1, min(max_steps, math.floor(target_s / max(first, 1e-3)))))
     t0 = time.perf_counter()
@@ -172,20 +229,39 @@ def cpu_oracle_sample(w, psi0, target_s=20.0, max_steps=10, threads=0):
     el = time.perf_counter() - t0
     value = w["n_modes"] * w["Nr"] * steps / el
     return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{steps} CN steps of the {w['workload']} workload ({w['n_modes']} modes x {w['Nr']} nodes) "
-                      f"after 1 warm-up step, oracle restatement (assembled CSR, OpenMP) on {cores} threads, "
-                      f"{el:.1f} s"}, steps, el
+            "sample": f"{steps} CN steps of the {w['workload']} workload ({w['n_modes']} modes x {w['Nr']} nodes, "
+                      f"tolerance {w['tolerance']:g}) after 1 warm-up step, oracle restatement (assembled CSR, "
+                      f"OpenMP) on {cores} threads, {el:.1f} s (set-up {setup:.0f} s)"}, steps, el
+
+
+def host_memory_gb():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 1e6
+    except OSError:
+        pass
+    return 0.0
+
+
+def oracle_memory_gb(w):
+    """Host memory of the oracle's assembled operators (about nine n^2 N complex128 arrays;
+    measured 13.8 GB at 91 modes x 4000 nodes)."""
+    return 13.8 * (w["n_modes"] / 91.0) ** 2 * (w["Nr"] / 4000.0)
 
 
 def run_reference(args):
     ws, rank, _ = dist_env()
-    w = dict(WORKLOAD)
+    w = dict(WORKLOADS[args.config])
     if rank != 0:
         return 0
-    from boson_cloud_binary_b200.initial_state import hydrogenic_on_primary
-    r = np.linspace(w["epsilon"], w["epsilon"] + w["L"], w["Nr"])
-    modes = [(l, m) for l in range(w["l_max"] + 1) for m in range(-l, l + 1) if (l - m) % 2 == 0]
-    psi0 = hydrogenic_on_primary(r, modes, w["mu"], w["q"], w["R"])
+    need, have = oracle_memory_gb(w), host_memory_gb()
+    if have and need > 0.7 * have:
+        print(json.dumps({"impl": "reference", "unavailable": f"the CPU oracle's assembled operators need about "
+                          f"{need:.0f} GB for {w['workload']}; the host has {have:.0f} GB available"}), flush=True)
+        return 0
+    psi0 = initial_state(w)
     base, steps, el = cpu_oracle_sample(w, psi0, target_s=30.0, max_steps=max(1, min(args.steps, 10)))
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": ws,
             "steps": steps, "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
@@ -197,6 +273,31 @@ def run_reference(args):
     return 0
 
 
+def timed_steps(cn, k0, steps):
+    """Device-event time (ms) of `steps` steps with the state resident in HBM, the launches
+    the steps made, and the solver iterations / passes of each step."""
+    iters = []
+    n0 = cn.launch_count()
+    cn.timer_start()
+    for q in range(steps):
+        d = cn.step(k0 + q)
+        iters.append(d["iterations"])
+    ms = cn.timer_stop()
+    return ms, cn.launch_count() - n0, iters
+
+
+def kernel_breakdown(cn, k0, steps):
+    cn.set_profiling(True)
+    cn.timer_start()
+    for q in range(steps):
+        cn.step(k0 + q)
+    prof_ms = cn.timer_stop()
+    names = ("apply", "tc_apply", "precond_solve", "precond_solve32", "precond_factor", "diagnostics")
+    kt = {name: cn.kernel_times(name) for name in names}
+    cn.set_profiling(False)
+    return {k: {"ms": v[0], "launches": v[1], "share_of_step": v[0] / prof_ms} for k, v in kt.items() if v[1] > 0}
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     dist = None
@@ -206,59 +307,73 @@ def run_ours(args):
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
-    from boson_cloud_binary_b200 import CrankNicolsonModes, select_device
-    from boson_cloud_binary_b200.initial_state import hydrogenic_on_primary
+    from boson_cloud_binary_b200 import CrankNicolsonModes, select_device, measure_fp64_peak
     select_device(local)
-    w = dict(WORKLOAD)
-    r = np.linspace(w["epsilon"], w["epsilon"] + w["L"], w["Nr"])
-    modes = [(l, m) for l in range(w["l_max"] + 1) for m in range(-l, l + 1) if (l - m) % 2 == 0]
-    psi0 = hydrogenic_on_primary(r, modes, w["mu"], w["q"], w["R"])
-    cn, _ = make_solver(CrankNicolsonModes, w, psi0)
+    w = dict(WORKLOADS[args.config])
+    mixed = w["precision"] == "mixed"
+    psi0 = initial_state(w)
+    cn = make_solver(CrankNicolsonModes, w, psi0, w["precision"])
+    ref = make_solver(CrankNicolsonModes, w, psi0, "fp64") if mixed else None
     T = cn.coupling_info()[1]
 
     def barrier():
         if dist is not None:
             dist.barrier()
 
-    k = 0
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        import torch
+        tt = torch.tensor([v], device=f"cuda:{local}")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
+    k = 1
     for _ in range(args.warmup):
-        k += 1
         cn.step(k)
-    # device-timed region, inputs resident in HBM (psi never leaves the GPU); no
-    # per-kernel events inside it
-    iters = []
+        if ref is not None:
+            ref.step(k)
+        k += 1
+    # clocks over a window of at least two seconds: a soak of the same steps (both arms,
+    # so their states stay aligned), then the timed region
     barrier()
     with ClockSampler(local) as clocks:
-        cn.timer_start()
-        for _ in range(args.steps):
+        t_soak = time.perf_counter()
+        while time.perf_counter() - t_soak < 2.0:
+            cn.step(k)
+            if ref is not None:
+                ref.step(k)
             k += 1
-            d = cn.step(k)
-            iters.append(d["iterations"])
-        ms = cn.timer_stop()
+        ms, launches, iters = timed_steps(cn, k, args.steps)
+    if ref is not None:
+        ms_ref, _, iters_ref = timed_steps(ref, k, args.steps)
+    k += args.steps
     barrier()
-    # per-kernel device time of the four hot kernel classes on a further stretch of
-    # the same run (events around every launch of those classes)
-    prof_steps = max(1, min(args.steps, 50))
-    cn.set_profiling(True)
-    cn.timer_start()
-    for _ in range(prof_steps):
-        k += 1
-        cn.step(k)
-    prof_ms = cn.timer_stop()
-    kt = {name: cn.kernel_times(name) for name in ("apply", "precond_solve", "precond_factor", "diagnostics")}
-    cn.set_profiling(False)
-    plan = cn.plan_info()
-    if dist is not None:
-        import torch
-        tt = torch.tensor([ms], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+    ms = max_over_ranks(ms)
     units = w["n_modes"] * w["Nr"] * args.steps * ws
     value = units / (ms / 1e3)
+    accuracy = None
+    if ref is not None:
+        ms_ref = max_over_ranks(ms_ref)
+        pa, pb = cn.psi, ref.psi
+        mu_dr = w["mu"] * (w["L"] / (w["Nr"] - 1))
+        ma, mb = mu_dr * np.sum(np.abs(pa) ** 2), mu_dr * np.sum(np.abs(pb) ** 2)
+        accuracy = {"steps_compared": k - 1, "U_lm_rel": float(np.linalg.norm(pa - pb) / np.linalg.norm(pb)),
+                    "mass_rel": float(abs(ma - mb) / mb), "R_rel": float(abs(cn.R - ref.R) / ref.R),
+                    "against": "the FP64 GPU path (the drop-in, pinned to the CPU oracle by the parity tests) "
+                               "from the same state, both at fp64 relative residual 1e-12"}
 
-    # end to end through the public API with host buffers: upload the state from
-    # pinned host memory, run the steps (each returns its diagnostics to the host),
-    # download the final state (the snapshot the reference writes at save_every).
+    # per-kernel device time on a further stretch of the same run (events around every
+    # launch of the hot kernel classes)
+    prof_steps = max(1, min(args.steps, 20))
+    kshare = kernel_breakdown(cn, k, prof_steps)
+    kshare_ref = kernel_breakdown(ref, k, prof_steps) if ref is not None else None
+    k += prof_steps
+    plan = cn.plan_info()
+
+    # end to end through the public API with host buffers: the state uploaded from pinned
+    # host memory, the steps (each returns its diagnostics to the host), the final state
+    # downloaded (the snapshot the reference writes at save_every)
     try:
         import torch
         host = torch.empty(2 * w["n_modes"] * w["Nr"], dtype=torch.float64, pin_memory=True).numpy()
@@ -270,63 +385,66 @@ def run_ours(args):
     t0 = time.perf_counter()
     cn.psi = host.view(np.complex128)
     for _ in range(args.steps):
-        k += 1
         cn.step(k)
+        k += 1
     host[:] = cn.psi.view(np.float64)
-    e2e_s = time.perf_counter() - t0
-    if dist is not None:
-        import torch
-        tt = torch.tensor([e2e_s], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        e2e_s = float(tt.item())
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
     state_bytes = 16 * w["n_modes"] * w["Nr"]
     e2e = {"value": units / e2e_s, "unit": UNIT, "h2d_bytes_per_step": state_bytes / args.steps,
            "d2h_bytes_per_step": diag_bytes + state_bytes / args.steps,
            "note": "state uploaded once and downloaded once per timed run (save_every = steps); "
                    "diagnostics returned to the host every step"}
 
+    # roofline of the dominant kernel class of the measured arm
     hbm, bf16, src = peaks()
-    from boson_cloud_binary_b200 import measure_fp64_peak
-    fp64_peak = measure_fp64_peak()
-    dom = max(kt, key=lambda kname: kt[kname][0])
-    tot, launches = kt[dom]
-    avg_s = tot / max(launches, 1) / 1e3
-    nbytes, nflops = algorithmic(dom, w, T)
-    # The schema's roofline is the HBM one; the operator kernel is bound by the FP64 FMA
-    # pipe instead, so its compute roofline (against the FP64 peak measured on this
-    # device by cnm_measure_fp64_peak) is reported beside it.
-    roof = {"kernel": dom, "bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm, "unit": "GB/s",
-            "frac": nbytes / avg_s / 1e9 / hbm, "traffic": NCU_TRAFFIC_BYTES,
-            "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
+    dom = max(kshare, key=lambda kname: kshare[kname]["ms"])
+    avg_s = kshare[dom]["ms"] / kshare[dom]["launches"] / 1e3
+    nbytes, nflops = algorithmic(dom, w, T, cn)
+    roof = {"kernel": dom, "avg_launch_us": avg_s * 1e6, "launches": kshare[dom]["launches"],
             "algorithmic_bytes_per_launch": nbytes, "algorithmic_flops_per_launch": nflops,
-            "avg_launch_us": avg_s * 1e6, "launches": launches,
-            "fp64": {"achieved_tflops": nflops / avg_s / 1e12, "peak_tflops": fp64_peak,
-                     "frac": nflops / avg_s / 1e12 / fp64_peak,
-                     "peak_source": "measured here (cnm_measure_fp64_peak: FP64 FMA chains, device events)"}}
-    kshare = {kname: {"ms": v[0], "launches": v[1], "share_of_step": v[0] / prof_ms} for kname, v in kt.items()}
+            "traffic": NCU_TRAFFIC.get((args.config, dom))}
+    if dom == "tc_apply":
+        roof.update({"bound": "tensor", "achieved": nflops / avg_s / 1e12, "peak": bf16, "unit": "TFLOP/s",
+                     "frac": nflops / avg_s / 1e12 / bf16,
+                     "peak_source": (f"{src} (MEASURED_PEAKS.json bf16_tflops: dense fp16 and bf16 rates are "
+                                     "the same)") if src == "measured" else "fallback",
+                     "hbm": {"achieved": nbytes / avg_s / 1e9, "peak": hbm, "unit": "GB/s",
+                             "frac": nbytes / avg_s / 1e9 / hbm}})
+    else:
+        fp64_peak = measure_fp64_peak()
+        roof.update({"bound": "hbm", "achieved": nbytes / avg_s / 1e9, "peak": hbm, "unit": "GB/s",
+                     "frac": nbytes / avg_s / 1e9 / hbm,
+                     "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
+                     "fp64": {"achieved_tflops": nflops / avg_s / 1e12, "peak_tflops": fp64_peak,
+                              "frac": nflops / avg_s / 1e12 / fp64_peak,
+                              "peak_source": "measured here (cnm_measure_fp64_peak: FP64 FMA chains, device "
+                                             "events)"}})
 
+    cfg = {k_: w[k_] for k_ in ("workload", "Nr", "L", "l_max", "n_modes", "mu", "q", "R", "dt", "precision",
+                                "tolerance")}
+    cfg.update({"parallelism": f"replicas{ws}", "l2": "working set > L2 (the state alone is "
+                f"{w['n_modes'] * w['Nr'] * 16 / 1e6:.0f} MB complex128)",
+                "iterations_mean": float(np.mean(iters)) if iters else None, "plan": plan,
+                "kernel_breakdown_steps": prof_steps})
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": w["workload"], "Nr": w["Nr"], "L": w["L"], "l_max": w["l_max"],
-                       "n_modes": w["n_modes"], "mu": w["mu"], "q": w["q"], "R": w["R"], "dt": w["dt"],
-                       "precision": "fp64", "parallelism": f"replicas{ws}",
-                       "l2": "working set > L2 (20 vectors of 14.4 MB plus pivots)",
-                       "bicgstab_iterations_mean": float(np.mean(iters)) if iters else None,
-                       "plan": plan, "kernel_breakdown_steps": prof_steps},
+            "vs_baseline": None, "dtype": "c64+c128" if mixed else "c128", "data": "synthetic", "config": cfg,
             "roofline": roof, "kernels": kshare, "e2e": e2e, "clocks": clocks.summary(),
-            "gpu_launches": None}
-    # launches of our kernels in the timed region (counted by the instrumented classes plus
-    # the streaming/scalar kernels per BiCGSTAB iteration and per step)
-    # per step: 1 right-hand-side apply, 1 factorisation, 1 Woodbury set-up, 1 residual
-    # apply, 1 diagnostics, start, mask, 3 sink projections, 1 hh table, 1 absorber
-    # moments, 1 projector, 1 slot sum = 15; per iteration 2 solves, 2 applies, 2
-    # Woodbury corrections, 1 update = 7 (with sinks, as in this workload)
-    it_total = int(np.sum(iters))
-    line["gpu_launches"] = int(it_total * 7 + args.steps * 15)
+            "gpu_launches": int(launches)}
+    if ref is not None:
+        line["fp64_arm"] = {"value": units / (ms_ref / 1e3), "ms_per_step": ms_ref / args.steps,
+                            "iterations_mean": float(np.mean(iters_ref)), "kernels": kshare_ref}
+        line["mixed_over_fp64"] = ms_ref / ms
+        line["accuracy"] = accuracy
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        base, _, _ = cpu_oracle_sample(w, psi0)
-        line["cpu_baseline"] = base
+        need, have = oracle_memory_gb(w), host_memory_gb()
+        if have and need > 0.7 * have:
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+                                    "sample": f"not run: the oracle's assembled operators need about {need:.0f} GB, "
+                                              f"{have:.0f} GB available"}
+        else:
+            base, _, _ = cpu_oracle_sample(w, psi0, target_s=20.0, max_steps=5)
+            line["cpu_baseline"] = base
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
@@ -338,8 +456,9 @@ def run_ours(args):
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=300)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--config", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()

@@ -76,7 +76,7 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
            "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel",
            "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy",
-           "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info", "cnm_mixed_trace")
+           "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info", "cnm_mixed_trace", "cnm_launch_count", "cnm_tc_blocks")
 
 def displaced_100_state(r, modes, mu, x_bh):
     """displaced_100_state (src/DisplacedAtom.cpp:12-76) on the device: the mode projection
@@ -107,7 +107,8 @@ def measure_fp64_peak():
 
 PRECISIONS = {"fp64": 0, "mixed": 1}
 
-KERNELS = {"apply": 0, "precond_solve": 1, "precond_factor": 2, "diagnostics": 3}
+KERNELS = {"apply": 0, "precond_solve": 1, "precond_factor": 2, "diagnostics": 3, "tc_apply": 4,
+           "precond_solve32": 5}
 
 _lib = None
 
@@ -148,6 +149,8 @@ def load_library():
     L.cnm_apply_lowp.argtypes = [p, i32, dp, dp]
     L.cnm_mixed_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), dp]
     L.cnm_mixed_trace.argtypes = [p, dp]
+    L.cnm_launch_count.argtypes = [p, C.POINTER(C.c_int64)]
+    L.cnm_tc_blocks.argtypes = [p, C.POINTER(i32), C.POINTER(i32)]
     L.cnm_sink_strength.argtypes = [p, i32, dp]
     L.cnm_sink_active.argtypes = [p, C.POINTER(i32)]
     L.cnm_sink_vector.argtypes = [p, i32, dp]
@@ -365,6 +368,19 @@ class CrankNicolsonModes:
         p, f, r = C.c_int32(), C.c_int32(), C.c_double()
         self._check(self._lib.cnm_mixed_info(self._h, C.byref(p), C.byref(f), C.byref(r)))
         return p.value, f.value, r.value
+
+    def tc_blocks(self):
+        """(padded mode count, non-zero 16-column Gaunt slices per multipole) of a mixed handle."""
+        kp = C.c_int32()
+        nb = np.zeros(2 * self.l_max + 1, np.int32)
+        self._check(self._lib.cnm_tc_blocks(self._h, C.byref(kp), nb.ctypes.data_as(C.POINTER(C.c_int32))))
+        return kp.value, nb
+
+    def launch_count(self):
+        """Kernels launched by this handle so far (cnm_launch_count)."""
+        v = C.c_int64()
+        self._check(self._lib.cnm_launch_count(self._h, C.byref(v)))
+        return v.value
 
     def mixed_trace(self):
         """Last residual check of the mixed solve (see cnm_mixed_trace)."""

@@ -220,7 +220,7 @@ struct KernelTimer {
     }
 };
 
-enum TimedKernel : int { TK_APPLY = 0, TK_PSOLVE = 1, TK_PFACTOR = 2, TK_DIAG = 3, TK_COUNT = 4 };
+enum TimedKernel : int { TK_APPLY = 0, TK_PSOLVE = 1, TK_PFACTOR = 2, TK_DIAG = 3, TK_TC = 4, TK_PSOLVE32 = 5, TK_COUNT = 6 };
 
 struct Solver {
     // constructor arguments and derived constants
@@ -707,7 +707,13 @@ struct Solver {
     }
 
     void sync() { CK(cudaStreamSynchronize(stream)); }
-    void launch_check() { CK(cudaGetLastError()); }
+    // kernels this handle has launched (counted at every launch site)
+    int64_t n_launches = 0;
+    void launch_check()
+    {
+        CK(cudaGetLastError());
+        ++n_launches;
+    }
 
     double ramp_end_time() const { return ramp_periods * initial_period; }
 
@@ -1133,6 +1139,7 @@ struct Solver {
             cfg.attrs = at;
             cfg.numAttrs = 2;
             kt_begin(TK_PFACTOR);
+            ++n_launches;
             CK(cudaLaunchKernelEx(&cfg, k_precond_factor_cl, grid(), table(), (const double *)d_hh.p, 0.5 * dtv,
                                   offdiag(dtv), pcl_per, dinv.p, d_status.p));
             kt_end(TK_PFACTOR);
@@ -1187,6 +1194,7 @@ struct Solver {
         cfg.attrs = at;
         cfg.numAttrs = 2;
         kt_begin(TK_PSOLVE);
+        ++n_launches;
         CK(cudaLaunchKernelEx(&cfg, k_precond_solve_cl, Nr, n_modes, pcl_per, offdiag(dtv), (const double2 *)dinv.p,
                               bv, xv, b2, x2, in, wd));
         kt_end(TK_PSOLVE);
@@ -1364,9 +1372,10 @@ struct Solver {
 
     void launch_tc(const TcArgs &a)
     {
-        kt_begin(TK_APPLY);
+        kt_begin(TK_TC);
+        ++n_launches;
         CK(launch_tc_apply(tcp, stream, grid(), d_mode_l.p, d_mode_m.p, K, tc_table(), a));
-        kt_end(TK_APPLY);
+        kt_end(TK_TC);
     }
 
     void mx_finish(int nblocks, int nslots, int stage)
@@ -1400,10 +1409,11 @@ struct Solver {
         cfg.attrs = at;
         cfg.numAttrs = 1;
         const double2 o = offdiag(op.dt);
-        kt_begin(TK_PSOLVE);
+        kt_begin(TK_PSOLVE32);
+        ++n_launches;
         CK(cudaLaunchKernelEx(&cfg, k_psolve32_cl, Nr, ps_per, make_float2((float)o.x, (float)o.y),
                               (const float2 *)dinv32.p, out, a));
-        kt_end(TK_PSOLVE);
+        kt_end(TK_PSOLVE32);
     }
 
     // One defect-correction pass on the current residual m_r (complex64): `iters`
@@ -2519,6 +2529,21 @@ int cnm_mixed_info(const cnm_handle *h, int32_t *passes, int32_t *fp64_applies, 
         if (fp64_applies) *fp64_applies = s.mx_fp64;
         if (residual) *residual = s.mx_residual;
     });
+}
+
+int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) {
+        if (!s.mixed) throw cnm::Error(CNM_ELOGIC, "no tensor-core operator on an fp64 handle");
+        if (kp) *kp = s.tg.kp;
+        if (nblk)
+            for (int l = 0; l < s.K; ++l) nblk[l] = s.tg.l_nblk[l];
+    });
+}
+
+int cnm_launch_count(const cnm_handle *h, int64_t *count)
+{
+    return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) { *count = s.n_launches; });
 }
 
 int cnm_mixed_trace(const cnm_handle *h, double *out)

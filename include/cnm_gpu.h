@@ -251,12 +251,18 @@ int cnm_sink_vector(const cnm_handle *h, int32_t body, double *out);
 
 /* --- measurement hooks (no counterpart in the reference) -------------------------
  * Device-event timing of the handle's stream, used by the benchmark: whole regions
- * (start/stop) and, while profiling is on, every launch of the four hot kernel
- * classes: 0 operator apply, 1 preconditioner solve, 2 pivot factorisation,
- * 3 fused diagnostics. */
+ * (start/stop) and, while profiling is on, every launch of the hot kernel classes:
+ * 0 fp64 operator apply, 1 fp64 preconditioner solve, 2 pivot factorisation, 3 fused
+ * diagnostics, 4 tensor-core operator apply, 5 fp32 preconditioner solve. */
 int cnm_set_profiling(cnm_handle *h, int32_t on);
 int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *launches);
 int cnm_timer_start(cnm_handle *h);
+/* Tensor-core operator layout of a CNM_MIXED handle: the padded mode count and, for each
+ * of the 2 l_max + 1 multipoles, the number of non-zero 16-column slices of its Gaunt
+ * matrix (one MMA per slice and 64-node half tile). */
+int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk);
+/* Kernels the handle has launched since its creation (every launch site counts). */
+int cnm_launch_count(const cnm_handle *h, int64_t *count);
 int cnm_timer_stop(cnm_handle *h, double *ms);
 /* Operator kernel selection (testing and measurement): 1 (default) uses the kernel
  * specialised at compile time for l_max <= 8 where it exists, 0 the generic
