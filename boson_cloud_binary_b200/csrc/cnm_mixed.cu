@@ -190,12 +190,12 @@ __device__ __forceinline__ uint32_t pack_f16(float lo, float hi)
 
 constexpr int TC_WORKERS = 256;              // operand producers and epilogue (warps 0-7)
 constexpr int TC_THREADS = TC_WORKERS + 32;  // + the copy / MMA warp (warp 8)
-constexpr int TC_ASTAGES = 3, TC_BSTAGES = 2;
+constexpr int TC_GMAX = 8, TC_BSTAGES = 2;  // at most 8 Gaunt stages (the plan sets how many)
 constexpr int TC_NT = 128;                   // nodes per tile: 2 x 64-node halves, one MMA M-tile each
 constexpr float TC_HCUT = 1e-9f;             // multipoles below this fraction of the monopole are skipped
 
 struct TcShared {
-    unsigned long long gfull[TC_ASTAGES], gfree[TC_ASTAGES], zfull[TC_BSTAGES], zfree[TC_BSTAGES];
+    unsigned long long gfull[TC_GMAX], gfree[TC_GMAX], zfull[TC_BSTAGES], zfree[TC_BSTAGES];
     unsigned long long accfull, accfree, tinfo, drain;
     uint32_t tmem_base;
     int lcut[2];
@@ -205,10 +205,11 @@ struct TcShared {
     int l_off[64], l_bytes[64], l_nblk[64];
 };
 
-// Bulk copy of multipole lv's Gaunt blocks into the G stage of use v (v % 3).
-__device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_stage, const uint8_t *blob, int v, int lv)
+// Bulk copy of multipole lv's Gaunt blocks into the G stage of use v (v % gst).
+__device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_stage, int gst, const uint8_t *blob, int v,
+                                           int lv)
 {
-    const int s = v % TC_ASTAGES;
+    const int s = v % gst;
     const uint32_t bar = smem_addr(&sh.gfull[s]);
     if (sh.l_bytes[lv] == 0) {  // no non-zero block: complete the phase without a copy
         mbar_arrive(bar);
@@ -230,7 +231,8 @@ __device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_sta
 // persistent CTAs, tile t = blockIdx.x + q gridDim.x.
 template <int KP>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int g_stage)
+    k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int g_stage,
+               int gst)
 {
     constexpr int LBO_Z = 32 * 128;            // bytes between 8-column groups of k in a Z stage
     constexpr int Z_STAGE = KP * 2 * TC_NT * 2;  // bytes of one Z stage (2 NT rows x KP fp16)
@@ -242,8 +244,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     __shared__ TcShared sh;
     const int n = g.n_modes, Nr = g.Nr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    uint8_t *Gst = tc_smem;                                              // TC_ASTAGES x g_stage
-    uint8_t *Zst = Gst + (size_t)TC_ASTAGES * g_stage;                   // TC_BSTAGES x Z_STAGE
+    uint8_t *Gst = tc_smem;                                              // gst x g_stage
+    uint8_t *Zst = Gst + (size_t)gst * g_stage;                          // TC_BSTAGES x Z_STAGE
+    // copies run gst - 1 uses ahead; a tile's first gst - 1 uses are copied before its cut is
+    // known, so every tile runs at least multipoles 0 .. gst - 2
+    const int lc_min = max(1, gst - 2);
     float *hs = reinterpret_cast<float *>(Zst + (size_t)TC_BSTAGES * Z_STAGE);  // K x TC_NT
     float2 *ph = reinterpret_cast<float2 *>(hs + (size_t)K * TC_NT);    // KP phases e^{i m_k theta}
     float *cent = reinterpret_cast<float *>(ph + KP);                   // KP: l (l + 1) / (2 mu)
@@ -253,7 +258,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     volatile int *abort = &sh.abort;
 
     if (tid == 0) {
-        for (int s = 0; s < TC_ASTAGES; ++s) {
+        for (int s = 0; s < gst; ++s) {
             mbar_init(smem_addr(&sh.gfull[s]), 1);
             mbar_init(smem_addr(&sh.gfree[s]), 1);
         }
@@ -301,11 +306,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             int copies = 0;
             int it = 0;
             const int first = blockIdx.x;
-            if (first < tiles) {
-                tc_issue_g(sh, Gst, g_stage, tt.blob, 0, 0);
-                tc_issue_g(sh, Gst, g_stage, tt.blob, 1, 1);
-                copies = 2;
-            }
+            if (first < tiles)
+                for (; copies < gst - 1; ++copies) tc_issue_g(sh, Gst, g_stage, gst, tt.blob, copies, copies);
             for (int tile = first; tile < tiles; tile += gridDim.x, ++it) {
                 mbar_wait(smem_addr(&sh.tinfo), it & 1, abort);
                 const int lc = sh.lcut[it & 1];
@@ -314,8 +316,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tc_fence_after();
                 bool firstmma = true;
                 for (int l = 0; l <= lc; ++l, ++u) {
-                    const int sg = u % TC_ASTAGES, sz = u % TC_BSTAGES;
-                    mbar_wait(smem_addr(&sh.gfull[sg]), (u / TC_ASTAGES) & 1, abort);
+                    const int sg = u % gst, sz = u % TC_BSTAGES;
+                    mbar_wait(smem_addr(&sh.gfull[sg]), (u / gst) & 1, abort);
                     mbar_wait(smem_addr(&sh.zfull[sz]), (u / TC_BSTAGES) & 1, abort);
                     tc_fence_after();
                     const uint32_t gbase = smem_addr(Gst + (size_t)sg * g_stage);
@@ -333,14 +335,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     tc_commit(smem_addr(&sh.gfree[sg]));
                     tc_commit(smem_addr(&sh.zfree[sz]));
-                    // refill: use u + 2 goes into the G stage of use u - 1
+                    // refill: use u + gst - 1 goes into the G stage of use u - 1 (in the next
+                    // tile it is one of multipoles 0 .. gst - 2, which every tile runs)
+                    const int ahead = gst - 1;
                     int lnext = -1;
-                    if (l + 2 <= lc) lnext = l + 2;
-                    else if (more) lnext = l + 2 - (lc + 1);
+                    if (l + ahead <= lc) lnext = l + ahead;
+                    else if (more) lnext = l + ahead - (lc + 1);
                     if (lnext >= 0) {
-                        if (u >= 1)
-                            mbar_wait(smem_addr(&sh.gfree[(u - 1) % TC_ASTAGES]), ((u - 1) / TC_ASTAGES) & 1, abort);
-                        tc_issue_g(sh, Gst, g_stage, tt.blob, u + 2, lnext);
+                        if (u >= 1) mbar_wait(smem_addr(&sh.gfree[(u - 1) % gst]), ((u - 1) / gst) & 1, abort);
+                        tc_issue_g(sh, Gst, g_stage, gst, tt.blob, u + ahead, lnext);
                         ++copies;
                     }
                 }
@@ -350,7 +353,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             tc_commit(smem_addr(&sh.drain));
             mbar_wait(smem_addr(&sh.drain), 0, abort, true);
             for (int v = u; v < copies; ++v)
-                mbar_wait(smem_addr(&sh.gfull[v % TC_ASTAGES]), (v / TC_ASTAGES) & 1, abort, true);
+                mbar_wait(smem_addr(&sh.gfull[v % gst]), (v / gst) & 1, abort, true);
         }
         __syncwarp();
     } else {
@@ -413,7 +416,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 atomicMax(&sh.pmax_bits, __float_as_int(zm * hmx[zc_node]));
             }
             workers_sync();
-            const int lc = max(1, sh.lcut_red);
+            const int lc = max(lc_min, sh.lcut_red);
             int se = 0;
             {
                 const float pm = __int_as_float(sh.pmax_bits);
@@ -477,7 +480,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             // on consecutive nodes of one mode (coalesced loads and stores)
             {
                 const int tile_nodes = min(TC_NT, Nr - i0);
-                constexpr int EB = 4;  // elements in flight per thread
+                constexpr int EB = 8;  // elements in flight per thread
 #pragma unroll 1
                 for (int e0 = tid; e0 < n * TC_NT; e0 += EB * TC_WORKERS) {
                     float2 x0[EB], xm[EB], xp[EB], w[EB];
@@ -597,8 +600,14 @@ bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
     p.nt = TC_NT;
     if (p.kp > 112 || K > 64) return false;
     p.a_stage = (g_stage_bytes + 127) / 128 * 128;
-    p.smem = (size_t)TC_ASTAGES * p.a_stage + (size_t)TC_BSTAGES * p.kp * 2 * TC_NT * 2 + (size_t)K * TC_NT * 4 +
-             (size_t)p.kp * 12 + (size_t)3 * TC_NT * 4 + 128;
+    const size_t fixed = (size_t)TC_BSTAGES * p.kp * 2 * TC_NT * 2 + (size_t)K * TC_NT * 4 + (size_t)p.kp * 12 +
+                         (size_t)3 * TC_NT * 4 + 128;
+    // as many Gaunt stages as fit (3 to 8, at most K: every tile runs gst - 1 multipoles)
+    const size_t budget = 220 * 1024;
+    p.gst = (int)std::min<size_t>(TC_GMAX, budget > fixed ? (budget - fixed) / std::max(p.a_stage, 128) : 0);
+    p.gst = std::min(p.gst, K);
+    if (p.gst < 3) return false;
+    p.smem = (size_t)p.gst * p.a_stage + fixed;
     // at least 120 KiB, so that one CTA (and its TMEM columns) is resident per SM and no
     // tcgen05.alloc has to wait for another CTA's columns
     p.smem = std::max<size_t>(p.smem, 120 * 1024);
@@ -622,7 +631,7 @@ cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, con
 {
 #define CNM_TC_LAUNCH(KP_)                                                                                      \
     if (p.kp == KP_) {                                                                                          \
-        k_tc_apply<KP_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage);   \
+        k_tc_apply<KP_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage, p.gst); \
         return cudaGetLastError();                                                                              \
     }
     CNM_TC_PLANS(CNM_TC_LAUNCH)

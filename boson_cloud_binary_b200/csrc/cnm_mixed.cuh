@@ -83,6 +83,7 @@ struct TcPlan {
     int tiles = 0, grid = 0;
     size_t smem = 0;
     int a_stage = 0;          // bytes of one Gaunt stage (largest multipole blob)
+    int gst = 3;              // Gaunt stages (copies run gst - 1 multipoles ahead)
 };
 bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p);
 cudaError_t tc_prepare(const TcPlan &p);
