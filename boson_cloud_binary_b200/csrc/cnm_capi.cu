@@ -456,8 +456,7 @@ struct Solver {
         apply_smem = (size_t)n_modes * (APPLY_TILE + 2 + APPLY_TILE + 1) * sizeof(double2) +
                      (size_t)std::max(K, 4) * APPLY_TILE * sizeof(double);
         diag_smem = apply_smem + (size_t)(2 * n_modes + 3) * (APPLY_THREADS / 32) * sizeof(double);
-        CK(cudaFuncSetAttribute(k_apply, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)apply_smem));
-        CK(set_operator_smem((int)apply_smem, (int)diag_smem));
+        CK(set_operator_smem((int)diag_smem));
         plan_operator(nsm);
         a5_groups = apply5_groups(l_max);
         if (a5_groups > 0) {
@@ -466,7 +465,6 @@ struct Solver {
             CK(set_apply5_smem());
             CK(set_diag5_smem());
         }
-        CK(cudaFuncSetAttribute(k_diagnostics, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)diag_smem));
         CK(cudaFuncSetAttribute(k_precond_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
         CK(cudaFuncSetAttribute(k_wood_setup_band, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)(2 * WOOD_BAND_MAX * sizeof(double2))));
@@ -1018,15 +1016,6 @@ struct Solver {
         const dim3 blocks3 = apply3_grid();
         kt_begin(TK_APPLY);
         ::cnm::launch_apply3(l_max, apply3_gsm, blocks3, apply3_smem, stream, grid(), table(), btable2(), aplan(), a);
-        launch_check();
-        kt_end(TK_APPLY);
-    }
-
-    void launch_apply_v2(const ApplyArgs &a)
-    {
-        const dim3 blocks = apply_grid();
-        kt_begin(TK_APPLY);
-        ::cnm::launch_apply(l_max, blocks, apply_smem, stream, grid(), table(), btable(), a);
         launch_check();
         kt_end(TK_APPLY);
     }

@@ -46,103 +46,6 @@ __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1
 
 // ------------------------------------------------------------------ operator application
 
-// One CTA owns APPLY_TILE consecutive radial nodes of every mode.  The tile of x
-// (with a one-node halo for the stencil), its phase-rotated copy z = D^dag x and
-// the tile of the hh table sit in shared memory; warp w computes rows
-// j = w, w + nwarps, ... with lane = node, so the coupling term list is read
-// warp-uniformly (broadcast) and every shared-memory access is conflict-free.
-__global__ void __launch_bounds__(APPLY_THREADS) k_apply(Grid g, CouplingTable ct, ApplyArgs a)
-{
-    extern __shared__ double2 smem2[];
-    const int n = g.n_modes, Nr = g.Nr;
-    const int K = 2 * ct.l_max + 1;
-    const int i0 = blockIdx.x * APPLY_TILE;
-    double2 *xs = smem2;                                   // n * (TILE + 2)
-    double2 *zs = xs + n * (APPLY_TILE + 2);               // n * TILE
-    double2 *ph = zs + n * APPLY_TILE;                     // n: exp(i m_k theta)
-    double *hs = reinterpret_cast<double *>(ph + n);       // K * TILE
-    const bool vp = a.vpart != V_NONE;
-
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        double s, c;
-        sincos((double)ct.mode_m[k] * a.theta, &s, &c);
-        ph[k] = cmake(c, s);
-    }
-    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
-        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
-        const int i = i0 - 1 + c;
-        xs[e] = (i >= 0 && i < Nr) ? a.x[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
-    }
-    if (vp)
-        for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
-            const int l = e / APPLY_TILE, c = e % APPLY_TILE;
-            const int i = i0 + c;
-            hs[e] = i < Nr ? a.hh[(int64_t)l * Nr + i] : 0.0;
-        }
-    __syncthreads();
-    if (vp)
-        for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
-            const int k = e / APPLY_TILE, c = e % APPLY_TILE;
-            zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
-        }
-    __syncthreads();
-
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-    const int c = lane;  // APPLY_TILE == 32
-    const int i = i0 + c;
-    if (i >= Nr) return;
-    const bool interior = i >= 1 && i <= Nr - 2;
-    const double alpha_d = 1.0 / (g.dr * g.dr);
-    const double ri = g.r[i];
-    for (int j = warp; j < n; j += nw) {
-        const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
-        double2 acc = cmake(0.0, 0.0);
-        if (a.use_h0 && interior) {
-            const int l = ct.mode_l[j];
-            const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
-            const double off = -alpha_d / (2 * g.mu);
-            const double2 xl = xs[j * (APPLY_TILE + 2) + c], xr = xs[j * (APPLY_TILE + 2) + c + 2];
-            acc = cadd(cscale(xv, diag), cscale(cadd(xl, xr), off));
-        }
-        if (vp && interior) {
-            double2 av = cmake(0.0, 0.0), am = cmake(0.0, 0.0);
-            const int pb = ct.pair_row_ptr[j], pe = ct.pair_row_ptr[j + 1];
-            for (int p = pb; p < pe; ++p) {
-                const int k = __ldg(ct.pair_col + p);
-                const int tb = __ldg(ct.pair_term_ptr + p), te = __ldg(ct.pair_term_ptr + p + 1);
-                double s = 0.0;
-                for (int t = tb; t < te; ++t) s += __ldg(ct.term_g + t) * hs[__ldg(ct.term_l + t) * APPLY_TILE + c];
-                const double2 zk = zs[k * APPLY_TILE + c];
-                av.x += s * zk.x;
-                av.y += s * zk.y;
-                if (a.vpart == V_DVDT) {
-                    const double sm = s * (double)ct.mode_m[k];
-                    am.x += sm * zk.x;
-                    am.y += sm * zk.y;
-                }
-            }
-            double2 vj;
-            if (a.vpart == V_DVDT) {
-                // (dV/dt x)_j = i s Omega e^{-i m_j theta} sum_k Ahat_jk (m_k - m_j) z_k
-                const double mj = (double)ct.mode_m[j];
-                const double2 d = cmake(am.x - mj * av.x, am.y - mj * av.y);
-                vj = cmuli(cscale(d, a.domega));
-            } else {
-                vj = av;
-            }
-            acc = cadd(acc, cmul(cconj(ph[j]), vj));
-        }
-        if (a.use_cap && g.capw) acc = cadd(acc, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));  // (-i w) x
-        double2 y = cadd(cmul(a.alpha, xv), cmul(a.beta, acc));
-        for (int s = 0; s < a.n_sinks; ++s)
-            if (i >= a.sink_lo[s] && i < a.sink_hi[s]) {
-                const double2 cf = cscale(a.sink_dots[s], a.sink_coef[s]);
-                y = cadd(y, cmul(cf, a.sink_v[s][(int64_t)j * Nr + i]));
-            }
-        a.y[(int64_t)j * Nr + i] = y;
-    }
-}
-
 // ------------------------------------------------------------------ register-blocked coupling
 
 // Multipole cut of one tile: the largest l* whose weight exceeds 1e-18 of the
@@ -257,54 +160,6 @@ struct TileCtx {
     double ri;
 };
 
-// Output of one chunk for k_apply2: stencil, potential, CAP, sinks, store, fused dots.
-template <int SMAX, int RB, int VP>
-__device__ __forceinline__ void apply_chunk(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
-                                            const ApplyArgs &a, const TileCtx &t, int ci, double (&dacc)[4])
-{
-    double2 acc[RB], accm[RB];
-    if (VP != V_NONE) coupling_chunk<SMAX, RB, VP == V_DVDT>(bt, ct.l_max, ci, t.lcut, t.zs, t.hs, ct.mode_m, t.lane, acc, accm);
-    const int Nr = g.Nr, c = t.lane, i = t.i;
-    if (i >= Nr) return;
-    const double alpha_d = 1.0 / (g.dr * g.dr);
-#pragma unroll
-    for (int rr = 0; rr < RB; ++rr) {
-        const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
-        const double2 xv = t.xs[j * (APPLY_TILE + 2) + c + 1];
-        double2 h = cmake(0.0, 0.0);
-        if (a.use_h0 && t.interior) {
-            const int l = ct.mode_l[j];
-            const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (t.ri * t.ri)) / (2 * g.mu);
-            const double off = -alpha_d / (2 * g.mu);
-            h = cadd(cscale(xv, diag), cscale(cadd(t.xs[j * (APPLY_TILE + 2) + c], t.xs[j * (APPLY_TILE + 2) + c + 2]), off));
-        }
-        if (VP != V_NONE && t.interior) {
-            double2 vj;
-            if (VP == V_DVDT) {
-                const double mj = (double)ct.mode_m[j];
-                vj = cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), a.domega));
-            } else {
-                vj = acc[rr];
-            }
-            h = cadd(h, cmul(cconj(t.ph[j]), vj));
-        }
-        if (a.use_cap && g.capw) h = cadd(h, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
-        double2 y = cadd(cmul(a.alpha, xv), cmul(a.beta, h));
-        for (int s2 = 0; s2 < a.n_sinks; ++s2)
-            if (i >= a.sink_lo[s2] && i < a.sink_hi[s2])
-                y = cadd(y, cmul(cscale(a.sink_dots[s2], a.sink_coef[s2]), a.sink_v[s2][(int64_t)j * Nr + i]));
-        a.y[(int64_t)j * Nr + i] = y;
-        for (int q = 0; q < a.n_dots; ++q) {
-            double2 d;
-            if (a.dot_kind[q] == 1) d = cconjmul(a.dot_ext[q][(int64_t)j * Nr + i], y);
-            else if (a.dot_kind[q] == 2) d = cconjmul(y, a.dot_ext[q][(int64_t)j * Nr + i]);
-            else d = cmake(cabs2(y), 0.0);
-            dacc[2 * q] += d.x;
-            dacc[2 * q + 1] += d.y;
-        }
-    }
-}
-
 // Fused diagnostics of one chunk (see k_diagnostics2).
 template <int SMAX, int RB>
 __device__ __forceinline__ void diag_chunk(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
@@ -361,91 +216,6 @@ __device__ __forceinline__ void diag_chunk(const Grid &g, const CouplingTable &c
         if (t.lane == 0) {
             red[j * nw + warp] = nrm;
             red[(n + j) * nw + warp] = en;
-        }
-    }
-}
-
-// Operator application, register-blocked.  grid.x = node tiles, grid.y splits the row
-// chunks of a tile between CTAs (chunk ci goes to CTA ci % gridDim.y); inside a CTA the
-// warps take its chunks round-robin.
-// SMAX: widest (l, l1) block (l_max + 1 rounded up); VP: the potential part (VPart).
-template <int SMAX, int VP>
-__global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply2(Grid g, CouplingTable ct, BlockTable bt, ApplyArgs a)
-{
-    extern __shared__ double2 smem2[];
-    __shared__ int s_lcut;
-    const int n = g.n_modes, Nr = g.Nr;
-    const int K = 2 * ct.l_max + 1;
-    const int i0 = blockIdx.x * APPLY_TILE;
-    double2 *xs = smem2;                              // n * (TILE + 2)
-    double2 *zs = xs + n * (APPLY_TILE + 2);          // n * TILE
-    double2 *ph = zs + n * APPLY_TILE;                // n
-    double *hs = reinterpret_cast<double *>(ph + n);  // max(K, 4) * TILE
-    constexpr bool vp = VP != V_NONE;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        double sn, cs;
-        sincos((double)ct.mode_m[k] * a.theta, &sn, &cs);
-        ph[k] = cmake(cs, sn);
-    }
-    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
-        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
-        const int i = i0 - 1 + c;
-        xs[e] = (i >= 0 && i < Nr) ? a.x[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
-    }
-    if (vp)
-        for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
-            const int l = e / APPLY_TILE, c = e % APPLY_TILE;
-            const int i = i0 + c;
-            hs[e] = i < Nr ? a.hh[(int64_t)l * Nr + i] : 0.0;
-        }
-    __syncthreads();
-    if (vp) {
-        for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
-            const int k = e / APPLY_TILE, c = e % APPLY_TILE;
-            zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
-        }
-        if (warp == 0) {
-            const int lc = tile_lcut(hs, K, lane);
-            if (lane == 0) s_lcut = lc;
-        }
-    }
-    __syncthreads();
-    TileCtx t;
-    t.xs = xs;
-    t.zs = zs;
-    t.ph = ph;
-    t.hs = hs;
-    t.lane = lane;
-    t.i = i0 + lane;
-    t.lcut = vp ? s_lcut : -1;
-    t.interior = t.i >= 1 && t.i <= Nr - 2;
-    t.ri = t.i < Nr ? g.r[t.i] : 1.0;
-    double dacc[4] = {0.0, 0.0, 0.0, 0.0};
-    for (int ci = blockIdx.y + gridDim.y * warp; ci < bt.n_chunks; ci += gridDim.y * nw) {
-        switch (bt.chunk_nrows[ci]) {
-        case 1: apply_chunk<SMAX, 1, VP>(g, ct, bt, a, t, ci, dacc); break;
-        case 2: apply_chunk<SMAX, 2, VP>(g, ct, bt, a, t, ci, dacc); break;
-        case 3: apply_chunk<SMAX, 3, VP>(g, ct, bt, a, t, ci, dacc); break;
-        default: apply_chunk<SMAX, 4, VP>(g, ct, bt, a, t, ci, dacc); break;
-        }
-    }
-    if (a.n_dots > 0) {
-        // deterministic CTA reduction of the fused inner products into per-CTA partials
-        __syncthreads();
-        double *red = hs;  // the hh tile is no longer needed
-#pragma unroll
-        for (int q = 0; q < 4; ++q) dacc[q] = warp_sum(dacc[q]);
-        if (lane == 0)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) red[q * 32 + warp] = dacc[q];
-        __syncthreads();
-        const int nblocks = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
-        if (threadIdx.x < 2 * a.n_dots) {
-            double sm = 0.0;
-            for (int w = 0; w < nw; ++w) sm += red[threadIdx.x * 32 + w];
-            a.dot_partials[(int64_t)threadIdx.x * nblocks + blk] = sm;
         }
     }
 }
@@ -805,13 +575,10 @@ static int smax_for(int l_max)
 
 #define CNM_FOR_SMAX(MACRO) MACRO(5) MACRO(9) MACRO(13) MACRO(17) MACRO(25)
 
-cudaError_t set_operator_smem(int apply_bytes, int diag_bytes)
+cudaError_t set_operator_smem(int diag_bytes)
 {
     cudaError_t e = cudaSuccess;
-#define CNM_ATTR(S)                                                                                          \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply2<S, V_NONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, apply_bytes); \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply2<S, V_POT>, cudaFuncAttributeMaxDynamicSharedMemorySize, apply_bytes);  \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_apply2<S, V_DVDT>, cudaFuncAttributeMaxDynamicSharedMemorySize, apply_bytes); \
+#define CNM_ATTR(S) \
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diagnostics2<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_bytes);
     CNM_FOR_SMAX(CNM_ATTR)
 #undef CNM_ATTR
@@ -870,22 +637,6 @@ void launch_apply3(int l_max, bool gsm, dim3 blocks, size_t smem, cudaStream_t s
 #undef CNM_LAUNCH3
 #undef CNM_LAUNCH3G
 }
-
-void launch_apply(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
-                  const BlockTable &bt, const ApplyArgs &a)
-{
-    const int smax = smax_for(l_max);
-#define CNM_LAUNCH(S)                                                                                        \
-    if (smax == S) {                                                                                         \
-        if (a.vpart == V_POT) k_apply2<S, V_POT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);         \
-        else if (a.vpart == V_DVDT) k_apply2<S, V_DVDT><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);  \
-        else k_apply2<S, V_NONE><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, a);                         \
-        return;                                                                                              \
-    }
-    CNM_FOR_SMAX(CNM_LAUNCH)
-#undef CNM_LAUNCH
-}
-
 void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
                         const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
                         const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
@@ -1025,71 +776,17 @@ __device__ __forceinline__ double2 mob_apply(const Mob &M, double2 p)
     return cdiv(cadd(cmul(M.m00, p), M.m01), cadd(cmul(M.m10, p), M.m11));
 }
 
-// Inverse Thomas pivots d_i = 1 / p_i of every radial block.  Grid (chunks, modes);
-// each CTA recomputes the pivot recurrence over its chunk preceded by a warm-up
-// window: the map p -> a - c/p contracts towards the local pivot, so the window
-// start value is forgotten to rounding.  Inside the CTA the recurrence is a
-// parallel scan of 2x2 Moebius matrices.
-__global__ void __launch_bounds__(SCAN_THREADS) k_precond_factor(Grid g, CouplingTable ct, const double *hh,
-                                                                  double half_dt, double2 off, int chunk, int window,
-                                                                  double2 *dinv, int *status)
-{
-    __shared__ Mob tmat[SCAN_THREADS];
-    const int Nr = g.Nr, j = blockIdx.y;
-    const int c0 = blockIdx.x * chunk, c1 = min(Nr, c0 + chunk);
-    const int lo = max(0, c0 - window), hi = c1;
-    const int len = hi - lo;
-    const int per = (len + blockDim.x - 1) / blockDim.x;
-    const int s0 = lo + threadIdx.x * per, s1 = min(hi, s0 + per);
-    const double2 c = cmul(off, off);
-    Mob acc;
-    acc.m00 = cmake(1, 0);
-    acc.m01 = cmake(0, 0);
-    acc.m10 = cmake(0, 0);
-    acc.m11 = cmake(1, 0);
-    for (int i = s0; i < s1; ++i) {
-        acc = mob_mul(pivot_map(a_diag(g, ct, hh, half_dt, j, i), i, Nr, c), acc);
-        mob_normalize(acc);
-    }
-    tmat[threadIdx.x] = acc;
-    __syncthreads();
-    // Hillis-Steele inclusive scan over threads (t composes after t-1).
-    for (int o = 1; o < (int)blockDim.x; o <<= 1) {
-        Mob mine = tmat[threadIdx.x];
-        Mob prev;
-        const bool has = threadIdx.x >= (unsigned)o;
-        if (has) prev = tmat[threadIdx.x - o];
-        __syncthreads();
-        if (has) {
-            mine = mob_mul(mine, prev);
-            mob_normalize(mine);
-            tmat[threadIdx.x] = mine;
-        }
-        __syncthreads();
-    }
-    // start value before node lo: any finite guess; exact when lo == 0 (node 0's map is constant)
-    double2 p = a_diag(g, ct, hh, half_dt, j, lo);
-    if (threadIdx.x > 0) p = mob_apply(tmat[threadIdx.x - 1], p);
-    for (int i = s0; i < s1; ++i) {
-        p = mob_apply(pivot_map(a_diag(g, ct, hh, half_dt, j, i), i, Nr, c), p);
-        if (i >= c0) {
-            const double m = cabs2(p);
-            if (!(m > 0.0) || !isfinite(m)) {
-                atomicOr(status, 1);
-                dinv[(int64_t)j * Nr + i] = cmake(0.0, 0.0);
-            } else {
-                dinv[(int64_t)j * Nr + i] = crcp(p);
-            }
-        }
-    }
-}
-
 // The pivot kernel above for a caller-supplied diagonal: a_i = diag[j * Nr + i] instead
 // of the diagonal rebuilt from the Hamiltonian.  Same chunking, window and scan.
+// With rho_max finite the pivots are also checked against the contraction the warm-up
+// windows were sized for: |off d_i| <= rho_max on every interior node, else bit 2 of
+// status (the windows would not forget their start values, and the solve would be
+// inexact).
 __global__ void __launch_bounds__(SCAN_THREADS) k_precond_factor_diag(const double2 *diag, int Nr, double2 off,
-                                                                       int chunk, int window, double2 *dinv,
-                                                                       int *status)
+                                                                       int chunk, int window, double rho_max,
+                                                                       double2 *dinv, int *status)
 {
+    const double off_abs = sqrt(cabs2(off));
     __shared__ Mob tmat[SCAN_THREADS];
     const int j = blockIdx.y;
     const int64_t base = (int64_t)j * Nr;
@@ -1134,6 +831,7 @@ __global__ void __launch_bounds__(SCAN_THREADS) k_precond_factor_diag(const doub
                 dinv[base + i] = cmake(0.0, 0.0);
             } else {
                 dinv[base + i] = crcp(p);
+                if (i >= 1 && i <= Nr - 2 && off_abs / sqrt(m) > rho_max) atomicOr(status, 2);
             }
         }
     }
@@ -1534,6 +1232,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     // complete on an mbarrier; the threads load the other inputs of a BiCGSTAB combination
     __shared__ __align__(8) unsigned long long stage_bar;
     const unsigned bar = (unsigned)__cvta_generic_to_shared(&stage_bar);
+    bool staged = true;
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(bar) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -1549,12 +1248,14 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         }
         if (!mbar_wait_parity(bar, 0u)) {
             // the copies did not complete in time: flag the solve as failed (the attempt
-            // is then not accepted) and wait once more for them before going on
+            // is then not accepted) and wait once more for them before going on; if that
+            // wait gives up too, this CTA still takes part in every cluster barrier but
+            // stores nothing (a copy's completion is then left unobserved)
             if (tid == 0 && in.fault) atomicOr(in.fault, 2);
-            mbar_wait_parity(bar, 0u);
+            staged = mbar_wait_parity(bar, 0u);
         }
     }
-    if (in.mode != PI_PLAIN) {
+    if (in.mode != PI_PLAIN && staged) {
         const double2 beta = in.kr->beta, omega = in.kr->omega, alpha = in.kr->alpha;
         // PI_P without p_old (first iteration: p_old = v = 0) is p = r
         const bool first = in.mode == PI_P && in.p_old == nullptr;
@@ -1717,7 +1418,8 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
         }
     }
     __syncthreads();
-    for (int e = tid; e < len; e += T) xv[base + e] = Y[e];
+    if (staged)
+        for (int e = tid; e < len; e += T) xv[base + e] = Y[e];
     if (wd.mode != WD_NONE) {
         // sink projections v_a^dag x of this CTA's nodes; the last CTA finishes the
         // Woodbury scalars
@@ -2164,20 +1866,6 @@ __global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, co
 
 // ---- BiCGSTAB (src/CrankNicolsonModes_matrices.cpp:47-91), device-resident scalars
 
-__global__ void k_bicg_p(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *p)
-{
-    const double2 beta = kr->beta, w = kr->omega;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
-        p[e] = cadd(r[e], cmul(beta, csub(p[e], cmul(w, v[e]))));
-}
-
-__global__ void k_bicg_s(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *s)
-{
-    const double2 al = kr->alpha;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
-        s[e] = csub(r[e], cmul(al, v[e]));
-}
-
 // x += alpha y + omega z; r = s - omega t; per-CTA partials of |r|^2 and r0 . r.
 __global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, Krylov *kr, double2 *x, const double2 *y,
                                                               const double2 *z, double2 *r, const double2 *s,
@@ -2206,20 +1894,6 @@ __global__ void __launch_bounds__(VEC_THREADS) k_bicg_update(int64_t n, Krylov *
     if (ticket) finish_stage(partials, gridDim.x, 3, red, kr, KS_UPDATE, ticket, scratch);
 }
 
-// Woodbury correction y = yP - sum_a W_a c_a on the vector (src/CrankNicolsonModes_matrices.cpp:146-153).
-__global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2 *yP, const double2 *W0,
-                           const double2 *W1, double2 *y)
-{
-    const double2 c0 = kr->wc[which][0], c1 = kr->wc[which][1];
-    const int k = kr->n_sinks;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        double2 corr = cmul(W0[e], c0);
-        if (k > 1) corr = cadd(corr, cmul(W1[e], c1));
-        y[e] = csub(yP[e], corr);
-    }
-}
-
-
 // Woodbury correction in place on the band of nodes [lo, hi) of every mode where the
 // W_a = P^{-1} v_a can be non-negligible: y -= sum_a W_a c_a (c from kr->wc[which]).
 __global__ void k_woodbury_band(int Nr, int n_modes, int lo, int hi, const Krylov *kr, int which, const double2 *W0,
@@ -2237,11 +1911,6 @@ __global__ void k_woodbury_band(int Nr, int n_modes, int lo, int hi, const Krylo
         if (k > 1) corr = cadd(corr, cmul(W1[q], c1));
         y[q] = csub(y[q], corr);
     }
-}
-
-__global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red)
-{
-    if (threadIdx.x == 0) bicg_stage(kr, stage, red);
 }
 
 // Woodbury set-up on the device (src/CrankNicolsonModes_matrices.cpp:133-145):
@@ -2275,23 +1944,6 @@ __device__ void wood_setup_dev(Krylov *kr, const double2 *vw, double c0, double 
 __global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1)
 {
     if (threadIdx.x == 0) wood_setup_dev(kr, vw, c0, c1);
-}
-
-// b = rhs / |rhs|, x = psi / |rhs| with |rhs|^2 = red[0]; a zero right-hand side is
-// flagged (kr->zero_rhs) and leaves b = x = 0.
-__global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
-                                double2 *b, double2 *x)
-{
-    const double nrm = sqrt(red[0]);
-    const double s = nrm > 0.0 ? 1.0 / nrm : 0.0;
-    if (blockIdx.x == 0 && threadIdx.x == 0) {
-        kr->rhs_norm = nrm;
-        kr->zero_rhs = nrm == 0.0;
-    }
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
-        b[e] = cscale(rhs[e], s);
-        x[e] = cscale(psi[e], s);
-    }
 }
 
 // Start of the solve in one pass: with s = 1/|rhs| (|rhs|^2 = red[0]),
@@ -2328,14 +1980,6 @@ __global__ void __launch_bounds__(VEC_THREADS) k_krylov_start(int64_t n, Krylov 
         __threadfence();
     }
     if (ticket) finish_stage(partials, gridDim.x, 4, red, kr, KS_INIT, ticket, scratch);
-}
-
-// candidate = x |rhs|.
-__global__ void k_scale_candidate(int64_t n, const Krylov *kr, const double2 *x, double2 *cand)
-{
-    const double s = kr->rhs_norm;
-    for (int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x)
-        cand[e] = cscale(x[e], s);
 }
 
 // Woodbury projections: with proj_a = v_a^dag yP (dots), c = G^{-1} proj and the sink
@@ -2481,136 +2125,6 @@ __global__ void __launch_bounds__(256) k_swave_projector(const double *r, int Nr
 
 // ------------------------------------------------------------------ diagnostics
 
-// One pass over nodes 0..idx_ex for every mode (src/CrankNicolsonModes_extraction.cpp:8-129):
-// with Hx, Vx and dV/dt x rebuilt on chip (same tiling as k_apply) it accumulates per CTA
-//   norms_j  = sum_{i < idx_ex} |psi|^2,  energies_j = sum_{i < idx_ex} Re conj(psi) (H psi),
-//   e_edge   = sum_j Re conj(psi) (H psi) at i = idx_ex,
-//   p_bin    = sum_{i <= idx_ex} Re conj(psi) (dVdt psi),
-//   dV       = sum_{i <= idx_ex} Re conj(dpsi/dt) (V psi),  dpsi/dt = -i H psi - Gamma psi / 2,
-// and stores dpsi/dt at idx_ex for the energy flux.  Partials layout: [slot][block],
-// slots 0..n-1 norms, n..2n-1 energies, 2n e_edge, 2n+1 p_bin, 2n+2 dV.
-__global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics(Grid g, CouplingTable ct, const double *hh,
-                                                                double theta, double domega, const double2 *psi,
-                                                                int idx_ex, int n_sinks, const double2 *sv0,
-                                                                const double2 *sv1, const double2 *sink_dots,
-                                                                double sink_coef0, double sink_coef1, int slo0,
-                                                                int shi0, int slo1, int shi1, double *partials,
-                                                                double2 *dpsi_edge, double2 *psi_edge)
-{
-    extern __shared__ double2 smem2[];
-    const int n = g.n_modes, Nr = g.Nr;
-    const int K = 2 * ct.l_max + 1;
-    const int i0 = blockIdx.x * APPLY_TILE;
-    double2 *xs = smem2;
-    double2 *zs = xs + n * (APPLY_TILE + 2);
-    double2 *ph = zs + n * APPLY_TILE;
-    double *hs = reinterpret_cast<double *>(ph + n);
-    double *red = hs + K * APPLY_TILE;  // (2n + 3) * nwarps
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        double s, c;
-        sincos((double)ct.mode_m[k] * theta, &s, &c);
-        ph[k] = cmake(c, s);
-    }
-    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
-        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
-        const int i = i0 - 1 + c;
-        xs[e] = (i >= 0 && i < Nr) ? psi[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
-    }
-    for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
-        const int l = e / APPLY_TILE, c = e % APPLY_TILE;
-        const int i = i0 + c;
-        hs[e] = i < Nr ? hh[(int64_t)l * Nr + i] : 0.0;
-    }
-    for (int e = threadIdx.x; e < (2 * n + 3) * nw; e += blockDim.x) red[e] = 0.0;
-    __syncthreads();
-    for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
-        const int k = e / APPLY_TILE, c = e % APPLY_TILE;
-        zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
-    }
-    __syncthreads();
-
-    const int c = lane;
-    const int i = i0 + c;
-    const bool active = i < Nr && i <= idx_ex;
-    const bool interior = i >= 1 && i <= Nr - 2;
-    const double alpha_d = 1.0 / (g.dr * g.dr);
-    double e_edge = 0.0, pb = 0.0, dv = 0.0;
-    for (int j = warp; j < n; j += nw) {
-        double nrm = 0.0, en = 0.0;
-        if (active) {
-            const double2 xv = xs[j * (APPLY_TILE + 2) + c + 1];
-            double2 hx = cmake(0.0, 0.0), vx = cmake(0.0, 0.0), dx = cmake(0.0, 0.0);
-            if (interior) {
-                const int l = ct.mode_l[j];
-                const double ri = g.r[i];
-                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (ri * ri)) / (2 * g.mu);
-                const double off = -alpha_d / (2 * g.mu);
-                hx = cadd(cscale(xv, diag),
-                          cscale(cadd(xs[j * (APPLY_TILE + 2) + c], xs[j * (APPLY_TILE + 2) + c + 2]), off));
-                double2 av = cmake(0.0, 0.0), am = cmake(0.0, 0.0);
-                for (int p = ct.pair_row_ptr[j]; p < ct.pair_row_ptr[j + 1]; ++p) {
-                    const int k = __ldg(ct.pair_col + p);
-                    double s = 0.0;
-                    for (int t = __ldg(ct.pair_term_ptr + p); t < __ldg(ct.pair_term_ptr + p + 1); ++t)
-                        s += __ldg(ct.term_g + t) * hs[__ldg(ct.term_l + t) * APPLY_TILE + c];
-                    const double2 zk = zs[k * APPLY_TILE + c];
-                    av.x += s * zk.x;
-                    av.y += s * zk.y;
-                    const double sm = s * (double)ct.mode_m[k];
-                    am.x += sm * zk.x;
-                    am.y += sm * zk.y;
-                }
-                const double mj = (double)ct.mode_m[j];
-                vx = cmul(cconj(ph[j]), av);
-                dx = cmul(cconj(ph[j]), cmuli(cscale(cmake(am.x - mj * av.x, am.y - mj * av.y), domega)));
-                hx = cadd(hx, vx);
-            }
-            if (g.capw) hx = cadd(hx, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
-            // dpsi/dt = -i H psi - Gamma psi / 2
-            double2 dp = cmake(hx.y, -hx.x);
-            if (n_sinks > 0 && i >= slo0 && i < shi0)
-                dp = cadd(dp, cmul(cscale(sink_dots[0], sink_coef0), sv0[(int64_t)j * Nr + i]));
-            if (n_sinks > 1 && i >= slo1 && i < shi1)
-                dp = cadd(dp, cmul(cscale(sink_dots[1], sink_coef1), sv1[(int64_t)j * Nr + i]));
-            const double ce = cconjmul(xv, hx).x;
-            if (i < idx_ex) {
-                nrm = cabs2(xv);
-                en = ce;
-            } else {
-                e_edge += ce;
-                dpsi_edge[j] = dp;
-                psi_edge[3 * j] = xs[j * (APPLY_TILE + 2) + c];
-                psi_edge[3 * j + 1] = xv;
-                psi_edge[3 * j + 2] = xs[j * (APPLY_TILE + 2) + c + 2];
-            }
-            pb += cconjmul(xv, dx).x;
-            dv += cconjmul(dp, vx).x;
-        }
-        nrm = warp_sum(nrm);
-        en = warp_sum(en);
-        if (lane == 0) {
-            red[j * nw + warp] = nrm;
-            red[(n + j) * nw + warp] = en;
-        }
-    }
-    e_edge = warp_sum(e_edge);
-    pb = warp_sum(pb);
-    dv = warp_sum(dv);
-    if (lane == 0) {
-        red[(2 * n) * nw + warp] = e_edge;
-        red[(2 * n + 1) * nw + warp] = pb;
-        red[(2 * n + 2) * nw + warp] = dv;
-    }
-    __syncthreads();
-    for (int q = threadIdx.x; q < 2 * n + 3; q += blockDim.x) {
-        double s = 0.0;
-        for (int w = 0; w < nw; ++w) s += red[q * nw + w];
-        partials[(int64_t)q * gridDim.x + blockIdx.x] = s;
-    }
-}
-
 // out[q] = sum_b partials[q][b]: one CTA per slot, coalesced loads, fixed-order tree.
 __global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out, const Krylov *gate)
 {
@@ -2623,21 +2137,6 @@ __global__ void k_sum_slots(const double *partials, int nblocks, int nslots, dou
     for (int b = threadIdx.x; b < nblocks; b += blockDim.x) acc[0] += partials[(int64_t)q * nblocks + b];
     block_sum<1>(acc, scratch);
     if (threadIdx.x == 0) out[q] = acc[0];
-}
-
-// Sum the per-CTA partials of nslots values into red[0..nslots) and run one scalar stage
-// of the recurrence on them, in one launch.
-__global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage)
-{
-    __shared__ double scratch[6 * 32];
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-        for (int q = 0; q < nslots; ++q) acc[q] += partials[(int64_t)q * nblocks + b];
-    block_sum<6>(acc, scratch);
-    if (threadIdx.x == 0) {
-        for (int q = 0; q < nslots; ++q) red[q] = acc[q];
-        bicg_stage(kr, stage, red);
-    }
 }
 
 // ------------------------------------------------------------------ initial states

@@ -66,18 +66,15 @@ enum Ticket : int { TK_APPLY_T = 0, TK_UPDATE_T = 1, TK_START_T = 2, TK_WOOD_T =
 
 __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
                            double scale, double a1, double a2);
-__global__ void k_apply(Grid g, CouplingTable ct, ApplyArgs a);
 // Register-blocked operator kernels (templated on the widest Gaunt block), launched
 // through these host functions.
-cudaError_t set_operator_smem(int apply_bytes, int diag_bytes);
+cudaError_t set_operator_smem(int diag_bytes);
 // Two-nodes-per-thread operator kernel on 64-node tiles with a two-row blocked table.
 constexpr int APPLY3_TILE = 64;
 cudaError_t set_apply3_smem(int bytes);
 const void *apply3_kernel(int l_max, int vpart, bool gsm);
 void launch_apply3(int l_max, bool gsm, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
                    const CouplingTable &ct, const BlockTable &bt, const ApplyPlan &pl, const ApplyArgs &a);
-void launch_apply(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
-                  const BlockTable &bt, const ApplyArgs &a);
 void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
                         const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
                         const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
@@ -86,9 +83,7 @@ void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, co
 __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
                             const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots, const Krylov *gate,
                             int gate_mode);
-__global__ void k_precond_factor(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off,
-                                 int chunk, int window, double2 *dinv, int *status);
-__global__ void k_precond_factor_diag(const double2 *diag, int Nr, double2 off, int chunk, int window,
+__global__ void k_precond_factor_diag(const double2 *diag, int Nr, double2 off, int chunk, int window, double rho_max,
                                       double2 *dinv, int *status);
 __global__ void k_precond_solve(int Nr, int chunk, int window, double2 off, const double2 *dinv,
                                 const double2 *b, double2 *x);
@@ -98,21 +93,13 @@ __global__ void k_sum_partials(const double *partials, int nblocks, int nslots, 
 __global__ void k_axpby(int64_t n, double2 a, const double2 *x, double2 b, const double2 *w, double2 *y);
 __global__ void k_scale_mask(int64_t n, int Nr, double s, const double *mask, const double2 *x, double2 *y,
                              const Krylov *kr);
-__global__ void k_bicg_p(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *p);
-__global__ void k_bicg_s(int64_t n, const Krylov *kr, const double2 *r, const double2 *v, double2 *s);
 __global__ void k_bicg_update(int64_t n, Krylov *kr, double2 *x, const double2 *y, const double2 *z, double2 *r,
                               const double2 *s, const double2 *t, const double2 *r0, double *partials, double *red,
                               unsigned *ticket);
-__global__ void k_woodbury(int64_t n, const Krylov *kr, int which, const double2 *yP, const double2 *W0,
-                           const double2 *W1, double2 *y);
-__global__ void k_bicg_scalar(Krylov *kr, int stage, const double *red);
 __global__ void k_wood_scalar(Krylov *kr, int which, const double2 *proj);
 __global__ void k_wood_setup(Krylov *kr, const double2 *vw, double c0, double c1);
-__global__ void k_normalize_rhs(int64_t n, Krylov *kr, const double *red, const double2 *rhs, const double2 *psi,
-                                double2 *b, double2 *x);
 __global__ void k_krylov_start(int64_t n, Krylov *kr, const double *red_in, const double2 *rhs, const double2 *psi,
                                double2 *x, double2 *r, double2 *r0, double *partials, double *red, unsigned *ticket);
-__global__ void k_scale_candidate(int64_t n, const Krylov *kr, const double2 *x, double2 *cand);
 __global__ void k_precond_solve2(int Nr, int chunk, int window, double2 off, const double2 *dinv, const double2 *b,
                                  double2 *x, PrecondInput in);
 __global__ void k_precond_factor2(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int chunk,
@@ -164,12 +151,7 @@ __global__ void k_abs_moments(const double *r, int Nr, int nq, const double *gl_
                               AbsorberPair ap);
 __global__ void k_swave_projector(const double *r, int Nr, int n_modes, double dr, const double *ang00,
                                   const int *mode_l, const int *mode_m, double theta, AbsorberPair ap);
-__global__ void k_diagnostics(Grid g, CouplingTable ct, const double *hh, double theta, double domega,
-                              const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
-                              const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0,
-                              int slo1, int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge);
 __global__ void k_sum_slots(const double *partials, int nblocks, int nslots, double *out, const Krylov *gate);
-__global__ void k_reduce_stage(const double *partials, int nblocks, int nslots, double *red, Krylov *kr, int stage);
 
 __global__ void k_fp64_peak(double *out, int iters, double b, double c);
 

@@ -56,15 +56,22 @@ cudaError_t scratch_for_current_device(double2 **out)
 }
 
 // Warm-up window of the chunked scans for an off-diagonal of modulus kappa (the same
-// rule as the handle's preconditioner).
-int scan_window(double kappa)
+// rule as the handle's windowed preconditioner): the forward and backward sweeps
+// contract by rho = kappa / |p+| per node, p+ the attracting pivot of a diagonal
+// 1 + 2 i kappa 0.99, and the window is long enough to forget the start value to
+// exp(-40) at that rate.  `rho` returns the rate the window assumes; the factorisation
+// flags any interior pivot whose actual rate |off / p_i| exceeds it.
+int scan_window(double kappa, double &rho)
 {
     const std::complex<double> a(1.0, 2.0 * kappa * 0.99), c(-kappa * kappa, 0.0);
     const std::complex<double> sq = std::sqrt(a * a - 4.0 * c);
     const double pp = std::max(std::abs((a + sq) * 0.5), std::abs((a - sq) * 0.5));
-    const double rho = kappa / pp;
+    rho = kappa / pp;
     const int w = rho < 1.0 ? (int)std::ceil(40.0 / -std::log(rho)) + 16 : 4096;
-    return std::max(32, std::min(4096, w));
+    const int wc = std::max(32, std::min(4096, w));
+    // the rate the clamped window still forgets to exp(-40)
+    rho = std::min(rho < 1.0 ? rho : 1.0, std::exp(-40.0 / (double)(wc - 16)));
+    return wc;
 }
 
 }  // namespace
@@ -84,10 +91,13 @@ extern "C" int cnm_radial_solve_noalloc(const double *diag, double off_re, doubl
     if (cudaMemsetAsync(status, 0, sizeof(int), st) != cudaSuccess) return CNM_ECUDA;
     const double2 off = make_double2(off_re, off_im);
     const int chunk = 2048;
-    const int window = scan_window(std::hypot(off_re, off_im));
+    double rho = 0.0;
+    const int window = scan_window(std::hypot(off_re, off_im), rho);
     const int chunks = (Nr + chunk - 1) / chunk;
+    // one chunk per mode: the sweeps start at the boundary and are exact, nothing to check
+    const double rho_max = chunks > 1 ? rho : INFINITY;
     k_precond_factor_diag<<<dim3(chunks, n_modes), SCAN_THREADS, 0, st>>>(
-        reinterpret_cast<const double2 *>(diag), Nr, off, chunk, window / 2 + 16, scratch, status);
+        reinterpret_cast<const double2 *>(diag), Nr, off, chunk, window / 2 + 16, rho_max, scratch, status);
     if (cudaGetLastError() != cudaSuccess) return CNM_ECUDA;
     const size_t smem = (size_t)(std::min(Nr, chunk + 2 * window) + SCAN_THREADS) * sizeof(double2);
     k_precond_solve<<<dim3(chunks, n_modes), SCAN_THREADS, smem, st>>>(

@@ -285,11 +285,16 @@ int cnm_plan_info(const cnm_handle *h, int32_t *scan_per, int32_t *scan_cluster,
  * fixed, pre-reserved device arena and allows no other allocation, a driver that
  * launches from a region where allocation is forbidden, a plug-in that only
  * receives device pointers -- and so cannot create a handle.  Solves, for every
- * mode j, the tridiagonal radial block of the preconditioner
- * (include/RadialBlockPreconditioner.hpp:44-98 of the reference):
+ * mode j, the tridiagonal system
  *     diag[j,i] x[j,i] + off (x[j,i-1] + x[j,i+1]) = b[j,i]   for 1 <= i <= Nr-2,
  *     diag[j,i] x[j,i] = b[j,i]                                for i = 0, Nr-1,
- * with the same kernels as cnm_apply(..., CNM_OP_PRECOND, ...).
+ * by chunked parallel Thomas sweeps (2048 nodes per chunk, each chunk started from a
+ * warm-up window).  The windows are sized for a diagonally dominant system: the
+ * sweeps must contract by |off / p_i| < rho per node (p_i the Thomas pivots), with rho
+ * the rate of the diagonal 1 + 1.98 i |off| (the CN radial blocks satisfy this).  With
+ * Nr <= 2048 there is one chunk per mode and the solve is exact for any non-singular
+ * system; beyond that a system that contracts more slowly is refused (CNM_EDEVICE),
+ * never solved inexactly.
  *   diag, b, x  device pointers to Nr * n_modes interleaved complex128 values,
  *               mode-major (x may not alias diag or b);
  *   off         the constant off-diagonal (re, im);
@@ -303,7 +308,8 @@ int cnm_plan_info(const cnm_handle *h, int32_t *scan_per, int32_t *scan_cluster,
  * shared-memory limit); make that first call before any stream capture.  Every call
  * shares the one array, so calls that overlap on the GPU (concurrent streams or
  * threads) race and must be serialised by the caller.  Returns CNM_EDEVICE if a
- * pivot is zero or not finite, CNM_ECUDA on a CUDA error. */
+ * pivot is zero or not finite or the system is not dominant enough for the chunked
+ * sweeps, CNM_ECUDA on a CUDA error. */
 #define CNM_NOALLOC_MAX_UNKNOWNS (1 << 20)
 int cnm_radial_solve_noalloc(const double *diag, double off_re, double off_im, int32_t Nr, int32_t n_modes,
                              const double *b, double *x, void *stream);
