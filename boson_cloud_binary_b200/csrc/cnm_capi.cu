@@ -300,6 +300,7 @@ struct Solver {
     bool mixed = false;
     TcGaunt tg;
     TcPlan tcp;
+    int64_t tc_replica_bytes = 0;
     DevBuf<uint8_t> d_tcblob;
     DevBuf<int> d_tc_loff, d_tc_lbytes, d_tc_slices, d_tc_lnblk;
     DevBuf<float2> m_r, m_y, m_v, m_s, m_z, m_t, m_d, m_xa, dinv32, m_r1, m_q;
@@ -485,8 +486,11 @@ struct Solver {
         for (int b : tg.l_bytes) amax = std::max(amax, b);
         if (!tc_plan(n_modes, K, Nr, amax, nsm, tcp))
             throw Error(CNM_EINVAL, "The mixed solve supports at most 112 modes (l_max <= 13)");
-        std::vector<uint8_t> bytes(tg.blob.size() * 2);
-        std::memcpy(bytes.data(), tg.blob.data(), bytes.size());
+        // TC_REPLICAS copies of the image (each 256-byte aligned); CTA b reads copy b % TC_REPLICAS
+        tc_replica_bytes = (int64_t)((tg.blob.size() * 2 + 255) / 256 * 256);
+        std::vector<uint8_t> bytes((size_t)tc_replica_bytes * TC_REPLICAS, 0);
+        for (int rcp = 0; rcp < TC_REPLICAS; ++rcp)
+            std::memcpy(bytes.data() + (size_t)rcp * tc_replica_bytes, tg.blob.data(), tg.blob.size() * 2);
         upload(d_tcblob, bytes);
         upload(d_tc_loff, tg.l_off);
         upload(d_tc_lbytes, tg.l_bytes);
@@ -1328,6 +1332,8 @@ struct Solver {
         t.slices = d_tc_slices.p;
         t.l_nblk = d_tc_lnblk.p;
         t.g_exp = tg.g_exp;
+        t.replicas = TC_REPLICAS;
+        t.replica_bytes = tc_replica_bytes;
         return t;
     }
 

@@ -63,20 +63,20 @@ TcGaunt build_tc_gaunt(const Coupling &c)
                     }
             if (!nz) continue;
             const size_t at = t.blob.size();
-            t.blob.resize(at + (size_t)16 * t.kp, 0);  // 32 kp bytes
+            t.blob.resize(at + 2048, 0);  // 4096 bytes: 128 rows j x 16 columns k
             for (int j = 0; j < n; ++j)
                 for (int k = 16 * s; k < std::min(n, 16 * s + 16); ++k) {
                     const double g = G[((size_t)l * n + j) * n + k];
                     fro += g * g;
                     const int kk = k - 16 * s;
-                    const size_t byte = (size_t)(kk / 8) * 16 * t.kp + (size_t)(j / 8) * 128 + (size_t)(j % 8) * 16 +
+                    const size_t byte = (size_t)(kk / 8) * 2048 + (size_t)(j / 8) * 128 + (size_t)(j % 8) * 16 +
                                         (size_t)(kk % 8) * 2;
                     t.blob[at + byte / 2] = f16_bits(std::ldexp(g, t.g_exp));
                 }
             t.slices[(size_t)l * 16 + t.l_nblk[l]] = s;
             t.l_nblk[l] += 1;
         }
-        t.l_bytes[l] = t.l_nblk[l] * 32 * t.kp;
+        t.l_bytes[l] = t.l_nblk[l] * 4096;
         t.fro_sum += std::sqrt(fro);
     }
     return t;
@@ -164,6 +164,18 @@ __device__ __forceinline__ void tc_commit(uint32_t bar)
                  : "memory");
 }
 
+// 8 consecutive fp32 columns of this warp's 32 TMEM lanes.
+__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8])
+{
+    uint32_t r[8];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+                 : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]);
+}
+
 // 16 consecutive fp32 columns of this warp's 32 TMEM lanes.
 __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
 {
@@ -178,7 +190,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
     for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, 256;" ::: "memory"); }
+__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
 
 __device__ __forceinline__ uint32_t pack_f16(float lo, float hi)
 {
@@ -188,8 +200,9 @@ __device__ __forceinline__ uint32_t pack_f16(float lo, float hi)
 
 // ==================================================================== tensor-core apply
 
-constexpr int TC_WORKERS = 256;              // operand producers and epilogue (warps 0-7)
-constexpr int TC_THREADS = TC_WORKERS + 32;  // + the copy / MMA warp (warp 8)
+constexpr int TC_WORKERS = 512;              // operand producers and epilogue (warps 0-15)
+constexpr int TC_THREADS = TC_WORKERS + 32;  // + the copy / MMA warp (warp 16)
+constexpr int TC_CTRL = TC_WORKERS / 32;     // the copy / MMA warp
 constexpr int TC_GMAX = 8, TC_BSTAGES = 2;  // at most 8 Gaunt stages (the plan sets how many)
 constexpr int TC_NT = 128;                   // nodes per tile: 2 x 64-node halves, one MMA M-tile each
 constexpr float TC_HCUT = 1e-9f;             // multipoles below this fraction of the monopole are skipped
@@ -236,14 +249,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 {
     constexpr int LBO_Z = 32 * 128;            // bytes between 8-column groups of k in a Z stage
     constexpr int Z_STAGE = KP * 2 * TC_NT * 2;  // bytes of one Z stage (2 NT rows x KP fp16)
-    constexpr int G_LBO = KP * 16;             // bytes between the two 8-column halves of a G block
-    constexpr int G_BLK = KP * 32;             // bytes of one G block (KP rows x 16 columns)
-    constexpr uint32_t IDESC = idesc_f16(128, KP);
-    constexpr uint32_t NCOLS = 2 * KP <= 32 ? 32 : 2 * KP <= 64 ? 64 : 2 * KP <= 128 ? 128 : 256;
+    constexpr int G_LBO = 2048;                // bytes between the two 8-column halves of a G block
+    constexpr int G_BLK = 4096;                // bytes of one G block (128 rows j x 16 columns k)
+    constexpr uint32_t IDESC = idesc_f16(128, 2 * TC_NT);
+    constexpr uint32_t NCOLS = 2 * TC_NT;      // one fp32 accumulator: 128 lanes (modes) x 256 columns
     extern __shared__ __align__(128) uint8_t tc_smem[];
     __shared__ TcShared sh;
     const int n = g.n_modes, Nr = g.Nr;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    // this CTA's replica of the Gaunt image: CTAs that start together would otherwise all
+    // read the same lines of L2 at once
+    const uint8_t *gblob = tt.blob + (size_t)(blockIdx.x % tt.replicas) * tt.replica_bytes;
     uint8_t *Gst = tc_smem;                                              // gst x g_stage
     uint8_t *Zst = Gst + (size_t)gst * g_stage;                          // TC_BSTAGES x Z_STAGE
     // copies run gst - 1 uses ahead; a tile's first gst - 1 uses are copied before its cut is
@@ -287,7 +303,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int l = k < n ? mode_l[k] : 0;
         cent[k] = (float)((double)(l * (l + 1)) / (2.0 * g.mu));
     }
-    if (warp == 8) {
+    if (warp == TC_CTRL) {
         // TMEM accumulators: 2 M-tiles x KP fp32 columns x 128 lanes
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&sh.tmem_base)),
                      "r"(NCOLS)
@@ -299,7 +315,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     tc_fence_after();
     const uint32_t tmem = sh.tmem_base;
 
-    if (warp == 8) {
+    if (warp == TC_CTRL) {
         // ---------------------------------------------------------- copies and MMAs
         if (lane == 0) {
             int u = 0;       // multipole uses issued so far (all tiles)
@@ -307,7 +323,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             int it = 0;
             const int first = blockIdx.x;
             if (first < tiles)
-                for (; copies < gst - 1; ++copies) tc_issue_g(sh, Gst, g_stage, gst, tt.blob, copies, copies);
+                for (; copies < gst - 1; ++copies) tc_issue_g(sh, Gst, g_stage, gst, gblob, copies, copies);
             for (int tile = first; tile < tiles; tile += gridDim.x, ++it) {
                 mbar_wait(smem_addr(&sh.tinfo), it & 1, abort);
                 const int lc = sh.lcut[it & 1];
@@ -323,14 +339,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint32_t gbase = smem_addr(Gst + (size_t)sg * g_stage);
                     const uint32_t zbase = smem_addr(Zst + (size_t)sz * Z_STAGE);
                     const int nb = sh.l_nblk[l];
+                    // one M = 128 (modes j), N = 256 (the tile's node-component rows), K = 16
+                    // MMA per non-zero slice of G_l*: every tcgen05.mma of K = 16 costs about the
+                    // same whatever its N, so N is kept at its maximum
                     for (int q = 0; q < nb; ++q) {
                         const int s16 = tt.slices[l * 16 + q];
-                        const uint64_t bd = sdesc(gbase + (uint32_t)(q * G_BLK), (uint32_t)G_LBO, 128u);
-#pragma unroll
-                        for (int mt = 0; mt < 2; ++mt) {
-                            const uint64_t ad = sdesc(zbase + (uint32_t)(s16 * 2 * LBO_Z + mt * 2048), (uint32_t)LBO_Z, 128u);
-                            tc_mma(tmem + (uint32_t)(mt * KP), ad, bd, IDESC, firstmma ? 0u : 1u);
-                        }
+                        const uint64_t ad = sdesc(gbase + (uint32_t)(q * G_BLK), (uint32_t)G_LBO, 128u);
+                        const uint64_t bd = sdesc(zbase + (uint32_t)(s16 * 2 * LBO_Z), (uint32_t)LBO_Z, 128u);
+                        tc_mma(tmem, ad, bd, IDESC, firstmma ? 0u : 1u);
                         firstmma = false;
                     }
                     tc_commit(smem_addr(&sh.gfree[sg]));
@@ -343,7 +359,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     else if (more) lnext = l + ahead - (lc + 1);
                     if (lnext >= 0) {
                         if (u >= 1) mbar_wait(smem_addr(&sh.gfree[(u - 1) % gst]), ((u - 1) / gst) & 1, abort);
-                        tc_issue_g(sh, Gst, g_stage, gst, tt.blob, u + ahead, lnext);
+                        tc_issue_g(sh, Gst, g_stage, gst, gblob, u + ahead, lnext);
                         ++copies;
                     }
                 }
@@ -358,9 +374,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         __syncwarp();
     } else {
         // ---------------------------------------------------------- workers
-        const int m = tid, zc_node = m >> 1, zc_comp = m & 1;  // operand row of this thread
+        // operand row m = 2 node + (Re | Im) and half of its columns k
+        constexpr int KH = KP / 2;
+        const int m = tid & 255, khalf = tid >> 8, zc_node = m >> 1, zc_comp = m & 1;
         const float ad = (float)(1.0 / (2.0 * g.mu * g.dr * g.dr));
-        const int mt = warp >> 2, q4 = warp & 3;               // epilogue: M-tile, lane quarter
+        // epilogue phase 1: TMEM lane quarter (warp % 4: modes j) and quarter of the columns
+        const int q4 = warp & 3, cq = warp >> 2;
         const float2 al = a.alpha, be = a.beta;
         double dacc[6] = {0, 0, 0, 0, 0, 0};
         // the launch's one complex64 reduction operand (kinds 1, 2) and complex128 one (kind 4)
@@ -374,16 +393,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         int u = 0, it = 0;
         for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
             const int i0 = tile * TC_NT;
-            // z_k of this row's node and component (e^{i m_k theta} x_k)
-            float zc[KP];
+            // z_k of this row's node and component (e^{i m_k theta} x_k), k in this thread's half
+            float zc[KH];
             {
                 const int i = i0 + zc_node;
 #pragma unroll
-                for (int k = 0; k < KP; ++k) {
+                for (int kk = 0; kk < KH; ++kk) {
+                    const int k = khalf * KH + kk;
                     float2 xv = make_float2(0.f, 0.f);
                     if (k < n && i < Nr) xv = __ldg(xg + (int64_t)k * Nr + i);
                     const float2 p = ph[k];
-                    zc[k] = zc_comp ? p.x * xv.y + p.y * xv.x : p.x * xv.x - p.y * xv.y;
+                    zc[kk] = zc_comp ? p.x * xv.y + p.y * xv.x : p.x * xv.x - p.y * xv.y;
                 }
             }
             // radial weights, 1/r^2 and CAP of the tile's nodes and the multipole cut (the
@@ -412,7 +432,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 // the tile's operand scale: S = 2^se with max |S h z| < 2^14 (fp16 range)
                 float zm = 0.f;
 #pragma unroll
-                for (int k = 0; k < KP; ++k) zm = fmaxf(zm, fabsf(zc[k]));
+                for (int k = 0; k < KH; ++k) zm = fmaxf(zm, fabsf(zc[k]));
                 atomicMax(&sh.pmax_bits, __float_as_int(zm * hmx[zc_node]));
             }
             workers_sync();
@@ -427,7 +447,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 se = min(100, max(-100, 14 - e2));
                 const float sz = ldexpf(1.f, se);
 #pragma unroll
-                for (int k = 0; k < KP; ++k) zc[k] *= sz;
+                for (int k = 0; k < KH; ++k) zc[k] *= sz;
             }
             const float wscale = ldexpf(1.f, -(se + tt.g_exp));  // undoes both operand scales
             workers_sync();
@@ -441,10 +461,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int l = 0; l <= lc; ++l, ++u) {
                 const int sz = u % TC_BSTAGES;
                 if (u >= TC_BSTAGES) mbar_wait(smem_addr(&sh.zfree[sz]), ((u / TC_BSTAGES) - 1) & 1, abort);
-                uint8_t *Z = Zst + (size_t)sz * Z_STAGE + (m >> 3) * 128 + (m & 7) * 16;
+                uint8_t *Z = Zst + (size_t)sz * Z_STAGE + (size_t)khalf * (KH / 8) * LBO_Z + (m >> 3) * 128 + (m & 7) * 16;
                 const float h = hs[l * TC_NT + zc_node];
 #pragma unroll
-                for (int gq = 0; gq < KP / 8; ++gq) {
+                for (int gq = 0; gq < KH / 8; ++gq) {
                     uint4 v;
                     v.x = pack_f16(h * zc[8 * gq + 0], h * zc[8 * gq + 1]);
                     v.y = pack_f16(h * zc[8 * gq + 2], h * zc[8 * gq + 3]);
@@ -462,14 +482,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             tc_fence_after();
             float *W = reinterpret_cast<float *>(Zst);
             {
-                const uint32_t taddr = tmem + ((uint32_t)(32 * q4) << 16) + (uint32_t)(mt * KP);
-                const int mrow = 128 * mt + 32 * q4 + lane;
+                const uint32_t taddr = tmem + ((uint32_t)(32 * q4) << 16);
+                const int j = 32 * q4 + lane;
 #pragma unroll 1
-                for (int jc = 0; jc < KP; jc += 16) {
-                    float wv[16];
-                    tmem_ld16(taddr + (uint32_t)jc, wv);
+                for (int col = cq * (TC_NT / 2); col < (cq + 1) * (TC_NT / 2); col += 8) {
+                    float wv[8];
+                    tmem_ld8(taddr + (uint32_t)col, wv);
+                    if (j < n)
 #pragma unroll
-                    for (int q = 0; q < 16; ++q) W[(jc + q) * (2 * TC_NT) + mrow] = wv[q];
+                        for (int q = 0; q < 8; ++q) W[j * (2 * TC_NT) + col + q] = wv[q];
                 }
             }
             tc_fence_before();
@@ -480,7 +501,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             // on consecutive nodes of one mode (coalesced loads and stores)
             {
                 const int tile_nodes = min(TC_NT, Nr - i0);
-                constexpr int EB = 8;  // elements in flight per thread
+                constexpr int EB = 4;  // elements in flight per thread
 #pragma unroll 1
                 for (int e0 = tid; e0 < n * TC_NT; e0 += EB * TC_WORKERS) {
                     float2 x0[EB], xm[EB], xp[EB], w[EB];
@@ -574,18 +595,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             for (int q = 0; q < 6; ++q) dacc[q] = warp_sum(dacc[q]);
             if (lane == 0)
 #pragma unroll
-                for (int q = 0; q < 6; ++q) red[q * 8 + warp] = dacc[q];
+                for (int q = 0; q < 6; ++q) red[q * TC_CTRL + warp] = dacc[q];
             workers_sync();
             if (tid < 2 * a.n_dots) {
                 double s = 0.0;
-                for (int w = 0; w < 8; ++w) s += red[tid * 8 + w];
+                for (int w = 0; w < TC_CTRL; ++w) s += red[tid * TC_CTRL + w];
                 a.partials[(int64_t)tid * gridDim.x + blockIdx.x] = s;
             }
         }
     }
     __syncthreads();
     if (tid == 0 && sh.abort && a.status) atomicOr(a.status, 16);
-    if (warp == 8) {
+    if (warp == TC_CTRL) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS) : "memory");
     }

@@ -16,8 +16,8 @@
 // Ahat(r) = sum_l* h_l*(r) G_l*, G_l* the real Gaunt matrix of multipole l* (rows j,
 // columns k).  For a tile of 128 nodes the kernel forms, per l*, the fp16 operand
 //   Z_l*[m, k] = h_l*(r_node) z_k(r_node)_(Re|Im),   m = 2 node + (0 | 1),
-// and accumulates  D[m, j] += sum_k Z_l*[m, k] G_l*[j, k]  in fp32 TMEM accumulators
-// (two M-tiles of 128 rows, N = the padded mode count, K = 16 per instruction); G_l*
+// and accumulates  D[j, m] += sum_k G_l*[j, k] Z_l*[m, k]  in one fp32 TMEM accumulator
+// (M = 128 modes, N = 256 node components, K = 16 per instruction); G_l*
 // arrives in shared memory by bulk copy from a pre-formatted fp16 image (scaled by a power
 // of two, as the operand is per tile, to sit near the top of the fp16 range).  Multipoles
 // whose radial weight is below 1e-9 of the monopole at every node of the tile are
@@ -32,9 +32,9 @@
 namespace cnm {
 
 // Shared-memory image of the Gaunt matrices for the tensor-core apply (host built).
-// Per multipole l* the blob holds its non-zero K slices (16 columns k each) as blocks of
-// 32 kp bytes in the canonical K-major, no-swizzle layout of tcgen05 (kp = padded modes):
-//   byte (k % 16 / 8) * 16 kp + (j / 8) * 128 + (j % 8) * 16 + (k % 8) * 2,  j < kp.
+// Per multipole l* the blob holds its non-zero K slices (16 columns k each) as 4096-byte
+// blocks in the canonical K-major, no-swizzle layout of tcgen05 (rows j padded to 128):
+//   byte (k % 16 / 8) * 2048 + (j / 8) * 128 + (j % 8) * 16 + (k % 8) * 2,  j < 128.
 struct TcGaunt {
     int n_modes = 0, kp = 0, K = 0;           // rows, padded columns (multiple of 16), multipoles
     std::vector<uint16_t> blob;               // fp16 bits, all multipoles back to back
@@ -48,10 +48,13 @@ TcGaunt build_tc_gaunt(const struct Coupling &c);
 
 // Device view of the image.
 struct TcTable {
-    const uint8_t *blob;
+    const uint8_t *blob;       // `replicas` copies of the image, replica_bytes apart
     const int *l_off, *l_bytes, *slices, *l_nblk;
     int g_exp;
+    int replicas;
+    int64_t replica_bytes;
 };
+constexpr int TC_REPLICAS = 16;
 
 // Arguments of one tensor-core operator application on complex64 vectors:
 //   y = alpha x + beta (c_h0 H0 x + V x + CAP x) + sum_a coef_a (v_a^dag x) v_a,
