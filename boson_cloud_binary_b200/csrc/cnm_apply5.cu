@@ -558,6 +558,11 @@ unsigned launch_diag5(int l_max, cudaStream_t st, const Grid &g, const double *g
     return blocks.x * blocks.y;
 }
 
+unsigned diag5_blocks(int l_max, int Nr)
+{
+    return diag5_groups(l_max) > 0 ? (unsigned)((Nr + A5_THREADS - 1) / A5_THREADS) * (unsigned)diag5_groups(l_max) : 0u;
+}
+
 unsigned apply5_blocks(int l_max, int Nr)
 {
     return (unsigned)((Nr + A5_THREADS - 1) / A5_THREADS) * (unsigned)apply5_groups(l_max);

@@ -15,6 +15,7 @@
 #include <cuda_runtime.h>
 
 #include "cnm_common.cuh"
+#include "cnm_kernels.cuh"
 #include "cnm_coupling.h"
 
 namespace cnm {
@@ -134,28 +135,11 @@ struct A5Host {
     int rowoff(int g, int l1, int j) const { return a5f::rowoff(L, G, g, l1, j); }
 };
 
-// Arguments of the specialised diagnostics kernel (the pass of k_diagnostics2: H psi,
-// V psi, dV/dt psi and dpsi/dt on nodes <= idx_ex, reduced into per-CTA partials
-// [slot][block]: slots 0..n-1 norms, n..2n-1 energies, 2n edge energy, 2n+1 p_bin,
-// 2n+2 dV; dpsi/dt and psi around idx_ex stored for the fluxes).
-struct DiagArgs {
-    const double *hh;
-    double theta, domega;
-    const double2 *psi;
-    int idx_ex;
-    int n_sinks;
-    const double2 *sv0, *sv1, *sink_dots;
-    double sink_coef0, sink_coef1;
-    int slo0, shi0, slo1, shi1;
-    double *partials;
-    double2 *dpsi_edge, *psi_edge;
-    const struct Krylov *gate;  // skip until the step's candidate is accepted (null: always run)
-};
-
 // Host side of the specialised kernels (0 groups: l_max not specialised).
 int apply5_groups(int l_max);
 size_t apply5_smem(int l_max);
 unsigned apply5_blocks(int l_max, int Nr);
+unsigned diag5_blocks(int l_max, int Nr);  // the diagnostics pass over every node (an upper bound)
 int diag5_groups(int l_max);
 // the weight table of a layout with G row groups (apply5_groups or diag5_groups)
 std::vector<double> apply5_table(int l_max, int G, const Coupling &c);

@@ -254,13 +254,10 @@ struct Solver {
     DevBuf<double> d_r, d_hh, d_hh_aux, d_capw, d_mask, d_glx, d_glw, d_partials, d_red, d_ang00;
     DevBuf<int> d_pair_row_ptr, d_pair_col, d_pair_term_ptr, d_term_l, d_diag_pair, d_mode_l, d_mode_m, d_status;
     DevBuf<double> d_term_g;
-    BlockedCoupling bcpl;         // 4-row chunks (diagnostics)
     CouplingPlan plan3;           // operator kernel work plan (its blocks: 1-2 row chunks in list order)
     bool apply3_gsm = false;      // group weights staged in shared memory
     DevBuf<int> d3_list_ptr, d3_group_goff;
     DevBuf<double> d_ir2;
-    DevBuf<int> d_chunk_l, d_chunk_nrows, d_chunk_rows, d_chunk_goff, d_l_off;
-    DevBuf<double> d_block_g;
     DevBuf<int> d2_chunk_l, d2_chunk_nrows, d2_chunk_rows, d2_chunk_goff, d2_l_off;
     DevBuf<double> d2_block_g;
     size_t apply3_smem = 0;
@@ -291,7 +288,7 @@ struct Solver {
     DevBuf<double> d_wpart;      // partials of the Woodbury projections
     // red slots past the diagnostics' 2 n + 3 sums: |rhs|^2 and the candidate's residual^2
     int RED_RHS = 0, RED_RES = 0;
-    size_t apply_smem = 0, diag_smem = 0;
+    size_t diag3_smem = 0;       // the diagnostics pass on the operator kernel's tiles
     // pinned host staging
     double *h_stage = nullptr;
     size_t h_stage_n = 0;
@@ -303,6 +300,7 @@ struct Solver {
     int64_t tc_replica_bytes = 0;
     DevBuf<uint8_t> d_tcblob;
     DevBuf<int> d_tc_loff, d_tc_lbytes, d_tc_slices, d_tc_lnblk;
+    DevBuf<int> d_tc_ctr;           // tile counter of the tensor-core apply (zero between launches)
     DevBuf<float2> m_r, m_y, m_v, m_s, m_z, m_t, m_d, m_xa, dinv32, m_r1, m_q;
     DevBuf<double2> m_r64, m_dots;  // m_dots: [0..1] sink projections, [2..3] corrected ones
     DevBuf<MixScalars> d_msc;
@@ -425,13 +423,6 @@ struct Solver {
         upload(d_mode_l, cpl.mode_l);
         upload(d_mode_m, cpl.mode_m);
         upload(d_ang00, cpl.ang00);
-        bcpl = block_coupling(cpl, ROW_BLOCK);
-        upload(d_chunk_l, bcpl.chunk_l);
-        upload(d_chunk_nrows, bcpl.chunk_nrows);
-        upload(d_chunk_rows, bcpl.chunk_rows);
-        upload(d_chunk_goff, bcpl.chunk_goff);
-        upload(d_l_off, bcpl.l_off);
-        upload(d_block_g, bcpl.g);
         {
             std::vector<double> ir2(Nr, 0.0);
             for (int i = 0; i < Nr; ++i) ir2[i] = r[i] > 0.0 ? 1.0 / (r[i] * r[i]) : 0.0;
@@ -450,15 +441,13 @@ struct Solver {
         RED_RES = 2 * n_modes + 12;
         d_red.alloc(std::max(64, 2 * n_modes + 16));
         d_tickets.alloc(TK_COUNT_T);
-        const int diag_blocks = 2 * ((Nr + APPLY_TILE - 1) / APPLY_TILE);  // node tiles x row split
-        d_partials.alloc(std::max<size_t>({(size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks,
-                                           (size_t)4 * 8 * ((Nr + 63) / 64)}));
-        // the hh tile doubles as the scratch of the fused reductions (4 x 32 doubles)
-        apply_smem = (size_t)n_modes * (APPLY_TILE + 2 + APPLY_TILE + 1) * sizeof(double2) +
-                     (size_t)std::max(K, 4) * APPLY_TILE * sizeof(double);
-        diag_smem = apply_smem + (size_t)(2 * n_modes + 3) * (APPLY_THREADS / 32) * sizeof(double);
-        CK(set_operator_smem((int)diag_smem));
         plan_operator(nsm);
+        // partials: the vector kernels' slots, the diagnostics pass's 2n + 3 slots per CTA
+        // (64-node tiles x row groups) and the operator kernel's fused reductions
+        const size_t tiles3 = (size_t)(Nr + APPLY3_TILE - 1) / APPLY3_TILE;
+        const size_t diag_blocks = std::max<size_t>(tiles3 * plan3.n_groups, diag5_blocks(l_max, Nr));
+        d_partials.alloc(std::max<size_t>({(size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks,
+                                           (size_t)4 * 8 * tiles3}));
         a5_groups = apply5_groups(l_max);
         if (a5_groups > 0) {
             upload(d_a5tab, apply5_table(l_max, apply5_groups(l_max), cpl));
@@ -496,6 +485,7 @@ struct Solver {
         upload(d_tc_lbytes, tg.l_bytes);
         upload(d_tc_slices, tg.slices);
         upload(d_tc_lnblk, tg.l_nblk);
+        d_tc_ctr.alloc(2);
         CK(tc_prepare(tcp));
         for (DevBuf<float2> *b : {&m_r, &m_y, &m_v, &m_s, &m_z, &m_t, &m_d, &m_xa, &dinv32, &m_r1, &m_q}) b->alloc(nN);
         m_r64.alloc(nN);
@@ -552,6 +542,11 @@ struct Solver {
             }
         }
         if (plan3.list_ptr.empty()) throw Error(CNM_EINVAL, "No resident configuration of the operator kernel");
+        // the diagnostics pass: the same tile (weights read through L1) and the per-row and
+        // per-warp sums of its reductions
+        diag3_smem = base + (size_t)(2 * n_modes + 3 * (APPLY_THREADS / 32)) * sizeof(double);
+        if (diag3_smem > (size_t)dyn_max) throw Error(CNM_EINVAL, "Too many modes for the diagnostics pass's shared tile");
+        CK(set_diag3_smem((int)diag3_smem));
         const BlockedCoupling &b = plan3.blocks;
         upload(d2_chunk_l, b.chunk_l);
         upload(d2_chunk_nrows, b.chunk_nrows);
@@ -672,19 +667,6 @@ struct Solver {
         c.mode_l = d_mode_l.p;
         c.mode_m = d_mode_m.p;
         return c;
-    }
-
-    BlockTable btable() const
-    {
-        BlockTable b;
-        b.n_chunks = bcpl.n_chunks;
-        b.chunk_l = d_chunk_l.p;
-        b.chunk_nrows = d_chunk_nrows.p;
-        b.chunk_rows = d_chunk_rows.p;
-        b.chunk_goff = d_chunk_goff.p;
-        b.l_off = d_l_off.p;
-        b.g = d_block_g.p;
-        return b;
     }
 
     BlockTable btable2() const
@@ -996,10 +978,6 @@ struct Solver {
         return a;
     }
 
-    // Row chunks of a tile are split across this many CTAs (one round of chunks per warp).
-    int apply_split() const { return bcpl.n_chunks > APPLY_THREADS / 32 ? 2 : 1; }
-    dim3 apply_grid() const { return dim3((unsigned)((Nr + APPLY_TILE - 1) / APPLY_TILE), (unsigned)apply_split()); }
-
     // Operator kernel grid: 64-node tiles x the plan's CTA groups.
     dim3 apply3_grid() const
     {
@@ -1235,38 +1213,34 @@ struct Solver {
         const Absorber *all[2] = {&abs1, &abs2};
         const bool have_sinks = absorption && cpl.mode00 >= 0;
         if (have_sinks) sink_dots(st, d_dots.p + 4, all, 2, GATE_ACCEPTED);
-        const dim3 dgrid = apply_grid();
-        unsigned dblocks = dgrid.x * dgrid.y;
+        unsigned dblocks = 0;
         kt_begin(TK_DIAG);
+        DiagArgs da;
+        da.hh = d_hh.p;
+        da.theta = op.theta;
+        da.domega = op.domega;
+        da.psi = st;
+        da.idx_ex = idx_ex;
+        da.n_sinks = k;
+        da.sv0 = k > 0 ? sk[0]->v.p : nullptr;
+        da.sv1 = k > 1 ? sk[1]->v.p : nullptr;
+        da.sink_dots = k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p;
+        da.sink_coef0 = k > 0 ? -0.5 * sk[0]->strength : 0.0;
+        da.sink_coef1 = k > 1 ? -0.5 * sk[1]->strength : 0.0;
+        da.slo0 = k > 0 ? sk[0]->lo : 0;
+        da.shi0 = k > 0 ? sk[0]->hi : 0;
+        da.slo1 = k > 1 ? sk[1]->lo : 0;
+        da.shi1 = k > 1 ? sk[1]->hi : 0;
+        da.partials = d_partials.p;
+        da.dpsi_edge = d_edge.p;
+        da.psi_edge = d_edge.p + n_modes;
+        da.gate = d_kr.p;
         if (a5_groups > 0 && a5_enabled) {
-            DiagArgs da;
-            da.hh = d_hh.p;
-            da.theta = op.theta;
-            da.domega = op.domega;
-            da.psi = st;
-            da.idx_ex = idx_ex;
-            da.n_sinks = k;
-            da.sv0 = k > 0 ? sk[0]->v.p : nullptr;
-            da.sv1 = k > 1 ? sk[1]->v.p : nullptr;
-            da.sink_dots = k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p;
-            da.sink_coef0 = k > 0 ? -0.5 * sk[0]->strength : 0.0;
-            da.sink_coef1 = k > 1 ? -0.5 * sk[1]->strength : 0.0;
-            da.slo0 = k > 0 ? sk[0]->lo : 0;
-            da.shi0 = k > 0 ? sk[0]->hi : 0;
-            da.slo1 = k > 1 ? sk[1]->lo : 0;
-            da.shi1 = k > 1 ? sk[1]->hi : 0;
-            da.partials = d_partials.p;
-            da.dpsi_edge = d_edge.p;
-            da.psi_edge = d_edge.p + n_modes;
-            da.gate = d_kr.p;
             dblocks = ::cnm::launch_diag5(l_max, stream, grid(), d_d5tab.p, da);
         } else {
-            ::cnm::launch_diagnostics(
-                l_max, dgrid, diag_smem, stream, grid(), table(), btable(), d_hh.p, op.theta, op.domega, st,
-                idx_ex, k, k > 0 ? sk[0]->v.p : nullptr, k > 1 ? sk[1]->v.p : nullptr,
-                k > 0 ? d_dots.p + 4 + sink_slot(sk[0]) : d_dots.p, k > 0 ? -0.5 * sk[0]->strength : 0.0,
-                k > 1 ? -0.5 * sk[1]->strength : 0.0, k > 0 ? sk[0]->lo : 0, k > 0 ? sk[0]->hi : 0,
-                k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, d_partials.p, d_edge.p, d_edge.p + n_modes, d_kr.p);
+            const dim3 dgrid((unsigned)(std::min(idx_ex, Nr - 1) / APPLY3_TILE + 1), (unsigned)plan3.n_groups);
+            ::cnm::launch_diag3(l_max, dgrid, diag3_smem, stream, grid(), table(), btable2(), aplan(), da);
+            dblocks = dgrid.x * dgrid.y;
         }
         launch_check();
         kt_end(TK_DIAG);
@@ -1362,6 +1336,7 @@ struct Solver {
         }
         a.partials = m_part.p;
         a.status = d_status.p;
+        a.tile_ctr = d_tc_ctr.p;
         return a;
     }
 
@@ -2526,13 +2501,14 @@ int cnm_mixed_info(const cnm_handle *h, int32_t *passes, int32_t *fp64_applies, 
     });
 }
 
-int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk)
+int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk, int32_t *lc_min)
 {
     return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) {
         if (!s.mixed) throw cnm::Error(CNM_ELOGIC, "no tensor-core operator on an fp64 handle");
         if (kp) *kp = s.tg.kp;
         if (nblk)
             for (int l = 0; l < s.K; ++l) nblk[l] = s.tg.l_nblk[l];
+        if (lc_min) *lc_min = std::max(1, s.tcp.gst - 2);
     });
 }
 

@@ -46,273 +46,6 @@ __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1
 
 // ------------------------------------------------------------------ operator application
 
-// ------------------------------------------------------------------ register-blocked coupling
-
-// Multipole cut of one tile: the largest l* whose weight exceeds 1e-18 of the
-// monopole weight at some node of the tile.  Smaller terms cannot change an FP64
-// result (they lie far below the rounding of the diagonal), and at radii well
-// outside the binary they make up most of the Gaunt terms.
-__device__ int tile_lcut(const double *hs, int K, int lane)
-{
-    int lc = -1;
-    const double h0 = fabs(hs[lane]);
-    if (h0 > 0.0) {
-        lc = 0;
-        for (int l = K - 1; l > 0; --l)
-            if (fabs(hs[l * APPLY_TILE + lane]) > 1e-18 * h0) {
-                lc = l;
-                break;
-            }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) lc = max(lc, __shfl_xor_sync(0xffffffffu, lc, o));
-    return lc;
-}
-
-// One (row chunk, l1) block: for the S_EFF leading multipoles l* = L0 + 2s held in
-// registers, Ahat_jk = sum_s g[k][row][s] h_s for the RB rows of the chunk and the
-// l1 + 1 columns k = col0 .. col0 + ncols - 1, accumulated into acc (and into accm with
-// weight m_k for dV/dt).  Weights come in 16-byte pairs (even stride) and feed two
-// independent FMA chains.
-template <int S_EFF, int RB, bool DVDT>
-__device__ __forceinline__ void coupling_block(const double *__restrict__ g, int stride, int ncols, int col0,
-                                               const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
-                                               double2 (&acc)[RB], double2 (&accm)[RB])
-{
-    double h[S_EFF];
-#pragma unroll
-    for (int s2 = 0; s2 < S_EFF; ++s2) h[s2] = hs_l0[2 * s2 * APPLY_TILE + lane];
-    for (int kk = 0; kk < ncols; ++kk) {
-        const double2 z = zs[(col0 + kk) * APPLY_TILE + lane];
-        const double *gk = g + kk * RB * stride;
-        const double mk = DVDT ? (double)mode_m[col0 + kk] : 0.0;
-#pragma unroll
-        for (int rr = 0; rr < RB; ++rr) {
-            const double *gr = gk + rr * stride;
-            double a0 = 0.0, a1 = 0.0;
-#pragma unroll
-            for (int s2 = 0; s2 + 1 < S_EFF; s2 += 2) {
-                const double2 gg = __ldg(reinterpret_cast<const double2 *>(gr + s2));
-                a0 = fma(gg.x, h[s2], a0);
-                a1 = fma(gg.y, h[s2 + 1], a1);
-            }
-            if (S_EFF & 1) a0 = fma(__ldg(gr + S_EFF - 1), h[S_EFF - 1], a0);
-            const double a = a0 + a1;
-            acc[rr].x = fma(a, z.x, acc[rr].x);
-            acc[rr].y = fma(a, z.y, acc[rr].y);
-            if (DVDT) {
-                const double am = a * mk;
-                accm[rr].x = fma(am, z.x, accm[rr].x);
-                accm[rr].y = fma(am, z.y, accm[rr].y);
-            }
-        }
-    }
-}
-
-template <int SMAX, int RB, bool DVDT>
-__device__ __forceinline__ void coupling_dispatch(int s_eff, const double *g, int stride, int ncols, int col0,
-                                                  const double2 *zs, const double *hs_l0, const int *mode_m, int lane,
-                                                  double2 (&acc)[RB], double2 (&accm)[RB])
-{
-    // Blocks of up to SMAX multipoles: the instantiation for an l_max allocates
-    // registers for its own widest block only.
-#define CNM_CASE(S)                                                                                  \
-    case S:                                                                                          \
-        if (S <= SMAX)                                                                               \
-            coupling_block<(S <= SMAX ? S : 1), RB, DVDT>(g, stride, ncols, col0, zs, hs_l0, mode_m, \
-                                                          lane, acc, accm);                          \
-        break;
-    switch (s_eff) {
-        CNM_CASE(1) CNM_CASE(2) CNM_CASE(3) CNM_CASE(4) CNM_CASE(5) CNM_CASE(6) CNM_CASE(7) CNM_CASE(8)
-        CNM_CASE(9) CNM_CASE(10) CNM_CASE(11) CNM_CASE(12) CNM_CASE(13) CNM_CASE(14) CNM_CASE(15)
-        CNM_CASE(16) CNM_CASE(17) CNM_CASE(18) CNM_CASE(19) CNM_CASE(20) CNM_CASE(21) CNM_CASE(22)
-        CNM_CASE(23) CNM_CASE(24) CNM_CASE(25)
-    default: break;
-    }
-#undef CNM_CASE
-}
-
-// Ahat z (and Ahat M z) for the RB rows of one chunk at the warp's 32 nodes.
-template <int SMAX, int RB, bool DVDT>
-__device__ __forceinline__ void coupling_chunk(const BlockTable &bt, int l_max, int ci, int lcut, const double2 *zs,
-                                               const double *hs, const int *mode_m, int lane, double2 (&acc)[RB],
-                                               double2 (&accm)[RB])
-{
-#pragma unroll
-    for (int rr = 0; rr < RB; ++rr) acc[rr] = accm[rr] = cmake(0.0, 0.0);
-    if (lcut < 0) return;
-    const int l = bt.chunk_l[ci];
-    for (int l1 = 0; l1 <= l_max; ++l1) {
-        const int L0 = abs(l - l1), S = min(l, l1) + 1;
-        if (lcut < L0) continue;
-        const int s_eff = min(S, (lcut - L0) / 2 + 1);
-        coupling_dispatch<SMAX, RB, DVDT>(s_eff, bt.g + bt.chunk_goff[ci * (l_max + 1) + l1], (S + 1) & ~1, l1 + 1,
-                                          bt.l_off[l1], zs, hs + L0 * APPLY_TILE, mode_m, lane, acc, accm);
-    }
-}
-
-// Everything an operator kernel's warp needs about its tile and node.
-struct TileCtx {
-    const double2 *xs, *zs, *ph;
-    const double *hs;
-    int lane, i, lcut;
-    bool interior;
-    double ri;
-};
-
-// Fused diagnostics of one chunk (see k_diagnostics2).
-template <int SMAX, int RB>
-__device__ __forceinline__ void diag_chunk(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
-                                           const TileCtx &t, int ci, bool active, int idx_ex, double domega,
-                                           int n_sinks, const double2 *sv0, const double2 *sv1,
-                                           const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0,
-                                           int shi0, int slo1, int shi1, double2 *dpsi_edge, double2 *psi_edge,
-                                           double *red, int nw, int warp, double &e_edge, double &pb, double &dv)
-{
-    double2 acc[RB], accm[RB];
-    coupling_chunk<SMAX, RB, true>(bt, ct.l_max, ci, t.lcut, t.zs, t.hs, ct.mode_m, t.lane, acc, accm);
-    const int Nr = g.Nr, c = t.lane, i = t.i, n = g.n_modes;
-    const double alpha_d = 1.0 / (g.dr * g.dr);
-#pragma unroll
-    for (int rr = 0; rr < RB; ++rr) {
-        const int j = bt.chunk_rows[ci * ROW_BLOCK + rr];
-        double nrm = 0.0, en = 0.0;
-        if (active) {
-            const double2 xv = t.xs[j * (APPLY_TILE + 2) + c + 1];
-            double2 hx = cmake(0.0, 0.0), vx = cmake(0.0, 0.0), dx = cmake(0.0, 0.0);
-            if (t.interior) {
-                const int l = ct.mode_l[j];
-                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) / (t.ri * t.ri)) / (2 * g.mu);
-                const double off = -alpha_d / (2 * g.mu);
-                hx = cadd(cscale(xv, diag),
-                          cscale(cadd(t.xs[j * (APPLY_TILE + 2) + c], t.xs[j * (APPLY_TILE + 2) + c + 2]), off));
-                const double mj = (double)ct.mode_m[j];
-                vx = cmul(cconj(t.ph[j]), acc[rr]);
-                dx = cmul(cconj(t.ph[j]), cmuli(cscale(cmake(accm[rr].x - mj * acc[rr].x, accm[rr].y - mj * acc[rr].y), domega)));
-                hx = cadd(hx, vx);
-            }
-            if (g.capw) hx = cadd(hx, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
-            double2 dp = cmake(hx.y, -hx.x);  // -i H psi
-            if (n_sinks > 0 && i >= slo0 && i < shi0)
-                dp = cadd(dp, cmul(cscale(sink_dots[0], sink_coef0), sv0[(int64_t)j * Nr + i]));
-            if (n_sinks > 1 && i >= slo1 && i < shi1)
-                dp = cadd(dp, cmul(cscale(sink_dots[1], sink_coef1), sv1[(int64_t)j * Nr + i]));
-            const double ce = cconjmul(xv, hx).x;
-            if (i < idx_ex) {
-                nrm = cabs2(xv);
-                en = ce;
-            } else {
-                e_edge += ce;
-                dpsi_edge[j] = dp;
-                psi_edge[3 * j] = t.xs[j * (APPLY_TILE + 2) + c];
-                psi_edge[3 * j + 1] = xv;
-                psi_edge[3 * j + 2] = t.xs[j * (APPLY_TILE + 2) + c + 2];
-            }
-            pb += cconjmul(xv, dx).x;
-            dv += cconjmul(dp, vx).x;
-        }
-        nrm = warp_sum(nrm);
-        en = warp_sum(en);
-        if (t.lane == 0) {
-            red[j * nw + warp] = nrm;
-            red[(n + j) * nw + warp] = en;
-        }
-    }
-}
-
-// Fused diagnostics, register-blocked (same outputs and partial layout as k_diagnostics).
-template <int SMAX>
-__global__ void __launch_bounds__(APPLY_THREADS) k_diagnostics2(Grid g, CouplingTable ct, BlockTable bt,
-                                                                 const double *hh, double theta, double domega,
-                                                                 const double2 *psi, int idx_ex, int n_sinks,
-                                                                 const double2 *sv0, const double2 *sv1,
-                                                                 const double2 *sink_dots, double sink_coef0,
-                                                                 double sink_coef1, int slo0, int shi0, int slo1,
-                                                                 int shi1, double *partials, double2 *dpsi_edge,
-                                                                 double2 *psi_edge, const Krylov *gate)
-{
-    if (gate && gate_closed(gate, GATE_ACCEPTED)) return;
-    extern __shared__ double2 smem2[];
-    __shared__ int s_lcut;
-    const int n = g.n_modes, Nr = g.Nr;
-    const int K = 2 * ct.l_max + 1;
-    const int i0 = blockIdx.x * APPLY_TILE;
-    double2 *xs = smem2;
-    double2 *zs = xs + n * (APPLY_TILE + 2);
-    double2 *ph = zs + n * APPLY_TILE;
-    double *hs = reinterpret_cast<double *>(ph + n);
-    double *red = hs + K * APPLY_TILE;  // (2n + 3) * nwarps
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
-
-    for (int k = threadIdx.x; k < n; k += blockDim.x) {
-        double sn, cs;
-        sincos((double)ct.mode_m[k] * theta, &sn, &cs);
-        ph[k] = cmake(cs, sn);
-    }
-    for (int e = threadIdx.x; e < n * (APPLY_TILE + 2); e += blockDim.x) {
-        const int j = e / (APPLY_TILE + 2), c = e % (APPLY_TILE + 2);
-        const int i = i0 - 1 + c;
-        xs[e] = (i >= 0 && i < Nr) ? psi[(int64_t)j * Nr + i] : cmake(0.0, 0.0);
-    }
-    for (int e = threadIdx.x; e < K * APPLY_TILE; e += blockDim.x) {
-        const int l = e / APPLY_TILE, c = e % APPLY_TILE;
-        const int i = i0 + c;
-        hs[e] = i < Nr ? hh[(int64_t)l * Nr + i] : 0.0;
-    }
-    for (int e = threadIdx.x; e < (2 * n + 3) * nw; e += blockDim.x) red[e] = 0.0;
-    __syncthreads();
-    for (int e = threadIdx.x; e < n * APPLY_TILE; e += blockDim.x) {
-        const int k = e / APPLY_TILE, c = e % APPLY_TILE;
-        zs[e] = cmul(ph[k], xs[k * (APPLY_TILE + 2) + c + 1]);
-    }
-    if (warp == 0) {
-        const int lc = tile_lcut(hs, K, lane);
-        if (lane == 0) s_lcut = lc;
-    }
-    __syncthreads();
-    TileCtx t;
-    t.xs = xs;
-    t.zs = zs;
-    t.ph = ph;
-    t.hs = hs;
-    t.lane = lane;
-    t.i = i0 + lane;
-    t.lcut = s_lcut;
-    t.interior = t.i >= 1 && t.i <= Nr - 2;
-    t.ri = t.i < Nr ? g.r[t.i] : 1.0;
-    const bool active = t.i < Nr && t.i <= idx_ex;
-    double e_edge = 0.0, pb = 0.0, dv = 0.0;
-    // tiles entirely beyond the extraction node hold no diagnostics
-    const bool tile_active = i0 <= idx_ex;
-    for (int ci = blockIdx.y + gridDim.y * warp; tile_active && ci < bt.n_chunks; ci += gridDim.y * nw) {
-#define CNM_DIAG(RB)                                                                                          \
-    diag_chunk<SMAX, RB>(g, ct, bt, t, ci, active, idx_ex, domega, n_sinks, sv0, sv1, sink_dots, sink_coef0, \
-                         sink_coef1, slo0, shi0, slo1, shi1, dpsi_edge, psi_edge, red, nw, warp, e_edge, pb, dv)
-        switch (bt.chunk_nrows[ci]) {
-        case 1: CNM_DIAG(1); break;
-        case 2: CNM_DIAG(2); break;
-        case 3: CNM_DIAG(3); break;
-        default: CNM_DIAG(4); break;
-        }
-#undef CNM_DIAG
-    }
-    e_edge = warp_sum(e_edge);
-    pb = warp_sum(pb);
-    dv = warp_sum(dv);
-    if (lane == 0) {
-        red[(2 * n) * nw + warp] = e_edge;
-        red[(2 * n + 1) * nw + warp] = pb;
-        red[(2 * n + 2) * nw + warp] = dv;
-    }
-    __syncthreads();
-    const int nblocks = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
-    for (int q = threadIdx.x; q < 2 * n + 3; q += blockDim.x) {
-        double sm = 0.0;
-        for (int w = 0; w < nw; ++w) sm += red[q * nw + w];
-        partials[(int64_t)q * nblocks + blk] = sm;
-    }
-}
-
 // ------------------------------------------------------------------ operator kernel, two nodes per thread
 
 // Tiles of TILE3 = 64 nodes: lane l of every warp owns nodes l and l + 32, so each
@@ -565,6 +298,167 @@ __global__ void __launch_bounds__(APPLY_THREADS, 2) k_apply3(Grid g, CouplingTab
     }
 }
 
+// ------------------------------------------------------------------ diagnostics pass, two nodes per thread
+
+// The diagnostics of one row chunk (src/CrankNicolsonModes_extraction.cpp:8-129) at the
+// lane's two nodes: H psi, V psi, dV/dt psi and dpsi/dt = -i H psi - Gamma psi / 2, the
+// mode's norm and energy sums (nodes < idx_ex, one value per row and tile in `rowred`),
+// the edge values at idx_ex, and the lane's p_bin and dV/dt sums.
+template <int SMAX, int RB>
+__device__ __forceinline__ void diag_chunk3(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
+                                            const double *gbase, int goff0, const DiagArgs &d, const double2 *zs,
+                                            const double2 *ph, const double *hs, int lane, int i0, int lcut, int ci,
+                                            double *rowred, double &e_edge, double &pb, double &dv)
+{
+    double2 acc[RB][2], accm[RB][2];
+    coupling_chunk3<SMAX, RB, true, false>(bt, gbase, goff0, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane, acc, accm);
+    const int Nr = g.Nr, n = g.n_modes;
+    const double alpha_d = 1.0 / (g.dr * g.dr), inv2mu = 1.0 / (2 * g.mu);
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) {
+        const int j = bt.chunk_rows[ci * 2 + rr];
+        const double2 *xr = d.psi + (int64_t)j * Nr;
+        double nrm = 0.0, en = 0.0;
+#pragma unroll
+        for (int nb = 0; nb < 2; ++nb) {
+            const int i = i0 + lane + 32 * nb;
+            if (i >= Nr || i > d.idx_ex) continue;
+            const bool interior = i >= 1 && i <= Nr - 2;
+            const double2 xv = xr[i];
+            double2 hx = cmake(0.0, 0.0), vx = cmake(0.0, 0.0), dx = cmake(0.0, 0.0);
+            if (interior) {
+                const int l = ct.mode_l[j];
+                const double diag = (2.0 * alpha_d + (double)(l * (l + 1)) * g.ir2[i]) * inv2mu;
+                const double off = -alpha_d * inv2mu;
+                hx = cadd(cscale(xv, diag), cscale(cadd(xr[i - 1], xr[i + 1]), off));
+                const double mj = (double)ct.mode_m[j];
+                vx = cmul(cconj(ph[j]), acc[rr][nb]);
+                dx = cmul(cconj(ph[j]), cmuli(cscale(cmake(accm[rr][nb].x - mj * acc[rr][nb].x,
+                                                           accm[rr][nb].y - mj * acc[rr][nb].y),
+                                                     d.domega)));
+                hx = cadd(hx, vx);
+            }
+            if (g.capw) hx = cadd(hx, cmake(g.capw[i] * xv.y, -g.capw[i] * xv.x));
+            double2 dp = cmake(hx.y, -hx.x);  // -i H psi
+            if (d.n_sinks > 0 && i >= d.slo0 && i < d.shi0)
+                dp = cadd(dp, cmul(cscale(d.sink_dots[0], d.sink_coef0), d.sv0[(int64_t)j * Nr + i]));
+            if (d.n_sinks > 1 && i >= d.slo1 && i < d.shi1)
+                dp = cadd(dp, cmul(cscale(d.sink_dots[1], d.sink_coef1), d.sv1[(int64_t)j * Nr + i]));
+            const double ce = cconjmul(xv, hx).x;
+            if (i < d.idx_ex) {
+                nrm += cabs2(xv);
+                en += ce;
+            } else {
+                e_edge += ce;
+                d.dpsi_edge[j] = dp;
+                d.psi_edge[3 * j] = i >= 1 ? xr[i - 1] : cmake(0.0, 0.0);
+                d.psi_edge[3 * j + 1] = xv;
+                d.psi_edge[3 * j + 2] = i + 1 < Nr ? xr[i + 1] : cmake(0.0, 0.0);
+            }
+            pb += cconjmul(xv, dx).x;
+            dv += cconjmul(dp, vx).x;
+        }
+        nrm = warp_sum(nrm);
+        en = warp_sum(en);
+        if (lane == 0) {
+            rowred[j] = nrm;
+            rowred[n + j] = en;
+        }
+    }
+}
+
+// The diagnostics pass on the operator kernel's tiles and work plan: CTA (64-node tile,
+// row group) over the tiles up to idx_ex; the group's warp lists of 1-2-row chunks, every
+// row in exactly one list.  Per-CTA partials [slot][block] (block = group x tiles +
+// tile): slots 0..n-1 norms, n..2n-1 energies (written by the row's group, zero in the
+// others), 2n edge energy, 2n+1 p_bin, 2n+2 dV.
+template <int SMAX>
+__global__ void __launch_bounds__(APPLY_THREADS, 2) k_diag3(Grid g, CouplingTable ct, BlockTable bt, ApplyPlan pl,
+                                                            DiagArgs d)
+{
+    if (d.gate && gate_closed(d.gate, GATE_ACCEPTED)) return;
+    extern __shared__ double2 smemd3[];
+    __shared__ int s_lcut;
+    const int n = g.n_modes, Nr = g.Nr;
+    const int K = 2 * ct.l_max + 1;
+    const int i0 = blockIdx.x * TILE3;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    double2 *zs = smemd3;                             // n * TILE3
+    double2 *ph = zs + n * TILE3;                     // n
+    double *hs = reinterpret_cast<double *>(ph + n);  // max(K, 4) * TILE3
+    double *rowred = hs + max(K, 4) * TILE3;          // 2n per-row sums + 3 x nw lane sums
+    const int grp = blockIdx.y;
+    const int goff0 = pl.group_goff[grp];
+    const double *gbase = bt.g + goff0;
+    for (int k = threadIdx.x; k < n; k += blockDim.x) {
+        double sn, cs;
+        sincos((double)ct.mode_m[k] * d.theta, &sn, &cs);
+        ph[k] = cmake(cs, sn);
+    }
+    for (int e = threadIdx.x; e < K * TILE3; e += blockDim.x) {
+        const int l = e / TILE3, c = e % TILE3;
+        const int i = i0 + c;
+        hs[e] = i < Nr ? d.hh[(int64_t)l * Nr + i] : 0.0;
+    }
+    for (int e = threadIdx.x; e < 2 * n + 3 * nw; e += blockDim.x) rowred[e] = 0.0;
+    __syncthreads();
+    for (int e = threadIdx.x; e < n * TILE3; e += blockDim.x) {
+        const int k = e / TILE3, c = e % TILE3;
+        const int i = i0 + c;
+        zs[e] = i < Nr ? cmul(ph[k], d.psi[(int64_t)k * Nr + i]) : cmake(0.0, 0.0);
+    }
+    if (warp == 0) {
+        // multipole cut over both halves of the tile (as in k_apply3)
+        int lc = -1;
+        for (int half = 0; half < 2; ++half) {
+            const int c = lane + 32 * half;
+            const double h0 = fabs(hs[c]);
+            if (h0 > 0.0) {
+                int lcc = 0;
+                for (int l = K - 1; l > 0; --l)
+                    if (fabs(hs[l * TILE3 + c]) > 1e-18 * h0) {
+                        lcc = l;
+                        break;
+                    }
+                lc = max(lc, lcc);
+            }
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) lc = max(lc, __shfl_xor_sync(0xffffffffu, lc, o));
+        if (lane == 0) s_lcut = lc;
+    }
+    __syncthreads();
+    const int lcut = s_lcut;
+    double e_edge = 0.0, pb = 0.0, dv = 0.0;
+    const int list = grp * nw + warp;
+    for (int ci = pl.list_ptr[list]; ci < pl.list_ptr[list + 1]; ++ci) {
+        if (bt.chunk_nrows[ci] == 1)
+            diag_chunk3<SMAX, 1>(g, ct, bt, gbase, goff0, d, zs, ph, hs, lane, i0, lcut, ci, rowred, e_edge, pb, dv);
+        else
+            diag_chunk3<SMAX, 2>(g, ct, bt, gbase, goff0, d, zs, ph, hs, lane, i0, lcut, ci, rowred, e_edge, pb, dv);
+    }
+    e_edge = warp_sum(e_edge);
+    pb = warp_sum(pb);
+    dv = warp_sum(dv);
+    double *lred = rowred + 2 * n;
+    if (lane == 0) {
+        lred[warp] = e_edge;
+        lred[nw + warp] = pb;
+        lred[2 * nw + warp] = dv;
+    }
+    __syncthreads();
+    const int nblocks = gridDim.x * gridDim.y, blk = blockIdx.y * gridDim.x + blockIdx.x;
+    for (int q = threadIdx.x; q < 2 * n + 3; q += blockDim.x) {
+        double sm = 0.0;
+        if (q < 2 * n) {
+            sm = rowred[q];
+        } else {
+            for (int w = 0; w < nw; ++w) sm += lred[(q - 2 * n) * nw + w];
+        }
+        d.partials[(int64_t)q * nblocks + blk] = sm;
+    }
+}
+
 // ---- launchers of the templated operator kernels
 
 static int smax_for(int l_max)
@@ -575,14 +469,24 @@ static int smax_for(int l_max)
 
 #define CNM_FOR_SMAX(MACRO) MACRO(5) MACRO(9) MACRO(13) MACRO(17) MACRO(25)
 
-cudaError_t set_operator_smem(int diag_bytes)
+cudaError_t set_diag3_smem(int bytes)
 {
     cudaError_t e = cudaSuccess;
-#define CNM_ATTR(S) \
-    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diagnostics2<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, diag_bytes);
-    CNM_FOR_SMAX(CNM_ATTR)
-#undef CNM_ATTR
+#define CNM_ATTRD(S) \
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_diag3<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    CNM_FOR_SMAX(CNM_ATTRD)
+#undef CNM_ATTRD
     return e;
+}
+
+const void *diag3_kernel(int l_max)
+{
+    const int smax = smax_for(l_max);
+#define CNM_PICKD(S) \
+    if (smax == S) return (const void *)k_diag3<S>;
+    CNM_FOR_SMAX(CNM_PICKD)
+#undef CNM_PICKD
+    return nullptr;
 }
 
 cudaError_t set_apply3_smem(int bytes)
@@ -637,23 +541,17 @@ void launch_apply3(int l_max, bool gsm, dim3 blocks, size_t smem, cudaStream_t s
 #undef CNM_LAUNCH3
 #undef CNM_LAUNCH3G
 }
-void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
-                        const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
-                        const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
-                        const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0, int slo1,
-                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge, const Krylov *gate)
+void launch_diag3(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
+                  const BlockTable &bt, const ApplyPlan &pl, const DiagArgs &d)
 {
     const int smax = smax_for(l_max);
-#define CNM_LAUNCH(S)                                                                                        \
-    if (smax == S) {                                                                                         \
-        k_diagnostics2<S><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, hh, theta, domega, psi, idx_ex,    \
-                                                               n_sinks, sv0, sv1, sink_dots, sink_coef0,     \
-                                                               sink_coef1, slo0, shi0, slo1, shi1, partials, \
-                                                               dpsi_edge, psi_edge, gate);                   \
-        return;                                                                                              \
+#define CNM_LAUNCHD(S)                                                           \
+    if (smax == S) {                                                             \
+        k_diag3<S><<<blocks, APPLY_THREADS, smem, st>>>(g, ct, bt, pl, d);       \
+        return;                                                                  \
     }
-    CNM_FOR_SMAX(CNM_LAUNCH)
-#undef CNM_LAUNCH
+    CNM_FOR_SMAX(CNM_LAUNCHD)
+#undef CNM_LAUNCHD
 }
 
 // ------------------------------------------------------------------ sink projections

@@ -5,7 +5,6 @@
 
 namespace cnm {
 
-constexpr int APPLY_TILE = 32;      // radial nodes per CTA in the operator kernels (= warp width)
 constexpr int APPLY_THREADS = 256;  // 8 warps share the rows of a tile
 constexpr int SCAN_THREADS = 256;   // preconditioner scan CTAs (per-thread chunk kernels)
 constexpr int SCAN2_THREADS = 512;  // staged preconditioner scan CTAs
@@ -66,20 +65,37 @@ enum Ticket : int { TK_APPLY_T = 0, TK_UPDATE_T = 1, TK_START_T = 2, TK_WOOD_T =
 
 __global__ void k_hh_table(double *hh, const double *r, int Nr, int K, double R1, double R2, double q,
                            double scale, double a1, double a2);
-// Register-blocked operator kernels (templated on the widest Gaunt block), launched
-// through these host functions.
-cudaError_t set_operator_smem(int diag_bytes);
-// Two-nodes-per-thread operator kernel on 64-node tiles with a two-row blocked table.
+// Two-nodes-per-thread operator kernel on 64-node tiles with a two-row blocked table
+// (templated on the widest Gaunt block), launched through these host functions.
 constexpr int APPLY3_TILE = 64;
 cudaError_t set_apply3_smem(int bytes);
 const void *apply3_kernel(int l_max, int vpart, bool gsm);
 void launch_apply3(int l_max, bool gsm, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
                    const CouplingTable &ct, const BlockTable &bt, const ApplyPlan &pl, const ApplyArgs &a);
-void launch_diagnostics(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g,
-                        const CouplingTable &ct, const BlockTable &bt, const double *hh, double theta, double domega,
-                        const double2 *psi, int idx_ex, int n_sinks, const double2 *sv0, const double2 *sv1,
-                        const double2 *sink_dots, double sink_coef0, double sink_coef1, int slo0, int shi0, int slo1,
-                        int shi1, double *partials, double2 *dpsi_edge, double2 *psi_edge, const Krylov *gate);
+// Arguments of the diagnostics pass (k_diag3, and k_diag5 for l_max <= 8): H psi,
+// V psi, dV/dt psi and dpsi/dt on nodes <= idx_ex, reduced into per-CTA partials
+// [slot][block]: slots 0..n-1 norms, n..2n-1 energies, 2n edge energy, 2n+1 p_bin,
+// 2n+2 dV; dpsi/dt and psi around idx_ex stored for the fluxes).
+struct DiagArgs {
+    const double *hh;
+    double theta, domega;
+    const double2 *psi;
+    int idx_ex;
+    int n_sinks;
+    const double2 *sv0, *sv1, *sink_dots;
+    double sink_coef0, sink_coef1;
+    int slo0, shi0, slo1, shi1;
+    double *partials;
+    double2 *dpsi_edge, *psi_edge;
+    const struct Krylov *gate;  // skip until the step's candidate is accepted (null: always run)
+};
+
+// The diagnostics pass on the operator kernel's tiles and work plan (grid: tiles up to
+// idx_ex x row groups; the partials' stride is the grid's size).
+cudaError_t set_diag3_smem(int bytes);
+const void *diag3_kernel(int l_max);
+void launch_diag3(int l_max, dim3 blocks, size_t smem, cudaStream_t st, const Grid &g, const CouplingTable &ct,
+                  const BlockTable &bt, const ApplyPlan &pl, const DiagArgs &d);
 __global__ void k_sink_dots(const double2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,
                             const double2 *v1, int lo0, int hi0, int lo1, int hi1, double2 *dots, const Krylov *gate,
                             int gate_mode);

@@ -164,30 +164,16 @@ __device__ __forceinline__ void tc_commit(uint32_t bar)
                  : "memory");
 }
 
-// 8 consecutive fp32 columns of this warp's 32 TMEM lanes.
-__device__ __forceinline__ void tmem_ld8(uint32_t taddr, float (&v)[8])
+// 32 consecutive fp32 columns of this warp's 32 TMEM lanes.
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
 {
-    uint32_t r[8];
-    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0,%1,%2,%3,%4,%5,%6,%7}, [%8];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+    uint32_t r[32];
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
                  : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-    for (int q = 0; q < 8; ++q) v[q] = __uint_as_float(r[q]);
-}
-
-// 16 consecutive fp32 columns of this warp's 32 TMEM lanes.
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16])
-{
-    uint32_t r[16];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-    for (int q = 0; q < 16; ++q) v[q] = __uint_as_float(r[q]);
+    for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
 }
 
 __device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
@@ -204,18 +190,30 @@ constexpr int TC_WORKERS = 512;              // operand producers and epilogue (
 constexpr int TC_THREADS = TC_WORKERS + 32;  // + the copy / MMA warp (warp 16)
 constexpr int TC_CTRL = TC_WORKERS / 32;     // the copy / MMA warp
 constexpr int TC_GMAX = 8, TC_BSTAGES = 2;  // at most 8 Gaunt stages (the plan sets how many)
-constexpr int TC_NT = 128;                   // nodes per tile: 2 x 64-node halves, one MMA M-tile each
+constexpr int TC_NT = 128;                   // nodes per tile: 256 node-component rows, the MMA's N
+constexpr int TC_KMAX = 32;                  // multipoles (2 l_max + 1) the kernel handles
+constexpr int TC_WS = 2 * TC_NT + 4;         // row stride (floats) of the accumulator image W[j][m]:
+                                             // 16-byte stores of 8 consecutive rows hit distinct banks
 constexpr float TC_HCUT = 1e-9f;             // multipoles below this fraction of the monopole are skipped
+
+// Bytes of the region that holds the Z stages and, in the epilogue, the accumulator image.
+__host__ __device__ constexpr size_t tc_zregion(int kp)
+{
+    return (size_t)TC_BSTAGES * kp * 2 * TC_NT * 2 > (size_t)kp * TC_WS * 4 ? (size_t)TC_BSTAGES * kp * 2 * TC_NT * 2
+                                                                              : (size_t)kp * TC_WS * 4;
+}
 
 struct TcShared {
     unsigned long long gfull[TC_GMAX], gfree[TC_GMAX], zfull[TC_BSTAGES], zfree[TC_BSTAGES];
     unsigned long long accfull, accfree, tinfo, drain;
     uint32_t tmem_base;
-    int lcut[2];
+    int lcut[2];        // multipole cut of the tile in flight (-1: no further tile)
+    int tile[2];        // tile index drawn from the launch's counter
     int lcut_red;
     int pmax_bits;      // largest |h z| of the tile (float bits, non-negative)
     int abort;
-    int l_off[64], l_bytes[64], l_nblk[64];
+    int l_off[TC_KMAX], l_bytes[TC_KMAX], l_nblk[TC_KMAX];
+    int slices[TC_KMAX * 16];
 };
 
 // Bulk copy of multipole lv's Gaunt blocks into the G stage of use v (v % gst).
@@ -233,15 +231,17 @@ __device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_sta
 }
 
 // y = alpha x + beta (H0 x + V x + CAP x) + sinks on complex64 vectors, the coupling on the
-// tensor cores.  A tile is TC_NT nodes; its 2 TC_NT rows m = 2 node + (0: Re, 1: Im) form
-// the MMA's A operand Z_l*[m, k] = h_l*(r_node) z_k(r_node)_(Re|Im) (two M-tiles of 128
-// rows), the Gaunt matrix G_l* is the B operand (N = KP rows j, K-major), and
-// D[m, j] = sum_l* sum_k Z_l*[m, k] G_l*[j, k] accumulates in TMEM (M-tile t at columns
-// [t KP, (t + 1) KP)).  Worker thread w produces row m = w of the A operand; in the
-// epilogue warp w reads TMEM lanes 32 (w % 4) .. of M-tile w / 4, i.e. 16 consecutive
-// nodes, Re and Im in adjacent lanes, so every global access of a warp is one 128-byte
-// line per mode.  Warp 8 copies G stages and issues the MMAs (one thread).  Grid:
-// persistent CTAs, tile t = blockIdx.x + q gridDim.x.
+// tensor cores.  A tile is TC_NT nodes; its 2 TC_NT node-component rows m = 2 node + (0: Re,
+// 1: Im) of Z_l*[m, k] = h_l*(r_node) z_k(r_node)_(Re|Im) form the MMA's B operand (N = 256,
+// K-major), the Gaunt matrix G_l* (M = 128 rows j, K-major) its A operand, and
+// D[j, m] = sum_l* sum_k G_l*[j, k] Z_l*[m, k] accumulates in one fp32 TMEM accumulator
+// (lane j, column m).  Worker thread w produces operand row m = w % 256 for half of the
+// columns k (w / 256); in the epilogue warp w reads TMEM lanes 32 (w % 4) .. (its quarter of
+// the modes j) and a quarter of the columns, writes them to shared memory, and the workers
+// then form one complex output per (mode, node), consecutive threads on consecutive nodes.
+// Warp 16 copies Gaunt stages and issues the MMAs (one thread).  Tiles are drawn from a
+// per-handle counter (tile_ctr[0]; the last CTA to finish resets it), so a CTA that got
+// light tiles (few multipoles above the cut, far from the bodies) takes more of them.
 template <int KP>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int g_stage,
@@ -261,16 +261,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // read the same lines of L2 at once
     const uint8_t *gblob = tt.blob + (size_t)(blockIdx.x % tt.replicas) * tt.replica_bytes;
     uint8_t *Gst = tc_smem;                                              // gst x g_stage
-    uint8_t *Zst = Gst + (size_t)gst * g_stage;                          // TC_BSTAGES x Z_STAGE
+    uint8_t *Zst = Gst + (size_t)gst * g_stage;                          // Z stages / accumulator image
     // copies run gst - 1 uses ahead; a tile's first gst - 1 uses are copied before its cut is
     // known, so every tile runs at least multipoles 0 .. gst - 2
     const int lc_min = max(1, gst - 2);
-    float *hs = reinterpret_cast<float *>(Zst + (size_t)TC_BSTAGES * Z_STAGE);  // K x TC_NT
+    float *hs = reinterpret_cast<float *>(Zst + tc_zregion(KP));        // K x TC_NT
     float2 *ph = reinterpret_cast<float2 *>(hs + (size_t)K * TC_NT);    // KP phases e^{i m_k theta}
     float *cent = reinterpret_cast<float *>(ph + KP);                   // KP: l (l + 1) / (2 mu)
     float *ir2s = cent + KP;                                             // TC_NT: 1 / r^2 of the tile
     float *caps = ir2s + TC_NT;                                          // TC_NT: CAP weights of the tile
-    float *hmx = caps + TC_NT;                                           // TC_NT: max_l* |h_l*| per node
     volatile int *abort = &sh.abort;
 
     if (tid == 0) {
@@ -296,6 +295,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         sh.l_bytes[l] = tt.l_bytes[l];
         sh.l_nblk[l] = tt.l_nblk[l];
     }
+    for (int e = tid; e < K * 16; e += TC_THREADS) sh.slices[e] = tt.slices[e];
     for (int k = tid; k < KP; k += TC_THREADS) {
         float s = 0.f, c = 0.f;
         if (k < n) sincosf((float)mode_m[k] * a.theta, &s, &c);
@@ -304,7 +304,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         cent[k] = (float)((double)(l * (l + 1)) / (2.0 * g.mu));
     }
     if (warp == TC_CTRL) {
-        // TMEM accumulators: 2 M-tiles x KP fp32 columns x 128 lanes
+        // TMEM accumulator: 128 lanes x 256 fp32 columns
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&sh.tmem_base)),
                      "r"(NCOLS)
                      : "memory");
@@ -320,14 +320,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (lane == 0) {
             int u = 0;       // multipole uses issued so far (all tiles)
             int copies = 0;
-            int it = 0;
-            const int first = blockIdx.x;
-            if (first < tiles)
-                for (; copies < gst - 1; ++copies) tc_issue_g(sh, Gst, g_stage, gst, gblob, copies, copies);
-            for (int tile = first; tile < tiles; tile += gridDim.x, ++it) {
+            // the first tile's first gst - 1 multipoles (copied even if this CTA draws no
+            // tile: the drain below waits for them)
+            for (; copies < gst - 1; ++copies) tc_issue_g(sh, Gst, g_stage, gst, gblob, copies, copies);
+            // a CTA runs at most `tiles` tiles; the bound only matters after a wait gave up
+            for (int it = 0; it < tiles; ++it) {
                 mbar_wait(smem_addr(&sh.tinfo), it & 1, abort);
                 const int lc = sh.lcut[it & 1];
-                const bool more = tile + (int)gridDim.x < tiles;
+                if (lc < 0) break;
                 if (it > 0) mbar_wait(smem_addr(&sh.accfree), (it - 1) & 1, abort);
                 tc_fence_after();
                 bool firstmma = true;
@@ -343,7 +343,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     // MMA per non-zero slice of G_l*: every tcgen05.mma of K = 16 costs about the
                     // same whatever its N, so N is kept at its maximum
                     for (int q = 0; q < nb; ++q) {
-                        const int s16 = tt.slices[l * 16 + q];
+                        const int s16 = sh.slices[l * 16 + q];
                         const uint64_t ad = sdesc(gbase + (uint32_t)(q * G_BLK), (uint32_t)G_LBO, 128u);
                         const uint64_t bd = sdesc(zbase + (uint32_t)(s16 * 2 * LBO_Z), (uint32_t)LBO_Z, 128u);
                         tc_mma(tmem, ad, bd, IDESC, firstmma ? 0u : 1u);
@@ -351,17 +351,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     tc_commit(smem_addr(&sh.gfree[sg]));
                     tc_commit(smem_addr(&sh.zfree[sz]));
-                    // refill: use u + gst - 1 goes into the G stage of use u - 1 (in the next
-                    // tile it is one of multipoles 0 .. gst - 2, which every tile runs)
+                    // refill: use u + gst - 1 goes into the G stage of use u - 1; past this
+                    // tile's cut it is one of the next tile's multipoles 0 .. gst - 2, which
+                    // every tile runs (copied whether or not a next tile comes)
                     const int ahead = gst - 1;
-                    int lnext = -1;
-                    if (l + ahead <= lc) lnext = l + ahead;
-                    else if (more) lnext = l + ahead - (lc + 1);
-                    if (lnext >= 0) {
-                        if (u >= 1) mbar_wait(smem_addr(&sh.gfree[(u - 1) % gst]), ((u - 1) / gst) & 1, abort);
-                        tc_issue_g(sh, Gst, g_stage, gst, gblob, u + ahead, lnext);
-                        ++copies;
-                    }
+                    const int lnext = l + ahead <= lc ? l + ahead : l + ahead - (lc + 1);
+                    if (u >= 1) mbar_wait(smem_addr(&sh.gfree[(u - 1) % gst]), ((u - 1) / gst) & 1, abort);
+                    tc_issue_g(sh, Gst, g_stage, gst, gblob, u + ahead, lnext);
+                    ++copies;
                 }
                 tc_commit(smem_addr(&sh.accfull));
             }
@@ -390,9 +387,45 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (a.dot_kind[d] == 4) ext64 = a.dot_ext64;
         }
         const float2 *__restrict__ xg = a.x;
-        int u = 0, it = 0;
-        for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++it) {
+        int u = 0;
+        for (int it = 0;; ++it) {
+            // the next tile (the barrier first: every worker has finished the previous
+            // epilogue and read the previous tile index)
+            if (tid == 0) sh.tile[it & 1] = atomicAdd(a.tile_ctr, 1);
+            workers_sync();
+            const int tile = sh.tile[it & 1];
+            if (tile >= tiles) {
+                if (tid == 0) {
+                    sh.lcut[it & 1] = -1;
+                    mbar_arrive(smem_addr(&sh.tinfo));
+                }
+                break;
+            }
             const int i0 = tile * TC_NT;
+            // radial weights of the tile (K x TC_NT, independent loads spread over the
+            // workers), 1/r^2 and the CAP weights of its nodes
+            {
+                constexpr int HPT = TC_KMAX * TC_NT / TC_WORKERS;
+                double hv[HPT];
+#pragma unroll
+                for (int q = 0; q < HPT; ++q) {
+                    const int e = tid + q * TC_WORKERS;
+                    const int l = e / TC_NT, i = i0 + (e % TC_NT);
+                    hv[q] = (l < K && a.use_v && i >= 1 && i <= Nr - 2) ? a.hh[(int64_t)l * Nr + i] : 0.0;
+                }
+                if (tid < TC_NT) {
+                    const int i = i0 + tid;
+                    ir2s[tid] = i < Nr ? (float)g.ir2[i] : 0.f;
+                } else if (tid < 2 * TC_NT) {
+                    const int i = i0 + tid - TC_NT;
+                    caps[tid - TC_NT] = (g.capw && i < Nr) ? (float)g.capw[i] : 0.f;
+                }
+#pragma unroll
+                for (int q = 0; q < HPT; ++q) {
+                    const int e = tid + q * TC_WORKERS;
+                    if (e < K * TC_NT) hs[e] = (float)hv[q];
+                }
+            }
             // z_k of this row's node and component (e^{i m_k theta} x_k), k in this thread's half
             float zc[KH];
             {
@@ -406,34 +439,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     zc[kk] = zc_comp ? p.x * xv.y + p.y * xv.x : p.x * xv.x - p.y * xv.y;
                 }
             }
-            // radial weights, 1/r^2 and CAP of the tile's nodes and the multipole cut (the
-            // barrier first: every worker has finished the previous epilogue)
-            workers_sync();
-            if (tid < TC_NT) {
-                const int i = i0 + tid;
-                int lcl = 0;
-                double h0 = 0.0;
-                float hm = 0.f;
-                for (int l = 0; l < K; ++l) {
-                    double h = 0.0;
-                    if (a.use_v && i >= 1 && i <= Nr - 2) h = a.hh[(int64_t)l * Nr + i];
-                    if (l == 0) h0 = fabs(h);
-                    else if (fabs(h) > (double)TC_HCUT * h0) lcl = l;
-                    hs[l * TC_NT + tid] = (float)h;
-                    hm = fmaxf(hm, fabsf((float)h));
-                }
-                if (lcl > 0) atomicMax(&sh.lcut_red, lcl);
-                hmx[tid] = hm;
-                ir2s[tid] = i < Nr ? (float)g.ir2[i] : 0.f;
-                caps[tid] = (g.capw && i < Nr) ? (float)g.capw[i] : 0.f;
-            }
             workers_sync();
             {
-                // the tile's operand scale: S = 2^se with max |S h z| < 2^14 (fp16 range)
+                // the multipole cut (the highest l* above TC_HCUT of the monopole at some node
+                // of the tile) and the operand scale S = 2^se with max |S h z| < 2^14: every
+                // thread evaluates its own node, a warp reduction, one atomic per warp
+                const float h0 = fabsf(hs[zc_node]);
+                int lcl = 0;
+                float hm = h0;
+                for (int l = 1; l < K; ++l) {
+                    const float h = fabsf(hs[l * TC_NT + zc_node]);
+                    if (h > TC_HCUT * h0) lcl = l;
+                    hm = fmaxf(hm, h);
+                }
                 float zm = 0.f;
 #pragma unroll
                 for (int k = 0; k < KH; ++k) zm = fmaxf(zm, fabsf(zc[k]));
-                atomicMax(&sh.pmax_bits, __float_as_int(zm * hmx[zc_node]));
+                const int lw = __reduce_max_sync(0xffffffffu, lcl);
+                const int pw = __reduce_max_sync(0xffffffffu, __float_as_int(zm * hm));  // non-negative floats
+                if (lane == 0) {
+                    if (lw > 0) atomicMax(&sh.lcut_red, lw);
+                    atomicMax(&sh.pmax_bits, pw);
+                }
             }
             workers_sync();
             const int lc = max(lc_min, sh.lcut_red);
@@ -457,7 +484,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 sh.pmax_bits = 0;
                 mbar_arrive(smem_addr(&sh.tinfo));
             }
-            // A operand rows, one multipole per stage
+            // B operand rows, one multipole per stage
             for (int l = 0; l <= lc; ++l, ++u) {
                 const int sz = u % TC_BSTAGES;
                 if (u >= TC_BSTAGES) mbar_wait(smem_addr(&sh.zfree[sz]), ((u / TC_BSTAGES) - 1) & 1, abort);
@@ -476,21 +503,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 __syncwarp();
                 if (lane == 0) mbar_arrive(smem_addr(&sh.zfull[sz]));
             }
-            // epilogue, phase 1: the accumulators to shared memory, W[j][m] (the Z stages are
-            // idle until this thread's next operand rows)
+            // epilogue, phase 1: the accumulator to shared memory, W[j][m] with row stride
+            // TC_WS (the Z stages are idle until the next tile's operand rows)
             mbar_wait(smem_addr(&sh.accfull), it & 1, abort);
             tc_fence_after();
             float *W = reinterpret_cast<float *>(Zst);
             {
                 const uint32_t taddr = tmem + ((uint32_t)(32 * q4) << 16);
                 const int j = 32 * q4 + lane;
+                float *wrow = W + (size_t)j * TC_WS;
 #pragma unroll 1
-                for (int col = cq * (TC_NT / 2); col < (cq + 1) * (TC_NT / 2); col += 8) {
-                    float wv[8];
-                    tmem_ld8(taddr + (uint32_t)col, wv);
+                for (int col = cq * (TC_NT / 2); col < (cq + 1) * (TC_NT / 2); col += 32) {
+                    float wv[32];
+                    tmem_ld32(taddr + (uint32_t)col, wv);
                     if (j < n)
 #pragma unroll
-                        for (int q = 0; q < 8; ++q) W[j * (2 * TC_NT) + col + q] = wv[q];
+                        for (int q = 0; q < 32; q += 4)
+                            *reinterpret_cast<float4 *>(wrow + col + q) = make_float4(wv[q], wv[q + 1], wv[q + 2], wv[q + 3]);
                 }
             }
             tc_fence_before();
@@ -498,13 +527,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             if (lane == 0) mbar_arrive(smem_addr(&sh.accfree));
             workers_sync();
             // phase 2: one complex output per (mode j, node) and thread, consecutive threads
-            // on consecutive nodes of one mode (coalesced loads and stores)
+            // on consecutive nodes of one mode (coalesced loads and stores); a warp's lanes
+            // hold 32 consecutive nodes, so the stencil's neighbours come by shuffles and
+            // only the first lane's left and the last lane's right neighbour are loaded
             {
                 const int tile_nodes = min(TC_NT, Nr - i0);
                 constexpr int EB = 4;  // elements in flight per thread
+                float2 *__restrict__ yg = a.y;
 #pragma unroll 1
                 for (int e0 = tid; e0 < n * TC_NT; e0 += EB * TC_WORKERS) {
-                    float2 x0[EB], xm[EB], xp[EB], w[EB];
+                    float2 x0[EB], xh[EB], w[EB];
+                    double2 ev[EB];
 #pragma unroll
                     for (int q = 0; q < EB; ++q) {
                         const int e = e0 + q * TC_WORKERS;
@@ -514,12 +547,27 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         const int64_t o = (int64_t)j * Nr + i;
                         const float2 zero = make_float2(0.f, 0.f);
                         x0[q] = ok ? __ldg(xg + o) : zero;
-                        xm[q] = (ok && i >= 1) ? __ldg(xg + o - 1) : zero;
-                        xp[q] = (ok && i + 1 < Nr) ? __ldg(xg + o + 1) : zero;
-                        w[q] = ok ? *reinterpret_cast<const float2 *>(W + j * (2 * TC_NT) + 2 * c) : zero;
+                        xh[q] = zero;
+                        if (ok && lane == 0 && i >= 1) xh[q] = __ldg(xg + o - 1);
+                        if (ok && lane == 31 && i + 1 < Nr) xh[q] = __ldg(xg + o + 1);
+                        w[q] = ok ? *reinterpret_cast<const float2 *>(W + j * TC_WS + 2 * c) : zero;
+                        ev[q] = make_double2(0.0, 0.0);
+                        if (ok && ext32) {
+                            const float2 t = __ldg(ext32 + o);
+                            ev[q] = make_double2(t.x, t.y);
+                        } else if (ok && ext64) {
+                            ev[q] = __ldg(ext64 + o);
+                        }
                     }
 #pragma unroll
                     for (int q = 0; q < EB; ++q) {
+                        float2 xm, xp;
+                        xm.x = __shfl_up_sync(0xffffffffu, x0[q].x, 1);
+                        xm.y = __shfl_up_sync(0xffffffffu, x0[q].y, 1);
+                        xp.x = __shfl_down_sync(0xffffffffu, x0[q].x, 1);
+                        xp.y = __shfl_down_sync(0xffffffffu, x0[q].y, 1);
+                        if (lane == 0) xm = xh[q];
+                        if (lane == 31) xp = xh[q];
                         const int e = e0 + q * TC_WORKERS;
                         const int j = e / TC_NT, c = e - j * TC_NT;
                         if (!(e < n * TC_NT && c < tile_nodes)) continue;
@@ -532,8 +580,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                 // H0 x = ad ((x - x_-) + (x - x_+)) + l (l + 1) / (2 mu r^2) x: the
                                 // differences of neighbours are exact for a smooth x
                                 const float cen = cent[j] * ir2s[c];
-                                hr = ad * ((x0[q].x - xm[q].x) + (x0[q].x - xp[q].x)) + cen * x0[q].x;
-                                hi = ad * ((x0[q].y - xm[q].y) + (x0[q].y - xp[q].y)) + cen * x0[q].y;
+                                hr = ad * ((x0[q].x - xm.x) + (x0[q].x - xp.x)) + cen * x0[q].x;
+                                hi = ad * ((x0[q].y - xm.y) + (x0[q].y - xp.y)) + cen * x0[q].y;
                             }
                             if (a.use_v) {  // conj(ph_j) w
                                 const float2 p = ph[j];
@@ -557,27 +605,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                                 yr += (float)(cr * vv.x - ci * vv.y);
                                 yi += (float)(cr * vv.y + ci * vv.x);
                             }
-                        a.y[o] = make_float2(yr, yi);
+                        yg[o] = make_float2(yr, yi);
                         const double yrd = yr, yid = yi;
 #pragma unroll
                         for (int d = 0; d < 3; ++d) {
                             if (d >= a.n_dots) break;
                             double dr_ = 0.0, di_ = 0.0;
                             const int kd = a.dot_kind[d];
-                            if (kd == 1 || kd == 2) {
-                                const float2 ev = __ldg(ext32 + o);
-                                if (kd == 1) {  // conj(e) y
-                                    dr_ = (double)ev.x * yrd + (double)ev.y * yid;
-                                    di_ = (double)ev.x * yid - (double)ev.y * yrd;
-                                } else {        // conj(y) e
-                                    dr_ = yrd * (double)ev.x + yid * (double)ev.y;
-                                    di_ = yrd * (double)ev.y - yid * (double)ev.x;
-                                }
+                            if (kd == 1) {  // conj(e) y
+                                dr_ = ev[q].x * yrd + ev[q].y * yid;
+                                di_ = ev[q].x * yid - ev[q].y * yrd;
+                            } else if (kd == 2) {  // conj(y) e
+                                dr_ = yrd * ev[q].x + yid * ev[q].y;
+                                di_ = yrd * ev[q].y - yid * ev[q].x;
                             } else if (kd == 3) {
                                 dr_ = yrd * yrd + yid * yid;
-                            } else {            // |e64 - y|^2
-                                const double2 e64 = __ldg(ext64 + o);
-                                const double ddr = e64.x - yrd, ddi = e64.y - yid;
+                            } else {  // |e64 - y|^2
+                                const double ddr = ev[q].x - yrd, ddi = ev[q].y - yid;
                                 dr_ = ddr * ddr + ddi * ddi;
                             }
                             dacc[2 * d] += dr_;
@@ -605,7 +649,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
     }
     __syncthreads();
-    if (tid == 0 && sh.abort && a.status) atomicOr(a.status, 16);
+    if (tid == 0) {
+        if (sh.abort && a.status) atomicOr(a.status, 16);
+        // the last CTA to finish resets the tile counter for the next launch on the stream
+        __threadfence();
+        if (atomicAdd(a.tile_ctr + 1, 1) == (int)gridDim.x - 1) {
+            atomicExch(a.tile_ctr, 0);
+            atomicExch(a.tile_ctr + 1, 0);
+        }
+    }
     if (warp == TC_CTRL) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(NCOLS) : "memory");
@@ -619,10 +671,9 @@ bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
 {
     p.kp = (n_modes + 15) / 16 * 16;
     p.nt = TC_NT;
-    if (p.kp > 112 || K > 64) return false;
+    if (p.kp > 112 || K > TC_KMAX) return false;
     p.a_stage = (g_stage_bytes + 127) / 128 * 128;
-    const size_t fixed = (size_t)TC_BSTAGES * p.kp * 2 * TC_NT * 2 + (size_t)K * TC_NT * 4 + (size_t)p.kp * 12 +
-                         (size_t)3 * TC_NT * 4 + 128;
+    const size_t fixed = tc_zregion(p.kp) + (size_t)K * TC_NT * 4 + (size_t)p.kp * 12 + (size_t)2 * TC_NT * 4 + 128;
     // as many Gaunt stages as fit (3 to 8, at most K: every tile runs gst - 1 multipoles)
     const size_t budget = 220 * 1024;
     p.gst = (int)std::min<size_t>(TC_GMAX, budget > fixed ? (budget - fixed) / std::max(p.a_stage, 128) : 0);

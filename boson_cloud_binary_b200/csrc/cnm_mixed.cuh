@@ -59,7 +59,9 @@ constexpr int TC_REPLICAS = 16;
 // Arguments of one tensor-core operator application on complex64 vectors:
 //   y = alpha x + beta (c_h0 H0 x + V x + CAP x) + sum_a coef_a (v_a^dag x) v_a,
 // with up to three fused fp64 reductions of y (per-CTA partials, [slot][block]):
-//   kind 1 conj(e) . y,  2 conj(y) . e,  3 |y|^2,  4 |e64 - y|^2 (e64 complex128).
+//   kind 1 conj(e) . y,  2 conj(y) . e,  3 |y|^2,  4 |e64 - y|^2 (e64 complex128);
+// a launch's reductions read at most one external operand (kinds 1 and 2 the same e,
+// and kind 4 not beside them).
 struct TcArgs {
     const float2 *x;
     float2 *y;
@@ -78,6 +80,7 @@ struct TcArgs {
     const double2 *dot_ext64;
     double *partials;         // [slot][gridDim.x]
     int *status;              // bit 4: an mbarrier wait gave up
+    int *tile_ctr;            // [2]: next tile, finished CTAs (zero between launches)
 };
 
 // Host entry points (cnm_mixed.cu).

@@ -257,10 +257,11 @@ int cnm_sink_vector(const cnm_handle *h, int32_t body, double *out);
 int cnm_set_profiling(cnm_handle *h, int32_t on);
 int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *launches);
 int cnm_timer_start(cnm_handle *h);
-/* Tensor-core operator layout of a CNM_MIXED handle: the padded mode count and, for each
- * of the 2 l_max + 1 multipoles, the number of non-zero 16-column slices of its Gaunt
- * matrix (one MMA per slice and 64-node half tile). */
-int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk);
+/* Tensor-core operator layout of a CNM_MIXED handle: the padded mode count, for each of
+ * the 2 l_max + 1 multipoles the number of non-zero 16-column slices of its Gaunt matrix
+ * (one M128 x N256 x K16 MMA per slice and 128-node tile), and the highest multipole every
+ * tile runs whatever its radial cut (any pointer may be NULL). */
+int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk, int32_t *lc_min);
 /* Kernels the handle has launched since its creation (every launch site counts). */
 int cnm_launch_count(const cnm_handle *h, int64_t *count);
 int cnm_timer_stop(cnm_handle *h, double *ms);

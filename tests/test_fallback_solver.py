@@ -39,3 +39,50 @@ def test_point_jacobi_fallback_matches_block_solve():
     assert err < 1e-11, f"fallback solve differs from the oracle's block solve by {err:.3e}"
     # the weaker preconditioner needs more iterations: the retry path really ran
     assert sum(its_fallback) > sum(its_block)
+
+
+def _gpu_case(max_iterations, accept_residual=1e-9, steps=3):
+    from boson_cloud_binary_b200 import CrankNicolsonModes  # noqa: F401
+    args = (48, 120.0, 0.2, 0.1, 3, 0.2, 0.01, 0.2, 0.0, 30.0, False, True, 10, 0.0, 10.0)
+    cn = make("gpu", *args)
+    cn.evolve_orbit = True
+    cn.theta = 0.3
+    cn.Omega = cn.Omega_0
+    cn.tolerance = 1e-14
+    cn.max_iterations = max_iterations
+    cn.accept_residual = accept_residual
+    i = np.arange(48 * cn.n_modes)
+    init = np.where((i % 48 == 0) | (i % 48 == 47), 0, (0.1 + 0.001 * i) * np.exp(1j * 0.1 * i))
+    cn.set_initial_state_full(init / np.linalg.norm(init))
+    cn.initialize()
+    cn.run(steps + 1, 60.0)
+    return cn
+
+
+@pytest.mark.gpu
+def test_failed_block_attempt_retries_with_point_jacobi():
+    """A radial-block attempt capped at one BiCGSTAB iteration misses the acceptance
+    residual 1e-9 (_matrices.cpp:158-174 then fall back, :175-186): the retry must run,
+    take more than the capped iteration, and land on the oracle's block solve."""
+    ref, _ = _run("oracle", True)
+    cn = _gpu_case(max_iterations=1)
+    its = []
+    for k in range(1, 4):
+        cn.step(k)
+        its.append(cn.last_solver_iterations)
+        assert cn.last_solver_residual <= 1e-9
+    # the accepted solve is the retry's: the capped attempt stops after one iteration
+    assert min(its) > 1, its
+    got = np.array(cn.psi)
+    err = np.linalg.norm(got - ref) / np.linalg.norm(ref)
+    assert err < 1e-11, f"fallback after a failed block attempt differs from the oracle by {err:.3e}"
+
+
+@pytest.mark.gpu
+def test_solve_error_when_both_attempts_fail():
+    """With an acceptance residual no solve reaches, the block attempt and the retry both
+    fail; the step raises the reference's std::runtime_error (SolveError, CNM_ESOLVE)."""
+    from boson_cloud_binary_b200.cnm import SolveError
+    cn = _gpu_case(max_iterations=1, accept_residual=1e-300)
+    with pytest.raises(SolveError):
+        cn.step(1)
