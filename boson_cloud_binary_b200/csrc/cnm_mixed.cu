@@ -131,6 +131,13 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t
                  : "memory");
 }
 
+// 8-byte asynchronous global -> shared copy (zero fill when `valid` is false: nothing is read)
+__device__ __forceinline__ void cp_async8(uint32_t dst, const void *src, bool valid)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;" ::"r"(dst), "l"(src), "r"(valid ? 8 : 0) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+
 __device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
 __device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
@@ -242,7 +249,9 @@ __device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_sta
 // Warp 16 copies Gaunt stages and issues the MMAs (one thread).  Tiles are drawn from a
 // per-handle counter (tile_ctr[0]; the last CTA to finish resets it), so a CTA that got
 // light tiles (few multipoles above the cut, far from the bodies) takes more of them.
-template <int KP>
+// DK fixes the launch's fused reductions at compile time: 0 none, 1 conj(e) . y,
+// 23 conj(y) . e and |y|^2, 4 |e64 - y|^2.
+template <int KP, int DK>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int g_stage,
                int gst)
@@ -378,14 +387,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // epilogue phase 1: TMEM lane quarter (warp % 4: modes j) and quarter of the columns
         const int q4 = warp & 3, cq = warp >> 2;
         const float2 al = a.alpha, be = a.beta;
-        double dacc[6] = {0, 0, 0, 0, 0, 0};
-        // the launch's one complex64 reduction operand (kinds 1, 2) and complex128 one (kind 4)
-        const float2 *__restrict__ ext32 = nullptr;
-        const double2 *__restrict__ ext64 = nullptr;
-        for (int d = 0; d < a.n_dots && d < 3; ++d) {
-            if (a.dot_kind[d] == 1 || a.dot_kind[d] == 2) ext32 = a.dot_ext[d];
-            if (a.dot_kind[d] == 4) ext64 = a.dot_ext64;
-        }
+        constexpr int NDOT = DK == 0 ? 0 : DK == 23 ? 2 : 1;
+        double dacc[4] = {0, 0, 0, 0};
+        // the launch's reduction operand: complex64 (kinds 1, 2) or complex128 (kind 4)
+        const float2 *__restrict__ ext32 = (DK == 1 || DK == 23) ? a.dot_ext[0] : nullptr;
+        const double2 *__restrict__ ext64 = DK == 4 ? a.dot_ext64 : nullptr;
         const float2 *__restrict__ xg = a.x;
         int u = 0;
         for (int it = 0;; ++it) {
@@ -404,9 +410,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int i0 = tile * TC_NT;
             // radial weights of the tile (K x TC_NT, independent loads spread over the
             // workers), 1/r^2 and the CAP weights of its nodes
+            constexpr int HPT = TC_KMAX * TC_NT / TC_WORKERS;
+            double hv[HPT];
             {
-                constexpr int HPT = TC_KMAX * TC_NT / TC_WORKERS;
-                double hv[HPT];
 #pragma unroll
                 for (int q = 0; q < HPT; ++q) {
                     const int e = tid + q * TC_WORKERS;
@@ -420,26 +426,37 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const int i = i0 + tid - TC_NT;
                     caps[tid - TC_NT] = (g.capw && i < Nr) ? (float)g.capw[i] : 0.f;
                 }
+            }
+            // z_k of this row's node and component (e^{i m_k theta} x_k), k in this thread's half,
+            // from the tile's x staged in the (idle) Z region by asynchronous copies: xs[k][c]
+            float zc[KH];
+            {
+                float2 *xs = reinterpret_cast<float2 *>(Zst);
+                constexpr int XPT = KP * TC_NT / TC_WORKERS;
+#pragma unroll
+                for (int q = 0; q < XPT; ++q) {
+                    const int e = tid + q * TC_WORKERS;
+                    const int k = e / TC_NT, i = i0 + (e % TC_NT);
+                    const bool valid = k < n && i < Nr;
+                    cp_async8(smem_addr(xs + e), valid ? (const void *)(xg + (int64_t)k * Nr + i) : (const void *)xg,
+                              valid);
+                }
+                // the radial weights land while the copies are in flight
 #pragma unroll
                 for (int q = 0; q < HPT; ++q) {
                     const int e = tid + q * TC_WORKERS;
                     if (e < K * TC_NT) hs[e] = (float)hv[q];
                 }
-            }
-            // z_k of this row's node and component (e^{i m_k theta} x_k), k in this thread's half
-            float zc[KH];
-            {
-                const int i = i0 + zc_node;
+                cp_async_wait_all();
+                workers_sync();
 #pragma unroll
                 for (int kk = 0; kk < KH; ++kk) {
                     const int k = khalf * KH + kk;
-                    float2 xv = make_float2(0.f, 0.f);
-                    if (k < n && i < Nr) xv = __ldg(xg + (int64_t)k * Nr + i);
+                    const float2 xv = xs[k * TC_NT + zc_node];
                     const float2 p = ph[k];
                     zc[kk] = zc_comp ? p.x * xv.y + p.y * xv.x : p.x * xv.x - p.y * xv.y;
                 }
             }
-            workers_sync();
             {
                 // the multipole cut (the highest l* above TC_HCUT of the monopole at some node
                 // of the tile) and the operand scale S = 2^se with max |S h z| < 2^14: every
@@ -537,6 +554,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll 1
                 for (int e0 = tid; e0 < n * TC_NT; e0 += EB * TC_WORKERS) {
                     float2 x0[EB], xh[EB], w[EB];
+                    // the reduction operand (complex64 widened, or complex128)
                     double2 ev[EB];
 #pragma unroll
                     for (int q = 0; q < EB; ++q) {
@@ -552,11 +570,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         if (ok && lane == 31 && i + 1 < Nr) xh[q] = __ldg(xg + o + 1);
                         w[q] = ok ? *reinterpret_cast<const float2 *>(W + j * TC_WS + 2 * c) : zero;
                         ev[q] = make_double2(0.0, 0.0);
-                        if (ok && ext32) {
-                            const float2 t = __ldg(ext32 + o);
-                            ev[q] = make_double2(t.x, t.y);
-                        } else if (ok && ext64) {
-                            ev[q] = __ldg(ext64 + o);
+                        if constexpr (DK == 1 || DK == 23) {
+                            if (ok) {
+                                const float2 t = __ldg(ext32 + o);
+                                ev[q] = make_double2(t.x, t.y);
+                            }
+                        } else if constexpr (DK == 4) {
+                            if (ok) ev[q] = __ldg(ext64 + o);
                         }
                     }
 #pragma unroll
@@ -607,41 +627,32 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                             }
                         yg[o] = make_float2(yr, yi);
                         const double yrd = yr, yid = yi;
-#pragma unroll
-                        for (int d = 0; d < 3; ++d) {
-                            if (d >= a.n_dots) break;
-                            double dr_ = 0.0, di_ = 0.0;
-                            const int kd = a.dot_kind[d];
-                            if (kd == 1) {  // conj(e) y
-                                dr_ = ev[q].x * yrd + ev[q].y * yid;
-                                di_ = ev[q].x * yid - ev[q].y * yrd;
-                            } else if (kd == 2) {  // conj(y) e
-                                dr_ = yrd * ev[q].x + yid * ev[q].y;
-                                di_ = yrd * ev[q].y - yid * ev[q].x;
-                            } else if (kd == 3) {
-                                dr_ = yrd * yrd + yid * yid;
-                            } else {  // |e64 - y|^2
-                                const double ddr = ev[q].x - yrd, ddi = ev[q].y - yid;
-                                dr_ = ddr * ddr + ddi * ddi;
-                            }
-                            dacc[2 * d] += dr_;
-                            dacc[2 * d + 1] += di_;
+                        if constexpr (DK == 1) {  // conj(e) y
+                            dacc[0] += ev[q].x * yrd + ev[q].y * yid;
+                            dacc[1] += ev[q].x * yid - ev[q].y * yrd;
+                        } else if constexpr (DK == 23) {  // conj(y) e, |y|^2
+                            dacc[0] += yrd * ev[q].x + yid * ev[q].y;
+                            dacc[1] += yrd * ev[q].y - yid * ev[q].x;
+                            dacc[2] += yrd * yrd + yid * yid;
+                        } else if constexpr (DK == 4) {  // |e64 - y|^2
+                            const double ddr = ev[q].x - yrd, ddi = ev[q].y - yid;
+                            dacc[0] += ddr * ddr + ddi * ddi;
                         }
                     }
                 }
             }
         }
         // per-CTA partials of the fused reductions (fixed order: warps, then lanes)
-        if (a.n_dots > 0) {
+        if constexpr (NDOT > 0) {
             double *red = reinterpret_cast<double *>(hs);  // the h tile is no longer read
             workers_sync();
 #pragma unroll
-            for (int q = 0; q < 6; ++q) dacc[q] = warp_sum(dacc[q]);
+            for (int q = 0; q < 2 * NDOT; ++q) dacc[q] = warp_sum(dacc[q]);
             if (lane == 0)
 #pragma unroll
-                for (int q = 0; q < 6; ++q) red[q * TC_CTRL + warp] = dacc[q];
+                for (int q = 0; q < 2 * NDOT; ++q) red[q * TC_CTRL + warp] = dacc[q];
             workers_sync();
-            if (tid < 2 * a.n_dots) {
+            if (tid < 2 * NDOT) {
                 double s = 0.0;
                 for (int w = 0; w < TC_CTRL; ++w) s += red[tid * TC_CTRL + w];
                 a.partials[(int64_t)tid * gridDim.x + blockIdx.x] = s;
@@ -691,9 +702,13 @@ bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
 cudaError_t tc_prepare(const TcPlan &p)
 {
     cudaError_t e = cudaSuccess;
+#define CNM_TC_ATTR1(KP_, DK_)                                                                                 \
+    if (e == cudaSuccess)                                                                                      \
+        e = cudaFuncSetAttribute(k_tc_apply<KP_, DK_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
 #define CNM_TC_ATTR(KP_) \
-    if (p.kp == KP_) e = cudaFuncSetAttribute(k_tc_apply<KP_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+    if (p.kp == KP_) { CNM_TC_ATTR1(KP_, 0) CNM_TC_ATTR1(KP_, 1) CNM_TC_ATTR1(KP_, 23) CNM_TC_ATTR1(KP_, 4) }
     CNM_TC_PLANS(CNM_TC_ATTR)
+#undef CNM_TC_ATTR1
 #undef CNM_TC_ATTR
     return e;
 }
@@ -701,13 +716,26 @@ cudaError_t tc_prepare(const TcPlan &p)
 cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, const int *mode_l, const int *mode_m,
                             int K, const TcTable &tt, const TcArgs &a)
 {
-#define CNM_TC_LAUNCH(KP_)                                                                                      \
-    if (p.kp == KP_) {                                                                                          \
-        k_tc_apply<KP_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage, p.gst); \
-        return cudaGetLastError();                                                                              \
+    // the launch's reduction set (the combinations the mixed solve uses)
+    int dk = -1;
+    if (a.n_dots == 0) dk = 0;
+    else if (a.n_dots == 1 && a.dot_kind[0] == 1) dk = 1;
+    else if (a.n_dots == 2 && a.dot_kind[0] == 2 && a.dot_kind[1] == 3) dk = 23;
+    else if (a.n_dots == 1 && a.dot_kind[0] == 4) dk = 4;
+    if (dk < 0) return cudaErrorInvalidValue;
+#define CNM_TC_LAUNCH1(KP_, DK_)                                                                                  \
+    if (dk == DK_) {                                                                                              \
+        k_tc_apply<KP_, DK_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage,  \
+                                                                p.gst);                                           \
+        return cudaGetLastError();                                                                                \
+    }
+#define CNM_TC_LAUNCH(KP_)                                                                          \
+    if (p.kp == KP_) {                                                                              \
+        CNM_TC_LAUNCH1(KP_, 0) CNM_TC_LAUNCH1(KP_, 1) CNM_TC_LAUNCH1(KP_, 23) CNM_TC_LAUNCH1(KP_, 4) \
     }
     CNM_TC_PLANS(CNM_TC_LAUNCH)
 #undef CNM_TC_LAUNCH
+#undef CNM_TC_LAUNCH1
     return cudaErrorInvalidConfiguration;
 }
 

@@ -153,14 +153,14 @@ bool read_mode_list(const std::string &path, std::vector<mode> &out)
 CrankNicolsonModes::CrankNicolsonModes(int Nx, double L_, double dt_i, double epsilon_, int l_max_, double mu_,
                                        double M_c_, double q_, double a_, double R_, bool counter_, bool absorption,
                                        int save_every_, double ramp_periods, double epsilon_smear,
-                                       std::string config_file)
+                                       std::string config_file, int precision)
     : Nr(Nx), save_every(save_every_), l_max(l_max_), n_modes(0), epsilon(epsilon_), mu(mu_), q(q_), R(R_),
       theta(0), phase(0), Omega(0), Omega_0(0), P(0), R1(0), R2(0), M1(1), M2(q_), a(a_), L(L_), dr(0), dt(dt_i),
       counter(counter_), M_c(M_c_), config_file_(std::move(config_file)), ramp_periods_(ramp_periods),
       initial_period_(2.0 * M_PI / std::sqrt((1 + q_) / std::pow(R_, 3)))
 {
     cnm_params p{Nx, L_, dt_i, epsilon_, l_max_, mu_, M_c_, q_, a_, R_, counter_ ? 1 : 0, absorption ? 1 : 0,
-                 save_every_, ramp_periods, epsilon_smear, CNM_FP64};
+                 save_every_, ramp_periods, epsilon_smear, precision};
     const int rc = cnm_create(&p, &h_);
     if (rc != CNM_OK) raise(rc, cnm_create_error());
     int32_t n = 0;

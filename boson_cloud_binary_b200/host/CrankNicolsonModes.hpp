@@ -29,9 +29,11 @@ struct mode {
 
 class CrankNicolsonModes {
 public:
+    // The reference's constructor (include/CrankNicolsonModes.hpp:84); `precision` (CNM_FP64, the
+    // default, or CNM_MIXED) selects the solver path of the device handle.
     CrankNicolsonModes(int Nx, double L, double dt, double epsilon, int l_max, double mu, double M_c, double q,
                        double a, double R, bool counter, bool absorption, int save_every, double ramp_periods,
-                       double epsilon_smear, std::string config_file);
+                       double epsilon_smear, std::string config_file, int precision = CNM_FP64);
     ~CrankNicolsonModes();
     CrankNicolsonModes(const CrankNicolsonModes &) = delete;
     CrankNicolsonModes &operator=(const CrankNicolsonModes &) = delete;
