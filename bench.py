@@ -52,7 +52,58 @@ WORKLOADS = {
     "c1": dict(BASE, workload="fp64_single_binary_fixed_orbit_l4_N3000", Nr=3000, L=300.0, l_max=4, n_modes=15,
                mu=0.2, q=0.1, R=30.0, dt=1.0, r_ex=250.0, evolve_orbit=False, precision="fp64", tolerance=1e-10),
 }
+WORKLOADS["c4"] = dict(BASE, workload="batched_sweep_64_binaries_seed0", precision="mixed", tolerance=1e-12,
+                       batch_file="bench_c4_binaries.json")
 METRIC = "CN mode*node*steps/s"
+
+
+def c4_binaries(count=64, seed=0):
+    """The batched sweep's binaries, drawn per binary in this order from
+    numpy.random.default_rng(seed): q ~ U[0.05, 1], R ~ U[20, 80], mu from {0.1, 0.15, 0.2,
+    0.3}, l_max from {4, 6, 8, 10}, N ~ U{4000..32000} (L = N / 10), the initial state: a
+    hydrogenic (2,1,1) or (3,2,2) atom on the primary, or a spherical Gaussian of width
+    sigma ~ U[5, 20] (sigma drawn only for a Gaussian).  dt = 0.5, absorption on."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(count):
+        q = float(rng.uniform(0.05, 1.0))
+        R = float(rng.uniform(20.0, 80.0))
+        mu = float(rng.choice([0.1, 0.15, 0.2, 0.3]))
+        l_max = int(rng.choice([4, 6, 8, 10]))
+        N = int(rng.integers(4000, 32001))
+        kind = int(rng.integers(0, 3))
+        if kind == 0:
+            state = {"kind": "hydrogenic", "n": 2, "l": 1, "m": 1}
+        elif kind == 1:
+            state = {"kind": "hydrogenic", "n": 3, "l": 2, "m": 2}
+        else:
+            state = {"kind": "gaussian", "sigma": float(rng.uniform(5.0, 20.0))}
+        out.append({"q": q, "R": R, "mu": mu, "l_max": l_max, "Nr": N, "L": N / 10.0, "dt": 0.5, "state": state})
+    return out
+
+
+def c4_load():
+    """The frozen list (bench_c4_binaries.json), checked against its generator."""
+    with open(os.path.join(ROOT, WORKLOADS["c4"]["batch_file"])) as f:
+        frozen = json.load(f)
+    if frozen != c4_binaries():
+        raise RuntimeError("bench_c4_binaries.json differs from c4_binaries(seed 0)")
+    return frozen
+
+
+def c4_modes(l_max):
+    return [(l, m) for l in range(l_max + 1) for m in range(-l, l + 1) if (l - m) % 2 == 0]
+
+
+def c4_state(b):
+    """Initial state of one binary of the sweep (device generator for the atoms)."""
+    from boson_cloud_binary_b200 import gaussian_state, hydrogenic_state
+    r = np.linspace(BASE["epsilon"], BASE["epsilon"] + b["L"], b["Nr"])
+    modes = c4_modes(b["l_max"])
+    st = b["state"]
+    if st["kind"] == "gaussian":
+        return gaussian_state(r, modes, st["sigma"])
+    return hydrogenic_state(r, modes, b["mu"], b["q"], b["R"], n=st["n"], l=st["l"], m=st["m"])
 UNIT = "mode*node*steps/s"
 
 # DRAM traffic (read + write) per launch of each measured kernel class, from the ncu
@@ -251,18 +302,84 @@ def oracle_memory_gb(w):
     return 13.8 * (w["n_modes"] / 91.0) ** 2 * (w["Nr"] / 4000.0)
 
 
+def c4_workload(b):
+    """One binary of the batched sweep as a single-binary workload dict."""
+    w = dict(BASE, workload="batched_sweep_binary", Nr=b["Nr"], L=b["L"], l_max=b["l_max"],
+             n_modes=len(c4_modes(b["l_max"])), mu=b["mu"], q=b["q"], R=b["R"], dt=b["dt"], r_ex=0.75 * b["L"],
+             precision="fp64", tolerance=WORKLOADS["c4"]["tolerance"])
+    return w
+
+
+def run_reference_batch(args):
+    """CPU arm of the batched sweep: the oracle on the three binaries with the smallest
+    assembled operators (the rest need tens of GB of host memory), a bounded sample of
+    steps each; the metric over the sample."""
+    binaries = sorted(c4_load(), key=lambda b: len(c4_modes(b["l_max"])) ** 2 * b["Nr"])[:3]
+    units, secs, parts, cores = 0, 0.0, [], 0
+    for b in binaries:
+        w = c4_workload(b)
+        base, steps, el = cpu_oracle_sample(w, c4_state_host(b), target_s=10.0, max_steps=max(1, min(args.steps, 4)))
+        units += w["n_modes"] * w["Nr"] * steps
+        secs += el
+        cores = base["cores"]
+        parts.append(f"{w['n_modes']}x{w['Nr']} ({steps} steps)")
+    value = units / secs
+    base = {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": "oracle restatement (assembled CSR, OpenMP) on the three binaries of the sweep with the "
+                      "smallest operators: " + ", ".join(parts) + f", {secs:.1f} s"}
+    return {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
+            "warmup": 1, "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c128", "data": "synthetic", "config": {"workload": WORKLOADS["c4"]["workload"],
+                                                           "precision": "fp64"},
+            "cpu_baseline": base, "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}
+
+
+def c4_state_host(b):
+    """The host generator's state of one binary (the CPU arm runs without a GPU)."""
+    from boson_cloud_binary_b200.cnm import gaussian_state
+    from boson_cloud_binary_b200.initial_state import hydrogenic_on_primary
+    r = np.linspace(BASE["epsilon"], BASE["epsilon"] + b["L"], b["Nr"])
+    modes = c4_modes(b["l_max"])
+    st = b["state"]
+    if st["kind"] == "gaussian":
+        return gaussian_state(r, modes, st["sigma"])
+    return hydrogenic_on_primary(r, modes, b["mu"], b["q"], b["R"], n=st["n"], l=st["l"], m=st["m"])
+
+
+def oracle_sample_workload(w, budget_gb=8.0):
+    """The workload the CPU oracle is timed on: the workload itself when its assembled
+    operators fit in `budget_gb` (and half the host's free memory), else the same binary
+    on fewer nodes at the same spacing (the oracle's cost per mode*node*step does not
+    depend on N: every operator is a pass over n^2 N stored entries).  Returns the
+    workload and a note."""
+    have = host_memory_gb()
+    budget = min(budget_gb, 0.5 * have) if have else budget_gb
+    need = oracle_memory_gb(w)
+    if need <= budget:
+        return w, ""
+    dr = w["L"] / (w["Nr"] - 1)
+    n2 = max(600, int(w["Nr"] * budget / need))
+    w2 = dict(w, Nr=n2, L=dr * (n2 - 1))
+    w2["r_ex"] = min(w["r_ex"], 0.75 * w2["L"])
+    return w2, (f"the same binary on {n2} of its {w['Nr']} nodes at its spacing dr = {dr:g} (the full grid's "
+                f"assembled operators need about {need:.0f} GB of host memory)")
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
-    w = dict(WORKLOADS[args.config])
     if rank != 0:
         return 0
-    need, have = oracle_memory_gb(w), host_memory_gb()
-    if have and need > 0.7 * have:
-        print(json.dumps({"impl": "reference", "unavailable": f"the CPU oracle's assembled operators need about "
-                          f"{need:.0f} GB for {w['workload']}; the host has {have:.0f} GB available"}), flush=True)
+    if args.config == "c4":
+        print(json.dumps(run_reference_batch(args)), flush=True)
         return 0
+    w_full = dict(WORKLOADS[args.config])
+    w, note = oracle_sample_workload(w_full)
     psi0 = initial_state(w)
     base, steps, el = cpu_oracle_sample(w, psi0, target_s=30.0, max_steps=max(1, min(args.steps, 10)))
+    if note:
+        base["sample"] += "; " + note
+    w = w_full
     line = {"impl": "reference", "metric": METRIC, "value": base["value"], "unit": UNIT, "n_gpus": ws,
             "steps": steps, "warmup": 1, "ms_per_step": 1e3 * el / steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "c128", "data": "synthetic",
@@ -443,19 +560,143 @@ def run_ours(args):
         line["mixed_over_fp64"] = ms_ref / ms
         line["accuracy"] = accuracy
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
-        need, have = oracle_memory_gb(w), host_memory_gb()
-        if have and need > 0.7 * have:
-            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
-                                    "sample": f"not run: the oracle's assembled operators need about {need:.0f} GB, "
-                                              f"{have:.0f} GB available"}
-        else:
-            base, _, _ = cpu_oracle_sample(w, psi0, target_s=20.0, max_steps=5)
-            line["cpu_baseline"] = base
+        ws_, note = oracle_sample_workload(w)
+        base, _, _ = cpu_oracle_sample(ws_, psi0 if ws_ is w else initial_state(ws_), target_s=20.0, max_steps=5)
+        if note:
+            base["sample"] += "; " + note
+        line["cpu_baseline"] = base
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+    return 0
+
+
+def run_batch(args):
+    """The batched sweep: 64 binaries of uneven N and l_max stepped together (cnm_batch_step:
+    every binary's step queued on its own stream before any is completed), mixed precision,
+    the same binaries in FP64 beside it.  Wall time of the synchronous batch steps (the
+    library returns after every binary's step completed)."""
+    ws, rank, local = dist_env()
+    from boson_cloud_binary_b200 import Batch, select_device
+    select_device(local)
+    w = dict(WORKLOADS["c4"])
+    binaries = c4_load()
+    states = [c4_state(b) for b in binaries]
+
+    def build(precision):
+        args_ = [(b["Nr"], b["L"], b["dt"], BASE["epsilon"], b["l_max"], b["mu"], BASE["M_c"], b["q"], 0.0, b["R"],
+                  BASE["counter"], BASE["absorption"], 10 ** 9, BASE["ramp_periods"], BASE["epsilon_smear"])
+                 for b in binaries]
+        bt = Batch(args_, precision=precision)
+        for b, cn, psi0 in zip(binaries, bt.binaries, states):
+            cn.set_initial_state_full(psi0)
+            cn.evolve_orbit = True
+            cn.steps_per_period = cn.P / b["dt"]
+            cn.tolerance = w["tolerance"]
+            cn.initialize()
+            cn.build_damping_mask(*BASE["mask"])
+            cn.run(10 ** 9, 0.75 * b["L"])
+            t_start = (BASE["ramp_periods"] + 1.0) * cn.P
+            cn.t_i = t_start
+            cn.refresh(t_start)
+        return bt
+
+    t0 = time.perf_counter()
+    mixed = build("mixed")
+    setup_s = time.perf_counter() - t0
+    fp64 = None if args.no_fp64_arm else build("fp64")
+    units_per_step = sum(len(c4_modes(b["l_max"])) * b["Nr"] for b in binaries)
+
+    def timed(bt, k0, steps):
+        n0 = sum(cn.launch_count() for cn in bt.binaries)
+        t = time.perf_counter()
+        for q in range(steps):
+            bt.step(k0 + q)
+        return time.perf_counter() - t, sum(cn.launch_count() for cn in bt.binaries) - n0
+
+    k = 1
+    for _ in range(args.warmup):
+        mixed.step(k)
+        if fp64 is not None:
+            fp64.step(k)
+        k += 1
+    with ClockSampler(local) as clocks:
+        t_soak = time.perf_counter()
+        while time.perf_counter() - t_soak < 2.0:
+            mixed.step(k)
+            if fp64 is not None:
+                fp64.step(k)
+            k += 1
+        el, launches = timed(mixed, k, args.steps)
+    el64 = timed(fp64, k, args.steps)[0] if fp64 is not None else None
+    k += args.steps
+    value = units_per_step * args.steps / el
+    # per-class kernel times over the binaries (device events on each binary's stream)
+    names = ("apply", "tc_apply", "precond_solve", "precond_solve32", "precond_factor", "diagnostics")
+    for cn in mixed.binaries:
+        cn.set_profiling(True)
+    prof_steps = max(1, min(args.steps, 5))
+    for q in range(prof_steps):
+        mixed.step(k + q)
+    k += prof_steps
+    kt = {name: [0.0, 0, 0.0] for name in names}   # ms, launches, algorithmic bytes
+    for b, cn in zip(binaries, mixed.binaries):
+        wb = {"n_modes": len(c4_modes(b["l_max"])), "Nr": b["Nr"], "l_max": b["l_max"]}
+        for name in names:
+            ms, nl = cn.kernel_times(name)
+            if nl > 0:
+                nbytes, _ = algorithmic(name, wb, cn.coupling_info()[1], cn) if name != "tc_apply" else \
+                    (3 * 8 * wb["n_modes"] * wb["Nr"] + 8 * (2 * wb["l_max"] + 1) * wb["Nr"], 0)
+                kt[name][0] += ms
+                kt[name][1] += nl
+                kt[name][2] += nbytes * nl
+        cn.set_profiling(False)
+    kshare = {n_: {"ms": v[0], "launches": v[1]} for n_, v in kt.items() if v[1] > 0}
+    dom = max(kshare, key=lambda n_: kshare[n_]["ms"])
+    hbm, _, src = peaks()
+    achieved = kt[dom][2] / (kt[dom][0] / 1e3) / 1e9
+    roof = {"kernel": dom, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+            "peak_source": f"{src} (MEASURED_PEAKS.json hbm_gbs)" if src == "measured" else "fallback",
+            "launches": kt[dom][1], "avg_launch_us": kt[dom][0] / kt[dom][1] * 1e3,
+            "algorithmic_bytes": "sum over the binaries' launches of each launch's algorithmic bytes", "traffic": None}
+    # end to end: every binary's state uploaded from pinned host memory, K steps, the states
+    # downloaded
+    try:
+        import torch
+        hosts = [torch.empty(2 * s_.size, dtype=torch.float64, pin_memory=True).numpy() for s_ in states]
+    except Exception:
+        hosts = [np.empty(2 * s_.size) for s_ in states]
+    for h_, cn in zip(hosts, mixed.binaries):
+        h_[:] = cn.psi.view(np.float64)
+    t0 = time.perf_counter()
+    for h_, cn in zip(hosts, mixed.binaries):
+        cn.psi = h_.view(np.complex128)
+    for q in range(args.steps):
+        mixed.step(k + q)
+    for h_, cn in zip(hosts, mixed.binaries):
+        h_[:] = cn.psi.view(np.float64)
+    e2e_s = time.perf_counter() - t0
+    state_bytes = sum(16 * s_.size for s_ in states)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "c64+c128", "data": "synthetic",
+            "config": {"workload": w["workload"], "binaries": len(binaries), "units_per_step": units_per_step,
+                       "precision": "mixed", "tolerance": w["tolerance"], "parallelism": f"replicas{ws}",
+                       "batch_file": w["batch_file"], "setup_s": setup_s,
+                       "l2": "working set > L2 (the states alone are %.0f MB complex128)" % (state_bytes / 1e6),
+                       "timing": "wall time of synchronous batch steps"},
+            "roofline": roof, "kernels": kshare,
+            "e2e": {"value": units_per_step * args.steps / e2e_s, "unit": UNIT,
+                    "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
+                    "note": "states uploaded once and downloaded once per timed run"},
+            "clocks": clocks.summary(), "gpu_launches": int(launches)}
+    if el64 is not None:
+        line["fp64_arm"] = {"value": units_per_step * args.steps / el64, "ms_per_step": 1e3 * el64 / args.steps}
+        line["mixed_over_fp64"] = el64 / el
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     return 0
 
 
@@ -474,6 +715,8 @@ def main():
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.config == "c4":
+        return run_batch(args)
     return run_ours(args)
 
 

@@ -76,7 +76,8 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_sink_vector", "cnm_save_checkpoint", "cnm_load_checkpoint", "cnm_replay_power_average", "cnm_select_device", "cnm_set_profiling", "cnm_kernel_times", "cnm_timer_start", "cnm_timer_stop",
            "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel",
            "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy",
-           "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info", "cnm_mixed_trace", "cnm_launch_count", "cnm_tc_blocks")
+           "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info", "cnm_mixed_trace", "cnm_launch_count", "cnm_tc_blocks",
+           "cnm_hydrogenic_state")
 
 def displaced_100_state(r, modes, mu, x_bh):
     """displaced_100_state (src/DisplacedAtom.cpp:12-76) on the device: the mode projection
@@ -93,6 +94,44 @@ def displaced_100_state(r, modes, mu, x_bh):
         msg = L.cnm_create_error().decode()
         raise ValueError(msg) if rc == CNM_EINVAL else CudaError(msg)
     return out.view(np.complex128)
+
+
+def hydrogenic_state(r, modes, mu, q, R, n=2, l=1, m=1, M1=1.0, n_theta=None, n_phi=None):
+    """cnm_hydrogenic_state: the mode projection of the hydrogenic (n, l, m) state of the
+    primary (mass M1, centred at x = R1 = q R / (1 + q)) computed on the device, complex
+    n_modes x Nr, normalised to sum |U|^2 dr = 1 (the reference's
+    initial_states/get_initial_state_COM_fast.py state; the quadrature defaults follow
+    initial_state.hydrogenic_on_primary)."""
+    L = load_library()
+    r = np.ascontiguousarray(np.asarray(r, float))
+    lmax = max(a for a, _ in modes)
+    n_theta = n_theta or max(48, 2 * (lmax + l) + 16)
+    n_phi = n_phi or 2 * n_theta
+    ls = np.array([a for a, _ in modes], np.int32)
+    ms = np.array([b for _, b in modes], np.int32)
+    out = np.zeros(2 * len(r) * len(modes))
+    rc = L.cnm_hydrogenic_state(_dptr(r), len(r), ls.ctypes.data_as(C.POINTER(C.c_int32)),
+                                ms.ctypes.data_as(C.POINTER(C.c_int32)), len(modes), float(mu), float(M1),
+                                float(q) / (1.0 + float(q)) * float(R), int(n), int(l), int(m), int(n_theta),
+                                int(n_phi), _dptr(out))
+    if rc != CNM_OK:
+        msg = L.cnm_create_error().decode()
+        raise ValueError(msg) if rc == CNM_EINVAL else CudaError(msg)
+    return out.view(np.complex128)
+
+
+def gaussian_state(r, modes, sigma):
+    """The reference's spherical Gaussian initial state (initial_states/get_initial_state_gaussian.py):
+    U_00 = sqrt(4 pi) r exp(-r^2 / (2 sigma^2)), every other mode zero, normalised on the grid
+    by the trapezoidal rule, complex n_modes x Nr."""
+    r = np.asarray(r, float)
+    out = np.zeros((len(modes), r.size), complex)
+    j00 = [i for i, lm in enumerate(modes) if tuple(lm) == (0, 0)]
+    if not j00 or not sigma > 0:
+        raise ValueError("the Gaussian state needs the (0, 0) mode and sigma > 0")
+    u = np.sqrt(4 * np.pi) * r * np.exp(-0.5 * (r / sigma) ** 2)
+    out[j00[0]] = u / np.sqrt(np.trapezoid(np.abs(u) ** 2, x=r))
+    return out.reshape(-1)
 
 
 def measure_fp64_peak():
@@ -171,6 +210,8 @@ def load_library():
     L.cnm_batch_step.argtypes = [p, i32, C.c_void_p]
     L.cnm_batch_destroy.argtypes = [p]
     L.cnm_displaced_100_state.argtypes = [dp, i32, C.POINTER(i32), C.POINTER(i32), i32, C.c_double, C.c_double, dp]
+    L.cnm_hydrogenic_state.argtypes = [dp, i32, C.POINTER(i32), C.POINTER(i32), i32, C.c_double, C.c_double,
+                                       C.c_double, i32, i32, i32, i32, i32, dp]
     _lib = L
     return L
 
@@ -463,16 +504,18 @@ class Batch:
     CrankNicolsonModes view of binary i for set-up and read-out; ``step(k)`` advances all
     of them by one step and returns their step diagnostics (scalars only)."""
 
-    def __init__(self, arg_lists):
+    def __init__(self, arg_lists, precision="fp64"):
         lib = load_library()
         n = len(arg_lists)
+        if precision not in PRECISIONS:
+            raise ValueError(f"precision must be one of {sorted(PRECISIONS)}")
         prms = (cnm_params * n)()
         for i, a in enumerate(arg_lists):
             (Nx, L, dt, epsilon, l_max, mu, M_c, q, aa, R, counter, absorption, save_every,
              ramp_periods, epsilon_smear) = a[:15]
             prms[i] = cnm_params(int(Nx), float(L), float(dt), float(epsilon), int(l_max), float(mu), float(M_c),
                                  float(q), float(aa), float(R), int(bool(counter)), int(bool(absorption)),
-                                 int(save_every), float(ramp_periods), float(epsilon_smear), 0)
+                                 int(save_every), float(ramp_periods), float(epsilon_smear), PRECISIONS[precision])
         b = C.c_void_p()
         rc = lib.cnm_batch_create(prms, n, C.byref(b))
         if rc != CNM_OK:
@@ -483,14 +526,19 @@ class Batch:
         for i, a in enumerate(arg_lists):
             h = C.c_void_p()
             lib.cnm_batch_handle(b, i, C.byref(h))
-            self.binaries.append(CrankNicolsonModes(*a[:15], _handle=h))
+            self.binaries.append(CrankNicolsonModes(*a[:15], _handle=h, precision=precision))
 
     def step(self, step_id):
         n = len(self.binaries)
         diags = (cnm_diag * n)()
         rc = self._lib.cnm_batch_step(self._b, int(step_id), C.cast(diags, C.c_void_p))
         if rc != CNM_OK:
-            raise SolveError(f"batch step {step_id} failed (status {rc})")
+            errs = []
+            for i, c in enumerate(self.binaries):
+                msg = self._lib.cnm_last_error(c._h)
+                if msg:
+                    errs.append(f"binary {i}: {msg.decode()}")
+            raise SolveError(f"batch step {step_id} failed (status {rc}): " + "; ".join(errs))
         out = []
         for i, c in enumerate(self.binaries):
             d = diags[i]

@@ -14,6 +14,7 @@
 #include "cnm_kernels.cuh"
 #include "cnm_apply5.cuh"
 #include "cnm_mixed.cuh"
+#include "cnm_initial.h"
 
 #include <cuda_runtime.h>
 
@@ -491,7 +492,7 @@ struct Solver {
         m_r64.alloc(nN);
         m_dots.alloc(8);
         d_msc.alloc(1);
-        m_part.alloc((size_t)8 * std::max(vec_blocks, tcp.grid));
+        m_part.alloc((size_t)8 * std::max(vec_blocks, tcp.tiles));
         // fp32 cluster solve: the fp64 solve's CTAs per cluster, nodes per thread from it
         ps_cs = pcl_cs;
         ps_per = pcl_per;
@@ -1406,7 +1407,7 @@ struct Solver {
                 a.dot_kind[0] = 1;
                 a.dot_ext[0] = m_r.p;  // r0
                 launch_tc(a);
-                mx_finish(tcp.grid, 2, first ? MX_ALPHA : MX_ALPHA2);
+                mx_finish(tcp.tiles, 2, first ? MX_ALPHA : MX_ALPHA2);
             }
             psolve32(1, nullptr, m_z.p, first ? m_r.p : m_r1.p, first ? m_s.p : m_q.p);
             wood32(sk, k, m_z.p);
@@ -1417,7 +1418,7 @@ struct Solver {
                 a.dot_ext[0] = first ? m_s.p : m_q.p;
                 a.dot_kind[1] = 3;
                 launch_tc(a);
-                mx_finish(tcp.grid, 4, MX_OMEGA);
+                mx_finish(tcp.tiles, 4, MX_OMEGA);
             }
             k_mx_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, x.p, m_y.p, m_z.p, m_d.p, first ? 1 : 0,
                                                                 last ? 1 : 0, m_part.p);
@@ -1459,7 +1460,7 @@ struct Solver {
         a.dot_kind[0] = 4;
         a.dot_ext64 = m_r64.p;
         launch_tc(a);
-        mx_finish(tcp.grid, 2, MX_TCRES);
+        mx_finish(tcp.tiles, 2, MX_TCRES);
     }
 
     // Calibration of the tensor-core residual check on the pass just verified in fp64:
@@ -1478,7 +1479,7 @@ struct Solver {
         a.dot_kind[0] = 4;
         a.dot_ext64 = cand.p;
         launch_tc(a);
-        mx_finish(tcp.grid, 2, MX_ECAL);
+        mx_finish(tcp.tiles, 2, MX_ECAL);
     }
 
     // psi candidate = mask x into cand, the diagnostics pass on it, the read-backs (the
@@ -2618,6 +2619,16 @@ int cnm_timer_stop(cnm_handle *h, double *ms)
         CK(cudaEventElapsedTime(&f, s.region_a, s.region_b));
         *ms = f;
     });
+}
+
+int cnm_hydrogenic_state(const double *r, int32_t Nr, const int32_t *l, const int32_t *m, int32_t n_modes, double mu,
+                         double M1, double x_center, int32_t n, int32_t la, int32_t ma, int32_t n_theta, int32_t n_phi,
+                         double *state)
+{
+    std::string err;
+    const int rc = cnm::hydrogenic_state(r, Nr, l, m, n_modes, mu, M1, x_center, n, la, ma, n_theta, n_phi, state, err);
+    if (rc != CNM_OK) g_create_error = err;
+    return rc;
 }
 
 int cnm_displaced_100_state(const double *r, int32_t Nr, const int32_t *l, const int32_t *m, int32_t n_modes,

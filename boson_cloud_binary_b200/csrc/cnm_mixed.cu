@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 #include "cnm_coupling.h"
@@ -221,6 +222,7 @@ struct TcShared {
     int abort;
     int l_off[TC_KMAX], l_bytes[TC_KMAX], l_nblk[TC_KMAX];
     int slices[TC_KMAX * 16];
+    double red[4 * 16];  // warp sums of a tile's fused reductions
 };
 
 // Bulk copy of multipole lv's Gaunt blocks into the G stage of use v (v % gst).
@@ -387,8 +389,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // epilogue phase 1: TMEM lane quarter (warp % 4: modes j) and quarter of the columns
         const int q4 = warp & 3, cq = warp >> 2;
         const float2 al = a.alpha, be = a.beta;
+        // the sinks' coefficients coef_a (v_a^dag x), fp64
+        double2 sk_c[2];
+#pragma unroll
+        for (int s2 = 0; s2 < 2; ++s2) {
+            sk_c[s2] = make_double2(0.0, 0.0);
+            if (s2 < a.n_sinks) {
+                const double2 dd = a.sink_dots[s2];
+                sk_c[s2] = make_double2(a.sink_coef[s2] * dd.x, a.sink_coef[s2] * dd.y);
+            }
+        }
         constexpr int NDOT = DK == 0 ? 0 : DK == 23 ? 2 : 1;
-        double dacc[4] = {0, 0, 0, 0};
         // the launch's reduction operand: complex64 (kinds 1, 2) or complex128 (kind 4)
         const float2 *__restrict__ ext32 = (DK == 1 || DK == 23) ? a.dot_ext[0] : nullptr;
         const double2 *__restrict__ ext64 = DK == 4 ? a.dot_ext64 : nullptr;
@@ -546,16 +557,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             // phase 2: one complex output per (mode j, node) and thread, consecutive threads
             // on consecutive nodes of one mode (coalesced loads and stores); a warp's lanes
             // hold 32 consecutive nodes, so the stencil's neighbours come by shuffles and
-            // only the first lane's left and the last lane's right neighbour are loaded
+            // only the first lane's left and the last lane's right neighbour are loaded.  The
+            // products of the fused reductions are formed in fp32 (their operands are fp32
+            // values; the residual check's difference in fp64) and summed per tile in fp32,
+            // then in fp64 across tiles.
             {
                 const int tile_nodes = min(TC_NT, Nr - i0);
-                constexpr int EB = 4;  // elements in flight per thread
+                constexpr int EB = 6;  // elements in flight per thread
+                using Ext = typename std::conditional<DK == 4, double2, float2>::type;
                 float2 *__restrict__ yg = a.y;
+                float tacc[3] = {0.f, 0.f, 0.f};
 #pragma unroll 1
                 for (int e0 = tid; e0 < n * TC_NT; e0 += EB * TC_WORKERS) {
-                    float2 x0[EB], xh[EB], w[EB];
-                    // the reduction operand (complex64 widened, or complex128)
-                    double2 ev[EB];
+                    float2 x0[EB], xh[EB];
+                    Ext ev[EB];
 #pragma unroll
                     for (int q = 0; q < EB; ++q) {
                         const int e = e0 + q * TC_WORKERS;
@@ -568,16 +583,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         xh[q] = zero;
                         if (ok && lane == 0 && i >= 1) xh[q] = __ldg(xg + o - 1);
                         if (ok && lane == 31 && i + 1 < Nr) xh[q] = __ldg(xg + o + 1);
-                        w[q] = ok ? *reinterpret_cast<const float2 *>(W + j * TC_WS + 2 * c) : zero;
-                        ev[q] = make_double2(0.0, 0.0);
-                        if constexpr (DK == 1 || DK == 23) {
-                            if (ok) {
-                                const float2 t = __ldg(ext32 + o);
-                                ev[q] = make_double2(t.x, t.y);
-                            }
-                        } else if constexpr (DK == 4) {
-                            if (ok) ev[q] = __ldg(ext64 + o);
-                        }
+                        if constexpr (DK == 1 || DK == 23) ev[q] = ok ? __ldg(ext32 + o) : zero;
+                        else if constexpr (DK == 4) ev[q] = ok ? __ldg(ext64 + o) : make_double2(0.0, 0.0);
                     }
 #pragma unroll
                     for (int q = 0; q < EB; ++q) {
@@ -593,7 +600,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         if (!(e < n * TC_NT && c < tile_nodes)) continue;
                         const int i = i0 + c;
                         const int64_t o = (int64_t)j * Nr + i;
-                        const float wr_ = w[q].x * wscale, wi_ = w[q].y * wscale;
+                        const float2 w = *reinterpret_cast<const float2 *>(W + j * TC_WS + 2 * c);
+                        const float wr_ = w.x * wscale, wi_ = w.y * wscale;
                         float hr = 0.f, hi = 0.f;
                         if (i >= 1 && i <= Nr - 2) {
                             if (a.use_h0) {
@@ -619,43 +627,41 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
                         for (int s2 = 0; s2 < 2; ++s2)
                             if (s2 < a.n_sinks && i >= a.sink_lo[s2] && i < a.sink_hi[s2]) {
-                                const double2 dd = a.sink_dots[s2];
                                 const double2 vv = a.sink_v[s2][o];
-                                const double cr = a.sink_coef[s2] * dd.x, ci = a.sink_coef[s2] * dd.y;
-                                yr += (float)(cr * vv.x - ci * vv.y);
-                                yi += (float)(cr * vv.y + ci * vv.x);
+                                yr += (float)(sk_c[s2].x * vv.x - sk_c[s2].y * vv.y);
+                                yi += (float)(sk_c[s2].x * vv.y + sk_c[s2].y * vv.x);
                             }
                         yg[o] = make_float2(yr, yi);
-                        const double yrd = yr, yid = yi;
                         if constexpr (DK == 1) {  // conj(e) y
-                            dacc[0] += ev[q].x * yrd + ev[q].y * yid;
-                            dacc[1] += ev[q].x * yid - ev[q].y * yrd;
+                            tacc[0] = fmaf(ev[q].x, yr, fmaf(ev[q].y, yi, tacc[0]));
+                            tacc[1] = fmaf(ev[q].x, yi, fmaf(-ev[q].y, yr, tacc[1]));
                         } else if constexpr (DK == 23) {  // conj(y) e, |y|^2
-                            dacc[0] += yrd * ev[q].x + yid * ev[q].y;
-                            dacc[1] += yrd * ev[q].y - yid * ev[q].x;
-                            dacc[2] += yrd * yrd + yid * yid;
+                            tacc[0] = fmaf(yr, ev[q].x, fmaf(yi, ev[q].y, tacc[0]));
+                            tacc[1] = fmaf(yr, ev[q].y, fmaf(-yi, ev[q].x, tacc[1]));
+                            tacc[2] = fmaf(yr, yr, fmaf(yi, yi, tacc[2]));
                         } else if constexpr (DK == 4) {  // |e64 - y|^2
-                            const double ddr = ev[q].x - yrd, ddi = ev[q].y - yid;
-                            dacc[0] += ddr * ddr + ddi * ddi;
+                            const float ddr = (float)(ev[q].x - (double)yr), ddi = (float)(ev[q].y - (double)yi);
+                            tacc[0] = fmaf(ddr, ddr, fmaf(ddi, ddi, tacc[0]));
                         }
                     }
                 }
-            }
-        }
-        // per-CTA partials of the fused reductions (fixed order: warps, then lanes)
-        if constexpr (NDOT > 0) {
-            double *red = reinterpret_cast<double *>(hs);  // the h tile is no longer read
-            workers_sync();
+                // the tile's partials [slot][tile] (warps, then the warp sums in order): the
+                // sums do not depend on which CTA ran the tile
+                if constexpr (NDOT > 0) {
+                    double v[4] = {(double)tacc[0], DK == 4 ? 0.0 : (double)tacc[1], DK == 23 ? (double)tacc[2] : 0.0,
+                                   0.0};
 #pragma unroll
-            for (int q = 0; q < 2 * NDOT; ++q) dacc[q] = warp_sum(dacc[q]);
-            if (lane == 0)
+                    for (int q = 0; q < 2 * NDOT; ++q) v[q] = warp_sum(v[q]);
+                    if (lane == 0)
 #pragma unroll
-                for (int q = 0; q < 2 * NDOT; ++q) red[q * TC_CTRL + warp] = dacc[q];
-            workers_sync();
-            if (tid < 2 * NDOT) {
-                double s = 0.0;
-                for (int w = 0; w < TC_CTRL; ++w) s += red[tid * TC_CTRL + w];
-                a.partials[(int64_t)tid * gridDim.x + blockIdx.x] = s;
+                        for (int q = 0; q < 2 * NDOT; ++q) sh.red[q * 16 + warp] = v[q];
+                    workers_sync();
+                    if (tid < 2 * NDOT) {
+                        double sum = 0.0;
+                        for (int w = 0; w < TC_CTRL; ++w) sum += sh.red[tid * 16 + w];
+                        a.partials[(int64_t)tid * tiles + tile] = sum;
+                    }
+                }
             }
         }
     }

@@ -78,7 +78,7 @@ struct TcArgs {
     int dot_kind[3];
     const float2 *dot_ext[3];
     const double2 *dot_ext64;
-    double *partials;         // [slot][gridDim.x]
+    double *partials;         // [slot][tile]: per-tile sums, independent of the CTA that ran the tile
     int *status;              // bit 4: an mbarrier wait gave up
     int *tile_ctr;            // [2]: next tile, finished CTAs (zero between launches)
 };

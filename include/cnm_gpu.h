@@ -186,6 +186,17 @@ int cnm_should_stop(const cnm_handle *h, int32_t *stop);
 int cnm_displaced_100_state(const double *r, int32_t Nr, const int32_t *l, const int32_t *m, int32_t n_modes,
                             double mu, double x_bh, double *state);
 
+/* The initial states of the sweeps (initial_states/get_initial_state_COM_fast.py of the
+ * reference, which writes them to MODESBIN files): the mode projection of the hydrogenic
+ * (n, la, ma) state of reduced mass mu about a body of mass M1 at x = x_center on the x axis,
+ *     U_j(r) = r int conj(Y_j) psi_nlm(r Omega - x_center e_x) dOmega,
+ * on the device, with n_theta Gauss-Legendre nodes in cos(theta) and n_phi uniform angles;
+ * normalised to sum |U|^2 dr = 1 on the (uniform) grid; U vanishes on the two end nodes.
+ * state: interleaved complex, n_modes x Nr (host buffer); at most 160 modes. */
+int cnm_hydrogenic_state(const double *r, int32_t Nr, const int32_t *l, const int32_t *m, int32_t n_modes, double mu,
+                         double M1, double x_center, int32_t n, int32_t la, int32_t ma, int32_t n_theta, int32_t n_phi,
+                         double *state);
+
 /* --- batched sweep (independent binaries) ------------------------------------------
  * A batch owns one handle per binary, each with its own stream.  cnm_batch_step
  * advances every binary by one step: it queues the device work of all binaries

@@ -69,3 +69,34 @@ def test_device_generator_matches_oracle(offset):
     assert np.linalg.norm(got - want) <= 1e-12 * np.linalg.norm(want)
     with pytest.raises(ValueError):
         _device_state(r, modes, 0.0, offset)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("n,l,m,lmax", [(2, 1, 1, 8), (3, 2, 2, 10), (3, 2, -2, 6), (2, 1, -1, 4), (1, 0, 0, 4)])
+def test_device_hydrogenic_state_matches_host_generator(n, l, m, lmax):
+    """The device projection of a translated hydrogenic (n, l, m) state (the state of the
+    reference's initial_states/get_initial_state_COM_fast.py) against the host generator of
+    the benchmark (scipy spherical harmonics and Laguerre polynomials) on the same
+    quadrature, to 1e-12 relative.  (States with l - m odd are odd in z and have no weight on
+    the solver's modes, which all have l - m even.)"""
+    from boson_cloud_binary_b200 import hydrogenic_state
+    from boson_cloud_binary_b200.initial_state import hydrogenic_on_primary
+    modes = _modes(lmax)
+    r = np.linspace(0.0, 120.0, 600)
+    mu, q, R = 0.3, 0.5, 30.0
+    dev = hydrogenic_state(r, modes, mu, q, R, n=n, l=l, m=m)
+    host = hydrogenic_on_primary(r, modes, mu, q, R, n=n, l=l, m=m)
+    assert np.linalg.norm(dev - host) / np.linalg.norm(host) < 1e-12
+
+
+def test_gaussian_state_is_the_reference_profile():
+    """initial_states/get_initial_state_gaussian.py: U_00 = sqrt(4 pi) r exp(-r^2/(2 sigma^2)),
+    normalised by the trapezoidal rule, every other mode zero."""
+    from boson_cloud_binary_b200.cnm import gaussian_state
+    r = np.linspace(0.0, 200.0, 2001)
+    modes = _modes(4)
+    u = gaussian_state(r, modes, 10.0).reshape(len(modes), -1)
+    assert np.count_nonzero(np.abs(u[1:]).sum(axis=1)) == 0
+    assert abs(np.trapezoid(np.abs(u[0]) ** 2, x=r) - 1.0) < 1e-14
+    ref = np.sqrt(4 * np.pi) * r * np.exp(-0.5 * (r / 10.0) ** 2)
+    assert np.allclose(u[0] / u[0][10], ref / ref[10], rtol=1e-14, atol=0)
