@@ -11,7 +11,9 @@ diagnostics and orbit); the FP64 arm is the complex128 drop-in.  `value` is the 
 arm; the FP64 arm, their ratio and the difference of the two solutions after the run are
 reported beside it.  Other workloads (--config): c2 (the FP64 drop-in on 45 modes x
 20000 nodes, the configuration the FP64 path was first measured on), c1 (15 modes x 3000
-nodes, fixed orbit).  Keys the configurations do not name take the reference's minimal-
+nodes, fixed orbit), c4 (the batched sweep: 64 binaries of uneven N and l_max from seed 0,
+bench_c4_binaries.json, mixed against FP64), c5 (the stress case on the FP64 path:
+equal-mass counter-rotating binary, (3,2,2) cloud, 153 modes x 65536 nodes, dt 0.25).  Keys the configurations do not name take the reference's minimal-
 example values: ramp_periods=2, epsilon=0, epsilon_smear=2, M_c=0.01, mask 0.85/1/6.  The
 timed steps start one initial period after the start-up ramp (absorbers, back-reaction
 and orbit evolution at full strength).  Synthetic input: the analytic 2p state projected
@@ -52,6 +54,9 @@ WORKLOADS = {
     "c1": dict(BASE, workload="fp64_single_binary_fixed_orbit_l4_N3000", Nr=3000, L=300.0, l_max=4, n_modes=15,
                mu=0.2, q=0.1, R=30.0, dt=1.0, r_ex=250.0, evolve_orbit=False, precision="fp64", tolerance=1e-10),
 }
+WORKLOADS["c5"] = dict(BASE, workload="fp64_stress_counter_rotating_l16_N65536", Nr=65536, L=6000.0, l_max=16,
+                       n_modes=153, mu=0.3, q=1.0, R=60.0, dt=0.25, counter=True, r_ex=5000.0, precision="fp64",
+                       tolerance=1e-10, state="3d hydrogenic (3,2,2) on the primary", atom=(3, 2, 2))
 WORKLOADS["c4"] = dict(BASE, workload="batched_sweep_64_binaries_seed0", precision="mixed", tolerance=1e-12,
                        batch_file="bench_c4_binaries.json")
 METRIC = "CN mode*node*steps/s"
@@ -183,11 +188,18 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def initial_state(w):
+def initial_state(w, device=False):
+    """The workload's hydrogenic atom on the primary projected on the modes: by the device
+    generator (cnm_hydrogenic_state) for the GPU arm, by the host generator for the CPU arm
+    (the same quadrature; the two agree to 1e-12)."""
     from boson_cloud_binary_b200.initial_state import hydrogenic_on_primary
     r = np.linspace(w["epsilon"], w["epsilon"] + w["L"], w["Nr"])
     modes = [(l, m) for l in range(w["l_max"] + 1) for m in range(-l, l + 1) if (l - m) % 2 == 0]
-    return hydrogenic_on_primary(r, modes, w["mu"], w["q"], w["R"])
+    n, l, m = w.get("atom", (2, 1, 1))
+    if device:
+        from boson_cloud_binary_b200 import hydrogenic_state
+        return hydrogenic_state(r, modes, w["mu"], w["q"], w["R"], n=n, l=l, m=m)
+    return hydrogenic_on_primary(r, modes, w["mu"], w["q"], w["R"], n=n, l=l, m=m)
 
 
 def make_solver(cls, w, psi0, precision=None):
@@ -428,7 +440,7 @@ def run_ours(args):
     select_device(local)
     w = dict(WORKLOADS[args.config])
     mixed = w["precision"] == "mixed"
-    psi0 = initial_state(w)
+    psi0 = initial_state(w, device=True)
     cn = make_solver(CrankNicolsonModes, w, psi0, w["precision"])
     ref = make_solver(CrankNicolsonModes, w, psi0, "fp64") if mixed and not args.no_fp64_arm else None
     T = cn.coupling_info()[1]

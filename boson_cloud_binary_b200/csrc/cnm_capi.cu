@@ -547,7 +547,9 @@ struct Solver {
         // per-warp sums of its reductions
         diag3_smem = base + (size_t)(2 * n_modes + 3 * (APPLY_THREADS / 32)) * sizeof(double);
         if (diag3_smem > (size_t)dyn_max) throw Error(CNM_EINVAL, "Too many modes for the diagnostics pass's shared tile");
-        CK(set_diag3_smem((int)diag3_smem));
+        // the attribute is shared by every handle of the process: the device's limit, not
+        // this handle's size (a smaller value set by another handle would fail this one's launch)
+        CK(set_diag3_smem(dyn_max));
         const BlockedCoupling &b = plan3.blocks;
         upload(d2_chunk_l, b.chunk_l);
         upload(d2_chunk_nrows, b.chunk_nrows);

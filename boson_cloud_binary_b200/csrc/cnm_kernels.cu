@@ -104,6 +104,28 @@ __device__ __forceinline__ void coupling_block3(const double *__restrict__ g, in
     }
 }
 
+// One (chunk, l1) block with its leading s_eff multipoles (dispatched to the compile-time width).
+template <int SMAX, int RB, bool DVDT, bool GSM>
+__device__ __forceinline__ void coupling_block_dispatch3(int s_eff, const double *g, int stride, int ncols, int col0,
+                                                         const double2 *zs, const double *hs_l0, const int *mode_m,
+                                                         int lane, double2 (&acc)[RB][2], double2 (&accm)[RB][2])
+{
+#define CNM_CASE3(S2)                                                                                            \
+    case S2:                                                                                                     \
+        if (S2 <= SMAX)                                                                                          \
+            coupling_block3<(S2 <= SMAX ? S2 : 1), RB, DVDT, GSM>(g, stride, ncols, col0, zs, hs_l0, mode_m,    \
+                                                                  lane, acc, accm);                              \
+        break;
+    switch (s_eff) {
+        CNM_CASE3(1) CNM_CASE3(2) CNM_CASE3(3) CNM_CASE3(4) CNM_CASE3(5) CNM_CASE3(6) CNM_CASE3(7)
+        CNM_CASE3(8) CNM_CASE3(9) CNM_CASE3(10) CNM_CASE3(11) CNM_CASE3(12) CNM_CASE3(13) CNM_CASE3(14)
+        CNM_CASE3(15) CNM_CASE3(16) CNM_CASE3(17) CNM_CASE3(18) CNM_CASE3(19) CNM_CASE3(20) CNM_CASE3(21)
+        CNM_CASE3(22) CNM_CASE3(23) CNM_CASE3(24) CNM_CASE3(25)
+    default: break;
+    }
+#undef CNM_CASE3
+}
+
 template <int SMAX, int RB, bool DVDT, bool GSM>
 __device__ __forceinline__ void coupling_chunk3(const BlockTable &bt, const double *gbase, int goff0, int l_max, int ci,
                                                 int lcut, const double2 *zs, const double *hs, const int *mode_m,
@@ -119,34 +141,19 @@ __device__ __forceinline__ void coupling_chunk3(const BlockTable &bt, const doub
         const int s_eff = min(S, (lcut - L0) / 2 + 1);
         const double *g = gbase + (bt.chunk_goff[ci * (l_max + 1) + l1] - goff0);
         const int stride = (S + 1) & ~1, col0 = bt.l_off[l1];
-        const double *hs_l0 = hs + L0 * TILE3;
-#define CNM_CASE3(S2)                                                                                            \
-    case S2:                                                                                                     \
-        if (S2 <= SMAX)                                                                                          \
-            coupling_block3<(S2 <= SMAX ? S2 : 1), RB, DVDT, GSM>(g, stride, l1 + 1, col0, zs, hs_l0, mode_m,   \
-                                                                  lane, acc, accm);                              \
-        break;
-        switch (s_eff) {
-            CNM_CASE3(1) CNM_CASE3(2) CNM_CASE3(3) CNM_CASE3(4) CNM_CASE3(5) CNM_CASE3(6) CNM_CASE3(7)
-            CNM_CASE3(8) CNM_CASE3(9) CNM_CASE3(10) CNM_CASE3(11) CNM_CASE3(12) CNM_CASE3(13) CNM_CASE3(14)
-            CNM_CASE3(15) CNM_CASE3(16) CNM_CASE3(17) CNM_CASE3(18) CNM_CASE3(19) CNM_CASE3(20) CNM_CASE3(21)
-            CNM_CASE3(22) CNM_CASE3(23) CNM_CASE3(24) CNM_CASE3(25)
-        default: break;
-        }
-#undef CNM_CASE3
+        coupling_block_dispatch3<SMAX, RB, DVDT, GSM>(s_eff, g, stride, l1 + 1, col0, zs, hs + L0 * TILE3, mode_m,
+                                                      lane, acc, accm);
     }
 }
 
-template <int SMAX, int RB, int VP, bool GSM>
-__device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
-                                             const double *gbase, int goff0, const ApplyArgs &a, const double2 *zs,
-                                             const double2 *ph, const double *hs, int lane, int i0, int lcut, int ci,
-                                             double (&dacc)[4])
+// The output rows of one chunk at the lane's two nodes from the coupling sums acc (accm for
+// dV/dt): stencil, centrifugal term, CAP, sinks, the store and the fused inner products.
+template <int RB, int VP>
+__device__ __forceinline__ void apply_epilogue3(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
+                                                const ApplyArgs &a, const double2 *ph, int lane, int i0, int ci,
+                                                const double2 (&acc)[RB][2], const double2 (&accm)[RB][2],
+                                                double (&dacc)[4])
 {
-    double2 acc[RB][2], accm[RB][2];
-    if (VP != V_NONE)
-        coupling_chunk3<SMAX, RB, VP == V_DVDT, GSM>(bt, gbase, goff0, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane,
-                                                     acc, accm);
     const int Nr = g.Nr;
     const double alpha_d = 1.0 / (g.dr * g.dr), inv2mu = 1.0 / (2 * g.mu);
 #pragma unroll
@@ -197,6 +204,21 @@ __device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable 
             }
         }
     }
+}
+
+template <int SMAX, int RB, int VP, bool GSM>
+__device__ __forceinline__ void apply_chunk3(const Grid &g, const CouplingTable &ct, const BlockTable &bt,
+                                             const double *gbase, int goff0, const ApplyArgs &a, const double2 *zs,
+                                             const double2 *ph, const double *hs, int lane, int i0, int lcut, int ci,
+                                             double (&dacc)[4])
+{
+    double2 acc[RB][2], accm[RB][2];
+#pragma unroll
+    for (int rr = 0; rr < RB; ++rr) acc[rr][0] = acc[rr][1] = accm[rr][0] = accm[rr][1] = cmake(0.0, 0.0);
+    if (VP != V_NONE)
+        coupling_chunk3<SMAX, RB, VP == V_DVDT, GSM>(bt, gbase, goff0, ct.l_max, ci, lcut, zs, hs, ct.mode_m, lane,
+                                                     acc, accm);
+    apply_epilogue3<RB, VP>(g, ct, bt, a, ph, lane, i0, ci, acc, accm, dacc);
 }
 
 // CTA (tile, group): the group's warp lists (ApplyPlan), one per warp; the group's

@@ -203,6 +203,7 @@ constexpr int TC_KMAX = 32;                  // multipoles (2 l_max + 1) the ker
 constexpr int TC_WS = 2 * TC_NT + 4;         // row stride (floats) of the accumulator image W[j][m]:
                                              // 16-byte stores of 8 consecutive rows hit distinct banks
 constexpr float TC_HCUT = 1e-9f;             // multipoles below this fraction of the monopole are skipped
+constexpr int TC_SMEM_MAX = 220 * 1024;      // dynamic shared memory of a plan (static ~3.3 KiB beside it)
 
 // Bytes of the region that holds the Z stages and, in the epilogue, the accumulator image.
 __host__ __device__ constexpr size_t tc_zregion(int kp)
@@ -692,7 +693,7 @@ bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
     p.a_stage = (g_stage_bytes + 127) / 128 * 128;
     const size_t fixed = tc_zregion(p.kp) + (size_t)K * TC_NT * 4 + (size_t)p.kp * 12 + (size_t)2 * TC_NT * 4 + 128;
     // as many Gaunt stages as fit (3 to 8, at most K: every tile runs gst - 1 multipoles)
-    const size_t budget = 220 * 1024;
+    const size_t budget = TC_SMEM_MAX;
     p.gst = (int)std::min<size_t>(TC_GMAX, budget > fixed ? (budget - fixed) / std::max(p.a_stage, 128) : 0);
     p.gst = std::min(p.gst, K);
     if (p.gst < 3) return false;
@@ -702,15 +703,17 @@ bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
     p.smem = std::max<size_t>(p.smem, 120 * 1024);
     p.tiles = (Nr + TC_NT - 1) / TC_NT;
     p.grid = std::min(p.tiles, n_sm);
-    return p.smem <= 225 * 1024;
+    return p.smem <= (size_t)TC_SMEM_MAX;
 }
 
 cudaError_t tc_prepare(const TcPlan &p)
 {
+    // the kernels' attribute is shared by every handle of the process: set it to the plan
+    // limit TC_SMEM_MAX, which every plan's shared memory stays within
     cudaError_t e = cudaSuccess;
 #define CNM_TC_ATTR1(KP_, DK_)                                                                                 \
     if (e == cudaSuccess)                                                                                      \
-        e = cudaFuncSetAttribute(k_tc_apply<KP_, DK_>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p.smem);
+        e = cudaFuncSetAttribute(k_tc_apply<KP_, DK_>, cudaFuncAttributeMaxDynamicSharedMemorySize, TC_SMEM_MAX);
 #define CNM_TC_ATTR(KP_) \
     if (p.kp == KP_) { CNM_TC_ATTR1(KP_, 0) CNM_TC_ATTR1(KP_, 1) CNM_TC_ATTR1(KP_, 23) CNM_TC_ATTR1(KP_, 4) }
     CNM_TC_PLANS(CNM_TC_ATTR)

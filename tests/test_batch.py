@@ -80,3 +80,22 @@ def test_mixed_batch_matches_single_binaries():
                 assert diags[i][key] == d[key], (i, k, key)
     for cb, cs in zip(batch.binaries, singles):
         assert np.array_equal(cb.psi, cs.psi)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", ["fp64", "mixed"])
+def test_handles_of_different_degrees_coexist(precision):
+    """Kernel attributes (dynamic shared memory limits) are process-wide: a handle created
+    after another one of a different l_max must not leave the first one unable to launch.
+    l_max 10 uses the generic operator and diagnostics kernels, l_max 4 the specialised ones."""
+    from boson_cloud_binary_b200 import CrankNicolsonModes
+    big = (600, 60.0, 0.5, 0.0, 10, 0.3, 0.01, 0.5, 0.0, 12.0, False, True, 100, 0.0, 2.0)
+    small = (600, 60.0, 0.5, 0.0, 4, 0.3, 0.01, 0.5, 0.0, 12.0, False, True, 100, 0.0, 2.0)
+    a = CrankNicolsonModes(*big, precision=precision)
+    _setup_smooth(a, big)
+    b = CrankNicolsonModes(*small, precision=precision)
+    _setup_smooth(b, small)
+    for k in range(1, 3):
+        a.step(k)
+        b.step(k)
+    assert np.isfinite(np.abs(a.psi)).all() and np.isfinite(np.abs(b.psi)).all()

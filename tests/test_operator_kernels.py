@@ -25,13 +25,14 @@ def test_specialised_and_generic_operator_kernels_agree(l_max):
         c.run(2, 50.0)
     rng = np.random.default_rng(7)
     x = rng.normal(size=cn.Nr * cn.n_modes) + 1j * rng.normal(size=cn.Nr * cn.n_modes)
-    for op in ("H", "V", "A", "B", "A_full", "schrodinger_rhs"):
+    for op in ("H", "V", "A", "B", "A_full", "schrodinger_rhs", "H0", "dVdt"):
         cn.set_operator_kernel(True)
         ys = cn.apply(op, x)
         cn.set_operator_kernel(False)
         yg = cn.apply(op, x)
         yo = orc.apply(op, x)
         scale = np.linalg.norm(yo)
+        assert scale > 0.0, op
         assert np.linalg.norm(ys - yg) <= 1e-13 * scale, f"{op}: kernels differ"
         assert np.linalg.norm(ys - yo) <= 1e-12 * scale, f"{op}: specialised kernel vs oracle"
     cn.set_operator_kernel(True)
