@@ -402,6 +402,23 @@ def run_reference(args):
     return 0
 
 
+def reduce_max(v, dist, device):
+    """The largest value over the ranks of the process group (v itself without one)."""
+    if dist is None:
+        return v
+    import torch
+    tt = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+    return float(tt.item())
+
+
+def whole_job(units_per_rank, ms_max, ws):
+    """Replicas: every rank advances its own binary, so the job's units are the ranks' sum and
+    its time the slowest rank's (ms_max, already maxed over the ranks)."""
+    units = units_per_rank * ws
+    return units, units / (ms_max / 1e3)
+
+
 def timed_steps(cn, k0, steps):
     """Device-event time (ms) of `steps` steps with the state resident in HBM, the launches
     the steps made, and the solver iterations / passes of each step."""
@@ -450,12 +467,7 @@ def run_ours(args):
             dist.barrier()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        import torch
-        tt = torch.tensor([v], device=f"cuda:{local}")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        return float(tt.item())
+        return reduce_max(v, dist, f"cuda:{local}")
 
     k = 1
     for _ in range(args.warmup):
@@ -479,8 +491,7 @@ def run_ours(args):
     k += args.steps
     barrier()
     ms = max_over_ranks(ms)
-    units = w["n_modes"] * w["Nr"] * args.steps * ws
-    value = units / (ms / 1e3)
+    units, value = whole_job(w["n_modes"] * w["Nr"] * args.steps, ms, ws)
     accuracy = None
     if ref is not None:
         ms_ref = max_over_ranks(ms_ref)
@@ -591,6 +602,13 @@ def run_batch(args):
     the same binaries in FP64 beside it.  Wall time of the synchronous batch steps (the
     library returns after every binary's step completed)."""
     ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     from boson_cloud_binary_b200 import Batch, select_device
     select_device(local)
     w = dict(WORKLOADS["c4"])
@@ -641,10 +659,15 @@ def run_batch(args):
             if fp64 is not None:
                 fp64.step(k)
             k += 1
+        if dist is not None:
+            dist.barrier()
         el, launches = timed(mixed, k, args.steps)
     el64 = timed(fp64, k, args.steps)[0] if fp64 is not None else None
     k += args.steps
-    value = units_per_step * args.steps / el
+    el = reduce_max(el, dist, f"cuda:{local}")
+    if el64 is not None:
+        el64 = reduce_max(el64, dist, f"cuda:{local}")
+    units_job, value = whole_job(units_per_step * args.steps, 1e3 * el, ws)
     # per-class kernel times over the binaries (device events on each binary's stream)
     names = ("apply", "tc_apply", "precond_solve", "precond_solve32", "precond_factor", "diagnostics")
     for cn in mixed.binaries:
@@ -689,7 +712,7 @@ def run_batch(args):
         mixed.step(k + q)
     for h_, cn in zip(hosts, mixed.binaries):
         h_[:] = cn.psi.view(np.float64)
-    e2e_s = time.perf_counter() - t0
+    e2e_s = reduce_max(time.perf_counter() - t0, dist, f"cuda:{local}")
     state_bytes = sum(16 * s_.size for s_ in states)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * el / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -700,15 +723,18 @@ def run_batch(args):
                        "l2": "working set > L2 (the states alone are %.0f MB complex128)" % (state_bytes / 1e6),
                        "timing": "wall time of synchronous batch steps"},
             "roofline": roof, "kernels": kshare,
-            "e2e": {"value": units_per_step * args.steps / e2e_s, "unit": UNIT,
+            "e2e": {"value": units_job / e2e_s, "unit": UNIT,
                     "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
                     "note": "states uploaded once and downloaded once per timed run"},
             "clocks": clocks.summary(), "gpu_launches": int(launches)}
     if el64 is not None:
-        line["fp64_arm"] = {"value": units_per_step * args.steps / el64, "ms_per_step": 1e3 * el64 / args.steps}
+        line["fp64_arm"] = {"value": units_job / el64, "ms_per_step": 1e3 * el64 / args.steps}
         line["mixed_over_fp64"] = el64 / el
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
     return 0
 
 
