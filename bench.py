@@ -460,6 +460,10 @@ def run_ours(args):
     psi0 = initial_state(w, device=True)
     cn = make_solver(CrankNicolsonModes, w, psi0, w["precision"])
     ref = make_solver(CrankNicolsonModes, w, psi0, "fp64") if mixed and not args.no_fp64_arm else None
+    # launch plans by timed search (the operator kernel's row groups, the tensor-core apply's
+    # Gaunt stages), before any timed work
+    tuning = cn.autotune() if not args.no_autotune else None
+    tuning_ref = ref.autotune() if ref is not None and not args.no_autotune else None
     T = cn.coupling_info()[1]
 
     def barrier():
@@ -570,7 +574,8 @@ def run_ours(args):
                                 "tolerance")}
     cfg.update({"parallelism": f"replicas{ws}", "l2": "working set > L2 (the state alone is "
                 f"{w['n_modes'] * w['Nr'] * 16 / 1e6:.0f} MB complex128)",
-                "iterations_mean": float(np.mean(iters)) if iters else None, "plan": plan,
+                "iterations_mean": float(np.mean(iters)) if iters else None, "plan": plan, "autotune": tuning,
+                "autotune_fp64_arm": tuning_ref,
                 "kernel_breakdown_steps": prof_steps})
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -746,6 +751,7 @@ def main():
     ap.add_argument("--config", default="c3", choices=sorted(WORKLOADS))
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the creation-time launch plans")
     ap.add_argument("--no-fp64-arm", action="store_true",
                     help="mixed workload only: skip the FP64 arm beside it (for profiling one arm)")
     args = ap.parse_args()

@@ -77,7 +77,7 @@ EXPORTS = ("cnm_create", "cnm_destroy", "cnm_last_error", "cnm_create_error", "c
            "cnm_plan_info", "cnm_measure_fp64_peak", "cnm_set_operator_kernel",
            "cnm_batch_create", "cnm_batch_size", "cnm_batch_handle", "cnm_batch_step", "cnm_batch_destroy",
            "cnm_displaced_100_state", "cnm_apply_lowp", "cnm_mixed_info", "cnm_mixed_trace", "cnm_launch_count", "cnm_tc_blocks",
-           "cnm_hydrogenic_state")
+           "cnm_hydrogenic_state", "cnm_autotune", "cnm_set_tuning", "cnm_device_name")
 
 def displaced_100_state(r, modes, mu, x_bh):
     """displaced_100_state (src/DisplacedAtom.cpp:12-76) on the device: the mode projection
@@ -202,6 +202,9 @@ def load_library():
     L.cnm_timer_start.argtypes = [p]
     L.cnm_timer_stop.argtypes = [p, dp]
     L.cnm_plan_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.cnm_autotune.argtypes = [p, C.POINTER(i32), C.POINTER(i32)]
+    L.cnm_set_tuning.argtypes = [p, i32, i32]
+    L.cnm_device_name.argtypes = [C.c_char_p, i32]
     L.cnm_measure_fp64_peak.argtypes = [dp]
     L.cnm_set_operator_kernel.argtypes = [p, i32]
     L.cnm_batch_create.argtypes = [C.POINTER(cnm_params), i32, C.POINTER(C.c_void_p)]
@@ -263,6 +266,7 @@ class CrankNicolsonModes:
             self.__dict__["_owned"] = False
         self.__dict__["_h"] = h
         self.__dict__["_lib"] = lib
+        self.__dict__["precision"] = precision
         n = C.c_int32()
         lib.cnm_n_modes(h, C.byref(n))
         l = np.zeros(n.value, np.int32)
@@ -483,6 +487,38 @@ class CrankNicolsonModes:
         """Select the operator kernel specialised for l_max <= 8 (True, default) or the
         generic plan-driven one (False)."""
         self._check(self._lib.cnm_set_operator_kernel(self._h, int(bool(specialised))))
+
+    def autotune(self, cache_file=None):
+        """Timed search of the launch plans (cnm_autotune): the operator kernel's row groups and,
+        on a mixed handle, the tensor-core apply's Gaunt stages.  With `cache_file` (JSON) the
+        choices are looked up by device, precision and shape and stored after a search.
+        Returns {"apply_groups", "tc_stages", "cached"}."""
+        import json
+        key = None
+        cache = {}
+        if cache_file:
+            dev = C.create_string_buffer(256)
+            self._lib.cnm_device_name(dev, 256)
+            key = f"{dev.value.decode()}|{self.precision}|l{self.l_max}|n{self.n_modes}|N{self.Nr}"
+            if os.path.exists(cache_file):
+                with open(cache_file) as f:
+                    cache = json.load(f)
+            if key in cache:
+                c = cache[key]
+                self._check(self._lib.cnm_set_tuning(self._h, int(c["apply_groups"]), int(c["tc_stages"])))
+                return dict(c, cached=True)
+        g, st = C.c_int32(), C.c_int32()
+        self._check(self._lib.cnm_autotune(self._h, C.byref(g), C.byref(st)))
+        out = {"apply_groups": g.value, "tc_stages": st.value}
+        if key is not None:
+            cache[key] = out
+            with open(cache_file, "w") as f:
+                json.dump(cache, f, indent=1, sort_keys=True)
+        return dict(out, cached=False)
+
+    def set_tuning(self, apply_groups=0, tc_stages=0):
+        """Apply launch-plan choices (cnm_set_tuning; 0 = the creation-time plan)."""
+        self._check(self._lib.cnm_set_tuning(self._h, int(apply_groups), int(tc_stages)))
 
     def plan_info(self):
         """Launch plan chosen for this device: {scan_per, scan_cluster, apply_groups,

@@ -290,6 +290,8 @@ struct Solver {
     // red slots past the diagnostics' 2 n + 3 sums: |rhs|^2 and the candidate's residual^2
     int RED_RHS = 0, RED_RES = 0;
     size_t diag3_smem = 0;       // the diagnostics pass on the operator kernel's tiles
+    int n_sm = 0;
+    int tc_amax = 0;             // bytes of the largest multipole's Gaunt image (tensor-core stages)
     // pinned host staging
     double *h_stage = nullptr;
     size_t h_stage_n = 0;
@@ -302,6 +304,7 @@ struct Solver {
     DevBuf<uint8_t> d_tcblob;
     DevBuf<int> d_tc_loff, d_tc_lbytes, d_tc_slices, d_tc_lnblk;
     DevBuf<int> d_tc_ctr;           // tile counter of the tensor-core apply (zero between launches)
+    DevBuf<unsigned> d_mx_ticket;   // finished blocks of a mixed-solve vector kernel (zero between launches)
     DevBuf<float2> m_r, m_y, m_v, m_s, m_z, m_t, m_d, m_xa, dinv32, m_r1, m_q;
     DevBuf<double2> m_r64, m_dots;  // m_dots: [0..1] sink projections, [2..3] corrected ones
     DevBuf<MixScalars> d_msc;
@@ -412,6 +415,7 @@ struct Solver {
         CK(cudaGetDevice(&dev));
         int nsm = 0;
         CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+        n_sm = nsm;
         CK(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
         vec_blocks = (int)std::max<int64_t>(1, std::min<int64_t>((nN + VEC_THREADS - 1) / VEC_THREADS, (int64_t)nsm * 4));
         upload(d_r, r);
@@ -446,7 +450,8 @@ struct Solver {
         // partials: the vector kernels' slots, the diagnostics pass's 2n + 3 slots per CTA
         // (64-node tiles x row groups) and the operator kernel's fused reductions
         const size_t tiles3 = (size_t)(Nr + APPLY3_TILE - 1) / APPLY3_TILE;
-        const size_t diag_blocks = std::max<size_t>(tiles3 * plan3.n_groups, diag5_blocks(l_max, Nr));
+        // (for any row-group count the autotuner may choose: up to 8 per tile)
+        const size_t diag_blocks = std::max<size_t>(tiles3 * 8, diag5_blocks(l_max, Nr));
         d_partials.alloc(std::max<size_t>({(size_t)6 * vec_blocks, (size_t)(2 * n_modes + 3) * diag_blocks,
                                            (size_t)4 * 8 * tiles3}));
         a5_groups = apply5_groups(l_max);
@@ -474,6 +479,7 @@ struct Solver {
         tg = build_tc_gaunt(cpl);
         int amax = 0;
         for (int b : tg.l_bytes) amax = std::max(amax, b);
+        tc_amax = amax;
         if (!tc_plan(n_modes, K, Nr, amax, nsm, tcp))
             throw Error(CNM_EINVAL, "The mixed solve supports at most 112 modes (l_max <= 13)");
         // TC_REPLICAS copies of the image (each 256-byte aligned); CTA b reads copy b % TC_REPLICAS
@@ -487,6 +493,7 @@ struct Solver {
         upload(d_tc_slices, tg.slices);
         upload(d_tc_lnblk, tg.l_nblk);
         d_tc_ctr.alloc(2);
+        d_mx_ticket.alloc(1);
         CK(tc_prepare(tcp));
         for (DevBuf<float2> *b : {&m_r, &m_y, &m_v, &m_s, &m_z, &m_t, &m_d, &m_xa, &dinv32, &m_r1, &m_q}) b->alloc(nN);
         m_r64.alloc(nN);
@@ -510,7 +517,7 @@ struct Solver {
     // warp lists (cnm::plan_coupling) and the resident CTAs per SM give an estimated
     // time  waves x heaviest warp list; the cheapest plan is kept.  A group's weights
     // are staged in shared memory when they fit beside the tile.
-    void plan_operator(int nsm)
+    void plan_operator(int nsm, int force_ng = 0)
     {
         int optin = 0, dev = 0;
         CK(cudaGetDevice(&dev));
@@ -524,7 +531,9 @@ struct Solver {
         if (base > (size_t)dyn_max) throw Error(CNM_EINVAL, "Too many modes for the operator kernel's shared tile");
         const int tiles = (Nr + APPLY3_TILE - 1) / APPLY3_TILE;
         double best = 0.0;
+        plan3 = CouplingPlan();
         for (int ng = 1; ng <= 8; ++ng) {
+            if (force_ng > 0 && ng != force_ng) continue;
             CouplingPlan pl = plan_coupling(cpl, ng, APPLY_THREADS / 32);
             const size_t with_g = base + (size_t)pl.max_group_g * sizeof(double);
             const bool gsm = with_g <= (size_t)dyn_max;
@@ -559,6 +568,113 @@ struct Solver {
         upload(d2_block_g, b.g);
         upload(d3_list_ptr, plan3.list_ptr);
         upload(d3_group_goff, plan3.group_goff);
+    }
+
+    // ------------------------------------------------------------ autotuner
+    // Device-event time (ms per launch) of `reps` operator applications A x (no sinks, no
+    // reductions) with the current plan, after one untimed launch.
+    double time_operator(int reps)
+    {
+        ApplyArgs a = base_args(psi.p, tmp.p);
+        a.alpha = cmake(1.0, 0.0);
+        a.beta = cmake(0.0, 0.5 * op.dt);
+        a.use_h0 = 1;
+        a.use_cap = 1;
+        a.vpart = V_POT;
+        launch_apply(a);
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, stream));
+        for (int q = 0; q < reps; ++q) launch_apply(a);
+        CK(cudaEventRecord(e1, stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return ms / reps;
+    }
+
+    // The same for the tensor-core apply on the complex64 copy of psi.
+    double time_tc(int reps)
+    {
+        k_to_f32<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, psi.p, m_xa.p);
+        launch_check();
+        TcArgs a = tc_a_args(m_xa.p, m_t.p, nullptr, 0, nullptr, op.dt);
+        launch_tc(a);
+        cudaEvent_t e0, e1;
+        CK(cudaEventCreate(&e0));
+        CK(cudaEventCreate(&e1));
+        CK(cudaEventRecord(e0, stream));
+        for (int q = 0; q < reps; ++q) launch_tc(a);
+        CK(cudaEventRecord(e1, stream));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        cudaEventDestroy(e0);
+        cudaEventDestroy(e1);
+        return ms / reps;
+    }
+
+    // Re-plans with the given choices (0 keeps the cost model's / the largest that fits).
+    void set_tuning(int apply_groups, int tc_stages)
+    {
+        if (apply_groups < 0 || apply_groups > 8 || tc_stages < 0 || tc_stages > TC_MAX_STAGES)
+            throw Error(CNM_EINVAL, "tuning choices out of range (row groups 0..8, stages 0..8)");
+        plan_operator(n_sm, apply_groups);
+        if (mixed) {
+            TcPlan p;
+            if (!tc_plan(n_modes, K, Nr, tc_amax, n_sm, p, tc_stages))
+                throw Error(CNM_EINVAL, "no tensor-core plan with that many stages");
+            tcp = p;
+        }
+    }
+
+    // Timed search: every row-group count of the operator kernel that has a resident
+    // configuration, then (mixed handles) every Gaunt-stage count of the tensor-core apply
+    // from 3 to the most that fit; the fastest of each is kept.
+    void autotune(int *apply_groups, int *tc_stages)
+    {
+        if (!initialized) throw Error(CNM_ELOGIC, "autotune needs an initialized solver (its operators and state)");
+        sync();
+        double best = 1e30;
+        int best_ng = 0;
+        for (int ng = 1; ng <= 8; ++ng) {
+            try {
+                plan_operator(n_sm, ng);
+            } catch (const Error &) {
+                continue;
+            }
+            const double ms = time_operator(5);
+            if (ms < best) {
+                best = ms;
+                best_ng = ng;
+            }
+        }
+        if (best_ng == 0) throw Error(CNM_EINVAL, "No resident configuration of the operator kernel");
+        plan_operator(n_sm, best_ng);
+        *apply_groups = best_ng;
+        *tc_stages = 0;
+        if (mixed) {
+            TcPlan full;
+            tc_plan(n_modes, K, Nr, tc_amax, n_sm, full);
+            double bt = 1e30;
+            int best_g = full.gst;
+            for (int g = 3; g <= full.gst; ++g) {
+                TcPlan p;
+                if (!tc_plan(n_modes, K, Nr, tc_amax, n_sm, p, g)) continue;
+                tcp = p;
+                const double ms = time_tc(5);
+                if (ms < bt) {
+                    bt = ms;
+                    best_g = g;
+                }
+            }
+            tc_plan(n_modes, K, Nr, tc_amax, n_sm, tcp, best_g);
+            *tc_stages = best_g;
+        }
+        sync();
     }
 
     // Cluster plan of the exact preconditioner scans.  Candidates: every odd count of
@@ -1340,6 +1456,8 @@ struct Solver {
         a.partials = m_part.p;
         a.status = d_status.p;
         a.tile_ctr = d_tc_ctr.p;
+        a.mx_stage = -1;
+        a.msc = d_msc.p;
         return a;
     }
 
@@ -1351,11 +1469,16 @@ struct Solver {
         kt_end(TK_TC);
     }
 
-    void mx_finish(int nblocks, int nslots, int stage)
+    // the last-block scalar stage of a mixed-solve vector kernel
+    MxFinish mxf(int stage)
     {
-        k_mx_finish<<<1, 256, 0, stream>>>(m_part.p, nblocks, nslots, d_msc.p, stage);
-        launch_check();
+        MxFinish f;
+        f.sc = d_msc.p;
+        f.stage = stage;
+        f.ticket = d_mx_ticket.p;
+        return f;
     }
+
 
     // out = P32^{-1} in (mode 0); mode 1: s = r - alpha v formed and stored to s_out,
     // out = P32^{-1} s; mode 2: out = P32^{-1} (r + beta (r0 - omega v)) with r0 = m_r
@@ -1408,8 +1531,8 @@ struct Solver {
                 a.n_dots = 1;
                 a.dot_kind[0] = 1;
                 a.dot_ext[0] = m_r.p;  // r0
+                a.mx_stage = first ? MX_ALPHA : MX_ALPHA2;
                 launch_tc(a);
-                mx_finish(tcp.tiles, 2, first ? MX_ALPHA : MX_ALPHA2);
             }
             psolve32(1, nullptr, m_z.p, first ? m_r.p : m_r1.p, first ? m_s.p : m_q.p);
             wood32(sk, k, m_z.p);
@@ -1419,18 +1542,16 @@ struct Solver {
                 a.dot_kind[0] = 2;
                 a.dot_ext[0] = first ? m_s.p : m_q.p;
                 a.dot_kind[1] = 3;
+                a.mx_stage = MX_OMEGA;
                 launch_tc(a);
-                mx_finish(tcp.tiles, 4, MX_OMEGA);
             }
             k_mx_update<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, x.p, m_y.p, m_z.p, m_d.p, first ? 1 : 0,
-                                                                last ? 1 : 0, m_part.p);
+                                                                last ? 1 : 0, m_part.p, mxf(last ? MX_D2 : -1));
             launch_check();
-            if (last) {
-                mx_finish(vec_blocks, 1, MX_D2);
-            } else {
-                k_mx_next<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, m_s.p, m_t.p, m_r.p, m_r1.p, m_part.p);
+            if (!last) {
+                k_mx_next<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, d_msc.p, m_s.p, m_t.p, m_r.p, m_r1.p, m_part.p,
+                                                                  mxf(MX_BETA));
                 launch_check();
-                mx_finish(vec_blocks, 2, MX_BETA);
             }
         }
         ++mx_passes;
@@ -1441,9 +1562,9 @@ struct Solver {
     {
         sink_dots(x.p, d_dots.p, sk, k);
         apply_A(x.p, tmp.p, sk, k, d_dots.p, dtv);
-        k_mx_resid<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, tmp.p, m_r64.p, diff, m_r.p, m_part.p);
+        k_mx_resid<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, tmp.p, m_r64.p, diff, m_r.p, m_part.p,
+                                                           mxf(MX_R64));
         launch_check();
-        mx_finish(vec_blocks, 1, MX_R64);
         ++mx_fp64;
     }
 
@@ -1461,8 +1582,8 @@ struct Solver {
         a.n_dots = 1;
         a.dot_kind[0] = 4;
         a.dot_ext64 = m_r64.p;
+        a.mx_stage = MX_TCRES;
         launch_tc(a);
-        mx_finish(tcp.tiles, 2, MX_TCRES);
     }
 
     // Calibration of the tensor-core residual check on the pass just verified in fp64:
@@ -1480,8 +1601,8 @@ struct Solver {
         a.n_dots = 1;
         a.dot_kind[0] = 4;
         a.dot_ext64 = cand.p;
+        a.mx_stage = MX_ECAL;
         launch_tc(a);
-        mx_finish(tcp.tiles, 2, MX_ECAL);
     }
 
     // psi candidate = mask x into cand, the diagnostics pass on it, the read-backs (the
@@ -1535,9 +1656,9 @@ struct Solver {
         k_to_f32<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dinv.p, dinv32.p);
         launch_check();
         if (k > 0) wood_setup(sk, k, dtv);
-        k_mx_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, psi.p, x.p, m_r64.p, m_r.p, m_part.p);
+        k_mx_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, psi.p, x.p, m_r64.p, m_r.p, m_part.p,
+                                                           mxf(MX_B2R0));
         launch_check();
-        mx_finish(vec_blocks, 2, MX_B2R0);
         mixed_pass(sk, k, dtv, 1);
         mixed_resid64(sk, k, dtv, cand.p);
         mixed_calibrate(sk, k, dtv);
@@ -2796,6 +2917,34 @@ int cnm_measure_fp64_peak(double *tflops)
         g_create_error = e.what();
         return CNM_ECUDA;
     }
+}
+
+int cnm_device_name(char *name, int32_t size)
+{
+    if (!name || size < 1) return CNM_EINVAL;
+    int dev = 0;
+    cudaDeviceProp prop;
+    if (cudaGetDevice(&dev) != cudaSuccess || cudaGetDeviceProperties(&prop, dev) != cudaSuccess) {
+        g_create_error = "cudaGetDeviceProperties failed";
+        return CNM_ECUDA;
+    }
+    std::snprintf(name, (size_t)size, "%s", prop.name);
+    return CNM_OK;
+}
+
+int cnm_autotune(cnm_handle *h, int32_t *apply_groups, int32_t *tc_stages)
+{
+    return guarded(h, [&](cnm::Solver &s) {
+        int g = 0, st = 0;
+        s.autotune(&g, &st);
+        if (apply_groups) *apply_groups = g;
+        if (tc_stages) *tc_stages = st;
+    });
+}
+
+int cnm_set_tuning(cnm_handle *h, int32_t apply_groups, int32_t tc_stages)
+{
+    return guarded(h, [&](cnm::Solver &s) { s.set_tuning(apply_groups, tc_stages); });
 }
 
 int cnm_plan_info(const cnm_handle *h, int32_t *scan_per, int32_t *scan_cluster, int32_t *apply_groups,

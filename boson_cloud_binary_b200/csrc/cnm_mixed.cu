@@ -192,6 +192,8 @@ __device__ __forceinline__ uint32_t pack_f16(float lo, float hi)
     return *reinterpret_cast<const uint32_t *>(&v);
 }
 
+__device__ void mx_stage(const double *acc, MixScalars *sc, int stage);
+
 // ==================================================================== tensor-core apply
 
 constexpr int TC_WORKERS = 512;              // operand producers and epilogue (warps 0-15)
@@ -224,6 +226,7 @@ struct TcShared {
     int l_off[TC_KMAX], l_bytes[TC_KMAX], l_nblk[TC_KMAX];
     int slices[TC_KMAX * 16];
     double red[4 * 16];  // warp sums of a tile's fused reductions
+    int last;            // this CTA finished last (runs the launch's scalar stage)
 };
 
 // Bulk copy of multipole lv's Gaunt blocks into the G stage of use v (v % gst).
@@ -265,6 +268,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     constexpr int G_BLK = 4096;                // bytes of one G block (128 rows j x 16 columns k)
     constexpr uint32_t IDESC = idesc_f16(128, 2 * TC_NT);
     constexpr uint32_t NCOLS = 2 * TC_NT;      // one fp32 accumulator: 128 lanes (modes) x 256 columns
+    constexpr int NDOT = DK == 0 ? 0 : DK == 23 ? 2 : 1;  // fused reductions (complex slots)
     extern __shared__ __align__(128) uint8_t tc_smem[];
     __shared__ TcShared sh;
     const int n = g.n_modes, Nr = g.Nr;
@@ -400,7 +404,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 sk_c[s2] = make_double2(a.sink_coef[s2] * dd.x, a.sink_coef[s2] * dd.y);
             }
         }
-        constexpr int NDOT = DK == 0 ? 0 : DK == 23 ? 2 : 1;
         // the launch's reduction operand: complex64 (kinds 1, 2) or complex128 (kind 4)
         const float2 *__restrict__ ext32 = (DK == 1 || DK == 23) ? a.dot_ext[0] : nullptr;
         const double2 *__restrict__ ext64 = DK == 4 ? a.dot_ext64 : nullptr;
@@ -420,6 +423,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             const int i0 = tile * TC_NT;
+            // the epilogue's reduction operand of this tile into L2 while the tile's multipole
+            // loop runs (one bulk prefetch per mode row, within the vector)
+            if constexpr (DK != 0) {
+                if (tid < n) {
+                    constexpr size_t es = DK == 4 ? sizeof(double2) : sizeof(float2);
+                    const char *base = DK == 4 ? (const char *)ext64 : (const char *)ext32;
+                    const size_t end = (size_t)n * Nr * es;
+                    size_t b0 = ((size_t)tid * Nr + i0) * es, b1 = b0 + (size_t)min(TC_NT, Nr - i0) * es;
+                    b0 &= ~(size_t)15;
+                    b1 = min((b1 + 15) & ~(size_t)15, end & ~(size_t)15);
+                    if (b1 > b0)
+                        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(base + b0), "r"((uint32_t)(b1 - b0))
+                                     : "memory");
+                }
+            }
             // radial weights of the tile (K x TC_NT, independent loads spread over the
             // workers), 1/r^2 and the CAP weights of its nodes
             constexpr int HPT = TC_KMAX * TC_NT / TC_WORKERS;
@@ -661,6 +679,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         double sum = 0.0;
                         for (int w = 0; w < TC_CTRL; ++w) sum += sh.red[tid * 16 + w];
                         a.partials[(int64_t)tid * tiles + tile] = sum;
+                        __threadfence();  // before this CTA's finish ticket
                     }
                 }
             }
@@ -671,9 +690,29 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         if (sh.abort && a.status) atomicOr(a.status, 16);
         // the last CTA to finish resets the tile counter for the next launch on the stream
         __threadfence();
-        if (atomicAdd(a.tile_ctr + 1, 1) == (int)gridDim.x - 1) {
+        sh.last = atomicAdd(a.tile_ctr + 1, 1) == (int)gridDim.x - 1;
+        if (sh.last) {
             atomicExch(a.tile_ctr, 0);
             atomicExch(a.tile_ctr + 1, 0);
+        }
+    }
+    __syncthreads();
+    if constexpr (NDOT > 0) {
+        // the launch's scalar stage of the inner iteration (a.mx_stage), by the last CTA: the
+        // per-tile partials summed in tile order, one warp per slot
+        if (sh.last && a.mx_stage >= 0) {
+            if (warp < 2 * NDOT) {
+                double v = 0.0;
+                for (int t = lane; t < tiles; t += 32) v += __ldcg(a.partials + (int64_t)warp * tiles + t);
+                v = warp_sum(v);
+                if (lane == 0) sh.red[warp] = v;
+            }
+            __syncthreads();
+            if (tid == 0) {
+                double acc[6] = {0, 0, 0, 0, 0, 0};
+                for (int q = 0; q < 2 * NDOT; ++q) acc[q] = sh.red[q];
+                mx_stage(acc, a.msc, a.mx_stage);
+            }
         }
     }
     if (warp == TC_CTRL) {
@@ -685,7 +724,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 // Kernels by padded mode count KP (the worker thread keeps KP z values in registers).
 #define CNM_TC_PLANS(X) X(16) X(32) X(48) X(64) X(80) X(96) X(112)
 
-bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
+bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p, int max_gst)
 {
     p.kp = (n_modes + 15) / 16 * 16;
     p.nt = TC_NT;
@@ -696,6 +735,7 @@ bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p)
     const size_t budget = TC_SMEM_MAX;
     p.gst = (int)std::min<size_t>(TC_GMAX, budget > fixed ? (budget - fixed) / std::max(p.a_stage, 128) : 0);
     p.gst = std::min(p.gst, K);
+    if (max_gst > 0) p.gst = std::min(p.gst, max_gst);
     if (p.gst < 3) return false;
     p.smem = (size_t)p.gst * p.a_stage + fixed;
     // at least 120 KiB, so that one CTA (and its TMEM columns) is resident per SM and no
@@ -955,10 +995,42 @@ __device__ __forceinline__ void partials_out(double (&v)[NV], double *partials)
         for (int q = 0; q < NV; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = v[q];
 }
 
+// partials_out, then (f.stage >= 0) the scalar stage by the last block to finish: the
+// blocks' partials summed in block order, and the ticket reset for the next launch.
+template <int NV>
+__device__ __forceinline__ void partials_finish(double (&v)[NV], double *partials, const MxFinish &f)
+{
+    __shared__ double scr[NV * 32];
+    __shared__ double scr6[6 * 32];
+    __shared__ int last;
+    block_sum<NV>(v, scr);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) partials[(int64_t)q * gridDim.x + blockIdx.x] = v[q];
+        last = 0;
+        if (f.stage >= 0) {
+            __threadfence();
+            last = atomicAdd(f.ticket, 1u) == gridDim.x - 1;
+        }
+    }
+    __syncthreads();
+    if (!last) return;
+    double acc[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] += __ldcg(partials + (int64_t)q * gridDim.x + b);
+    block_sum<6>(acc, scr6);
+    if (threadIdx.x == 0) {
+        mx_stage(acc, f.sc, f.stage);
+        *f.ticket = 0u;
+    }
+}
+
 // x = psi, r = b - A_full psi = 2 (b - psi) (A_full psi = 2 psi - b by construction of b);
 // partials: |r|^2, |b|^2.
 __global__ void __launch_bounds__(VEC_THREADS) k_mx_start(int64_t n, const double2 *b, const double2 *psi,
-                                                          double2 *x, double2 *r64, float2 *r32, double *partials)
+                                                          double2 *x, double2 *r64, float2 *r32, double *partials,
+                                                          MxFinish f)
 {
     double acc[2] = {0.0, 0.0};
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -970,14 +1042,15 @@ __global__ void __launch_bounds__(VEC_THREADS) k_mx_start(int64_t n, const doubl
         acc[0] += rr * rr + ri * ri;
         acc[1] += bv.x * bv.x + bv.y * bv.y;
     }
-    partials_out<2>(acc, partials);
+    partials_finish<2>(acc, partials, f);
 }
 
 // r64 = b - A_full x, r32 = r64; with diff set, diff = r64_before - r64_after (the change
 // the last correction made, against which its tensor-core image is calibrated); partial
 // |r64|^2.
 __global__ void __launch_bounds__(VEC_THREADS) k_mx_resid(int64_t n, const double2 *b, const double2 *ax,
-                                                          double2 *r64, double2 *diff, float2 *r32, double *partials)
+                                                          double2 *r64, double2 *diff, float2 *r32, double *partials,
+                                                          MxFinish f)
 {
     double acc[1] = {0.0};
     for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < n; e += (int64_t)gridDim.x * blockDim.x) {
@@ -991,7 +1064,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_mx_resid(int64_t n, const doubl
         r32[e] = make_float2((float)rr, (float)ri);
         acc[0] += rr * rr + ri * ri;
     }
-    partials_out<1>(acc, partials);
+    partials_finish<1>(acc, partials, f);
 }
 
 // The pass's correction d (complex64): d = alpha y + omega z (first iteration) or
@@ -1000,7 +1073,7 @@ __global__ void __launch_bounds__(VEC_THREADS) k_mx_resid(int64_t n, const doubl
 // Partial |d|^2.
 __global__ void __launch_bounds__(VEC_THREADS) k_mx_update(int64_t n, const MixScalars *sc, double2 *x,
                                                            const float2 *y, const float2 *z, float2 *d, int first,
-                                                           int apply, double *partials)
+                                                           int apply, double *partials, MxFinish f)
 {
     const double2 al = sc->alpha, om = sc->omega;
     double acc[1] = {0.0};
@@ -1023,14 +1096,14 @@ __global__ void __launch_bounds__(VEC_THREADS) k_mx_update(int64_t n, const MixS
         }
         acc[0] += (double)df.x * df.x + (double)df.y * df.y;
     }
-    partials_out<1>(acc, partials);
+    partials_finish<1>(acc, partials, f);
 }
 
 // Inner residual after an iteration, r1 = s - omega t, and the partial conj(r0) . r1 of the
 // next iteration's rho.
 __global__ void __launch_bounds__(VEC_THREADS) k_mx_next(int64_t n, const MixScalars *sc, const float2 *s,
                                                          const float2 *t, const float2 *r0, float2 *r1,
-                                                         double *partials)
+                                                         double *partials, MxFinish f)
 {
     const double2 om = sc->omega;
     const float2 omf = make_float2((float)om.x, (float)om.y);
@@ -1042,20 +1115,15 @@ __global__ void __launch_bounds__(VEC_THREADS) k_mx_next(int64_t n, const MixSca
         acc[0] += (double)rv.x * r.x + (double)rv.y * r.y;
         acc[1] += (double)rv.x * r.y - (double)rv.y * r.x;
     }
-    partials_out<2>(acc, partials);
+    partials_finish<2>(acc, partials, f);
 }
 
 // Sum the partials in a fixed order and run one scalar step of the inner iteration.
-__global__ void k_mx_finish(const double *partials, int nblocks, int nslots, MixScalars *sc, int stage)
+
+// One scalar step of the inner iteration from the summed reductions acc (run by the last
+// CTA of the launch whose reductions they are).
+__device__ void mx_stage(const double *acc, MixScalars *sc, int stage)
 {
-    __shared__ double scr[6 * 32];
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x)
-#pragma unroll
-        for (int q = 0; q < 6; ++q)
-            if (q < nslots) acc[q] += partials[(int64_t)q * nblocks + b];
-    block_sum<6>(acc, scr);
-    if (threadIdx.x != 0) return;
     switch (stage) {
     case MX_B2R0:
         sc->rr = acc[0];

@@ -81,6 +81,8 @@ struct TcArgs {
     double *partials;         // [slot][tile]: per-tile sums, independent of the CTA that ran the tile
     int *status;              // bit 4: an mbarrier wait gave up
     int *tile_ctr;            // [2]: next tile, finished CTAs (zero between launches)
+    int mx_stage;             // scalar stage run by the last CTA on the reductions (-1: none)
+    struct MixScalars *msc;
 };
 
 // Host entry points (cnm_mixed.cu).
@@ -91,7 +93,9 @@ struct TcPlan {
     int a_stage = 0;          // bytes of one Gaunt stage (largest multipole blob)
     int gst = 3;              // Gaunt stages (copies run gst - 1 multipoles ahead)
 };
-bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p);
+// max_gst > 0 caps the Gaunt stages (the autotuner's candidates); 0 takes as many as fit.
+bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p, int max_gst = 0);
+constexpr int TC_MAX_STAGES = 8;
 cudaError_t tc_prepare(const TcPlan &p);
 cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, const int *mode_l, const int *mode_m,
                             int K, const TcTable &tt, const TcArgs &a);
@@ -129,16 +133,22 @@ struct Ps32Args {
 constexpr int PS32_THREADS = 256;
 __global__ void k_psolve32_cl(int Nr, int per, float2 off, const float2 *dinv, float2 *x, Ps32Args in);
 
+// The scalar stage a vector kernel's last block runs on its reductions (stage -1: none; the
+// ticket counts finished blocks and is zero between launches).
+struct MxFinish {
+    MixScalars *sc;
+    int stage;
+    unsigned *ticket;
+};
 // Vector kernels of the mixed solve (fp64 accumulations into per-CTA partials).
 __global__ void k_mx_start(int64_t n, const double2 *b, const double2 *psi, double2 *x, double2 *r64, float2 *r32,
-                           double *partials);
+                           double *partials, MxFinish f);
 __global__ void k_mx_resid(int64_t n, const double2 *b, const double2 *ax, double2 *r64, double2 *diff, float2 *r32,
-                           double *partials);
+                           double *partials, MxFinish f);
 __global__ void k_mx_update(int64_t n, const MixScalars *sc, double2 *x, const float2 *y, const float2 *z, float2 *d,
-                            int first, int apply, double *partials);
+                            int first, int apply, double *partials, MxFinish f);
 __global__ void k_mx_next(int64_t n, const MixScalars *sc, const float2 *s, const float2 *t, const float2 *r0,
-                          float2 *r1, double *partials);
-__global__ void k_mx_finish(const double *partials, int nblocks, int nslots, MixScalars *sc, int stage);
+                          float2 *r1, double *partials, MxFinish f);
 __global__ void k_to_f32(int64_t n, const double2 *a, float2 *b);
 __global__ void k_to_f64(int64_t n, const float2 *a, double2 *b);
 __global__ void k_sink_dots32(const float2 *x, int Nr, int n_modes, int n_sinks, const double2 *v0,

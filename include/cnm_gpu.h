@@ -284,6 +284,17 @@ int cnm_set_operator_kernel(cnm_handle *h, int32_t specialised);
  * register-resident chain microbenchmark timed with device events: the denominator of
  * the FP64 roofline of the operator kernels. */
 int cnm_measure_fp64_peak(double *tflops);
+/* Autotuner (no counterpart in the reference, which has no device plans): times every
+ * row-group count of the operator kernel that has a resident configuration (five
+ * applications of A to the current state each, device events on the handle's stream) and,
+ * on a CNM_MIXED handle, every Gaunt-stage count of the tensor-core apply from 3 to the most
+ * that fit; keeps the fastest of each and reports them.  Needs an initialized handle.
+ * cnm_set_tuning applies choices found earlier (0 = the creation-time plan: the cost
+ * model's row groups, as many stages as fit), e.g. from a cache keyed by device and shape. */
+int cnm_autotune(cnm_handle *h, int32_t *apply_groups, int32_t *tc_stages);
+/* The current device's name (the autotuner cache's key), NUL-terminated in name[size]. */
+int cnm_device_name(char *name, int32_t size);
+int cnm_set_tuning(cnm_handle *h, int32_t apply_groups, int32_t tc_stages);
 /* Launch plan chosen at creation for this device: nodes per thread and CTAs per cluster
  * of the exact preconditioner scans (0, 0 when the windowed scans are used), row groups
  * of the operator kernel in use (the kernel specialised for l_max <= 8 when it is

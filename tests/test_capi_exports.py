@@ -16,7 +16,8 @@ def declared_entry_points():
     names = []
     for h in os.listdir(os.path.join(ROOT, "include")):
         if h.endswith(".h"):
-            text = open(os.path.join(ROOT, "include", h)).read()
+            with open(os.path.join(ROOT, "include", h)) as f:
+                text = f.read()
             names += re.findall(r"^[a-z_ *]+?\b(cnm_[a-z0-9_]+)\s*\(", text, re.M)
     return sorted(set(names))
 

@@ -65,3 +65,39 @@ def test_specialised_and_generic_diagnostics_agree(l_max):
         for key in ("flux", "energy_flux", "norms", "energies"):
             a, b = np.asarray(d_s[key]), np.asarray(d_g[key])
             assert np.linalg.norm(a - b) <= 1e-11 * max(1e-300, np.linalg.norm(b)) + 1e-300, key
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision,l_max", [("fp64", 12), ("mixed", 8)])
+def test_autotuner_choices_keep_the_operator(precision, l_max, tmp_path):
+    """The autotuner's timed search changes launch plans only: the operator (and, for a
+    mixed handle, the step) computed after tuning, after re-applying the choices from its
+    JSON cache, and with the creation-time plan agree to rounding."""
+    from boson_cloud_binary_b200 import CrankNicolsonModes
+    from boson_cloud_binary_b200 import hydrogenic_state
+    args = (800, 80.0, 0.5, 0.0, l_max, 0.3, 0.01, 0.5, 0.0, 15.0, False, True, 10, 0.0, 2.0)
+    cn = CrankNicolsonModes(*args, precision=precision)
+    cn.set_initial_state_full(hydrogenic_state(cn.r, cn.modes, 0.3, 0.5, 15.0))
+    cn.evolve_orbit = False
+    cn.tolerance = 1e-12
+    cn.initialize()
+    cn.run(10, 60.0)
+    rng = np.random.default_rng(3)
+    x = rng.normal(size=cn.Nr * cn.n_modes) + 1j * rng.normal(size=cn.Nr * cn.n_modes)
+    y0 = cn.apply("A", x)
+    cache = str(tmp_path / "tune.json")
+    t1 = cn.autotune(cache_file=cache)
+    assert not t1["cached"] and 1 <= t1["apply_groups"] <= 8
+    assert (t1["tc_stages"] >= 3) if precision == "mixed" else (t1["tc_stages"] == 0)
+    y1 = cn.apply("A", x)
+    t2 = cn.autotune(cache_file=cache)
+    assert t2["cached"] and t2["apply_groups"] == t1["apply_groups"] and t2["tc_stages"] == t1["tc_stages"]
+    y2 = cn.apply("A", x)
+    scale = np.linalg.norm(y0)
+    assert np.linalg.norm(y1 - y0) <= 1e-13 * scale and np.linalg.norm(y2 - y0) <= 1e-13 * scale
+    cn.set_tuning(0, 0)
+    assert np.linalg.norm(cn.apply("A", x) - y0) <= 1e-13 * scale
+    cn.set_tuning(t1["apply_groups"], t1["tc_stages"])
+    if precision == "mixed":
+        cn.step(1)   # (rebuilds the operators: apply("A") changes after it)
+        assert cn.mixed_info()[2] <= 1e-12

@@ -34,7 +34,7 @@ def test_replica_aggregation_two_ranks():
     import torch.multiprocessing as mp
     ws = 2
     port = _free_port()
-    with mp.Manager() as mgr:
+    with mp.get_context("spawn").Manager() as mgr:
         out = mgr.dict()
         mp.start_processes(_worker, args=(ws, port, out), nprocs=ws, start_method="spawn", join=True)
         res = dict(out)
