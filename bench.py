@@ -235,20 +235,20 @@ def hh_table(w, cn):
 
 
 def tc_mma_flops(w, cn):
-    """Tensor-core flops one tensor-core apply issues: per 128-node tile, multipoles 0 .. the
-    tile's cut (the highest one above 1e-9 of the monopole at some node of the tile, and at
-    least the multipoles every tile runs), one M128 x N256 x K16 MMA per non-zero 16-column
-    Gaunt slice (M = 128 mode rows, padded; N = the tile's 256 node components)."""
-    kp, nblk, lc_min = cn.tc_blocks()
+    """Tensor-core flops one tensor-core apply issues: per tile of nt nodes, multipoles 0 ..
+    the tile's cut (the highest one above 1e-9 of the monopole at some node of the tile, and
+    at least the multipoles every tile runs), one M128 x N(2 nt) x K16 MMA per non-zero
+    16-column Gaunt slice (M = 128 mode rows, padded; N = the tile's 2 nt node components)."""
+    kp, nblk, lc_min, nt = cn.tc_blocks()
     hh = hh_table(w, cn)
     N = w["Nr"]
     slices = 0
-    for i0 in range(0, N, 128):
-        h = np.abs(hh[:, i0:i0 + 128])
+    for i0 in range(0, N, nt):
+        h = np.abs(hh[:, i0:i0 + nt])
         keep = (h[1:] > 1e-9 * h[0][None, :]).any(axis=1)
         lc = max(lc_min, int(np.max(np.nonzero(keep)[0]) + 1) if keep.any() else 0)
         slices += int(np.sum(nblk[:lc + 1]))
-    return slices * 2 * 128 * 256 * 16
+    return slices * 2 * 128 * (2 * nt) * 16
 
 
 def algorithmic(kernel, w, n_terms, cn=None):

@@ -189,7 +189,7 @@ def load_library():
     L.cnm_mixed_info.argtypes = [p, C.POINTER(i32), C.POINTER(i32), dp]
     L.cnm_mixed_trace.argtypes = [p, dp]
     L.cnm_launch_count.argtypes = [p, C.POINTER(C.c_int64)]
-    L.cnm_tc_blocks.argtypes = [p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
+    L.cnm_tc_blocks.argtypes = [p, C.POINTER(i32), C.POINTER(i32), C.POINTER(i32), C.POINTER(i32)]
     L.cnm_sink_strength.argtypes = [p, i32, dp]
     L.cnm_sink_active.argtypes = [p, C.POINTER(i32)]
     L.cnm_sink_vector.argtypes = [p, i32, dp]
@@ -416,12 +416,12 @@ class CrankNicolsonModes:
 
     def tc_blocks(self):
         """(padded mode count, non-zero 16-column Gaunt slices per multipole, highest multipole
-        every tile runs) of a mixed handle."""
-        kp, lc_min = C.c_int32(), C.c_int32()
+        every tile runs, nodes per tile) of a mixed handle."""
+        kp, lc_min, nt = C.c_int32(), C.c_int32(), C.c_int32()
         nb = np.zeros(2 * self.l_max + 1, np.int32)
         self._check(self._lib.cnm_tc_blocks(self._h, C.byref(kp), nb.ctypes.data_as(C.POINTER(C.c_int32)),
-                                            C.byref(lc_min)))
-        return kp.value, nb, lc_min.value
+                                            C.byref(lc_min), C.byref(nt)))
+        return kp.value, nb, lc_min.value, nt.value
 
     def launch_count(self):
         """Kernels launched by this handle so far (cnm_launch_count)."""

@@ -305,6 +305,7 @@ struct Solver {
     DevBuf<int> d_tc_loff, d_tc_lbytes, d_tc_slices, d_tc_lnblk;
     DevBuf<int> d_tc_ctr;           // tile counter of the tensor-core apply (zero between launches)
     DevBuf<unsigned> d_mx_ticket;   // finished blocks of a mixed-solve vector kernel (zero between launches)
+    bool pivots32 = false;          // the last factorisation also wrote the fp32 pivots dinv32
     DevBuf<float2> m_r, m_y, m_v, m_s, m_z, m_t, m_d, m_xa, dinv32, m_r1, m_q;
     DevBuf<double2> m_r64, m_dots;  // m_dots: [0..1] sink projections, [2..3] corrected ones
     DevBuf<MixScalars> d_msc;
@@ -633,7 +634,7 @@ struct Solver {
 
     // Timed search: every row-group count of the operator kernel that has a resident
     // configuration, then (mixed handles) every Gaunt-stage count of the tensor-core apply
-    // from 3 to the most that fit; the fastest of each is kept.
+    // from TC_MIN_STAGES to the most that fit; the fastest of each is kept.
     void autotune(int *apply_groups, int *tc_stages)
     {
         if (!initialized) throw Error(CNM_ELOGIC, "autotune needs an initialized solver (its operators and state)");
@@ -661,7 +662,7 @@ struct Solver {
             tc_plan(n_modes, K, Nr, tc_amax, n_sm, full);
             double bt = 1e30;
             int best_g = full.gst;
-            for (int g = 3; g <= full.gst; ++g) {
+            for (int g = TC_MIN_STAGES; g <= full.gst; ++g) {
                 TcPlan p;
                 if (!tc_plan(n_modes, K, Nr, tc_amax, n_sm, p, g)) continue;
                 tcp = p;
@@ -1080,6 +1081,14 @@ struct Solver {
         launch_check();
     }
 
+    // The same for a complex64 vector (the mixed solve's inner iterations; k >= 1).
+    void sink_dots32(const float2 *xv, double2 *dots, const Absorber *const *sk, int k)
+    {
+        k_sink_dots32<<<1, 1024, 0, stream>>>(xv, Nr, n_modes, k, sk[0]->v.p, k > 1 ? sk[1]->v.p : nullptr, sk[0]->lo,
+                                             sk[0]->hi, k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, dots);
+        launch_check();
+    }
+
     ApplyArgs base_args(const double2 *xv, double2 *yv) const
     {
         ApplyArgs a;
@@ -1214,6 +1223,7 @@ struct Solver {
 
     void factorize(double dtv)
     {
+        pivots32 = false;
         CK(cudaMemsetAsync(d_status.p, 0, sizeof(int), stream));
         if (jacobi) {
             k_jacobi_diag<<<vec_blocks, VEC_THREADS, 0, stream>>>(grid(), table(), d_hh.p, 0.5 * dtv, dinv.p);
@@ -1230,9 +1240,11 @@ struct Solver {
             cfg.numAttrs = 2;
             kt_begin(TK_PFACTOR);
             ++n_launches;
+            float2 *const d32 = mixed ? dinv32.p : nullptr;
             CK(cudaLaunchKernelEx(&cfg, k_precond_factor_cl, grid(), table(), (const double *)d_hh.p, 0.5 * dtv,
-                                  offdiag(dtv), pcl_per, dinv.p, d_status.p));
+                                  offdiag(dtv), pcl_per, dinv.p, d32, d_status.p));
             kt_end(TK_PFACTOR);
+            pivots32 = d32 != nullptr;
             return;
         }
         choose_window(dtv);
@@ -1573,10 +1585,7 @@ struct Solver {
     void mixed_resid_tc(const Absorber *const *sk, int k, double dtv)
     {
         if (k > 0) {
-            k_sink_dots32<<<1, 1024, 0, stream>>>(m_d.p, Nr, n_modes, k, sk[0]->v.p, k > 1 ? sk[1]->v.p : nullptr,
-                                                 sk[0]->lo, sk[0]->hi, k > 1 ? sk[1]->lo : 0,
-                                                 k > 1 ? sk[1]->hi : 0, m_dots.p + 4);
-            launch_check();
+            sink_dots32(m_d.p, m_dots.p + 4, sk, k);
         }
         TcArgs a = tc_a_args(m_d.p, m_t.p, sk, k, m_dots.p + 4, dtv);
         a.n_dots = 1;
@@ -1592,10 +1601,7 @@ struct Solver {
     void mixed_calibrate(const Absorber *const *sk, int k, double dtv)
     {
         if (k > 0) {
-            k_sink_dots32<<<1, 1024, 0, stream>>>(m_d.p, Nr, n_modes, k, sk[0]->v.p, k > 1 ? sk[1]->v.p : nullptr,
-                                                 sk[0]->lo, sk[0]->hi, k > 1 ? sk[1]->lo : 0,
-                                                 k > 1 ? sk[1]->hi : 0, m_dots.p + 4);
-            launch_check();
+            sink_dots32(m_d.p, m_dots.p + 4, sk, k);
         }
         TcArgs a = tc_a_args(m_d.p, m_t.p, sk, k, m_dots.p + 4, dtv);
         a.n_dots = 1;
@@ -1653,8 +1659,10 @@ struct Solver {
         CK(cudaMemcpyAsync(d_kr.p, &h_kr_init, sizeof(kr), cudaMemcpyHostToDevice, stream));
         jacobi = false;
         factorize(dtv);
-        k_to_f32<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dinv.p, dinv32.p);
-        launch_check();
+        if (!pivots32) {
+            k_to_f32<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, dinv.p, dinv32.p);
+            launch_check();
+        }
         if (k > 0) wood_setup(sk, k, dtv);
         k_mx_start<<<vec_blocks, VEC_THREADS, 0, stream>>>(nN, rhs.p, psi.p, x.p, m_r64.p, m_r.p, m_part.p,
                                                            mxf(MX_B2R0));
@@ -1736,10 +1744,7 @@ struct Solver {
     void wood32(const Absorber *const *sk, int k, float2 *yv)
     {
         if (k == 0) return;
-        k_sink_dots32<<<1, 1024, 0, stream>>>(yv, Nr, n_modes, k, sk[0]->v.p, k > 1 ? sk[1]->v.p : nullptr,
-                                             sk[0]->lo, sk[0]->hi, k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0,
-                                             m_dots.p);
-        launch_check();
+        sink_dots32(yv, m_dots.p, sk, k);
         const int64_t nb = (int64_t)std::max(1, wband_hi - wband_lo) * n_modes;
         const unsigned blocks = (unsigned)std::max<int64_t>(1, std::min<int64_t>((nb + 255) / 256, vec_blocks));
         k_wood32<<<blocks, 256, 0, stream>>>(Nr, n_modes, wband_lo, wband_hi, d_kr.p, m_dots.p, W0.p, W1.p, yv,
@@ -2337,10 +2342,7 @@ struct Solver {
             a.use_cap = ab_cap ? 1 : 0;
             k = active_sinks(sk);
             if (k > 0) {
-                k_sink_dots32<<<1, 1024, 0, stream>>>(m_xa.p, Nr, n_modes, k, sk[0]->v.p,
-                                                     k > 1 ? sk[1]->v.p : nullptr, sk[0]->lo, sk[0]->hi,
-                                                     k > 1 ? sk[1]->lo : 0, k > 1 ? sk[1]->hi : 0, m_dots.p + 6);
-                launch_check();
+                sink_dots32(m_xa.p, m_dots.p + 6, sk, k);
             }
             {
                 TcArgs b = tc_a_args(m_xa.p, m_t.p, sk, k, m_dots.p + 6, op.dt);
@@ -2625,7 +2627,7 @@ int cnm_mixed_info(const cnm_handle *h, int32_t *passes, int32_t *fp64_applies, 
     });
 }
 
-int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk, int32_t *lc_min)
+int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk, int32_t *lc_min, int32_t *nt)
 {
     return guarded(const_cast<cnm_handle *>(h), [&](cnm::Solver &s) {
         if (!s.mixed) throw cnm::Error(CNM_ELOGIC, "no tensor-core operator on an fp64 handle");
@@ -2633,6 +2635,7 @@ int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk, int32_t *lc_m
         if (nblk)
             for (int l = 0; l < s.K; ++l) nblk[l] = s.tg.l_nblk[l];
         if (lc_min) *lc_min = std::max(1, s.tcp.gst - 2);
+        if (nt) *nt = s.tcp.nt;
     });
 }
 
@@ -2917,6 +2920,27 @@ int cnm_measure_fp64_peak(double *tflops)
         g_create_error = e.what();
         return CNM_ECUDA;
     }
+}
+
+int cnm_host_alloc(int64_t bytes, void **ptr)
+{
+    if (!ptr) return CNM_EINVAL;
+    *ptr = nullptr;
+    if (bytes <= 0) return CNM_EINVAL;
+    const cudaError_t e = cudaMallocHost(ptr, (size_t)bytes);
+    if (e != cudaSuccess) {
+        *ptr = nullptr;
+        cudaGetLastError();
+        g_create_error = std::string("cudaMallocHost failed: ") + cudaGetErrorString(e);
+        return CNM_ECUDA;
+    }
+    return CNM_OK;
+}
+
+int cnm_host_free(void *ptr)
+{
+    if (!ptr) return CNM_OK;
+    return cudaFreeHost(ptr) == cudaSuccess ? CNM_OK : CNM_ECUDA;
 }
 
 int cnm_device_name(char *name, int32_t size)

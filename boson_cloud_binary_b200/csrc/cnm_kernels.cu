@@ -1588,7 +1588,7 @@ __global__ void __launch_bounds__(WSB_THREADS) k_wood_setup_band(int Nr, int n_m
 // rescaled by powers of two as they grow).  Grid (cluster size, modes).
 __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, CouplingTable ct, const double *hh,
                                                                     double half_dt, double2 off, int per,
-                                                                    double2 *dinv, int *status)
+                                                                    double2 *dinv, float2 *dinv32, int *status)
 {
     pdl_wait();
     namespace cg = cooperative_groups;
@@ -1713,6 +1713,8 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
     __syncthreads();
     const int64_t base = (int64_t)j * Nr + c0;
     for (int e = tid; e < len; e += T) dinv[base + e] = A[e];
+    if (dinv32)  // the mixed solve's fp32 copy of the pivots
+        for (int e = tid; e < len; e += T) dinv32[base + e] = make_float2((float)A[e].x, (float)A[e].y);
     cl.barrier_wait();
 }
 

@@ -152,7 +152,7 @@ constexpr int WSB_THREADS = 512;
 __global__ void k_wood_setup_band(int Nr, int n_modes, int blo, int bhi, double2 off, const double2 *dinv,
                                   WoodBand wb);
 __global__ void k_precond_factor_cl(Grid g, CouplingTable ct, const double *hh, double half_dt, double2 off, int per,
-                                    double2 *dinv, int *status);
+                                    double2 *dinv, float2 *dinv32, int *status);
 // One or two absorbers: support [lo, hi), projector range [wlo, whi) (the support and
 // the previous one), moments and projector buffers, the parity flag of the second body.
 struct AbsorberPair {

@@ -184,7 +184,12 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32])
     for (int q = 0; q < 32; ++q) v[q] = __uint_as_float(r[q]);
 }
 
-__device__ __forceinline__ void workers_sync() { asm volatile("bar.sync 1, 512;" ::: "memory"); }
+// Named barrier 1 over the W worker threads (the copy / MMA warp does not take part).
+template <int W>
+__device__ __forceinline__ void workers_sync()
+{
+    asm volatile("bar.sync 1, %0;" ::"n"(W) : "memory");
+}
 
 __device__ __forceinline__ uint32_t pack_f16(float lo, float hi)
 {
@@ -196,22 +201,36 @@ __device__ void mx_stage(const double *acc, MixScalars *sc, int stage);
 
 // ==================================================================== tensor-core apply
 
-constexpr int TC_WORKERS = 512;              // operand producers and epilogue (warps 0-15)
-constexpr int TC_THREADS = TC_WORKERS + 32;  // + the copy / MMA warp (warp 16)
-constexpr int TC_CTRL = TC_WORKERS / 32;     // the copy / MMA warp
 constexpr int TC_GMAX = 8, TC_BSTAGES = 2;  // at most 8 Gaunt stages (the plan sets how many)
-constexpr int TC_NT = 128;                   // nodes per tile: 256 node-component rows, the MMA's N
 constexpr int TC_KMAX = 32;                  // multipoles (2 l_max + 1) the kernel handles
-constexpr int TC_WS = 2 * TC_NT + 4;         // row stride (floats) of the accumulator image W[j][m]:
-                                             // 16-byte stores of 8 consecutive rows hit distinct banks
 constexpr float TC_HCUT = 1e-9f;             // multipoles below this fraction of the monopole are skipped
-constexpr int TC_SMEM_MAX = 220 * 1024;      // dynamic shared memory of a plan (static ~3.3 KiB beside it)
+
+// The launch shape by padded mode count KP.  Nodes per tile NT (2 NT node-component rows,
+// the MMA's N) and CTAs per SM: 128 nodes and one CTA per SM.  The kernel also runs 64-node
+// tiles with two CTAs per SM (one CTA's loads and epilogue beside the other's multipole
+// loop; KP <= 96, where two CTAs' shared memory fits): on 91 modes x 40000 nodes that
+// measured the same per launch (103.9 against 104.0 us), since both leave 2.1 tiles per CTA
+// and the launch ends with the CTAs that run a third.  One worker thread per operand row and
+// half of the columns k (4 NT workers, operand producers and epilogue), plus the copy / MMA
+// warp.
+__host__ __device__ constexpr int tc_nt(int) { return 128; }
+__host__ __device__ constexpr int tc_ctas(int kp) { return tc_nt(kp) == 64 ? 2 : 1; }
+__host__ __device__ constexpr int tc_workers(int kp) { return 4 * tc_nt(kp); }
+__host__ __device__ constexpr int tc_threads(int kp) { return tc_workers(kp) + 32; }
+// Row stride (floats) of the accumulator image W[j][m]: 2 NT + 4, so that 16-byte stores of
+// 8 consecutive rows hit distinct banks.
+__host__ __device__ constexpr int tc_ws(int kp) { return 2 * tc_nt(kp) + 4; }
+// Dynamic shared memory of a plan: with two CTAs per SM each stays below half of the SM's
+// 228 KiB less the per-CTA reservation and the ~3.2 KiB of static shared memory.
+__host__ __device__ constexpr int tc_smem_max(int kp) { return tc_ctas(kp) == 2 ? 108 * 1024 : 220 * 1024; }
+constexpr int TC_SMEM_MAX = 220 * 1024;  // the kernels' shared-memory attribute (every plan stays within it)
 
 // Bytes of the region that holds the Z stages and, in the epilogue, the accumulator image.
 __host__ __device__ constexpr size_t tc_zregion(int kp)
 {
-    return (size_t)TC_BSTAGES * kp * 2 * TC_NT * 2 > (size_t)kp * TC_WS * 4 ? (size_t)TC_BSTAGES * kp * 2 * TC_NT * 2
-                                                                              : (size_t)kp * TC_WS * 4;
+    return (size_t)TC_BSTAGES * kp * 2 * tc_nt(kp) * 2 > (size_t)kp * tc_ws(kp) * 4
+               ? (size_t)TC_BSTAGES * kp * 2 * tc_nt(kp) * 2
+               : (size_t)kp * tc_ws(kp) * 4;
 }
 
 struct TcShared {
@@ -225,7 +244,7 @@ struct TcShared {
     int abort;
     int l_off[TC_KMAX], l_bytes[TC_KMAX], l_nblk[TC_KMAX];
     int slices[TC_KMAX * 16];
-    double red[4 * 16];  // warp sums of a tile's fused reductions
+    double red[4 * 16];  // warp sums of a tile's fused reductions (at most 16 worker warps)
     int last;            // this CTA finished last (runs the launch's scalar stage)
 };
 
@@ -244,13 +263,13 @@ __device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_sta
 }
 
 // y = alpha x + beta (H0 x + V x + CAP x) + sinks on complex64 vectors, the coupling on the
-// tensor cores.  A tile is TC_NT nodes; its 2 TC_NT node-component rows m = 2 node + (0: Re,
-// 1: Im) of Z_l*[m, k] = h_l*(r_node) z_k(r_node)_(Re|Im) form the MMA's B operand (N = 256,
+// tensor cores.  A tile is NT nodes; its 2 NT node-component rows m = 2 node + (0: Re,
+// 1: Im) of Z_l*[m, k] = h_l*(r_node) z_k(r_node)_(Re|Im) form the MMA's B operand (N = 2 NT,
 // K-major), the Gaunt matrix G_l* (M = 128 rows j, K-major) its A operand, and
 // D[j, m] = sum_l* sum_k G_l*[j, k] Z_l*[m, k] accumulates in one fp32 TMEM accumulator
-// (lane j, column m).  Worker thread w produces operand row m = w % 256 for half of the
-// columns k (w / 256); in the epilogue warp w reads TMEM lanes 32 (w % 4) .. (its quarter of
-// the modes j) and a quarter of the columns, writes them to shared memory, and the workers
+// (lane j, column m).  Worker thread w produces operand row m = w % 2 NT for half of the
+// columns k (w / 2 NT); in the epilogue warp w reads TMEM lanes 32 (w % 4) .. (its quarter of
+// the modes j) and its share of the columns, writes them to shared memory, and the workers
 // then form one complex output per (mode, node), consecutive threads on consecutive nodes.
 // Warp 16 copies Gaunt stages and issues the MMAs (one thread).  Tiles are drawn from a
 // per-handle counter (tile_ctr[0]; the last CTA to finish resets it), so a CTA that got
@@ -258,16 +277,19 @@ __device__ __forceinline__ void tc_issue_g(TcShared &sh, uint8_t *Gst, int g_sta
 // DK fixes the launch's fused reductions at compile time: 0 none, 1 conj(e) . y,
 // 23 conj(y) . e and |y|^2, 4 |e64 - y|^2.
 template <int KP, int DK>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(tc_threads(KP), tc_ctas(KP))
     k_tc_apply(Grid g, const int *mode_l, const int *mode_m, int K, TcTable tt, TcArgs a, int tiles, int g_stage,
                int gst)
 {
-    constexpr int LBO_Z = 32 * 128;            // bytes between 8-column groups of k in a Z stage
+    constexpr int TC_NT = tc_nt(KP), TC_WORKERS = tc_workers(KP), TC_THREADS = tc_threads(KP);
+    constexpr int TC_CTRL = TC_WORKERS / 32;   // the copy / MMA warp
+    constexpr int TC_WS = tc_ws(KP);
+    constexpr int LBO_Z = 2 * TC_NT / 8 * 128;   // bytes between 8-column groups of k in a Z stage
     constexpr int Z_STAGE = KP * 2 * TC_NT * 2;  // bytes of one Z stage (2 NT rows x KP fp16)
     constexpr int G_LBO = 2048;                // bytes between the two 8-column halves of a G block
     constexpr int G_BLK = 4096;                // bytes of one G block (128 rows j x 16 columns k)
     constexpr uint32_t IDESC = idesc_f16(128, 2 * TC_NT);
-    constexpr uint32_t NCOLS = 2 * TC_NT;      // one fp32 accumulator: 128 lanes (modes) x 256 columns
+    constexpr uint32_t NCOLS = 2 * TC_NT;      // one fp32 accumulator: 128 lanes (modes) x 2 NT columns
     constexpr int NDOT = DK == 0 ? 0 : DK == 23 ? 2 : 1;  // fused reductions (complex slots)
     extern __shared__ __align__(128) uint8_t tc_smem[];
     __shared__ TcShared sh;
@@ -320,7 +342,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         cent[k] = (float)((double)(l * (l + 1)) / (2.0 * g.mu));
     }
     if (warp == TC_CTRL) {
-        // TMEM accumulator: 128 lanes x 256 fp32 columns
+        // TMEM accumulator: 128 lanes x 2 NT fp32 columns
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(&sh.tmem_base)),
                      "r"(NCOLS)
                      : "memory");
@@ -355,7 +377,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const uint32_t gbase = smem_addr(Gst + (size_t)sg * g_stage);
                     const uint32_t zbase = smem_addr(Zst + (size_t)sz * Z_STAGE);
                     const int nb = sh.l_nblk[l];
-                    // one M = 128 (modes j), N = 256 (the tile's node-component rows), K = 16
+                    // one M = 128 (modes j), N = 2 NT (the tile's node-component rows), K = 16
                     // MMA per non-zero slice of G_l*: every tcgen05.mma of K = 16 costs about the
                     // same whatever its N, so N is kept at its maximum
                     for (int q = 0; q < nb; ++q) {
@@ -389,10 +411,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---------------------------------------------------------- workers
         // operand row m = 2 node + (Re | Im) and half of its columns k
         constexpr int KH = KP / 2;
-        const int m = tid & 255, khalf = tid >> 8, zc_node = m >> 1, zc_comp = m & 1;
+        const int m = tid & (2 * TC_NT - 1), khalf = tid / (2 * TC_NT), zc_node = m >> 1, zc_comp = m & 1;
         const float ad = (float)(1.0 / (2.0 * g.mu * g.dr * g.dr));
-        // epilogue phase 1: TMEM lane quarter (warp % 4: modes j) and quarter of the columns
+        // epilogue phase 1: TMEM lane quarter (warp % 4: modes j) and a share of the columns
+        // (one share per group of four warps)
         const int q4 = warp & 3, cq = warp >> 2;
+        constexpr int CQ_SPAN = 2 * TC_NT / (TC_WORKERS / 128);
         const float2 al = a.alpha, be = a.beta;
         // the sinks' coefficients coef_a (v_a^dag x), fp64
         double2 sk_c[2];
@@ -413,7 +437,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             // the next tile (the barrier first: every worker has finished the previous
             // epilogue and read the previous tile index)
             if (tid == 0) sh.tile[it & 1] = atomicAdd(a.tile_ctr, 1);
-            workers_sync();
+            workers_sync<TC_WORKERS>();
             const int tile = sh.tile[it & 1];
             if (tile >= tiles) {
                 if (tid == 0) {
@@ -478,7 +502,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     if (e < K * TC_NT) hs[e] = (float)hv[q];
                 }
                 cp_async_wait_all();
-                workers_sync();
+                workers_sync<TC_WORKERS>();
 #pragma unroll
                 for (int kk = 0; kk < KH; ++kk) {
                     const int k = khalf * KH + kk;
@@ -509,7 +533,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     atomicMax(&sh.pmax_bits, pw);
                 }
             }
-            workers_sync();
+            workers_sync<TC_WORKERS>();
             const int lc = max(lc_min, sh.lcut_red);
             int se = 0;
             {
@@ -524,7 +548,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 for (int k = 0; k < KH; ++k) zc[k] *= sz;
             }
             const float wscale = ldexpf(1.f, -(se + tt.g_exp));  // undoes both operand scales
-            workers_sync();
+            workers_sync<TC_WORKERS>();
             if (tid == 0) {
                 sh.lcut[it & 1] = lc;
                 sh.lcut_red = 0;
@@ -560,7 +584,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int j = 32 * q4 + lane;
                 float *wrow = W + (size_t)j * TC_WS;
 #pragma unroll 1
-                for (int col = cq * (TC_NT / 2); col < (cq + 1) * (TC_NT / 2); col += 32) {
+                for (int col = cq * CQ_SPAN; col < (cq + 1) * CQ_SPAN; col += 32) {
                     float wv[32];
                     tmem_ld32(taddr + (uint32_t)col, wv);
                     if (j < n)
@@ -572,7 +596,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(smem_addr(&sh.accfree));
-            workers_sync();
+            workers_sync<TC_WORKERS>();
             // phase 2: one complex output per (mode j, node) and thread, consecutive threads
             // on consecutive nodes of one mode (coalesced loads and stores); a warp's lanes
             // hold 32 consecutive nodes, so the stencil's neighbours come by shuffles and
@@ -674,7 +698,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     if (lane == 0)
 #pragma unroll
                         for (int q = 0; q < 2 * NDOT; ++q) sh.red[q * 16 + warp] = v[q];
-                    workers_sync();
+                    workers_sync<TC_WORKERS>();
                     if (tid < 2 * NDOT) {
                         double sum = 0.0;
                         for (int w = 0; w < TC_CTRL; ++w) sum += sh.red[tid * 16 + w];
@@ -727,23 +751,24 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p, int max_gst)
 {
     p.kp = (n_modes + 15) / 16 * 16;
-    p.nt = TC_NT;
     if (p.kp > 112 || K > TC_KMAX) return false;
+    p.nt = tc_nt(p.kp);
     p.a_stage = (g_stage_bytes + 127) / 128 * 128;
-    const size_t fixed = tc_zregion(p.kp) + (size_t)K * TC_NT * 4 + (size_t)p.kp * 12 + (size_t)2 * TC_NT * 4 + 128;
-    // as many Gaunt stages as fit (3 to 8, at most K: every tile runs gst - 1 multipoles)
-    const size_t budget = TC_SMEM_MAX;
+    const size_t fixed = tc_zregion(p.kp) + (size_t)K * p.nt * 4 + (size_t)p.kp * 12 + (size_t)2 * p.nt * 4 + 128;
+    // as many Gaunt stages as fit (2 to 8, at most K: every tile runs gst - 1 multipoles)
+    const size_t budget = tc_smem_max(p.kp);
     p.gst = (int)std::min<size_t>(TC_GMAX, budget > fixed ? (budget - fixed) / std::max(p.a_stage, 128) : 0);
     p.gst = std::min(p.gst, K);
     if (max_gst > 0) p.gst = std::min(p.gst, max_gst);
-    if (p.gst < 3) return false;
+    if (p.gst < TC_MIN_STAGES) return false;
     p.smem = (size_t)p.gst * p.a_stage + fixed;
-    // at least 120 KiB, so that one CTA (and its TMEM columns) is resident per SM and no
-    // tcgen05.alloc has to wait for another CTA's columns
-    p.smem = std::max<size_t>(p.smem, 120 * 1024);
-    p.tiles = (Nr + TC_NT - 1) / TC_NT;
-    p.grid = std::min(p.tiles, n_sm);
-    return p.smem <= (size_t)TC_SMEM_MAX;
+    // one CTA per SM (KP 112): at least 120 KiB, so that no second CTA shares the SM and no
+    // tcgen05.alloc waits for another CTA's columns; two per SM (2 x 2 NT = 256 TMEM columns)
+    // never wait either
+    if (tc_ctas(p.kp) == 1) p.smem = std::max<size_t>(p.smem, 120 * 1024);
+    p.tiles = (Nr + p.nt - 1) / p.nt;
+    p.grid = std::min(p.tiles, tc_ctas(p.kp) * n_sm);
+    return p.smem <= (size_t)tc_smem_max(p.kp);
 }
 
 cudaError_t tc_prepare(const TcPlan &p)
@@ -774,8 +799,8 @@ cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, con
     if (dk < 0) return cudaErrorInvalidValue;
 #define CNM_TC_LAUNCH1(KP_, DK_)                                                                                  \
     if (dk == DK_) {                                                                                              \
-        k_tc_apply<KP_, DK_><<<p.grid, TC_THREADS, p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles, p.a_stage,  \
-                                                                p.gst);                                           \
+        k_tc_apply<KP_, DK_><<<p.grid, tc_threads(KP_), p.smem, st>>>(g, mode_l, mode_m, K, tt, a, p.tiles,       \
+                                                                     p.a_stage, p.gst);                            \
         return cudaGetLastError();                                                                                \
     }
 #define CNM_TC_LAUNCH(KP_)                                                                          \

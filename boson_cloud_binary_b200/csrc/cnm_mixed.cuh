@@ -95,7 +95,7 @@ struct TcPlan {
 };
 // max_gst > 0 caps the Gaunt stages (the autotuner's candidates); 0 takes as many as fit.
 bool tc_plan(int n_modes, int K, int Nr, int g_stage_bytes, int n_sm, TcPlan &p, int max_gst = 0);
-constexpr int TC_MAX_STAGES = 8;
+constexpr int TC_MAX_STAGES = 8, TC_MIN_STAGES = 2;
 cudaError_t tc_prepare(const TcPlan &p);
 cudaError_t launch_tc_apply(const TcPlan &p, cudaStream_t st, const Grid &g, const int *mode_l, const int *mode_m,
                             int K, const TcTable &tt, const TcArgs &a);

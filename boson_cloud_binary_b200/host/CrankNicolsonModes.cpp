@@ -1,6 +1,7 @@
 // CrankNicolsonModes.cpp -- host side of the drop-in class: scalars, writers, run,
 // checkpoints and resume, over the C ABI of include/cnm_gpu.h.
 #include "CrankNicolsonModes.hpp"
+#include "cnm_snapshot_text.hpp"
 
 #include <algorithm>
 #include <chrono>
@@ -17,6 +18,7 @@
 #include <regex>
 #include <sstream>
 #include <stdexcept>
+#include <thread>
 
 namespace fs = std::filesystem;
 
@@ -131,6 +133,20 @@ bool parse_snapshot(const std::string &path, size_t size, std::vector<dcomplex> 
     return true;
 }
 
+// One state snapshot as text: "re im" per value in the default stream format (the bytes
+// of src/CrankNicolsonModes_utils.cpp:48-64), formatted on up to 8 threads.
+void write_snapshot_file(const std::string &path, const dcomplex *v, size_t n)
+{
+    std::ofstream out(path, std::ios::binary);
+    if (!out) {
+        std::cerr << "Could not open file: " << path << "\n";
+        return;
+    }
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    for (const std::string &piece : snapshot_text(v, n, std::min(8u, hw)))
+        out.write(piece.data(), (std::streamsize)piece.size());
+}
+
 // The (l, m) list of a run's modes.txt ("l,m" per line); false when there is no file.
 bool read_mode_list(const std::string &path, std::vector<mode> &out)
 {
@@ -178,8 +194,59 @@ CrankNicolsonModes::CrankNicolsonModes(int Nx, double L_, double dt_i, double ep
 
 CrankNicolsonModes::~CrankNicolsonModes()
 {
-    flush_diagnostics();
+    out_.stop();  // every queued write has run
+    for (auto &[stream, name] : diagnostic_files())
+        if (stream->is_open()) stream->flush();
+    for (auto &[ptr, pinned] : pool_all_) {
+        if (pinned) cnm_host_free(ptr);
+        else std::free(ptr);
+    }
     if (h_) cnm_destroy(h_);
+}
+
+OutputQueue &CrankNicolsonModes::output()
+{
+    if (out_.inline_mode == async_output) {
+        out_.drain();  // writes queued under the previous setting go first
+        out_.inline_mode = !async_output;
+    }
+    return out_;
+}
+
+void CrankNicolsonModes::wait_output() { out_.drain(); }
+
+std::shared_ptr<dcomplex> CrankNicolsonModes::state_to_buffer()
+{
+    const size_t n = (size_t)Nr * n_modes;
+    void *p = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(pool_m_);
+        if (!pool_free_.empty()) {
+            p = pool_free_.back();
+            pool_free_.pop_back();
+        }
+    }
+    if (!p) {
+        const bool pinned = cnm_host_alloc((int64_t)(n * sizeof(dcomplex)), &p) == CNM_OK;
+        if (!pinned && !(p = std::malloc(n * sizeof(dcomplex)))) throw std::bad_alloc();
+        std::lock_guard<std::mutex> lk(pool_m_);
+        pool_all_.emplace_back(p, pinned);
+    }
+    std::shared_ptr<dcomplex> buf(static_cast<dcomplex *>(p), [this](dcomplex *q) {
+        std::lock_guard<std::mutex> lk(pool_m_);
+        pool_free_.push_back(q);
+    });
+    check(cnm_get_state(h_, reinterpret_cast<double *>(buf.get()), (int64_t)n));
+    psi.assign(buf.get(), buf.get() + n);
+    return buf;
+}
+
+void CrankNicolsonModes::post_snapshot(int step_id, std::shared_ptr<const dcomplex> data, const std::string &name)
+{
+    std::stringstream fn;
+    fn << output_folder_ << "/" << name << "/snapshot_" << std::setw(6) << std::setfill('0') << step_id << ".txt";
+    const size_t n = (size_t)Nr * n_modes;
+    output().post([path = fn.str(), data = std::move(data), n]() { write_snapshot_file(path, data.get(), n); }, true);
 }
 
 void CrankNicolsonModes::check(int rc) const
@@ -339,26 +406,28 @@ void CrankNicolsonModes::step(int step_id)
         if (evolve_orbit) std::cout << " | R = " << d.R;
         std::cout << std::flush;
     }
-    write_quantity_line(d.R, R_file);
-    write_quantity_line(d.theta, theta_file);
-    write_quantity_line(d.Omega, Omega_file);
-    write_quantity_line(d.M1, M_1_file);
-    write_quantity_line(d.q, q_file);
-    write_quantity_line(d.t, time_file);
-    write_quantity_line_modes(ef, energy_flux_file);
-    write_quantity_line_modes(fl, flux_file);
-    write_quantity_line(d.energy, energy_file);
-    write_quantity_line(d.p_bin, p_bin_file);
-    write_quantity_line(d.p_bin_inst, p_bin_inst_file);
-    write_quantity_line(d.dV_bin_dt, d_V_bin_dt_file);
-    write_quantity_line_modes(nm, norms_file);
-    write_quantity_line_modes(en, energy_modes_file);
-    const bool snapshot = step_id % save_every == 0;
-    if (sync_every_step || snapshot) sync_state();
-    if (snapshot) {
-        save_snapshot(step_id, psi, "psi");
+    output().post([this, d, ef = std::move(ef), fl = std::move(fl), nm = std::move(nm), en = std::move(en)]() {
+        write_quantity_line(d.R, R_file);
+        write_quantity_line(d.theta, theta_file);
+        write_quantity_line(d.Omega, Omega_file);
+        write_quantity_line(d.M1, M_1_file);
+        write_quantity_line(d.q, q_file);
+        write_quantity_line(d.t, time_file);
+        write_quantity_line_modes(ef, energy_flux_file);
+        write_quantity_line_modes(fl, flux_file);
+        write_quantity_line(d.energy, energy_file);
+        write_quantity_line(d.p_bin, p_bin_file);
+        write_quantity_line(d.p_bin_inst, p_bin_inst_file);
+        write_quantity_line(d.dV_bin_dt, d_V_bin_dt_file);
+        write_quantity_line_modes(nm, norms_file);
+        write_quantity_line_modes(en, energy_modes_file);
+    });
+    if (step_id % save_every == 0) {
+        post_snapshot(step_id, state_to_buffer(), "psi");
         flush_diagnostics();
         save_checkpoint(step_id);
+    } else if (sync_every_step) {
+        sync_state();
     }
 }
 
@@ -383,8 +452,7 @@ void CrankNicolsonModes::run(int n_steps, double r_ex)
     if (verbose) std::cout << "Output folder: " << output_folder_ << std::endl;
     open_diagnostics(std::ios::out);
     save_run_info();
-    sync_state();
-    save_snapshot(0, psi, "psi");
+    post_snapshot(0, state_to_buffer(), "psi");
     save_snapshot(0, schrodinger_rhs(psi), "psi_dt");
     save_checkpoint(0);
     evolve(1, n_steps);
@@ -402,6 +470,7 @@ void CrankNicolsonModes::evolve(int first_step, int n_steps)
     if (verbose) std::cout << std::endl;
     flush_diagnostics();
     sync_state();
+    wait_output();  // the run's files are complete when it returns
     if (verbose) std::cout << "Simulation completed!" << std::endl;
 }
 
@@ -434,14 +503,8 @@ void CrankNicolsonModes::save_run_info()
 // src/CrankNicolsonModes_utils.cpp:48-64.
 void CrankNicolsonModes::save_snapshot(int step_id, const std::vector<dcomplex> &state, const std::string &name)
 {
-    std::stringstream fn;
-    fn << output_folder_ << "/" << name << "/snapshot_" << std::setw(6) << std::setfill('0') << step_id << ".txt";
-    std::ofstream out(fn.str());
-    if (!out) {
-        std::cerr << "Could not open file: " << fn.str() << "\n";
-        return;
-    }
-    for (const dcomplex &v : state) out << v.real() << " " << v.imag() << "\n";
+    auto keep = std::make_shared<std::vector<dcomplex>>(state);
+    post_snapshot(step_id, std::shared_ptr<const dcomplex>(keep, keep->data()), name);
 }
 
 void CrankNicolsonModes::write_quantity_line_modes(const std::vector<double> &quantity, std::ofstream &file)
@@ -460,8 +523,10 @@ void CrankNicolsonModes::write_quantity_line(double quantity, std::ofstream &fil
 
 void CrankNicolsonModes::flush_diagnostics()
 {
-    for (auto &[stream, name] : diagnostic_files())
-        if (stream->is_open()) stream->flush();
+    output().post([this] {
+        for (auto &[stream, name] : diagnostic_files())
+            if (stream->is_open()) stream->flush();
+    });
 }
 
 // src/CrankNicolsonModes_restart.cpp:107-137.
@@ -480,6 +545,7 @@ std::vector<std::pair<std::ofstream *, std::string>> CrankNicolsonModes::diagnos
 
 void CrankNicolsonModes::open_diagnostics(std::ios::openmode mode)
 {
+    wait_output();
     for (auto &[stream, name] : diagnostic_files()) {
         if (stream->is_open()) stream->close();
         stream->open(output_folder_ + "/" + name, mode);
@@ -490,35 +556,40 @@ void CrankNicolsonModes::open_diagnostics(std::ios::openmode mode)
 // ------------------------------------------------------------------ checkpoints
 
 // src/CrankNicolsonModes_restart.cpp:139-177: the bytes come from the device state
-// (cnm_save_checkpoint); the file is replaced atomically through a .tmp file.
+// (cnm_save_checkpoint) now; the file, replaced atomically through a .tmp file, is written
+// after the snapshot and the diagnostic rows queued before it.
 void CrankNicolsonModes::save_checkpoint(int step_id)
 {
     push();
     int64_t size = 0;
     check(cnm_save_checkpoint(h_, step_id, nullptr, 0, &size));
-    std::vector<char> bytes((size_t)size);
-    check(cnm_save_checkpoint(h_, step_id, bytes.data(), size, &size));
-    const std::string final_path = output_folder_ + "/checkpoint.bin", tmp_path = final_path + ".tmp";
-    {
-        std::ofstream out(tmp_path, std::ios::binary | std::ios::trunc);
-        if (!out) {
-            std::cerr << "Could not write checkpoint " << tmp_path << "\n";
-            return;
+    auto bytes = std::make_shared<std::vector<char>>((size_t)size);
+    check(cnm_save_checkpoint(h_, step_id, bytes->data(), size, &size));
+    const std::string final_path = output_folder_ + "/checkpoint.bin";
+    output().post([final_path, bytes]() {
+        const std::string tmp_path = final_path + ".tmp";
+        {
+            std::ofstream out(tmp_path, std::ios::binary | std::ios::trunc);
+            if (!out) {
+                std::cerr << "Could not write checkpoint " << tmp_path << "\n";
+                return;
+            }
+            out.write(bytes->data(), (std::streamsize)bytes->size());
+            if (!out) {
+                std::cerr << "Could not write checkpoint " << tmp_path << "\n";
+                return;
+            }
         }
-        out.write(bytes.data(), (std::streamsize)bytes.size());
-        if (!out) {
-            std::cerr << "Could not write checkpoint " << tmp_path << "\n";
-            return;
-        }
-    }
-    std::error_code err;
-    fs::rename(tmp_path, final_path, err);
-    if (err) std::cerr << "Could not replace checkpoint: " << err.message() << "\n";
+        std::error_code err;
+        fs::rename(tmp_path, final_path, err);
+        if (err) std::cerr << "Could not replace checkpoint: " << err.message() << "\n";
+    });
 }
 
 // src/CrankNicolsonModes_restart.cpp:179-233.
 bool CrankNicolsonModes::load_checkpoint(int step_id)
 {
+    wait_output();
     std::ifstream in(output_folder_ + "/checkpoint.bin", std::ios::binary);
     if (!in) return false;
     std::vector<char> bytes((std::istreambuf_iterator<char>(in)), std::istreambuf_iterator<char>());
@@ -593,6 +664,7 @@ void CrankNicolsonModes::reconstruct_state_from_diagnostics(int step_id)
 void CrankNicolsonModes::resume(const std::string &folder, int n_steps, double r_ex)
 {
     if (verbose) std::cout << "Resuming the run in " << folder << std::endl;
+    wait_output();
     push();
     set_extraction_radius(r_ex, n_steps);
     pull();

@@ -7,16 +7,21 @@
 // B200 path never assembles them.  The numerics run on the GPU through
 // include/cnm_gpu.h; this class keeps the host side of the reference: the public
 // scalar members, the Simulation_* folder, the 14 diagnostic files, snapshots,
-// checkpoints and resume.
+// checkpoints and resume.  Files are written by a background thread in the order the
+// synchronous code would write them (cnm_output_queue.hpp); snapshots are copied off
+// the device into page-locked buffers and formatted there.
 #pragma once
 
 #include <complex>
 #include <fstream>
+#include <memory>
+#include <mutex>
 #include <string>
 #include <utility>
 #include <vector>
 
 #include "cnm_gpu.h"
+#include "cnm_output_queue.hpp"
 
 using dcomplex = std::complex<double>;
 
@@ -85,6 +90,11 @@ public:
     bool verbose = true;
     /// BiCGSTAB tolerance (the reference hard-codes 1e-10).
     double tolerance = 1e-10;
+    /// Write diagnostics, snapshots and checkpoints on the background thread (the bytes
+    /// are the same either way); off, they are written before step() returns.
+    bool async_output = true;
+    /// Wait until every file write queued so far is done.
+    void wait_output();
     const std::string &output_folder() const { return output_folder_; }
 
 private:
@@ -97,6 +107,17 @@ private:
     double orbits_average_ = 2.0;
     double ramp_periods_;
     double initial_period_;
+
+    OutputQueue out_;
+    std::mutex pool_m_;
+    std::vector<void *> pool_free_;                  // snapshot buffers of Nr * n_modes values
+    std::vector<std::pair<void *, bool>> pool_all_;  // (buffer, page-locked)
+
+    // A snapshot buffer filled with the device state (the public mirror psi is refreshed
+    // from it); it returns to the pool when the last holder drops it.
+    std::shared_ptr<dcomplex> state_to_buffer();
+    void post_snapshot(int step_id, std::shared_ptr<const dcomplex> data, const std::string &name);
+    OutputQueue &output();
 
     void check(int rc) const;
     void push();  // public scalars -> device solver

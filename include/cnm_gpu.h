@@ -150,6 +150,12 @@ int cnm_set_initial_state_full(cnm_handle *h, const double *psi0, int64_t n);
 /* Raw access to member psi (no scaling). */
 int cnm_set_state(cnm_handle *h, const double *psi, int64_t n);
 int cnm_get_state(const cnm_handle *h, double *psi, int64_t n);
+/* Page-locked host memory for state copies (cnm_get_state into it runs at the full
+ * device-to-host rate): cnm_host_alloc returns *ptr = NULL and CNM_ECUDA when the
+ * allocation fails (cnm_create_error() says why); cnm_host_free(NULL) does nothing.
+ * No counterpart in the reference, whose state lives in host memory. */
+int cnm_host_alloc(int64_t bytes, void **ptr);
+int cnm_host_free(void *ptr);
 
 /* --- set-up ------------------------------------------------------------------- */
 
@@ -270,9 +276,9 @@ int cnm_kernel_times(cnm_handle *h, int32_t which, double *total_ms, int64_t *la
 int cnm_timer_start(cnm_handle *h);
 /* Tensor-core operator layout of a CNM_MIXED handle: the padded mode count, for each of
  * the 2 l_max + 1 multipoles the number of non-zero 16-column slices of its Gaunt matrix
- * (one M128 x N256 x K16 MMA per slice and 128-node tile), and the highest multipole every
- * tile runs whatever its radial cut (any pointer may be NULL). */
-int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk, int32_t *lc_min);
+ * (one M128 x N(2 nt) x K16 MMA per slice and tile), the highest multipole every tile runs
+ * whatever its radial cut, and the nodes per tile nt (any pointer may be NULL). */
+int cnm_tc_blocks(const cnm_handle *h, int32_t *kp, int32_t *nblk, int32_t *lc_min, int32_t *nt);
 /* Kernels the handle has launched since its creation (every launch site counts). */
 int cnm_launch_count(const cnm_handle *h, int64_t *count);
 int cnm_timer_stop(cnm_handle *h, double *ms);

@@ -8,6 +8,7 @@
 //     (6-digit snapshots: every diagnostic within 2e-4 of the uninterrupted run);
 //   * a truncated last snapshot is skipped for the previous one;
 //   * a folder with another mode list, or without snapshots, is refused;
+//   * the background writer leaves the same bytes as writing before step() returns;
 // plus the MODESBIN reader.
 //
 //   host_check <work_dir>        exit status 0 on success
@@ -68,11 +69,12 @@ std::unique_ptr<CrankNicolsonModes> make_solver(int l_max = 2)
 constexpr double kREx = 40.0;
 
 // A fresh run of n_steps in work/name; returns its folder.
-fs::path new_run(const fs::path &work, const std::string &name, int n_steps)
+fs::path new_run(const fs::path &work, const std::string &name, int n_steps, bool async_output = true)
 {
     fs::create_directories(work / name);
     fs::current_path(work / name);
     auto cn = make_solver();
+    cn->async_output = async_output;
     cn->run(n_steps, kREx);
     return fs::absolute(cn->output_folder());
 }
@@ -188,6 +190,11 @@ int main(int argc, char **argv)
     const int n_full = 41, n_cut = 25;  // snapshots every 10 steps: the cut run ends 4 rows past snapshot 20
     const fs::path reference = new_run(work, "reference", n_full);
 
+    {  // synchronous writing: the same folder
+        const fs::path run = new_run(work, "synchronous", n_full, false);
+        require_identical(reference, run, "synchronous writer");
+        std::printf("background writer: folder identical to synchronous writing\n");
+    }
     {  // exact resume from the checkpoint
         const fs::path run = new_run(work, "interrupted", n_cut);
         require(read_rows(run / "t.txt").size() == (size_t)(n_cut - 1), "interrupted run has the wrong row count");

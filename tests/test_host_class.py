@@ -17,6 +17,17 @@ def test_host_check_binary_built():
     assert os.path.exists(CHECK), "build the package (make -C boson_cloud_binary_b200) first"
 
 
+def test_output_queue_order_bound_and_drain():
+    """The background writer of the C++ class (host/cnm_output_queue.hpp), on the CPU:
+    posting order kept, drain complete, at most two snapshot jobs in flight, failures
+    reported without stopping the queue."""
+    check = os.path.join(ROOT, "boson_cloud_binary_b200", "cnm_output_queue_check")
+    assert os.path.exists(check), "build the package (make -C boson_cloud_binary_b200) first"
+    res = subprocess.run([check], capture_output=True, text=True, timeout=120)
+    assert res.returncode == 0, res.stdout + res.stderr
+    assert "output_queue_check: OK" in res.stdout
+
+
 @pytest.mark.gpu
 def test_host_class_run_and_resume(tmp_path):
     res = subprocess.run([CHECK, str(tmp_path)], capture_output=True, text=True, timeout=600)
