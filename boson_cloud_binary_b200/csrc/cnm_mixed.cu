@@ -856,6 +856,7 @@ __global__ void __launch_bounds__(PS32_THREADS) k_psolve32_cl(int Nr, int per, f
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ float2 ps32[];
     __shared__ Aff32 wagg[PS32_THREADS / 32];
+    __shared__ Aff32 wex_s[PS32_THREADS / 32];  // exclusive prefix (forward) / suffix (backward) of wagg
     __shared__ Aff32 cagg_f, cagg_b;
     constexpr int T = PS32_THREADS, NW = PS32_THREADS / 32;
     const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
@@ -907,12 +908,16 @@ __global__ void __launch_bounds__(PS32_THREADS) k_psolve32_cl(int Nr, int per, f
     if (lane == 31) wagg[warp] = acc;
     __syncthreads();
     if (warp == 0) {
+        // the CTA total, and every warp's exclusive prefix for the apply pass below
         Aff32 cc = lane < NW ? wagg[lane] : aff32_id();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const Aff32 prev = shfl_aff32(cc, o, true);
             if (lane >= o) cc = aff32_then(prev, cc);
         }
+        Aff32 ex = shfl_aff32(cc, 1, true);
+        if (lane == 0) ex = aff32_id();
+        if (lane < NW) wex_s[lane] = ex;
         if (lane == 31) cagg_f = cc;
     }
     cl.sync();
@@ -925,32 +930,22 @@ __global__ void __launch_bounds__(PS32_THREADS) k_psolve32_cl(int Nr, int per, f
             if (lane >= o) cc = aff32_then(prev, cc);
         }
         const float2 ycta = make_float2(__shfl_sync(0xffffffffu, cc.B.x, 31), __shfl_sync(0xffffffffu, cc.B.y, 31));
-        Aff32 w = lane < NW ? wagg[lane] : aff32_id();
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const Aff32 prev = shfl_aff32(w, o, true);
-            if (lane >= o) w = aff32_then(prev, w);
-        }
-        Aff32 wex = shfl_aff32(w, 1, true);
-        if (lane == 0) wex = aff32_id();
-        const float2 ys = aff32_apply(wex, ycta);
-        ywarp = make_float2(__shfl_sync(0xffffffffu, ys.x, warp), __shfl_sync(0xffffffffu, ys.y, warp));
+        ywarp = aff32_apply(wex_s[warp], ycta);
     }
+    // forward apply, and with it (ascending) the thread's backward map
+    // bcc = f_s0 o ... o f_s1-1, f_e(x) = y_e - u_e d_e x: x_i = y_i - u_i d_i x_{i+1}
+    Aff32 bcc = aff32_id();
     {
         float2 y = aff32_apply(excl, ywarp);
         for (int e = s0; e < s1; ++e) {
             const int i = c0 + e;
             const float2 l = (i >= 1 && i <= Nr - 2) ? off : make_float2(0.f, 0.f);
-            y = fmul2(D[e], fsub2(Y[e], fmul2(l, y)));
+            const float2 d = D[e];
+            y = fmul2(d, fsub2(Y[e], fmul2(l, y)));
             Y[e] = y;
+            const float2 ud = fmul2(l, d);
+            bcc = aff32_then(Aff32{make_float2(-ud.x, -ud.y), y}, bcc);
         }
-    }
-    // backward: x_i = y_i - u_i d_i x_{i+1}
-    Aff32 bcc = aff32_id();
-    for (int e = s1 - 1; e >= s0; --e) {
-        const int i = c0 + e;
-        const float2 ud = fmul2((i >= 1 && i <= Nr - 2) ? off : make_float2(0.f, 0.f), D[e]);
-        bcc = aff32_then(bcc, Aff32{make_float2(-ud.x, -ud.y), Y[e]});
     }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -963,12 +958,16 @@ __global__ void __launch_bounds__(PS32_THREADS) k_psolve32_cl(int Nr, int per, f
     if (lane == 0) wagg[warp] = bcc;
     __syncthreads();
     if (warp == 0) {
+        // the CTA total, and every warp's exclusive suffix for the apply pass below
         Aff32 cc = lane < NW ? wagg[lane] : aff32_id();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const Aff32 nxt = shfl_aff32(cc, o, false);
             if (lane + o < 32) cc = aff32_then(nxt, cc);
         }
+        Aff32 ex = shfl_aff32(cc, 1, false);
+        if (lane == 31) ex = aff32_id();
+        if (lane < NW) wex_s[lane] = ex;
         if (lane == 0) cagg_b = cc;
     }
     cl.sync();
@@ -981,16 +980,7 @@ __global__ void __launch_bounds__(PS32_THREADS) k_psolve32_cl(int Nr, int per, f
             if (lane + o < 32) cc = aff32_then(nxt, cc);
         }
         const float2 xcta = make_float2(__shfl_sync(0xffffffffu, cc.B.x, 0), __shfl_sync(0xffffffffu, cc.B.y, 0));
-        Aff32 w = lane < NW ? wagg[lane] : aff32_id();
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const Aff32 nxt = shfl_aff32(w, o, false);
-            if (lane + o < 32) w = aff32_then(nxt, w);
-        }
-        Aff32 wex = shfl_aff32(w, 1, false);
-        if (lane == 31) wex = aff32_id();
-        const float2 xs = aff32_apply(wex, xcta);
-        xwarp = make_float2(__shfl_sync(0xffffffffu, xs.x, warp), __shfl_sync(0xffffffffu, xs.y, warp));
+        xwarp = aff32_apply(wex_s[warp], xcta);
     }
     // remote reads of cagg_b happen before this arrive; the wait is the last statement
     cl.barrier_arrive();
