@@ -1134,6 +1134,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double2 smc[];
     __shared__ Aff wagg[PCL_THREADS / 32];
+    __shared__ Aff wex_s[PCL_THREADS / 32];  // exclusive prefix (forward) / suffix (backward) of wagg
     __shared__ Aff cagg_f, cagg_b;
     const int rank = (int)cl.block_rank(), cs = (int)cl.num_blocks();
     const int second = blockIdx.y >= (unsigned)n_modes;
@@ -1229,13 +1230,17 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     if (lane == 31) wagg[warp] = acc;
     __syncthreads();
     if (warp == 0) {
-        // CTA total: ordered scan of the warp totals in lanes 0..NW-1
+        // CTA total: ordered scan of the warp totals in lanes 0..NW-1; each warp's exclusive
+        // prefix is kept for the apply pass
         Aff c = lane < NW ? wagg[lane] : aff_identity();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const Aff prev = shfl_up_aff(c, o);
             if (lane >= o) c = aff_then(prev, c);
         }
+        Aff ex = shfl_up_aff(c, 1);
+        if (lane == 0) ex = aff_identity();
+        if (lane < NW) wex_s[lane] = ex;
         if (lane == 31) cagg_f = c;
     }
     cl.sync();
@@ -1252,36 +1257,22 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
             if (lane >= o) c = aff_then(prev, c);
         }
         const double2 ycta = cmake(__shfl_sync(0xffffffffu, c.B.x, 31), __shfl_sync(0xffffffffu, c.B.y, 31));
-        // start values of the warps: exclusive scan of the warp totals; lane w holds warp w's
-        Aff w = lane < NW ? wagg[lane] : aff_identity();
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const Aff prev = shfl_up_aff(w, o);
-            if (lane >= o) w = aff_then(prev, w);
-        }
-        Aff wex = shfl_up_aff(w, 1);
-        if (lane == 0) wex = aff_identity();
-        const double2 ys = aff_apply(wex, ycta);
-        ywarp = cmake(__shfl_sync(0xffffffffu, ys.x, warp), __shfl_sync(0xffffffffu, ys.y, warp));
+        ywarp = aff_apply(wex_s[warp], ycta);
     }
+    // ---- forward apply and, composed as it goes, the thread's backward map
+    // bcc = f_s0 o ... o f_s1-1 with f_e(x) = y_e - u_e d_e x (x_i = y_i - u_i d_i x_{i+1})
+    Aff bcc = aff_identity();
     {
         double2 y = aff_apply(excl, ywarp);
         for (int e = s0; e < s1; ++e) {
             const int i = c0 + e;
             const double2 l = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
-            y = cmul(D[e], csub(Y[e], cmul(l, y)));
+            const double2 d = D[e];
+            y = cmul(d, csub(Y[e], cmul(l, y)));
             Y[e] = y;
+            const Aff m{cmake(-(l.x * d.x - l.y * d.y), -(l.x * d.y + l.y * d.x)), y};
+            bcc = aff_then(m, bcc);
         }
-    }
-
-    // ---- backward: x_i = y_i - u_i d_i x_{i+1}
-    Aff bcc = aff_identity();
-    for (int e = s1 - 1; e >= s0; --e) {
-        const int i = c0 + e;
-        const double2 d = D[e];
-        const double2 u = (i >= 1 && i <= Nr - 2) ? off : cmake(0, 0);
-        const Aff m{cmake(-(u.x * d.x - u.y * d.y), -(u.x * d.y + u.y * d.x)), Y[e]};
-        bcc = aff_then(bcc, m);
     }
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -1290,17 +1281,21 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
     }
     Aff bexcl = shfl_down_aff(bcc, 1);
     if (lane == 31) bexcl = aff_identity();
-    __syncthreads();  // every thread has read wagg[] of the forward sweep
+    __syncthreads();  // every thread has read wex_s[] of the forward sweep
     if (lane == 0) wagg[warp] = bcc;
     __syncthreads();
     if (warp == 0) {
-        // CTA total of the backward maps: ordered suffix scan of the warp totals
+        // CTA total of the backward maps: ordered suffix scan of the warp totals; each
+        // warp's exclusive suffix is kept for the apply pass
         Aff c = lane < NW ? wagg[lane] : aff_identity();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const Aff nxt = shfl_down_aff(c, o);
             if (lane + o < 32) c = aff_then(nxt, c);
         }
+        Aff ex = shfl_down_aff(c, 1);
+        if (lane == 31) ex = aff_identity();
+        if (lane < NW) wex_s[lane] = ex;
         if (lane == 0) cagg_b = c;
     }
     cl.sync();
@@ -1314,16 +1309,7 @@ __global__ void __launch_bounds__(PCL_THREADS, 3) k_precond_solve_cl(int Nr, int
             if (lane + o < 32) c = aff_then(nxt, c);
         }
         const double2 xcta = cmake(__shfl_sync(0xffffffffu, c.B.x, 0), __shfl_sync(0xffffffffu, c.B.y, 0));
-        Aff w = lane < NW ? wagg[lane] : aff_identity();
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const Aff nxt = shfl_down_aff(w, o);
-            if (lane + o < 32) w = aff_then(nxt, w);
-        }
-        Aff wex = shfl_down_aff(w, 1);
-        if (lane == 31) wex = aff_identity();
-        const double2 xs = aff_apply(wex, xcta);
-        xwarp = cmake(__shfl_sync(0xffffffffu, xs.x, warp), __shfl_sync(0xffffffffu, xs.y, warp));
+        xwarp = aff_apply(wex_s[warp], xcta);
     }
     // the other CTAs read cagg_b only before this arrive; the matching wait is the
     // last statement, so a CTA's shared memory outlives every remote read of it
