@@ -1581,6 +1581,7 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
     cg::cluster_group cl = cg::this_cluster();
     extern __shared__ double2 smc[];
     __shared__ Mob wmob[PCL_THREADS / 32];
+    __shared__ Mob wex_s[PCL_THREADS / 32];  // each warp's exclusive prefix of wmob
     __shared__ Mob cmob;
     const int rank = (int)cl.block_rank();
     const int Nr = g.Nr, j = blockIdx.y;
@@ -1637,6 +1638,7 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
     if (lane == 31) wmob[warp] = acc;
     __syncthreads();
     if (warp == 0) {
+        // the CTA total, and each warp's exclusive prefix for its start pivot below
         Mob m = lane < NW ? wmob[lane] : mob_identity();
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -1646,6 +1648,9 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
                 mob_normalize(m);
             }
         }
+        Mob ex = shfl_up_mob(m, 1);
+        if (lane == 0) ex = mob_identity();
+        if (lane < NW) wex_s[lane] = ex;
         if (lane == 31) cmob = m;
     }
     cl.sync();
@@ -1664,19 +1669,7 @@ __global__ void __launch_bounds__(PCL_THREADS) k_precond_factor_cl(Grid g, Coupl
         }
         double2 pc = lane == 31 ? mob_apply(m, cmake(1.0, 0.0)) : cmake(0.0, 0.0);
         pc = cmake(__shfl_sync(0xffffffffu, pc.x, 31), __shfl_sync(0xffffffffu, pc.y, 31));
-        Mob w = lane < NW ? wmob[lane] : mob_identity();
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const Mob prev = shfl_up_mob(w, o);
-            if (lane >= o) {
-                w = mob_mul(w, prev);
-                mob_normalize(w);
-            }
-        }
-        Mob wex = shfl_up_mob(w, 1);
-        if (lane == 0) wex = mob_identity();
-        const double2 ps = mob_apply(wex, pc);
-        p = cmake(__shfl_sync(0xffffffffu, ps.x, warp), __shfl_sync(0xffffffffu, ps.y, warp));
+        p = mob_apply(wex_s[warp], pc);
     }
     cl.barrier_arrive();
     if (lane > 0) p = mob_apply(excl, p);
