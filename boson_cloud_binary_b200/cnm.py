@@ -363,7 +363,8 @@ class CrankNicolsonModes:
     def run(self, n_steps, r_ex):
         """The computational part of run(): extraction radius, t = 0, operator refresh.
 
-        (The text output of a run lives in boson_cloud_binary_b200.output.)"""
+        (The text output of a run -- diagnostic files, snapshots, checkpoints -- is written by
+        the C++ drop-in class in host/.)"""
         self._check(self._lib.cnm_prepare_run(self._h, int(n_steps), float(r_ex)))
         self.__dict__["t"] = [0.0]
 
